@@ -1,0 +1,423 @@
+"""hazmath_b200 -- B200-native UA-AMG preconditioned Krylov solve (HAZmath drop-in).
+
+The product is the CUDA shared library ``libhazb200.so`` built from ``csrc/``
+(sm_100a).  This module is its Python host mirror through ctypes: the
+HAZmath structures (``dCSRmat``, ``dvector``, ``AMG_param``,
+``linear_itsolver_param``, ``precond_data``, ``AMG_data``), the drop-in entry
+points with HAZmath's names and argument meaning, and a thin ``Solver``
+wrapper over the persistent device handle.  There is no CPU fallback: if the
+library is missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhazb200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "hazmath_b200.h")
+
+INT = C.c_int
+SHORT = C.c_short
+REAL = C.c_double
+
+# constants of include/macro.h (same values)
+SUCCESS = 0
+ERROR_INPUT_PAR = -13
+ERROR_MAT_SIZE = -15
+ERROR_ALLOC_MEM = -20
+ERROR_DATA_STRUCTURE = -21
+ERROR_DATA_ZERODIAG = -22
+ERROR_AMG_SMOOTH_TYPE = -31
+ERROR_AMG_COARSEING = -33
+ERROR_SOLVER_TYPE = -40
+ERROR_SOLVER_STAG = -42
+ERROR_SOLVER_SOLSTAG = -43
+ERROR_SOLVER_TOLSMALL = -44
+ERROR_SOLVER_MISC = -47
+ERROR_SOLVER_MAXIT = -48
+SOLVER_CG = 1
+SOLVER_UMFPACK = 32
+STOP_REL_RES, STOP_REL_PRECRES, STOP_MOD_REL_RES = 1, 2, 3
+PREC_AMG = 2
+UA_AMG = 1
+VMB, HEC, HEM = 1, 4, 5
+V_CYCLE, W_CYCLE = 1, 2
+SMOOTHER_JACOBI, SMOOTHER_GS, SMOOTHER_SGS = 1, 2, 3
+SMOOTHER_SOR, SMOOTHER_SSOR, SMOOTHER_GSOR, SMOOTHER_SGSOR = 5, 6, 7, 8
+SMOOTHER_L1DIAG = 10
+HZB_PREC_FP64, HZB_PREC_MIXED = 0, 1
+HZB_GS_EXACT, HZB_GS_MULTICOLOR = 0, 1
+HZB_MATCH_EXACT, HZB_MATCH_PARALLEL = 0, 1
+MAX_AMG_LVL = 20
+
+
+class dCSRmat(C.Structure):
+    _fields_ = [("row", INT), ("col", INT), ("nnz", INT), ("IA", C.POINTER(INT)),
+                ("JA", C.POINTER(INT)), ("val", C.POINTER(REAL))]
+
+
+class dvector(C.Structure):
+    _fields_ = [("row", INT), ("val", C.POINTER(REAL))]
+
+
+class linear_itsolver_param(C.Structure):
+    _fields_ = [("linear_itsolver_type", SHORT), ("linear_precond_type", SHORT),
+                ("linear_stop_type", SHORT), ("linear_maxit", INT), ("linear_tol", REAL),
+                ("linear_restart", INT), ("linear_print_level", SHORT),
+                ("HX_smooth_iter", SHORT), ("AL_scaling_param", REAL)]
+
+
+class AMG_param(C.Structure):
+    _fields_ = [("AMG_type", SHORT), ("print_level", SHORT), ("maxit", INT), ("tol", REAL),
+                ("max_levels", SHORT), ("coarse_dof", INT), ("cycle_type", SHORT),
+                ("smoother", SHORT), ("presmooth_iter", SHORT), ("postsmooth_iter", SHORT),
+                ("relaxation", REAL), ("polynomial_degree", SHORT), ("coarse_solver", SHORT),
+                ("coarse_scaling", SHORT), ("amli_degree", SHORT),
+                ("amli_coef", C.POINTER(REAL)), ("nl_amli_krylov_type", SHORT),
+                ("aggregation_type", SHORT), ("strong_coupled", REAL),
+                ("max_aggregation", INT), ("smooth_filter", SHORT),
+                ("tentative_smooth", REAL), ("Schwarz_levels", INT),
+                ("Schwarz_mmsize", INT), ("Schwarz_maxlvl", INT), ("Schwarz_type", INT),
+                ("Schwarz_blksolver", INT), ("HAZDIR", C.c_char_p),
+                ("Schwarz_on_blk", C.POINTER(INT)), ("Schwarz_patch_type", C.POINTER(INT)),
+                ("damping_param", REAL), ("BSR_alpha", REAL), ("BSR_omega", REAL),
+                ("fpwr", REAL), ("smoother_function", C.c_void_p)]
+
+
+class precond(C.Structure):
+    _fields_ = [("data", C.c_void_p),
+                ("fct", C.CFUNCTYPE(None, C.POINTER(REAL), C.POINTER(REAL), C.c_void_p)),
+                ("setup_time", REAL)]
+
+
+class Schwarz_data(C.Structure):
+    _fields_ = [("A", dCSRmat), ("nblk", INT), ("iblock", C.POINTER(INT)),
+                ("jblock", C.POINTER(INT)), ("rhsloc1", dvector), ("xloc1", dvector),
+                ("Schwarz_type", SHORT), ("blk_solver", INT), ("memt", INT),
+                ("mask", C.POINTER(INT)), ("maxbs", INT), ("maxbnnz", INT),
+                ("blk_data", C.c_void_p), ("numeric", C.c_void_p), ("swzparam", C.c_void_p)]
+
+
+class AMG_data(C.Structure):
+    _fields_ = [("max_levels", SHORT), ("num_levels", SHORT), ("A", dCSRmat), ("R", dCSRmat),
+                ("P", dCSRmat), ("b", dvector), ("x", dvector), ("M", dCSRmat),
+                ("Numeric", C.c_void_p), ("near_kernel_dim", INT),
+                ("near_kernel_basis", C.c_void_p), ("Schwarz_levels", INT),
+                ("Schwarz", Schwarz_data), ("w", dvector), ("cycle_type", INT),
+                ("wdata", C.c_void_p)]
+
+
+class precond_data(C.Structure):
+    _fields_ = [("AMG_type", SHORT), ("print_level", SHORT), ("maxit", INT),
+                ("max_levels", SHORT), ("tol", REAL), ("cycle_type", SHORT),
+                ("smoother", SHORT), ("presmooth_iter", SHORT), ("postsmooth_iter", SHORT),
+                ("relaxation", REAL), ("polynomial_degree", SHORT), ("coarse_solver", SHORT),
+                ("coarse_scaling", SHORT), ("amli_degree", SHORT),
+                ("nl_amli_krylov_type", SHORT), ("amli_coef", C.POINTER(REAL)),
+                ("mgl_data", C.POINTER(AMG_data)), ("fpwr", REAL), ("A", C.c_void_p),
+                ("A_nk", C.c_void_p), ("P_nk", C.c_void_p), ("R_nk", C.c_void_p),
+                ("r", C.c_void_p), ("w", C.POINTER(REAL))]
+
+
+class hzb_param(C.Structure):
+    _fields_ = [("precision", SHORT), ("gs_schedule", SHORT), ("matching", SHORT),
+                ("export_hierarchy", SHORT), ("use_omega", SHORT),
+                ("omega", C.POINTER(C.c_float)), ("device", INT), ("fallback_check", SHORT),
+                ("use_graph", SHORT), ("reserved", SHORT * 6)]
+
+
+class hzb_stats(C.Structure):
+    _fields_ = [("num_levels", INT), ("rows", INT * MAX_AMG_LVL), ("nnz", INT * MAX_AMG_LVL),
+                ("iterations", INT), ("final_relres", REAL), ("setup_seconds", REAL),
+                ("solve_seconds", REAL), ("strong_coupled", REAL), ("condest", REAL),
+                ("omega_contraction", REAL * 2), ("omega_used", INT), ("launches", INT)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libhazb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m hazmath_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        L.hzb_last_error.restype = C.c_char_p
+        L.amg_data_create.restype = P(AMG_data)
+        L.amg_setup_ua.restype = SHORT
+        L.hzb_create.argtypes = [P(C.c_void_p), P(AMG_param), P(linear_itsolver_param),
+                                 P(hzb_param)]
+        for name in ("hzb_setup_device", "hzb_solve_device", "hzb_precond_device",
+                     "hzb_set_omega_device", "hzb_level_copy", "hzb_get_stats",
+                     "hzb_setup_host", "hzb_solve_host", "hzb_destroy"):
+            getattr(L, name).argtypes = None
+        L.hzb_setup_device.argtypes = [C.c_void_p, INT, INT, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hzb_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hzb_solve_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hzb_setup_host.argtypes = [C.c_void_p, P(dCSRmat)]
+        L.hzb_precond_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hzb_set_omega_device.argtypes = [C.c_void_p, C.c_void_p]
+        L.hzb_level_copy.argtypes = [C.c_void_p, INT, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
+        L.hzb_get_stats.argtypes = [C.c_void_p, P(hzb_stats)]
+        L.hzb_destroy.argtypes = [C.c_void_p]
+        L.hzb_dcsr_aAxpy_device.argtypes = [REAL, INT, INT, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hzb_smoother_device.argtypes = [SHORT, SHORT, INT, REAL, INT, INT, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hzb_aggregation_hem_device.argtypes = [INT, INT, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, REAL, C.c_void_p, P(INT)]
+        L.hzb_rap_agg_device.argtypes = [INT, INT, C.c_void_p, C.c_void_p, C.c_void_p, INT,
+                                         C.c_void_p, P(INT), P(C.c_void_p), P(C.c_void_p),
+                                         P(C.c_void_p)]
+        L.dcsr_pcg.argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL, INT,
+                               SHORT, SHORT]
+        L.python_wrapper_krylov_amg.argtypes = [P(INT), P(INT), C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p, C.c_void_p, P(REAL),
+                                                P(INT), P(INT)]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().hzb_last_error().decode()
+
+
+def declared_symbols(header: str = HEADER) -> list[str]:
+    """Function names declared in include/hazmath_b200.h."""
+    import re
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    # declarations start in column 0; struct fields are indented
+    names = re.findall(r"^(?:const\s+)?[A-Za-z_][A-Za-z_0-9]*\s*\**\s*([A-Za-z_][A-Za-z_0-9]*)\s*\(",
+                       text, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "return")))
+
+
+# ---------------------------------------------------------------------------
+# parameter helpers (HAZmath's init functions, run in the library)
+# ---------------------------------------------------------------------------
+def amg_param(**kw) -> AMG_param:
+    """AMG_param from param_amg_init, then keyword overrides."""
+    p = AMG_param()
+    lib().param_amg_init(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def itsolver_param(**kw) -> linear_itsolver_param:
+    p = linear_itsolver_param()
+    lib().param_linear_solver_init(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def b200_param(**kw) -> hzb_param:
+    p = hzb_param()
+    lib().hzb_param_init(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def survey_amg(**kw) -> AMG_param:
+    """The UA-AMG setting of the benchmark configurations: HEM, theta = 0,
+    V(1,1) Gauss-Seidel, coarse direct solve at <= 2000 rows."""
+    base = dict(AMG_type=UA_AMG, cycle_type=V_CYCLE, smoother=SMOOTHER_GS,
+                presmooth_iter=1, postsmooth_iter=1, aggregation_type=HEM,
+                strong_coupled=0.0, max_aggregation=20, coarse_dof=2000, max_levels=20,
+                coarse_solver=SOLVER_UMFPACK, maxit=1, tol=1e-6)
+    base.update(kw)
+    return amg_param(**base)
+
+
+class _HostCSR:
+    """Keeps numpy arrays alive behind a dCSRmat."""
+
+    def __init__(self, ia, ja, val):
+        self.ia = np.ascontiguousarray(ia, np.int32)
+        self.ja = np.ascontiguousarray(ja, np.int32)
+        self.val = np.ascontiguousarray(val, np.float64)
+        n = len(self.ia) - 1
+        self.mat = dCSRmat(n, n, int(self.ia[-1]), self.ia.ctypes.data_as(C.POINTER(INT)),
+                           self.ja.ctypes.data_as(C.POINTER(INT)),
+                           self.val.ctypes.data_as(C.POINTER(REAL)))
+
+
+def _dvec(a: np.ndarray) -> dvector:
+    return dvector(len(a), a.ctypes.data_as(C.POINTER(REAL)))
+
+
+# ---------------------------------------------------------------------------
+# drop-in calls on numpy arrays (host pointers, as the reference takes them)
+# ---------------------------------------------------------------------------
+def linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, itparam, amgparam, b200=None):
+    """itsolver.c:846 semantics; x (float64 array) is updated in place.
+    Returns the iteration count or a negative ERROR_* code."""
+    A = _HostCSR(ia, ja, val)
+    assert x.dtype == np.float64 and x.flags.c_contiguous
+    bb = np.ascontiguousarray(b, np.float64)
+    if b200 is None:
+        return lib().linear_solver_dcsr_krylov_amg(C.byref(A.mat), C.byref(_dvec(bb)),
+                                                   C.byref(_dvec(x)), C.byref(itparam),
+                                                   C.byref(amgparam))
+    return lib().hzb_solver_dcsr_krylov_amg(C.byref(A.mat), C.byref(_dvec(bb)),
+                                            C.byref(_dvec(x)), C.byref(itparam),
+                                            C.byref(amgparam), C.byref(b200))
+
+
+def linear_solver_amg(ia, ja, val, b, x, amgparam):
+    A = _HostCSR(ia, ja, val)
+    bb = np.ascontiguousarray(b, np.float64)
+    return lib().linear_solver_amg(C.byref(A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),
+                                   C.byref(amgparam))
+
+
+def python_wrapper_krylov_amg(ia, ja, val, b, u, tol=1e-8, maxit=500, print_lvl=0):
+    ia = np.ascontiguousarray(ia, np.int32)
+    ja = np.ascontiguousarray(ja, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    n, nnz = INT(len(ia) - 1), INT(int(ia[-1]))
+    lib().python_wrapper_krylov_amg(C.byref(n), C.byref(nnz), ia.ctypes.data, ja.ctypes.data,
+                                    val.ctypes.data, b.ctypes.data, u.ctypes.data,
+                                    C.byref(REAL(tol)), C.byref(INT(maxit)),
+                                    C.byref(INT(print_lvl)))
+
+
+class AMGHierarchy:
+    """amg_data_create + amg_setup_ua on a host matrix; the pieces a caller
+    assembles itself (HAZNICS create_precond_amg style): precond_amg as a
+    preconditioner for dcsr_pcg, mgcycle, amg_data_free."""
+
+    def __init__(self, ia, ja, val, amgparam: AMG_param):
+        self._A = _HostCSR(ia, ja, val)
+        self.param = amgparam
+        L = lib()
+        self.mgl = L.amg_data_create(amgparam.max_levels)
+        self.mgl[0].A = self._A.mat   # the caller's arrays, as dcsr_cp'd in the reference
+        self._owned_A0 = True
+        self.status = L.amg_setup_ua(self.mgl, C.byref(amgparam))
+        self.pcdata = precond_data()
+        L.precond_data_null(C.byref(self.pcdata))
+        L.param_amg_to_prec(C.byref(self.pcdata), C.byref(amgparam))
+        self.pcdata.max_levels = self.mgl[0].num_levels
+        self.pcdata.mgl_data = self.mgl
+        self.pc = precond()
+        self.pc.data = C.cast(C.pointer(self.pcdata), C.c_void_p)
+        self.pc.fct = C.cast(L.precond_amg, type(self.pc.fct))
+
+    @property
+    def num_levels(self) -> int:
+        return self.mgl[0].num_levels
+
+    def level(self, l: int):
+        A = self.mgl[l].A
+        n, nnz = A.row, A.nnz
+        ia = np.ctypeslib.as_array(A.IA, (n + 1,)).copy()
+        ja = np.ctypeslib.as_array(A.JA, (nnz,)).copy()
+        val = np.ctypeslib.as_array(A.val, (nnz,)).copy()
+        return ia, ja, val
+
+    def agg(self, l: int):
+        P = self.mgl[l].P
+        ia = np.ctypeslib.as_array(P.IA, (P.row + 1,))
+        ja = np.ctypeslib.as_array(P.JA, (max(P.nnz, 1),))
+        out = np.full(P.row, -1, np.int32)
+        has = ia[1:] > ia[:-1]
+        out[has] = ja[ia[:-1][has]]
+        return out
+
+    def precond(self, r):
+        r = np.ascontiguousarray(r, np.float64).copy()
+        z = np.zeros_like(r)
+        lib().precond_amg(r.ctypes.data_as(C.POINTER(REAL)), z.ctypes.data_as(C.POINTER(REAL)),
+                          C.cast(C.pointer(self.pcdata), C.c_void_p))
+        return z
+
+    def pcg(self, b, x, tol=1e-8, maxit=500, stop_type=STOP_REL_RES, prtlvl=0):
+        bb = np.ascontiguousarray(b, np.float64)
+        return lib().dcsr_pcg(C.byref(self._A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),
+                              C.byref(self.pc), tol, maxit, stop_type, prtlvl)
+
+    def free(self):
+        if self.mgl:
+            # level 0 A belongs to the caller here: detach before freeing
+            self.mgl[0].A = dCSRmat()
+            lib().amg_data_free(self.mgl, C.byref(self.param))
+            self.mgl = None
+
+
+class Solver:
+    """Persistent device handle (hzb_create / hzb_setup_* / hzb_solve_*)."""
+
+    def __init__(self, amg: AMG_param | None = None, it: linear_itsolver_param | None = None,
+                 b200: hzb_param | None = None):
+        self.amg = amg or survey_amg()
+        self.it = it or itsolver_param(linear_itsolver_type=SOLVER_CG,
+                                       linear_precond_type=PREC_AMG, linear_tol=1e-8,
+                                       linear_maxit=500)
+        self.b200 = b200 or b200_param()
+        h = C.c_void_p()
+        rc = lib().hzb_create(C.byref(h), C.byref(self.amg), C.byref(self.it),
+                              C.byref(self.b200))
+        if rc:
+            raise RuntimeError(f"hzb_create: {rc} {last_error()}")
+        self.h = h
+        self._keep = None
+
+    def setup_device(self, n, nnz, ia_ptr, ja_ptr, val_ptr) -> int:
+        return lib().hzb_setup_device(self.h, n, nnz, ia_ptr, ja_ptr, val_ptr)
+
+    def setup_host(self, ia, ja, val) -> int:
+        self._keep = _HostCSR(ia, ja, val)
+        return lib().hzb_setup_host(self.h, C.byref(self._keep.mat))
+
+    def solve_device(self, b_ptr, x_ptr) -> int:
+        return lib().hzb_solve_device(self.h, b_ptr, x_ptr)
+
+    def solve_host(self, b, x) -> int:
+        bb = np.ascontiguousarray(b, np.float64)
+        return lib().hzb_solve_host(self.h, bb.ctypes.data, x.ctypes.data)
+
+    def precond_device(self, r_ptr, z_ptr) -> int:
+        return lib().hzb_precond_device(self.h, r_ptr, z_ptr)
+
+    def set_omega_device(self, omega_ptr) -> int:
+        return lib().hzb_set_omega_device(self.h, omega_ptr)
+
+    def stats(self) -> hzb_stats:
+        st = hzb_stats()
+        lib().hzb_get_stats(self.h, C.byref(st))
+        return st
+
+    def level(self, l: int):
+        st = self.stats()
+        n, nnz = st.rows[l], st.nnz[l]
+        ia = np.empty(n + 1, np.int32)
+        ja = np.empty(nnz, np.int32)
+        val = np.empty(nnz)
+        agg = np.empty(n, np.int32)
+        rc = lib().hzb_level_copy(self.h, l, ia.ctypes.data, ja.ctypes.data, val.ctypes.data,
+                                  agg.ctypes.data)
+        if rc:
+            raise RuntimeError(f"hzb_level_copy: {rc} {last_error()}")
+        return ia, ja, val, agg
+
+    def close(self):
+        if self.h:
+            lib().hzb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

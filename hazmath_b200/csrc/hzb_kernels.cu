@@ -1,0 +1,640 @@
+// hzb_kernels.cu -- sparse, vector and smoother kernels (FP64 parity + FP32).
+//
+// Compiled with -fmad=false: a*b+c is rounded twice, as in the reference's
+// C loops built without FMA.  Row sums run sequentially in CSR order inside
+// one thread; coalescing comes from staging each row bundle's entries in
+// shared memory (the CSR-stream schedule), not from splitting rows.
+#include "hzb_kernels.cuh"
+#include <cstdio>
+#include <mutex>
+
+namespace hzb {
+
+// ---------------------------------------------------------------------------
+// bookkeeping
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static thread_local long long g_launches = 0;
+
+void set_error(cudaError_t e, const char *file, int line) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s (%s:%d)", cudaGetErrorString(e), file, line);
+    g_err = buf;
+}
+void set_error_msg(const std::string &m) { g_err = m; }
+const char *last_error() { return g_err.c_str(); }
+void count_launch(int k) { g_launches += k; }
+long long launch_count() { return g_launches; }
+
+int sm_count() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cached = v > 0 ? v : 148;
+    }
+    return cached;
+}
+
+// ---------------------------------------------------------------------------
+// SpMV: row bundles staged in shared memory
+// ---------------------------------------------------------------------------
+__global__ void k_bundle_cap(int n, const int *__restrict__ ia, int *cap) {
+    __shared__ int sh[32];
+    int best = 0;
+    const int nb = (n + SPMV_ROWS - 1) / SPMV_ROWS;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+         b += gridDim.x * blockDim.x) {
+        int r0 = b * SPMV_ROWS, r1 = min(r0 + SPMV_ROWS, n);
+        best = max(best, ia[r1] - ia[r0]);
+    }
+    best = block_max(best, sh);
+    if (threadIdx.x == 0) atomicMax(cap, best);
+}
+
+int bundle_capacity(int n, const int *ia, cudaStream_t s, int *cap) {
+    int *d = nullptr;
+    HZB_TRY(dalloc(&d, 1));
+    cudaMemsetAsync(d, 0, sizeof(int), s);
+    const int nb = div_up(n, SPMV_ROWS);
+    k_bundle_cap<<<grid_for(nb), 256, 0, s>>>(n, ia, d);
+    count_launch();
+    cudaError_t e = cudaMemcpyAsync(cap, d, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+    return SUCCESS;
+}
+
+template <typename T, int MODE>
+__device__ __forceinline__ void spmv_store(int row, T t, const T *b, T *y, T alpha) {
+    if (MODE == SPMV_Y || MODE == SPMV_Y_DOT) {
+        y[row] = t;
+    } else if (MODE == SPMV_RES) {
+        y[row] = b[row] - t;
+    } else {
+        if (alpha == T(1)) y[row] += t;
+        else if (alpha == T(-1)) y[row] -= t;
+        else y[row] += t * alpha;
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(SPMV_ROWS)
+k_spmv_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+              const T *__restrict__ val, const T *__restrict__ x,
+              const T *__restrict__ b, T *__restrict__ y, T alpha,
+              T *__restrict__ part, int cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sv = reinterpret_cast<T *>(smem_raw);
+    int *sc = reinterpret_cast<int *>(sv + ((cap + 1) & ~1));
+    const int r0 = blockIdx.x * SPMV_ROWS;
+    const int r1 = min(r0 + SPMV_ROWS, n);
+    const int s = __ldg(ia + r0), e = __ldg(ia + r1);
+    const int cnt = e - s;
+    for (int k = threadIdx.x; k < cnt; k += SPMV_ROWS) {
+        sv[k] = __ldg(val + s + k);
+        sc[k] = __ldg(ja + s + k);
+    }
+    __syncthreads();
+    const int row = r0 + threadIdx.x;
+    T t = T(0), prod = T(0);
+    if (row < r1) {
+        const int b0 = __ldg(ia + row) - s, b1 = __ldg(ia + row + 1) - s;
+        for (int k = b0; k < b1; ++k) t += sv[k] * __ldg(x + sc[k]);
+        spmv_store<T, MODE>(row, t, b, y, alpha);
+        if (MODE == SPMV_Y_DOT) prod = t * __ldg(x + row);
+    }
+    if (MODE == SPMV_Y_DOT) {
+        __shared__ T sh[32];
+        prod = block_sum(prod, sh);
+        if (threadIdx.x == 0) part[blockIdx.x] = prod;
+    }
+}
+
+// Rows too long for the staged bundle: one thread per row from global memory.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(SPMV_ROWS)
+k_spmv_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+            const T *__restrict__ val, const T *__restrict__ x,
+            const T *__restrict__ b, T *__restrict__ y, T alpha,
+            T *__restrict__ part) {
+    const int row = blockIdx.x * SPMV_ROWS + threadIdx.x;
+    T t = T(0), prod = T(0);
+    if (row < n) {
+        const int b0 = ia[row], b1 = ia[row + 1];
+        for (int k = b0; k < b1; ++k) t += val[k] * __ldg(x + ja[k]);
+        spmv_store<T, MODE>(row, t, b, y, alpha);
+        if (MODE == SPMV_Y_DOT) prod = t * x[row];
+    }
+    if (MODE == SPMV_Y_DOT) {
+        __shared__ T sh[32];
+        prod = block_sum(prod, sh);
+        if (threadIdx.x == 0) part[blockIdx.x] = prod;
+    }
+}
+
+int spmv_blocks(int n) { return div_up(n > 0 ? n : 1, SPMV_ROWS); }
+
+template <typename T, int MODE>
+static int spmv_mode(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha,
+                     T *part, cudaStream_t s) {
+    if (A.n <= 0) return SUCCESS;
+    const int grid = spmv_blocks(A.n);
+    const size_t smem = (size_t)((A.bundle_cap + 1) & ~1) * sizeof(T) +
+                        (size_t)A.bundle_cap * sizeof(int);
+    if (A.bundle_cap > 0 && smem <= SPMV_SMEM_MAX) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_spmv_bundle<T, MODE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        k_spmv_bundle<T, MODE><<<grid, SPMV_ROWS, smem, s>>>(
+            A.n, A.ia, A.ja, A.val, x, b, y, alpha, part, A.bundle_cap);
+    } else {
+        k_spmv_rows<T, MODE><<<grid, SPMV_ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val,
+                                                       x, b, y, alpha, part);
+    }
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+template <typename T>
+int spmv(const DCsr<T> &A, int mode, const T *x, const T *b, T *y, T alpha,
+         T *part, cudaStream_t s) {
+    switch (mode) {
+    case SPMV_Y: return spmv_mode<T, SPMV_Y>(A, x, b, y, alpha, part, s);
+    case SPMV_RES: return spmv_mode<T, SPMV_RES>(A, x, b, y, alpha, part, s);
+    case SPMV_AXPY: return spmv_mode<T, SPMV_AXPY>(A, x, b, y, alpha, part, s);
+    case SPMV_Y_DOT: return spmv_mode<T, SPMV_Y_DOT>(A, x, b, y, alpha, part, s);
+    }
+    return ERROR_INPUT_PAR;
+}
+template int spmv<double>(const DCsr<double> &, int, const double *, const double *,
+                          double *, double, double *, cudaStream_t);
+template int spmv<float>(const DCsr<float> &, int, const float *, const float *,
+                         float *, float, float *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Transfers (P = aggregate map, R = P^T with ascending fine rows)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_restrict(int nc, const int *__restrict__ ria,
+                           const int *__restrict__ rja, const T *__restrict__ w,
+                           T *__restrict__ bc) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc;
+         c += gridDim.x * blockDim.x) {
+        T t = T(0);
+        for (int k = ria[c]; k < ria[c + 1]; ++k) t += w[rja[k]];
+        bc[c] = t;
+    }
+}
+
+template <typename T>
+int restrict_agg(int nc, const int *ria, const int *rja, const T *w, T *bc,
+                 cudaStream_t s) {
+    if (nc <= 0) return SUCCESS;
+    k_restrict<T><<<grid_for(nc), 256, 0, s>>>(nc, ria, rja, w, bc);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int restrict_agg<double>(int, const int *, const int *, const double *,
+                                  double *, cudaStream_t);
+template int restrict_agg<float>(int, const int *, const int *, const float *,
+                                 float *, cudaStream_t);
+
+template <typename T>
+__global__ void k_prolong(int n, const int *__restrict__ agg,
+                          const T *__restrict__ xc, T *__restrict__ x, T alpha) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        T t = T(0);
+        const int c = agg[i];
+        if (c >= 0) t += xc[c];
+        if (alpha == T(1)) x[i] += t;
+        else if (alpha == T(-1)) x[i] -= t;
+        else x[i] += t * alpha;
+    }
+}
+
+template <typename T>
+int prolong_agg(int n, const int *agg, const T *xc, T *x, T alpha,
+                cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    k_prolong<T><<<grid_for(n), 256, 0, s>>>(n, agg, xc, x, alpha);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int prolong_agg<double>(int, const int *, const double *, double *,
+                                 double, cudaStream_t);
+template int prolong_agg<float>(int, const int *, const float *, float *, float,
+                                cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Point smoothers
+// ---------------------------------------------------------------------------
+// Jacobi, w = 1: t = b_i - sum_{j != i} a_ij x_j;  x_i = (1-w) x_i + w t / d_i
+__global__ void k_jacobi(int n, const int *__restrict__ ia,
+                         const int *__restrict__ ja, const double *__restrict__ a,
+                         const double *__restrict__ dj, const double *__restrict__ b,
+                         const double *__restrict__ x, double *__restrict__ xn) {
+    const double w = 1.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        double t = b[i];
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+            if (ja[k] != i) t -= a[k] * x[ja[k]];
+        const double d = dj[i];
+        xn[i] = (fabs(d) > SMALLREAL) ? (1 - w) * x[i] + w * t / d : x[i];
+    }
+}
+
+int jacobi_sweep(const DCsr<double> &A, const double *dj, const double *b,
+                 const double *x, double *xn, cudaStream_t s) {
+    if (A.n <= 0) return SUCCESS;
+    k_jacobi<<<grid_for(A.n), 256, 0, s>>>(A.n, A.ia, A.ja, A.val, dj, b, x, xn);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+// l1-Jacobi: t = b_i - sum_j a_ij x_j, d = sum_j |a_ij| (both in CSR order);
+// x_i += omega_i * (t / d).  Rows are staged per bundle like the SpMV.
+template <typename T>
+__global__ void __launch_bounds__(SPMV_ROWS)
+k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+            const T *__restrict__ a, const T *__restrict__ b,
+            const T *__restrict__ x, T *__restrict__ xn,
+            const float *__restrict__ omega, int cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sv = reinterpret_cast<T *>(smem_raw);
+    int *sc = reinterpret_cast<int *>(sv + ((cap + 1) & ~1));
+    const int r0 = blockIdx.x * SPMV_ROWS;
+    const int r1 = min(r0 + SPMV_ROWS, n);
+    const int s = __ldg(ia + r0), e = __ldg(ia + r1);
+    const int cnt = e - s;
+    if (cap > 0) {
+        for (int k = threadIdx.x; k < cnt; k += SPMV_ROWS) {
+            sv[k] = __ldg(a + s + k);
+            sc[k] = __ldg(ja + s + k);
+        }
+        __syncthreads();
+    }
+    const int i = r0 + threadIdx.x;
+    if (i >= r1) return;
+    T t = b[i], d = T(0);
+    const int b0 = __ldg(ia + i), b1 = __ldg(ia + i + 1);
+    if (cap > 0) {
+        for (int k = b0 - s; k < b1 - s; ++k) {
+            const T v = sv[k];
+            t -= v * __ldg(x + sc[k]);
+            d += fabs(v);
+        }
+    } else {
+        for (int k = b0; k < b1; ++k) {
+            const T v = a[k];
+            t -= v * __ldg(x + ja[k]);
+            d += fabs(v);
+        }
+    }
+    T xi = x[i];
+    if (fabs(d) > T(SMALLREAL)) {
+        if (omega) xi += T(omega[i]) * (t / d);
+        else xi += t / d;
+    }
+    xn[i] = xi;
+}
+
+template <typename T>
+int l1_sweep(const DCsr<T> &A, const T *b, const T *x, T *xn,
+             const float *omega, cudaStream_t s) {
+    if (A.n <= 0) return SUCCESS;
+    const int grid = spmv_blocks(A.n);
+    size_t smem = (size_t)((A.bundle_cap + 1) & ~1) * sizeof(T) +
+                  (size_t)A.bundle_cap * sizeof(int);
+    int cap = A.bundle_cap;
+    if (cap <= 0 || smem > SPMV_SMEM_MAX) { cap = 0; smem = 0; }
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_l1_bundle<T>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_l1_bundle<T><<<grid, SPMV_ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn,
+                                                 omega, cap);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int l1_sweep<double>(const DCsr<double> &, const double *, const double *,
+                              double *, const float *, cudaStream_t);
+template int l1_sweep<float>(const DCsr<float> &, const float *, const float *,
+                             float *, const float *, cudaStream_t);
+
+// Gauss-Seidel family on independent rows.  x is read with plain loads:
+// in gs_run earlier sets of the same CTA wrote it.
+// Row `skip` is left untouched: the backward sweep of smoother_dcsr_sgs starts
+// at row n-2 (smoother.c:225); the host passes kind | GS_SKIP_LAST for it.
+template <typename T>
+__device__ __forceinline__ void gs_row(int i, int kind, const int *ia,
+                                       const int *ja, const T *a, const T *d,
+                                       T w, const T *b, T *x, int skip) {
+    if (i == skip) return;
+    T t = b[i];
+    const int k1 = ia[i + 1];
+    for (int k = ia[i]; k < k1; ++k) {
+        const int j = ja[k];
+        if (j != i) t -= a[k] * x[j];
+    }
+    const T di = d[i];
+    if (kind == 0) {
+        x[i] = t * di;
+    } else if (kind == 1) {
+        if (fabs(di) > T(SMALLREAL)) x[i] = w * (t / di) + (1 - w) * x[i];
+    } else {
+        if (fabs(di) > T(SMALLREAL)) x[i] = t / di;
+    }
+}
+
+template <typename T>
+__global__ void k_gs_rows(int cnt, const int *__restrict__ rows,
+                          const int *__restrict__ ia, const int *__restrict__ ja,
+                          const T *__restrict__ a, const T *__restrict__ d,
+                          int kind, T w, const T *__restrict__ b, T *x,
+                          int skip) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt;
+         q += gridDim.x * blockDim.x)
+        gs_row<T>(rows[q], kind, ia, ja, a, d, w, b, x, skip);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_gs_run(const int *__restrict__ rows, const int *__restrict__ set_ptr,
+         int first, int last, const int *__restrict__ ia,
+         const int *__restrict__ ja, const T *__restrict__ a,
+         const T *__restrict__ d, int kind, T w, const T *__restrict__ b, T *x,
+         int skip) {
+    for (int sidx = first; sidx < last; ++sidx) {
+        const int q0 = set_ptr[sidx], q1 = set_ptr[sidx + 1];
+        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x)
+            gs_row<T>(rows[q], kind, ia, ja, a, d, w, b, x, skip);
+        __syncthreads();
+    }
+}
+
+template <typename T>
+int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt, const T *d,
+            T w, const T *b, T *x, cudaStream_t s) {
+    if (cnt <= 0) return SUCCESS;
+    const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
+    k_gs_rows<T><<<grid_for(cnt), 256, 0, s>>>(cnt, rows, A.ia, A.ja, A.val, d,
+                                               kind & 15, w, b, x, skip);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template <typename T>
+int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
+           int first, int last, const T *d, T w, const T *b, T *x,
+           cudaStream_t s) {
+    if (last <= first) return SUCCESS;
+    const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
+    k_gs_run<T><<<1, 1024, 0, s>>>(rows, set_ptr, first, last, A.ia, A.ja,
+                                   A.val, d, kind & 15, w, b, x, skip);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int gs_rows<double>(const DCsr<double> &, int, const int *, int,
+                             const double *, double, const double *, double *,
+                             cudaStream_t);
+template int gs_rows<float>(const DCsr<float> &, int, const int *, int,
+                            const float *, float, const float *, float *,
+                            cudaStream_t);
+template int gs_run<double>(const DCsr<double> &, int, const int *, const int *,
+                            int, int, const double *, double, const double *,
+                            double *, cudaStream_t);
+template int gs_run<float>(const DCsr<float> &, int, const int *, const int *,
+                           int, int, const float *, float, const float *,
+                           float *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Reductions (deterministic: fixed grid for a given n, ordered final sum)
+// ---------------------------------------------------------------------------
+constexpr int RED_BLOCK = 256;
+int reduce_blocks(int n) {
+    int g = div_up(n > 0 ? n : 1, RED_BLOCK * 4);
+    int cap = sm_count() * 4;
+    return g < cap ? g : cap;
+}
+
+__global__ void k_reduce_final(const double *__restrict__ part, int np,
+                               double *out, int is_max) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    // each thread folds a contiguous slice in order
+    const int per = (np + blockDim.x - 1) / blockDim.x;
+    const int b0 = threadIdx.x * per, b1 = min(b0 + per, np);
+    for (int k = b0; k < b1; ++k) v = is_max ? fmax(v, part[k]) : v + part[k];
+    v = is_max ? block_max(v, sh) : block_sum(v, sh);
+    if (threadIdx.x == 0) out[0] = v;
+}
+
+int reduce_final(const double *part, int np, double *out, cudaStream_t s) {
+    k_reduce_final<<<1, 256, 0, s>>>(part, np, out, 0);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+int reduce_final_max(const double *part, int np, double *out, cudaStream_t s) {
+    k_reduce_final<<<1, 256, 0, s>>>(part, np, out, 1);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+__global__ void k_dot_partial(int n, const double *__restrict__ x,
+                              const double *__restrict__ y, double *part) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        v += x[i] * y[i];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+int dot_partial(int n, const double *x, const double *y, double *part,
+                cudaStream_t s) {
+    k_dot_partial<<<reduce_blocks(n), RED_BLOCK, 0, s>>>(n, x, y, part);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+int dot(int n, const double *x, const double *y, double *part, double *out,
+        cudaStream_t s) {
+    HZB_TRY(dot_partial(n, x, y, part, s));
+    return reduce_final(part, reduce_blocks(n), out, s);
+}
+
+// part4 layout: [0..G) (r,r)  [G..2G) max|u|  [2G..3G) (u,u)  [3G..4G) (p,p)
+__global__ void k_pcg_update(int n, const double *__restrict__ num,
+                             const double *__restrict__ den, double *u,
+                             double *r, const double *__restrict__ p,
+                             const double *__restrict__ t, double *part4) {
+    __shared__ double sh[32];
+    const double alpha = num[0] / den[0];
+    double rr = 0.0, um = 0.0, uu = 0.0, pp = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const double pi = p[i];
+        double ui = u[i];
+        if (alpha == 1.0) ui += pi;
+        else if (alpha == -1.0) ui -= pi;
+        else ui += alpha * pi;
+        const double ma = -alpha;
+        double ri = r[i];
+        const double ti = t[i];
+        if (ma == 1.0) ri += ti;
+        else if (ma == -1.0) ri -= ti;
+        else ri += ma * ti;
+        u[i] = ui;
+        r[i] = ri;
+        rr += ri * ri;
+        um = fmax(um, fabs(ui));
+        uu += ui * ui;
+        pp += pi * pi;
+    }
+    const int G = gridDim.x;
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) part4[blockIdx.x] = rr;
+    um = block_max(um, sh);
+    if (threadIdx.x == 0) part4[G + blockIdx.x] = um;
+    uu = block_sum(uu, sh);
+    if (threadIdx.x == 0) part4[2 * G + blockIdx.x] = uu;
+    pp = block_sum(pp, sh);
+    if (threadIdx.x == 0) part4[3 * G + blockIdx.x] = pp;
+}
+
+int pcg_update(int n, const double *num, const double *den, double *u,
+               double *r, const double *p, const double *t, double *part4,
+               cudaStream_t s) {
+    k_pcg_update<<<reduce_blocks(n), RED_BLOCK, 0, s>>>(n, num, den, u, r, p, t,
+                                                        part4);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+__global__ void k_pcg_axpby(int n, const double *__restrict__ num,
+                            const double *__restrict__ den,
+                            const double *__restrict__ z, double *p) {
+    const double beta = num[0] / den[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        p[i] = 1.0 * z[i] + beta * p[i];
+}
+
+int pcg_axpby(int n, const double *num, const double *den, const double *z,
+              double *p, cudaStream_t s) {
+    k_pcg_axpby<<<grid_for(n), 256, 0, s>>>(n, num, den, z, p);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+template <typename T>
+__global__ void k_copy(int n, const T *__restrict__ x, T *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        y[i] = x[i];
+}
+template <typename T>
+__global__ void k_zero(int n, T *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        y[i] = T(0);
+}
+template <typename T>
+int vcopy(int n, const T *x, T *y, cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    k_copy<T><<<grid_for(n), 256, 0, s>>>(n, x, y);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template <typename T>
+int vzero(int n, T *y, cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    k_zero<T><<<grid_for(n), 256, 0, s>>>(n, y);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int vcopy<double>(int, const double *, double *, cudaStream_t);
+template int vcopy<float>(int, const float *, float *, cudaStream_t);
+template int vcopy<int>(int, const int *, int *, cudaStream_t);
+template int vzero<double>(int, double *, cudaStream_t);
+template int vzero<float>(int, float *, cudaStream_t);
+
+__global__ void k_d2f(int n, const double *__restrict__ x, float *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
+}
+__global__ void k_f2d(int n, const float *__restrict__ x, double *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        y[i] = (double)x[i];
+}
+int d2f(int n, const double *x, float *y, cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    k_d2f<<<grid_for(n), 256, 0, s>>>(n, x, y);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+int f2d(int n, const float *x, double *y, cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    k_f2d<<<grid_for(n), 256, 0, s>>>(n, x, y);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+int csr_val_d2f(int nnz, const double *x, float *y, cudaStream_t s) {
+    return d2f(nnz, x, y, s);
+}
+
+// ---------------------------------------------------------------------------
+// Coarse level: y = Ainv x, one warp per row, FP64 accumulation
+// ---------------------------------------------------------------------------
+template <typename TI>
+__global__ void k_gemv(int n, const double *__restrict__ M,
+                       const TI *__restrict__ x, TI *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < n; r += nwarps) {
+        const double *row = M + (size_t)r * n;
+        double t = 0.0;
+        for (int c = lane; c < n; c += 32) t += row[c] * (double)x[c];
+        t = warp_sum(t);
+        if (lane == 0) y[r] = (TI)t;
+    }
+}
+
+template <typename TI>
+int dense_gemv(int n, const double *Ainv, const TI *x, TI *y, cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    const int grid = div_up((long long)n * 32, 256);
+    k_gemv<TI><<<grid, 256, 0, s>>>(n, Ainv, x, y);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int dense_gemv<double>(int, const double *, const double *, double *,
+                                cudaStream_t);
+template int dense_gemv<float>(int, const double *, const float *, float *,
+                               cudaStream_t);
+
+}  // namespace hzb

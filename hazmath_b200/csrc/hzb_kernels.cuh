@@ -1,0 +1,105 @@
+// hzb_kernels.cuh -- host launchers of the sparse / vector / smoother kernels.
+//
+// Arithmetic contract of the FP64 kernels: this translation unit set is
+// compiled with -fmad=false, every row sum runs in one thread in CSR order
+// starting from 0.0 (or from b_i for the smoothers), so each value is
+// rounded exactly as the reference's sequential C loops round it.
+#pragma once
+#include "hzb_common.cuh"
+
+namespace hzb {
+
+// A CSR matrix resident in device memory (int32 pattern).
+template <typename T>
+struct DCsr {
+    int n = 0, nnz = 0;
+    const int *ia = nullptr, *ja = nullptr;
+    const T *val = nullptr;
+    int bundle_cap = 0;   // max entries in any SPMV_ROWS-row bundle (0: none)
+};
+
+constexpr int SPMV_ROWS = 128;          // rows per CTA in the row-bundle SpMV
+constexpr int SPMV_SMEM_MAX = 160 * 1024;
+
+enum SpmvMode { SPMV_Y = 0, SPMV_RES = 1, SPMV_AXPY = 2, SPMV_Y_DOT = 3 };
+
+// Largest number of stored entries in any SPMV_ROWS-row bundle of A.
+int bundle_capacity(int n, const int *ia, cudaStream_t s, int *cap);
+
+// y = A x (SPMV_Y); y = b - A x (SPMV_RES); y += alpha A x with the
+// reference's +-1 special cases (SPMV_AXPY); y = A x and partial dot(y, x)
+// into part[blockIdx] (SPMV_Y_DOT, part sized by spmv_blocks()).
+template <typename T>
+int spmv(const DCsr<T> &A, int mode, const T *x, const T *b, T *y, T alpha,
+         T *part, cudaStream_t s);
+int spmv_blocks(int n);
+
+// b_c[c] = sum over R row c of w (R rows list fine indices ascending).
+template <typename T>
+int restrict_agg(int nc, const int *ria, const int *rja, const T *w, T *bc,
+                 cudaStream_t s);
+// x_i (+/-)= alpha * x_c[agg_i] as dcsr_aAxpy_agg does for unit P.
+template <typename T>
+int prolong_agg(int n, const int *agg, const T *xc, T *x, T alpha,
+                cudaStream_t s);
+// fused: x_i += x_c[agg_i] (alpha = 1), then the first l1-Jacobi sweep
+// reads the updated x -- kept separate in parity mode.
+
+// Jacobi (w = 1) sweep reading x, writing xn (reference smoother.c:35-100).
+int jacobi_sweep(const DCsr<double> &A, const double *dj, const double *b,
+                 const double *x, double *xn, cudaStream_t s);
+// l1-Jacobi sweep: xn = x + omega * (b - A x) / l1 (omega == nullptr: 1).
+template <typename T>
+int l1_sweep(const DCsr<T> &A, const T *b, const T *x, T *xn,
+             const float *omega, cudaStream_t s);
+// Gauss-Seidel family on a list of independent rows (one level set / colour).
+//   kind 0: x_i = t * d_i            (GS, d_i = 1/a_ii)
+//   kind 1: x_i = w (t/d_i) + (1-w) x_i  if |d_i| > 1e-20   (SOR)
+//   kind 2: x_i = t / d_i               if |d_i| > 1e-20   (SGS)
+//   | GS_SKIP_LAST: leave row n-1 untouched (SGS backward sweep)
+constexpr int GS_SKIP_LAST = 16;
+template <typename T>
+int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt,
+            const T *d, T w, const T *b, T *x, cudaStream_t s);
+// One CTA runs level sets [first, last) back to back, __syncthreads between
+// sets (all sets of the run hold <= 1024 rows).
+template <typename T>
+int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
+           int first, int last, const T *d, T w, const T *b, T *x,
+           cudaStream_t s);
+
+// Deterministic reductions: partial sums per block, then an ordered final
+// sum into out[0].
+int reduce_final(const double *part, int nparts, double *out, cudaStream_t s);
+int reduce_final_max(const double *part, int nparts, double *out,
+                     cudaStream_t s);
+int dot_partial(int n, const double *x, const double *y, double *part,
+                cudaStream_t s);
+int dot(int n, const double *x, const double *y, double *part, double *out,
+        cudaStream_t s);
+int reduce_blocks(int n);
+
+// PCG update (krylov.c:198-224 + norms of checks I/II): alpha = num/den
+// (device scalars); u += alpha p; r += (-alpha) t; per-block partials of
+// (r,r), max|u|, (u,u), (p,p) into part4 (4 x reduce_blocks(n)).
+int pcg_update(int n, const double *num, const double *den, double *u,
+               double *r, const double *p, const double *t, double *part4,
+               cudaStream_t s);
+// p = 1.0 * z + beta * p with beta = num/den computed on device.
+int pcg_axpby(int n, const double *num, const double *den, const double *z,
+              double *p, cudaStream_t s);
+// y = x (copy), y = 0
+template <typename T>
+int vcopy(int n, const T *x, T *y, cudaStream_t s);
+template <typename T>
+int vzero(int n, T *y, cudaStream_t s);
+// precision conversions
+int d2f(int n, const double *x, float *y, cudaStream_t s);
+int f2d(int n, const float *x, double *y, cudaStream_t s);
+int csr_val_d2f(int nnz, const double *x, float *y, cudaStream_t s);
+
+// Dense coarse solve y = Ainv x (row-major n x n FP64 inverse).
+template <typename TI>
+int dense_gemv(int n, const double *Ainv, const TI *x, TI *y, cudaStream_t s);
+
+}  // namespace hzb

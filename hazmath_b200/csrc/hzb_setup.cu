@@ -1,0 +1,980 @@
+// hzb_setup.cu -- setup-phase kernels of the UA-AMG hierarchy.
+// Compiled with -fmad=false like the cycle kernels: the Galerkin sums are
+// rounded in the reference's order.
+#include "hzb_setup.cuh"
+#include <algorithm>
+#include <vector>
+
+namespace hzb {
+
+// ---------------------------------------------------------------------------
+// exclusive scan (int32)
+// ---------------------------------------------------------------------------
+constexpr int SCAN_BLOCK = 256, SCAN_ITEMS = 8, SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_exscan(int v, int *sh, int *total) {
+    // inclusive warp scan
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    if (wid == 0) {
+        int w = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) sh[lane] = w;   // inclusive warp totals
+    }
+    __syncthreads();
+    const int before = wid > 0 ? sh[wid - 1] : 0;
+    *total = sh[nw - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void k_scan_tiles(const int *__restrict__ in, int n, int *tiles) {
+    __shared__ int sh[32];
+    const int base = blockIdx.x * SCAN_TILE;
+    int v = 0;
+    for (int k = threadIdx.x; k < SCAN_TILE; k += SCAN_BLOCK) {
+        int i = base + k;
+        if (i < n) v += in[i];
+    }
+    int tot;
+    block_exscan(v, sh, &tot);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_tilesums(int *tiles, int nt) {
+    __shared__ int sh[32];
+    int carry = 0;
+    for (int b = 0; b < nt; b += blockDim.x) {
+        int i = b + threadIdx.x;
+        int v = i < nt ? tiles[i] : 0;
+        int tot;
+        int ex = block_exscan(v, sh, &tot);
+        if (i < nt) tiles[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) tiles[nt] = carry;
+}
+
+__global__ void k_scan_apply(const int *__restrict__ in, int *out, int n,
+                             const int *__restrict__ tiles) {
+    __shared__ int sh[32];
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        int i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        sum += v[k];
+    }
+    int tot;
+    int ex = block_exscan(sum, sh, &tot) + tiles[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        int i = base + k;
+        if (i < n) out[i] = ex;
+        ex += v[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tiles[gridDim.x];
+}
+
+int scan_tmp_size(int n) { return div_up(n > 0 ? n : 1, SCAN_TILE) + 1; }
+
+int scan_exclusive(const int *in, int *out, int n, int *tmp, cudaStream_t s) {
+    if (n <= 0) {
+        HZB_CUDA(cudaMemsetAsync(out, 0, sizeof(int), s));
+        return SUCCESS;
+    }
+    const int nt = div_up(n, SCAN_TILE);
+    k_scan_tiles<<<nt, SCAN_BLOCK, 0, s>>>(in, n, tmp);
+    k_scan_tilesums<<<1, 1024, 0, s>>>(tmp, nt);
+    k_scan_apply<<<nt, SCAN_BLOCK, 0, s>>>(in, out, n, tmp);
+    count_launch(3);
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// strength graph
+// ---------------------------------------------------------------------------
+__global__ void k_first_diag(int n, const int *__restrict__ ia,
+                             const int *__restrict__ ja, const double *__restrict__ a,
+                             double *d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        double v = 0.0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+            if (ja[k] == i) { v = a[k]; break; }
+        d[i] = v;
+    }
+}
+
+__device__ __forceinline__ bool strong(int i, int j, double v, double th2,
+                                       const double *d) {
+    return j == i || ((v * v) >= th2 * fabs(d[i] * d[j]) && v < 0e0);
+}
+
+__global__ void k_strength_count(int n, const int *__restrict__ ia,
+                                 const int *__restrict__ ja,
+                                 const double *__restrict__ a,
+                                 const double *__restrict__ d, double th2,
+                                 int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        int c = 0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) c += strong(i, ja[k], a[k], th2, d);
+        cnt[i] = c;
+    }
+}
+
+__global__ void k_strength_fill(int n, const int *__restrict__ ia,
+                                const int *__restrict__ ja,
+                                const double *__restrict__ a,
+                                const double *__restrict__ d, double th2,
+                                const int *__restrict__ nia, int *nja,
+                                double *nval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        int p = nia[i];
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+            if (strong(i, ja[k], a[k], th2, d)) { nja[p] = ja[k]; nval[p] = a[k]; ++p; }
+    }
+}
+
+int strength_graph(const DCsr<double> &A, double theta, int *nia, int *nja,
+                   double *nval, int *nnnz, int *tmp, cudaStream_t s) {
+    const int n = A.n;
+    double *d = nullptr;
+    int *cnt = nullptr;
+    HZB_TRY(dalloc(&d, n));
+    int rc = dalloc(&cnt, n);
+    if (rc) { dfree(d); return rc; }
+    const double th2 = theta * theta;
+    const int g = grid_for(n);
+    k_first_diag<<<g, 256, 0, s>>>(n, A.ia, A.ja, A.val, d);
+    k_strength_count<<<g, 256, 0, s>>>(n, A.ia, A.ja, A.val, d, th2, cnt);
+    count_launch(2);
+    rc = scan_exclusive(cnt, nia, n, tmp, s);
+    if (!rc) {
+        k_strength_fill<<<g, 256, 0, s>>>(n, A.ia, A.ja, A.val, d, th2, nia, nja, nval);
+        count_launch();
+        cudaError_t e = cudaMemcpyAsync(nnnz, nia + n, sizeof(int),
+                                        cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; }
+    }
+    dfree(d);
+    dfree(cnt);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// heavy edge matching, reference order: one warp walks the vertices in
+// ascending order; the 32 lanes examine a row's neighbours together.
+// ---------------------------------------------------------------------------
+// Candidate order of heavy_edg(w, id, iz-1, 0): the largest weight wins, and
+// among equal weights the later position in the row (backward scan, strict >).
+__device__ __forceinline__ void better_last(double &w, int &p, double w2, int p2) {
+    if (p2 >= 0 && (p < 0 || w2 > w || (w2 == w && p2 > p))) { w = w2; p = p2; }
+}
+// heavy_edg(w, id, 0, iz-1): largest weight, among equals the earlier position.
+__device__ __forceinline__ void better_first(double &w, int &p, double w2, int p2) {
+    if (p2 >= 0 && (p < 0 || w2 > w || (w2 == w && p2 < p))) { w = w2; p = p2; }
+}
+
+__global__ void __launch_bounds__(32)
+k_hem_seq(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+          const double *__restrict__ a, int *mask_, int *cnt_, int *out) {
+    volatile int *mask = mask_;
+    volatile int *cnt = cnt_;
+    const int lane = threadIdx.x;
+    for (int k = lane; k < n; k += 32) {
+        mask[k] = (ia[k + 1] - ia[k] > 1) ? -1 : -2;   // pass 0
+        cnt[k] = 0;
+    }
+    __syncwarp();
+    int nc = 0;
+    for (int k = 0; k < n; ++k) {                      // pass 1
+        if (mask[k] != -1) continue;
+        const int b0 = ia[k], b1 = ia[k + 1];
+        double bw = 0.0;
+        int bp = -1;
+        for (int p = b0 + lane; p < b1; p += 32) {
+            const int j = ja[p];
+            if (j != k && mask[j] < 0) better_last(bw, bp, fabs(a[p]), p);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w2 = __shfl_xor_sync(0xffffffffu, bw, o);
+            int p2 = __shfl_xor_sync(0xffffffffu, bp, o);
+            better_last(bw, bp, w2, p2);
+        }
+        if (bp >= 0) {
+            if (lane == 0) {
+                const int pick = ja[bp];
+                mask[k] = nc;
+                mask[pick] = nc;
+                cnt[nc] = 2;
+            }
+            ++nc;
+        }
+        __syncwarp();
+    }
+    int status = 0;
+    for (int k = 0; k < n; ++k) {                      // pass 2
+        if (mask[k] != -1) continue;
+        const int b0 = ia[k], b1 = ia[k + 1];
+        double bw = 0.0;
+        int bp = -1, bc = -1;
+        for (int p = b0 + lane; p < b1; p += 32) {
+            const int kc = mask[ja[p]];
+            if (kc >= 0) {
+                double w2 = (double)(-cnt[kc]);
+                int oldp = bp;
+                better_first(bw, bp, w2, p);
+                if (bp != oldp) bc = kc;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w2 = __shfl_xor_sync(0xffffffffu, bw, o);
+            int p2 = __shfl_xor_sync(0xffffffffu, bp, o);
+            int c2 = __shfl_xor_sync(0xffffffffu, bc, o);
+            int oldp = bp;
+            better_first(bw, bp, w2, p2);
+            if (bp != oldp) bc = c2;
+        }
+        if (bp < 0) { status = -1; break; }
+        if (lane == 0) {
+            mask[k] = bc;
+            cnt[bc] = cnt[bc] + 1;
+        }
+        __syncwarp();
+    }
+    __syncwarp();
+    for (int k = lane; k < n; k += 32)                 // pass 3
+        if (mask[k] < 0) mask[k] = UNPT;
+    if (lane == 0) { out[0] = nc; out[1] = status; }
+}
+
+int hem_exact(int n, const int *nia, const int *nja, const double *nval,
+              int *agg, int *nagg, int *work_n, cudaStream_t s) {
+    int *out = nullptr;
+    HZB_TRY(dalloc(&out, 2));
+    k_hem_seq<<<1, 32, 0, s>>>(n, nia, nja, nval, agg, work_n, out);
+    count_launch();
+    int h[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(h, out, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(out);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+    *nagg = h[0];
+    return h[1] < 0 ? ERROR_AMG_COARSEING : SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// deterministic parallel matching (fast mode)
+//   rounds: every free vertex points at its preferred free neighbour (the
+//   reference's preference: heaviest |a_ij|, later row position on ties);
+//   mutual pairs match, numbered by the lower vertex through a scan.
+//   Leftovers join the adjacent aggregate with the fewest members counted
+//   before the leftover pass (first such neighbour on ties).
+// ---------------------------------------------------------------------------
+__global__ void k_pm_init(int n, const int *__restrict__ ia, int *state) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x)
+        state[k] = (ia[k + 1] - ia[k] > 1) ? -1 : -2;   // -1 free, -2 isolated
+}
+
+__global__ void k_pm_point(int n, const int *__restrict__ ia,
+                           const int *__restrict__ ja, const double *__restrict__ a,
+                           const int *__restrict__ state, int *ptr) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x) {
+        int best = -1;
+        if (state[k] == -1) {
+            double bw = 0.0;
+            int bp = -1;
+            for (int p = ia[k]; p < ia[k + 1]; ++p) {
+                const int j = ja[p];
+                if (j != k && state[j] == -1) better_last(bw, bp, fabs(a[p]), p);
+            }
+            if (bp >= 0) best = ja[bp];
+        }
+        ptr[k] = best;
+    }
+}
+
+// flag[k] = 1 if k is the lower end of a mutual pair
+__global__ void k_pm_mutual(int n, const int *__restrict__ ptr, int *flag,
+                            int *any) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x) {
+        const int j = ptr[k];
+        int f = (j >= 0 && ptr[j] == k && k < j) ? 1 : 0;
+        flag[k] = f;
+        if (f) *any = 1;
+    }
+}
+
+__global__ void k_pm_assign(int n, const int *__restrict__ ptr,
+                            const int *__restrict__ flag,
+                            const int *__restrict__ pos, int base, int *state) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x)
+        if (flag[k]) {
+            const int c = base + pos[k];
+            state[k] = c;
+            state[ptr[k]] = c;
+        }
+}
+
+__global__ void k_pm_sizes(int n, const int *__restrict__ state, int *size) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x)
+        if (state[k] >= 0) atomicAdd(size + state[k], 1);
+}
+
+__global__ void k_pm_leftover(int n, const int *__restrict__ ia,
+                              const int *__restrict__ ja,
+                              const int *__restrict__ state,
+                              const int *__restrict__ size, int *out, int *bad) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x) {
+        int st = state[k];
+        if (st == -1) {
+            int bc = -1, bs = 0;
+            for (int p = ia[k]; p < ia[k + 1]; ++p) {
+                const int c = state[ja[p]];
+                if (c >= 0 && (bc < 0 || size[c] < bs)) { bc = c; bs = size[c]; }
+            }
+            if (bc < 0) *bad = 1;
+            st = bc;
+        }
+        out[k] = st < 0 ? UNPT : st;
+    }
+}
+
+int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
+                 int *agg, int *nagg, int *work, cudaStream_t s) {
+    // work layout (ints): state n | ptr n | flag n | pos n+1 | size n | scan tmp
+    int *state = work, *ptr = work + n, *flag = work + 2 * n, *pos = work + 3 * n;
+    int *size = work + 4 * n + 1, *tmp = work + 5 * n + 1;
+    int *dflag = nullptr;
+    HZB_TRY(dalloc(&dflag, 2));
+    const int g = grid_for(n);
+    k_pm_init<<<g, 256, 0, s>>>(n, nia, state);
+    count_launch();
+    int nc = 0;
+    for (int round = 0; round < 64; ++round) {
+        cudaMemsetAsync(dflag, 0, sizeof(int), s);
+        k_pm_point<<<g, 256, 0, s>>>(n, nia, nja, nval, state, ptr);
+        k_pm_mutual<<<g, 256, 0, s>>>(n, ptr, flag, dflag);
+        count_launch(2);
+        int any = 0, cnt = 0;
+        int rc = scan_exclusive(flag, pos, n, tmp, s);
+        if (rc) { dfree(dflag); return rc; }
+        cudaMemcpyAsync(&any, dflag, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&cnt, pos + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { dfree(dflag); set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+        if (!any) break;
+        k_pm_assign<<<g, 256, 0, s>>>(n, ptr, flag, pos, nc, state);
+        count_launch();
+        nc += cnt;
+    }
+    cudaMemsetAsync(size, 0, sizeof(int) * (nc > 0 ? nc : 1), s);
+    cudaMemsetAsync(dflag + 1, 0, sizeof(int), s);
+    k_pm_sizes<<<g, 256, 0, s>>>(n, state, size);
+    k_pm_leftover<<<g, 256, 0, s>>>(n, nia, nja, state, size, agg, dflag + 1);
+    count_launch(2);
+    int bad = 0;
+    cudaMemcpyAsync(&bad, dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    dfree(dflag);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+    *nagg = nc;
+    return bad ? ERROR_AMG_COARSEING : SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// R = P^T pattern with ascending fine indices per row
+// ---------------------------------------------------------------------------
+__global__ void k_agg_count(int n, const int *__restrict__ agg, int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        if (agg[i] >= 0) atomicAdd(cnt + agg[i], 1);
+}
+__global__ void k_agg_fill(int n, const int *__restrict__ agg,
+                           const int *__restrict__ ria, int *fillc, int *rja) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const int c = agg[i];
+        if (c >= 0) rja[ria[c] + atomicAdd(fillc + c, 1)] = i;
+    }
+}
+__global__ void k_sort_rows(int nr, const int *__restrict__ ia, int *ja) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nr;
+         r += gridDim.x * blockDim.x) {
+        const int b0 = ia[r], b1 = ia[r + 1];
+        for (int p = b0 + 1; p < b1; ++p) {      // insertion sort (short rows)
+            int v = ja[p], q = p - 1;
+            while (q >= b0 && ja[q] > v) { ja[q + 1] = ja[q]; --q; }
+            ja[q + 1] = v;
+        }
+    }
+}
+
+int restriction_pattern(int n, int nc, const int *agg, int *ria, int *rja,
+                        int *tmp, cudaStream_t s) {
+    int *cnt = nullptr;
+    HZB_TRY(dalloc(&cnt, nc));
+    HZB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (nc > 0 ? nc : 1), s));
+    k_agg_count<<<grid_for(n), 256, 0, s>>>(n, agg, cnt);
+    count_launch();
+    int rc = scan_exclusive(cnt, ria, nc, tmp, s);
+    if (!rc) {
+        cudaMemsetAsync(cnt, 0, sizeof(int) * (nc > 0 ? nc : 1), s);
+        k_agg_fill<<<grid_for(n), 256, 0, s>>>(n, agg, ria, cnt, rja);
+        k_sort_rows<<<grid_for(nc), 256, 0, s>>>(nc, ria, rja);
+        count_launch(2);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; }
+    }
+    dfree(cnt);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin product A_c = R A P for unit aggregation P (exact order)
+// ---------------------------------------------------------------------------
+__global__ void k_rap_bound(int nc, const int *__restrict__ ria,
+                            const int *__restrict__ rja, const int *__restrict__ ia,
+                            int *ub) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc;
+         c += gridDim.x * blockDim.x) {
+        int u = 1;
+        for (int q = ria[c]; q < ria[c + 1]; ++q) {
+            const int i = rja[q];
+            u += ia[i + 1] - ia[i];
+        }
+        ub[c] = u;
+    }
+}
+
+// One thread per coarse row builds its slot list in scratch: slot 0 is the
+// diagonal (0.0, accumulated); other columns in first-encounter order; a new
+// column takes the entry's value, a known column adds it.
+__global__ void k_rap_build(int nc, const int *__restrict__ ria,
+                            const int *__restrict__ rja, const int *__restrict__ ia,
+                            const int *__restrict__ ja, const double *__restrict__ a,
+                            const int *__restrict__ agg, const int *__restrict__ off,
+                            int *scol, double *sval, int *rowcnt) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc;
+         c += gridDim.x * blockDim.x) {
+        int *cols = scol + off[c];
+        double *vals = sval + off[c];
+        int cnt = 1;
+        cols[0] = c;
+        vals[0] = 0.0;
+        for (int q = ria[c]; q < ria[c + 1]; ++q) {
+            const int i = rja[q];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                const int cc = agg[ja[k]];
+                if (cc < 0) continue;
+                int pos = -1;
+                for (int t = 0; t < cnt; ++t)
+                    if (cols[t] == cc) { pos = t; break; }
+                if (pos >= 0) {
+                    vals[pos] += a[k];
+                } else {
+                    cols[cnt] = cc;
+                    vals[cnt] = a[k];
+                    ++cnt;
+                }
+            }
+        }
+        rowcnt[c] = cnt;
+    }
+}
+
+__global__ void k_rap_compact(int nc, const int *__restrict__ off,
+                              const int *__restrict__ cia,
+                              const int *__restrict__ scol,
+                              const double *__restrict__ sval, int *cja,
+                              double *cval) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc;
+         c += gridDim.x * blockDim.x) {
+        const int src = off[c], dst = cia[c], m = cia[c + 1] - cia[c];
+        for (int t = 0; t < m; ++t) {
+            cja[dst + t] = scol[src + t];
+            cval[dst + t] = sval[src + t];
+        }
+    }
+}
+
+int rap_agg(const DCsr<double> &A, int nc, const int *agg, const int *ria,
+            const int *rja, int **cia_out, int **cja_out, double **cval_out,
+            int *cnnz, cudaStream_t s) {
+    *cia_out = nullptr; *cja_out = nullptr; *cval_out = nullptr;
+    int *ub = nullptr, *off = nullptr, *tmp = nullptr, *rowcnt = nullptr;
+    int *scol = nullptr, *cia = nullptr, *cja = nullptr;
+    double *sval = nullptr, *cval = nullptr;
+    int rc = SUCCESS, total = 0;
+    const int g = grid_for(nc);
+    cudaError_t e;
+    if ((rc = dalloc(&ub, nc))) goto fail;
+    if ((rc = dalloc(&off, nc + 1))) goto fail;
+    if ((rc = dalloc(&tmp, scan_tmp_size(nc + 1)))) goto fail;
+    if ((rc = dalloc(&rowcnt, nc))) goto fail;
+    if ((rc = dalloc(&cia, nc + 1))) goto fail;
+    k_rap_bound<<<g, 256, 0, s>>>(nc, ria, rja, A.ia, ub);
+    count_launch();
+    if ((rc = scan_exclusive(ub, off, nc, tmp, s))) goto fail;
+    e = cudaMemcpyAsync(&total, off + nc, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto fail; }
+    if ((rc = dalloc(&scol, total))) goto fail;
+    if ((rc = dalloc(&sval, total))) goto fail;
+    k_rap_build<<<g, 128, 0, s>>>(nc, ria, rja, A.ia, A.ja, A.val, agg, off, scol,
+                                  sval, rowcnt);
+    count_launch();
+    if ((rc = scan_exclusive(rowcnt, cia, nc, tmp, s))) goto fail;
+    e = cudaMemcpyAsync(cnnz, cia + nc, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto fail; }
+    if ((rc = dalloc(&cja, *cnnz))) goto fail;
+    if ((rc = dalloc(&cval, *cnnz))) goto fail;
+    k_rap_compact<<<g, 256, 0, s>>>(nc, off, cia, scol, sval, cja, cval);
+    count_launch();
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto fail; }
+    dfree(ub); dfree(off); dfree(tmp); dfree(rowcnt); dfree(scol); dfree(sval);
+    *cia_out = cia; *cja_out = cja; *cval_out = cval;
+    return SUCCESS;
+fail:
+    dfree(ub); dfree(off); dfree(tmp); dfree(rowcnt); dfree(scol); dfree(sval);
+    dfree(cia); dfree(cja); dfree(cval);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// smoother diagonals
+// ---------------------------------------------------------------------------
+__global__ void k_diags(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                        const double *__restrict__ a, double *djac, double *dgs,
+                        double *dsor, int *gs_ok, int *sor_ok, int *missing) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        double dj = 0.0, dg = 0.0, ds = 0.0;
+        int okg = 0, oks = 0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            if (ja[k] != i) continue;
+            dj = a[k];
+            ds = a[k];
+            oks = 1;
+            if (fabs(a[k]) > SMALLREAL) { dg = 1.e+0 / a[k]; okg = 1; }
+        }
+        djac[i] = dj;
+        dgs[i] = dg;
+        dsor[i] = ds;
+        gs_ok[i] = okg;
+        sor_ok[i] = oks;
+        if (!okg || !oks) atomicAdd(missing, 1);
+    }
+}
+
+// Rows without a (usable) diagonal keep the previous row's d in the
+// reference's sweep; resolve that carry sequentially (rare path).
+__global__ void k_diag_carry(int n, const double *__restrict__ dgs,
+                             const double *__restrict__ dsor,
+                             const int *__restrict__ gs_ok,
+                             const int *__restrict__ sor_ok, double *gf,
+                             double *gb, double *sf, double *sb) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double c1 = 0.0, c2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        if (gs_ok[i]) c1 = dgs[i];
+        if (sor_ok[i]) c2 = dsor[i];
+        gf[i] = c1;
+        sf[i] = c2;
+    }
+    c1 = 0.0; c2 = 0.0;
+    for (int i = n - 1; i >= 0; --i) {
+        if (gs_ok[i]) c1 = dgs[i];
+        if (sor_ok[i]) c2 = dsor[i];
+        gb[i] = c1;
+        sb[i] = c2;
+    }
+}
+
+int smoother_diagonals(const DCsr<double> &A, double *d_jac, double *d_gs_f,
+                       double *d_gs_b, double *d_sor_f, double *d_sor_b,
+                       cudaStream_t s) {
+    const int n = A.n;
+    int *ok = nullptr;
+    HZB_TRY(dalloc(&ok, 2 * (size_t)n + 1));
+    int *missing = ok + 2 * (size_t)n;
+    HZB_CUDA(cudaMemsetAsync(missing, 0, sizeof(int), s));
+    k_diags<<<grid_for(n), 256, 0, s>>>(n, A.ia, A.ja, A.val, d_jac, d_gs_f, d_sor_f,
+                                        ok, ok + n, missing);
+    count_launch();
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, missing, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { dfree(ok); set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+    if (h) {
+        double *tg = nullptr, *ts = nullptr;
+        int rc = dalloc(&tg, n);
+        if (!rc) rc = dalloc(&ts, n);
+        if (rc) { dfree(tg); dfree(ok); return rc; }
+        cudaMemcpyAsync(tg, d_gs_f, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(ts, d_sor_f, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        k_diag_carry<<<1, 32, 0, s>>>(n, tg, ts, ok, ok + n, d_gs_f, d_gs_b, d_sor_f,
+                                      d_sor_b);
+        count_launch();
+        e = cudaStreamSynchronize(s);
+        dfree(tg); dfree(ts);
+        if (e != cudaSuccess) { dfree(ok); set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+    } else {
+        cudaMemcpyAsync(d_gs_b, d_gs_f, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d_sor_b, d_sor_f, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+    }
+    dfree(ok);
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// A^T with ascending column indices per row (dcsr_transz, p = NULL)
+// ---------------------------------------------------------------------------
+__global__ void k_tr_count(int n, const int *__restrict__ ia,
+                           const int *__restrict__ ja, int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) atomicAdd(cnt + ja[k], 1);
+}
+__global__ void k_tr_fill(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                          const double *__restrict__ a, const int *__restrict__ tia,
+                          int *fillc, int *tja, double *tval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            const int q = tia[ja[k]] + atomicAdd(fillc + ja[k], 1);
+            tja[q] = i;
+            tval[q] = a[k];
+        }
+}
+// rows of the transpose in ascending order (stable for equal indices is not
+// needed: a row index appears once per source row entry)
+__global__ void k_tr_sort(int n, const int *__restrict__ tia, int *tja, double *tval) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n;
+         r += gridDim.x * blockDim.x) {
+        const int b0 = tia[r], b1 = tia[r + 1];
+        for (int p = b0 + 1; p < b1; ++p) {
+            const int v = tja[p];
+            const double x = tval[p];
+            int q = p - 1;
+            while (q >= b0 && tja[q] > v) { tja[q + 1] = tja[q]; tval[q + 1] = tval[q]; --q; }
+            tja[q + 1] = v;
+            tval[q + 1] = x;
+        }
+    }
+}
+
+int transpose_csr(const DCsr<double> &A, int **tia_out, int **tja_out,
+                  double **tval_out, cudaStream_t s) {
+    const int n = A.n;
+    int *tia = nullptr, *tja = nullptr, *cnt = nullptr, *tmp = nullptr;
+    double *tval = nullptr;
+    int rc = SUCCESS;
+    const int g = grid_for(n);
+    if ((rc = dalloc(&tia, n + 1)) || (rc = dalloc(&tja, A.nnz)) ||
+        (rc = dalloc(&tval, A.nnz)) || (rc = dalloc(&cnt, n)) ||
+        (rc = dalloc(&tmp, scan_tmp_size(n + 1)))) goto fail;
+    cudaMemsetAsync(cnt, 0, sizeof(int) * n, s);
+    k_tr_count<<<g, 256, 0, s>>>(n, A.ia, A.ja, cnt);
+    count_launch();
+    if ((rc = scan_exclusive(cnt, tia, n, tmp, s))) goto fail;
+    cudaMemsetAsync(cnt, 0, sizeof(int) * n, s);
+    k_tr_fill<<<g, 256, 0, s>>>(n, A.ia, A.ja, A.val, tia, cnt, tja, tval);
+    k_tr_sort<<<g, 256, 0, s>>>(n, tia, tja, tval);
+    count_launch(2);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error(cudaGetLastError(), __FILE__, __LINE__);
+        rc = ERROR_SOLVER_MISC;
+        goto fail;
+    }
+    dfree(cnt); dfree(tmp);
+    *tia_out = tia; *tja_out = tja; *tval_out = tval;
+    return SUCCESS;
+fail:
+    dfree(tia); dfree(tja); dfree(tval); dfree(cnt); dfree(tmp);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// level schedules (Kahn rounds on the DAG lower -> higher or reverse)
+// ---------------------------------------------------------------------------
+void Schedule::release() {
+    dfree(rows);
+    dfree(set_ptr);
+    h_ptr.clear();
+    run_first.clear();
+    run_last.clear();
+}
+
+__global__ void k_transpose_count(int n, const int *__restrict__ ia,
+                                  const int *__restrict__ ja, int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) atomicAdd(cnt + ja[k], 1);
+}
+__global__ void k_transpose_fill(int n, const int *__restrict__ ia,
+                                 const int *__restrict__ ja,
+                                 const int *__restrict__ tia, int *fillc, int *tja) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            const int j = ja[k];
+            tja[tia[j] + atomicAdd(fillc + j, 1)] = i;
+        }
+}
+
+// dependency count: neighbours that come earlier in the sweep
+__global__ void k_indeg(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                        const int *__restrict__ tia, const int *__restrict__ tja,
+                        int backward, int *indeg, int *rows, int *tail) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        int c = 0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            const int j = ja[k];
+            c += backward ? (j > i) : (j < i);
+        }
+        for (int k = tia[i]; k < tia[i + 1]; ++k) {
+            const int j = tja[k];
+            c += backward ? (j > i) : (j < i);
+        }
+        indeg[i] = c;
+        if (c == 0) rows[atomicAdd(tail, 1)] = i;
+    }
+}
+
+__global__ void k_kahn_round(int head, int cnt, const int *__restrict__ ia,
+                             const int *__restrict__ ja, const int *__restrict__ tia,
+                             const int *__restrict__ tja, int backward, int *indeg,
+                             int *rows, int *tail) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt;
+         q += gridDim.x * blockDim.x) {
+        const int i = rows[head + q];
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            const int j = ja[k];
+            if (backward ? (j < i) : (j > i))
+                if (atomicSub(indeg + j, 1) == 1) rows[atomicAdd(tail, 1)] = j;
+        }
+        for (int k = tia[i]; k < tia[i + 1]; ++k) {
+            const int j = tja[k];
+            if (backward ? (j < i) : (j > i))
+                if (atomicSub(indeg + j, 1) == 1) rows[atomicAdd(tail, 1)] = j;
+        }
+    }
+}
+
+static void make_runs(Schedule *sch) {
+    const int ns = (int)sch->h_ptr.size() - 1;
+    int k = 0;
+    while (k < ns) {
+        int k2 = k;
+        while (k2 < ns && sch->h_ptr[k2 + 1] - sch->h_ptr[k2] <= 1024) ++k2;
+        if (k2 > k) {   // run of small sets
+            sch->run_first.push_back(k);
+            sch->run_last.push_back(k2);
+            k = k2;
+        } else {        // one large set: a grid-wide launch (marked by -1)
+            sch->run_first.push_back(k);
+            sch->run_last.push_back(-1);
+            ++k;
+        }
+    }
+}
+
+int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,
+                Schedule *sch, cudaStream_t s) {
+    sch->release();
+    int *tia = nullptr, *tja = nullptr, *fillc = nullptr, *indeg = nullptr;
+    int *tail = nullptr, *tmp = nullptr;
+    int rc = SUCCESS;
+    std::vector<int> ptr;
+    cudaError_t e;
+    const int g = grid_for(n);
+    if ((rc = dalloc(&tia, n + 1))) goto done;
+    if ((rc = dalloc(&tja, nnz))) goto done;
+    if ((rc = dalloc(&fillc, n))) goto done;
+    if ((rc = dalloc(&indeg, n))) goto done;
+    if ((rc = dalloc(&tail, 1))) goto done;
+    if ((rc = dalloc(&tmp, scan_tmp_size(n + 1)))) goto done;
+    if ((rc = dalloc(&sch->rows, n))) goto done;
+    cudaMemsetAsync(fillc, 0, sizeof(int) * n, s);
+    cudaMemsetAsync(tail, 0, sizeof(int), s);
+    k_transpose_count<<<g, 256, 0, s>>>(n, ia, ja, fillc);
+    count_launch();
+    if ((rc = scan_exclusive(fillc, tia, n, tmp, s))) goto done;
+    cudaMemsetAsync(fillc, 0, sizeof(int) * n, s);
+    k_transpose_fill<<<g, 256, 0, s>>>(n, ia, ja, tia, fillc, tja);
+    k_indeg<<<g, 256, 0, s>>>(n, ia, ja, tia, tja, backward, indeg, sch->rows, tail);
+    count_launch(2);
+    {
+        int head = 0, cur = 0;
+        e = cudaMemcpyAsync(&cur, tail, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+        ptr.push_back(0);
+        while (cur > head) {
+            ptr.push_back(cur);
+            const int cnt = cur - head;
+            k_kahn_round<<<grid_for(cnt), 256, 0, s>>>(head, cnt, ia, ja, tia, tja,
+                                                       backward, indeg, sch->rows, tail);
+            count_launch();
+            head = cur;
+            e = cudaMemcpyAsync(&cur, tail, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+        }
+        if (head != n) {   // a cycle cannot occur in index order; guard anyway
+            set_error_msg("gs_schedule: incomplete level schedule");
+            rc = ERROR_DATA_STRUCTURE;
+            goto done;
+        }
+    }
+    sch->h_ptr = ptr;
+    if ((rc = dalloc(&sch->set_ptr, ptr.size()))) goto done;
+    e = cudaMemcpyAsync(sch->set_ptr, ptr.data(), sizeof(int) * ptr.size(),
+                        cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+    make_runs(sch);
+done:
+    dfree(tia); dfree(tja); dfree(fillc); dfree(indeg); dfree(tail); dfree(tmp);
+    if (rc) sch->release();
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// multicolouring (Jones-Plassmann, hashed priorities, smallest free colour)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned hash_u32(unsigned x) {
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return x;
+}
+
+__global__ void k_jp_round(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                           const int *__restrict__ col_in, int *col_out, int *left) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        int c = col_in[i];
+        if (c >= 0) { col_out[i] = c; continue; }
+        const unsigned pi = hash_u32((unsigned)i);
+        bool top = true;
+        unsigned long long used = 0ull;   // colours 0..63 taken by neighbours
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            const int j = ja[k];
+            if (j == i) continue;
+            const int cj = col_in[j];
+            if (cj >= 0) {
+                if (cj < 64) used |= 1ull << cj;
+            } else {
+                const unsigned pj = hash_u32((unsigned)j);
+                if (pj > pi || (pj == pi && j > i)) { top = false; }
+            }
+        }
+        if (top) {
+            int cc = 0;
+            while (cc < 64 && (used >> cc & 1ull)) ++cc;
+            col_out[i] = cc;
+        } else {
+            col_out[i] = -1;
+            atomicAdd(left, 1);
+        }
+    }
+}
+
+__global__ void k_color_count(int n, const int *__restrict__ col, int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        atomicAdd(cnt + col[i], 1);
+}
+__global__ void k_color_fill(int n, const int *__restrict__ col,
+                             const int *__restrict__ ptr, int *fillc, int *rows) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        rows[ptr[col[i]] + atomicAdd(fillc + col[i], 1)] = i;
+}
+
+int multicolor(int n, const int *ia, const int *ja, Schedule *sch, cudaStream_t s) {
+    sch->release();
+    int *c0 = nullptr, *c1 = nullptr, *left = nullptr, *cnt = nullptr, *ptr = nullptr;
+    int *tmp = nullptr;
+    int rc = SUCCESS, ncol = 0;
+    cudaError_t e;
+    const int g = grid_for(n);
+    std::vector<int> hp;
+    if ((rc = dalloc(&c0, n))) goto done;
+    if ((rc = dalloc(&c1, n))) goto done;
+    if ((rc = dalloc(&left, 1))) goto done;
+    if ((rc = dalloc(&cnt, 65))) goto done;
+    if ((rc = dalloc(&ptr, 66))) goto done;
+    if ((rc = dalloc(&tmp, scan_tmp_size(66)))) goto done;
+    if ((rc = dalloc(&sch->rows, n))) goto done;
+    cudaMemsetAsync(c0, 0xff, sizeof(int) * n, s);
+    for (int round = 0; round < 4096; ++round) {
+        int hl = 0;
+        cudaMemsetAsync(left, 0, sizeof(int), s);
+        k_jp_round<<<g, 256, 0, s>>>(n, ia, ja, c0, c1, left);
+        count_launch();
+        std::swap(c0, c1);
+        e = cudaMemcpyAsync(&hl, left, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+        if (!hl) break;
+    }
+    cudaMemsetAsync(cnt, 0, sizeof(int) * 65, s);
+    k_color_count<<<g, 256, 0, s>>>(n, c0, cnt);
+    count_launch();
+    if ((rc = scan_exclusive(cnt, ptr, 65, tmp, s))) goto done;
+    hp.resize(66);
+    e = cudaMemcpyAsync(hp.data(), ptr, sizeof(int) * 66, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+    if (hp[65] != n) { set_error_msg("multicolor: more than 64 colours"); rc = ERROR_DATA_STRUCTURE; goto done; }
+    cudaMemsetAsync(cnt, 0, sizeof(int) * 65, s);
+    k_color_fill<<<g, 256, 0, s>>>(n, c0, ptr, cnt, sch->rows);
+    count_launch();
+    ncol = 0;
+    while (ncol < 65 && hp[ncol + 1] > hp[ncol]) ++ncol;
+    sch->h_ptr.assign(hp.begin(), hp.begin() + ncol + 1);
+    if ((rc = dalloc(&sch->set_ptr, ncol + 1))) goto done;
+    e = cudaMemcpyAsync(sch->set_ptr, sch->h_ptr.data(), sizeof(int) * (ncol + 1),
+                        cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+    make_runs(sch);
+done:
+    dfree(c0); dfree(c1); dfree(left); dfree(cnt); dfree(ptr); dfree(tmp);
+    if (rc) sch->release();
+    return rc;
+}
+
+}  // namespace hzb

@@ -1,0 +1,76 @@
+// hzb_setup.cuh -- setup-phase kernels: strength graph, heavy edge matching,
+// restriction pattern, Galerkin product, smoother diagonals, level schedules,
+// colouring, dense coarse factorisation.
+#pragma once
+#include <vector>
+#include "hzb_kernels.cuh"
+
+namespace hzb {
+
+// out[0..n] = exclusive scan of in[0..n), out[n] = total.  tmp: >= scan_tmp(n)
+int scan_tmp_size(int n);
+int scan_exclusive(const int *in, int *out, int n, int *tmp, cudaStream_t s);
+
+// strength graph Neigh (construct_strongly_coupled, amg_setup_ua.c:375-455);
+// nia sized n+1, nja/nval sized nnz; returns its nnz through *nnnz.
+int strength_graph(const DCsr<double> &A, double theta, int *nia, int *nja,
+                   double *nval, int *nnnz, int *tmp, cudaStream_t s);
+
+// heavy edge matching (aggregation_hem, amg_setup_ua.c:913-1050), exact
+// reference visiting order, on the strength graph.  agg: n outputs.
+// Returns SUCCESS, or ERROR_AMG_COARSEING where the reference exits (an
+// isolated point on the second pass).
+int hem_exact(int n, const int *nia, const int *nja, const double *nval,
+              int *agg, int *nagg, int *work_n, cudaStream_t s);
+// deterministic parallel matching (mutual heaviest neighbour rounds + the
+// same leftover rule against pre-pass-2 sizes); not bit-exact.
+int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
+                 int *agg, int *nagg, int *work, cudaStream_t s);
+
+// R = P^T: rows of R list fine indices ascending (dcsr_trans, sparse.c:770).
+int restriction_pattern(int n, int nc, const int *agg, int *ria, int *rja,
+                        int *tmp, cudaStream_t s);
+
+// A_c = R A P (dcsr_rap_agg, sparse.c:2557-2690), reference slot order and
+// summation order.  Allocates *cia (nc+1), *cja, *cval.
+int rap_agg(const DCsr<double> &A, int nc, const int *agg, const int *ria,
+            const int *rja, int **cia, int **cja, double **cval, int *cnnz,
+            cudaStream_t s);
+
+// A^T with ascending column indices in every row (dcsr_transz with p = NULL,
+// sparse.c); allocates the three arrays.
+int transpose_csr(const DCsr<double> &A, int **tia, int **tja, double **tval,
+                  cudaStream_t s);
+
+// Per-row diagonals used by the smoothers (d_jac: last diagonal entry or 0;
+// d_gs_f/_b: 1/a_ii of the last usable diagonal entry with the reference's
+// carry-over from the previous row in sweep order; d_sor_f/_b: last diagonal
+// entry with carry-over).
+int smoother_diagonals(const DCsr<double> &A, double *d_jac, double *d_gs_f,
+                       double *d_gs_b, double *d_sor_f, double *d_sor_b,
+                       cudaStream_t s);
+
+// Level schedule of lexicographic Gauss-Seidel: rows grouped into sets that
+// depend only on earlier sets (forward: on lower-numbered neighbours in A or
+// A^T; backward: higher).  perm (n) and host set pointers.
+struct Schedule {
+    int *rows = nullptr;           // device, n
+    int *set_ptr = nullptr;        // device, nsets+1
+    std::vector<int> h_ptr;        // host copy of set_ptr
+    std::vector<int> run_first;    // runs of small sets for one CTA: [first,last)
+    std::vector<int> run_last;
+    void release();
+};
+int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,
+                Schedule *sch, cudaStream_t s);
+// Colour classes (Jones-Plassmann with hashed priorities, smallest free
+// colour): rows sorted by colour, host colour pointers.
+int multicolor(int n, const int *ia, const int *ja, Schedule *sch,
+               cudaStream_t s);
+
+// Coarsest level: dense inverse (row-major, n x n) of the SPD coarse matrix
+// through a Cholesky factorisation.  Returns ERROR_DATA_ZERODIAG if a pivot
+// is not positive.
+int dense_inverse(const DCsr<double> &A, double **Ainv, cudaStream_t s);
+
+}  // namespace hzb

@@ -1,0 +1,850 @@
+// hzb_solver.cu -- UA-AMG hierarchy setup, V/W cycles and Krylov loops.
+//
+// Control flow mirrors the reference line by line (cited per function); all
+// vector work is device kernels on one stream, the host only sequences them
+// and reads back the scalars the reference's branches test.
+#include "hzb_solver.cuh"
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace hzb {
+
+// ---------------------------------------------------------------------------
+// small kernels local to the Krylov loops
+// ---------------------------------------------------------------------------
+__global__ void k_dot2_partial(int n, const double *__restrict__ z,
+                               const double *__restrict__ t,
+                               const double *__restrict__ r, double *part) {
+    __shared__ double sh[32];
+    double a = 0.0, b = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const double zi = z[i];
+        a += zi * t[i];
+        b += zi * r[i];
+    }
+    a = block_sum(a, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+    b = block_sum(b, sh);
+    if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = b;
+}
+
+// flexible-CG direction: p = z + beta p, beta = -(z, A p_old) / (p_old, A p_old)
+__global__ void k_fcg_p(int n, const double *__restrict__ zt,
+                        const double *__restrict__ pap,
+                        const double *__restrict__ z, double *p) {
+    const double beta = -zt[0] / pap[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+__global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
+
+// ---------------------------------------------------------------------------
+// containers
+// ---------------------------------------------------------------------------
+void Level::release() {
+    if (own_A) { dfree(ia); dfree(ja); dfree(val); }
+    ia = ja = nullptr; val = nullptr;
+    dfree(val32);
+    dfree(agg); dfree(ria); dfree(rja);
+    dfree(b); dfree(x); dfree(w); dfree(t);
+    dfree(b32); dfree(x32); dfree(w32); dfree(t32);
+    dfree(d_jac); dfree(d_gs_f); dfree(d_gs_b); dfree(d_sor_f); dfree(d_sor_b);
+    dfree(d_gs32);
+    dfree(tia); dfree(tja); dfree(tval);
+    fwd.release(); bwd.release(); col.release();
+}
+
+// scalar slots of KrylovWork::sc
+enum { SC_T1 = 0, SC_T2 = 1, SC_RR = 2, SC_UM = 3, SC_UU = 4, SC_PP = 5,
+       SC_T3 = 6, SC_ZT = 7, SC_X = 8, SC_N = 16 };
+
+int KrylovWork::alloc(int nn) {
+    release();
+    n = nn;
+    const int G = reduce_blocks(n);
+    const int np = 4 * G + spmv_blocks(n) + 8;
+    HZB_TRY(dalloc(&p, n));
+    HZB_TRY(dalloc(&z, n));
+    HZB_TRY(dalloc(&r, n));
+    HZB_TRY(dalloc(&t, n));
+    HZB_TRY(dalloc(&part, np));
+    HZB_TRY(dalloc(&sc, SC_N));
+    HZB_CUDA(cudaMallocHost((void **)&h_sc, SC_N * sizeof(double)));
+    return SUCCESS;
+}
+void KrylovWork::release() {
+    dfree(p); dfree(z); dfree(r); dfree(t); dfree(part); dfree(sc);
+    if (h_sc) cudaFreeHost(h_sc);
+    h_sc = nullptr;
+    n = 0;
+}
+
+static int fetch(hzb_solver *S, KrylovWork &w) {
+    HZB_CUDA(cudaMemcpyAsync(w.h_sc, w.sc, SC_N * sizeof(double),
+                             cudaMemcpyDeviceToHost, S->s));
+    HZB_CUDA(cudaStreamSynchronize(S->s));
+    return SUCCESS;
+}
+
+// ||x||^2 into sc[slot] (deterministic)
+static int norm2sq(hzb_solver *S, KrylovWork &w, int n, const double *x, int slot) {
+    return dot(n, x, x, w.part, w.sc + slot, S->s);
+}
+
+// ---------------------------------------------------------------------------
+// smoothing (mgcycle.c:76-240 dispatch) on one level
+// ---------------------------------------------------------------------------
+static int run_sets(hzb_solver *S, const DCsr<double> &A, const Schedule &sc,
+                    int kind, const double *d, double w, const double *b,
+                    double *x, bool reverse) {
+    const int ns = (int)sc.h_ptr.size() - 1;
+    if (!reverse) {
+        for (size_t q = 0; q < sc.run_first.size(); ++q) {
+            const int f = sc.run_first[q], l = sc.run_last[q];
+            if (l < 0) {
+                HZB_TRY(gs_rows<double>(A, kind, sc.rows + sc.h_ptr[f],
+                                        sc.h_ptr[f + 1] - sc.h_ptr[f], d, w, b, x, S->s));
+            } else {
+                HZB_TRY(gs_run<double>(A, kind, sc.rows, sc.set_ptr, f, l, d, w, b, x, S->s));
+            }
+        }
+    } else {
+        for (int k = ns - 1; k >= 0; --k)
+            HZB_TRY(gs_rows<double>(A, kind, sc.rows + sc.h_ptr[k],
+                                    sc.h_ptr[k + 1] - sc.h_ptr[k], d, w, b, x, S->s));
+    }
+    return SUCCESS;
+}
+
+// forward Gauss-Seidel-type sweep (rows ascending) / backward (descending)
+static int gs_sweep(hzb_solver *S, Level &L, int kind, bool forward, double w) {
+    const DCsr<double> A = L.A64();
+    const bool mc = S->bp.gs_schedule == HZB_GS_MULTICOLOR;
+    const bool is_gs = (kind & 15) == 0;
+    const double *d = is_gs ? (forward ? L.d_gs_f : L.d_gs_b)
+                            : (forward ? L.d_sor_f : L.d_sor_b);
+    if (mc) return run_sets(S, A, L.col, kind, d, w, L.b, L.x, !forward);
+    return run_sets(S, A, forward ? L.fwd : L.bwd, kind, d, w, L.b, L.x, false);
+}
+
+int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
+    Level &L = S->lv[l];
+    const int sweeps = pre ? cyc.presmooth_iter : cyc.postsmooth_iter;
+    const double w = cyc.relaxation;
+    const DCsr<double> A = L.A64();
+    switch (cyc.smoother) {
+    case SMOOTHER_JACOBI:
+        for (int k = 0; k < sweeps; ++k) {
+            HZB_TRY(jacobi_sweep(A, L.d_jac, L.b, L.x, L.t, S->s));
+            HZB_TRY(vcopy(L.n, L.t, L.x, S->s));
+        }
+        return SUCCESS;
+    case SMOOTHER_L1DIAG: {
+        const float *om = (l == 0 && S->omega_active) ? S->omega : nullptr;
+        for (int k = 0; k < sweeps; ++k) {
+            HZB_TRY(l1_sweep<double>(A, L.b, L.x, L.t, om, S->s));
+            HZB_TRY(vcopy(L.n, L.t, L.x, S->s));
+        }
+        return SUCCESS;
+    }
+    case SMOOTHER_GS:
+        for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, pre, w));
+        return SUCCESS;
+    case SMOOTHER_SGS:
+        for (int k = 0; k < sweeps; ++k) {
+            HZB_TRY(gs_sweep(S, L, 2, true, w));
+            HZB_TRY(gs_sweep(S, L, 2 | GS_SKIP_LAST, false, w));
+        }
+        return SUCCESS;
+    case SMOOTHER_SOR:
+        for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, pre, w));
+        return SUCCESS;
+    case SMOOTHER_SSOR:
+        for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, true, w));
+        for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, false, w));
+        return SUCCESS;
+    case SMOOTHER_GSOR:
+        if (pre) {
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, true, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, false, w));
+        } else {
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, true, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, false, w));
+        }
+        return SUCCESS;
+    case SMOOTHER_SGSOR:
+        if (pre) {
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, true, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, false, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, true, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, false, w));
+        } else {
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, true, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 1, false, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, true, w));
+            for (int k = 0; k < sweeps; ++k) HZB_TRY(gs_sweep(S, L, 0, false, w));
+        }
+        return SUCCESS;
+    }
+    set_error_msg("unsupported smoother type");
+    return ERROR_AMG_SMOOTH_TYPE;
+}
+
+static bool smoother_needs_gs(int sm) {
+    return sm == SMOOTHER_GS || sm == SMOOTHER_SGS || sm == SMOOTHER_SOR ||
+           sm == SMOOTHER_SSOR || sm == SMOOTHER_GSOR || sm == SMOOTHER_SGSOR;
+}
+
+// ---------------------------------------------------------------------------
+// V / W cycle, mgcycle (mgcycle.c:245-415)
+// ---------------------------------------------------------------------------
+static int coarse_solve64(hzb_solver *S, const AMG_param &cyc) {
+    Level &C = S->lv[S->nl - 1];
+    if (cyc.coarse_solver == SOLVER_UMFPACK && S->Ainv)
+        return dense_gemv<double>(C.n, S->Ainv, C.b, C.x, S->s);
+    // coarse_itsolver (mgcycle.c:34-52): plain CG to tol*1e-2, maxit 20 n
+    double rel = 0.0;
+    int it = pcg(S, C.A64(), C.b, C.x, PC_NONE, nullptr, cyc.tol * 1e-2, 20 * C.n,
+                 STOP_REL_RES, 0, S->kwc, &rel, nullptr);
+    return it == ERROR_SOLVER_MISC ? it : SUCCESS;
+}
+
+int cycle64(hzb_solver *S, const AMG_param &cyc) {
+    const int nl = S->nl;
+    int num_lvl[MAX_AMG_LVL] = {0};
+    int l = 0;
+    double alpha = 1.0;
+forward:
+    while (l < nl - 1) {
+        Level &L = S->lv[l];
+        num_lvl[l]++;
+        HZB_TRY(smooth64(S, l, true, cyc));
+        HZB_TRY(spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, S->s));
+        HZB_TRY(restrict_agg<double>(L.nc, L.ria, L.rja, L.w, S->lv[l + 1].b, S->s));
+        ++l;
+        HZB_TRY(vzero<double>(S->lv[l].n, S->lv[l].x, S->s));
+    }
+    HZB_TRY(coarse_solve64(S, cyc));
+    while (l > 0) {
+        --l;
+        Level &L = S->lv[l];
+        if (cyc.coarse_scaling == ON) {
+            Level &C = S->lv[l + 1];
+            KrylovWork &w = S->kw;
+            HZB_TRY(dot(C.n, C.x, C.b, w.part, w.sc + SC_X, S->s));
+            HZB_TRY(spmv<double>(C.A64(), SPMV_Y, C.x, nullptr, C.t, 1.0, nullptr, S->s));
+            HZB_TRY(dot(C.n, C.x, C.t, w.part, w.sc + SC_X + 1, S->s));
+            HZB_TRY(fetch(S, w));
+            alpha = w.h_sc[SC_X] / w.h_sc[SC_X + 1];
+            alpha = std::min(alpha, 2.0);
+        }
+        HZB_TRY(prolong_agg<double>(L.n, L.agg, S->lv[l + 1].x, L.x, alpha, S->s));
+        HZB_TRY(smooth64(S, l, false, cyc));
+        if (num_lvl[l] < cyc.cycle_type) break;
+        else num_lvl[l] = 0;
+    }
+    if (l > 0) goto forward;
+    return SUCCESS;
+}
+
+// precond_amg (precond.c:164-184)
+int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
+    Level &L0 = S->lv[0];
+    double *sb = L0.b, *sx = L0.x;
+    L0.b = const_cast<double *>(r);
+    L0.x = z;
+    int rc = vzero<double>(L0.n, z, S->s);
+    for (int i = 0; rc == SUCCESS && i < cyc.maxit; ++i) rc = cycle64(S, cyc);
+    L0.b = sb;
+    L0.x = sx;
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 cycle (mixed precision): same structure, single-precision vectors and
+// matrix values, FP32 accumulation; the coarse solve reads the FP64 inverse.
+// ---------------------------------------------------------------------------
+static int smooth32(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
+    Level &L = S->lv[l];
+    const int sweeps = pre ? cyc.presmooth_iter : cyc.postsmooth_iter;
+    const DCsr<float> A = L.A32();
+    switch (cyc.smoother) {
+    case SMOOTHER_L1DIAG:
+    case SMOOTHER_JACOBI: {
+        const float *om = (l == 0 && S->omega_active) ? S->omega : nullptr;
+        for (int k = 0; k < sweeps; ++k) {
+            // ping-pong x <-> t; an odd count ends with a copy back to x
+            const bool odd = (k & 1) == 0;
+            HZB_TRY(l1_sweep<float>(A, L.b32, odd ? L.x32 : L.t32, odd ? L.t32 : L.x32,
+                                    om, S->s));
+        }
+        if (sweeps & 1) HZB_TRY(vcopy<float>(L.n, L.t32, L.x32, S->s));
+        return SUCCESS;
+    }
+    case SMOOTHER_GS: {
+        const Schedule &sc = L.col;
+        const int ns = (int)sc.h_ptr.size() - 1;
+        for (int k = 0; k < sweeps; ++k)
+            for (int q = 0; q < ns; ++q) {
+                const int c = pre ? q : ns - 1 - q;
+                HZB_TRY(gs_rows<float>(A, 0, sc.rows + sc.h_ptr[c],
+                                       sc.h_ptr[c + 1] - sc.h_ptr[c], L.d_gs32, 1.0f,
+                                       L.b32, L.x32, S->s));
+            }
+        return SUCCESS;
+    }
+    }
+    set_error_msg("mixed precision supports the l1-Jacobi and multicolour GS smoothers");
+    return ERROR_AMG_SMOOTH_TYPE;
+}
+
+int cycle32(hzb_solver *S, const AMG_param &cyc) {
+    const int nl = S->nl;
+    int num_lvl[MAX_AMG_LVL] = {0};
+    int l = 0;
+forward:
+    while (l < nl - 1) {
+        Level &L = S->lv[l];
+        num_lvl[l]++;
+        HZB_TRY(smooth32(S, l, true, cyc));
+        HZB_TRY(spmv<float>(L.A32(), SPMV_RES, L.x32, L.b32, L.w32, 1.0f, nullptr, S->s));
+        HZB_TRY(restrict_agg<float>(L.nc, L.ria, L.rja, L.w32, S->lv[l + 1].b32, S->s));
+        ++l;
+        HZB_TRY(vzero<float>(S->lv[l].n, S->lv[l].x32, S->s));
+    }
+    {
+        Level &C = S->lv[nl - 1];
+        HZB_TRY(dense_gemv<float>(C.n, S->Ainv, C.b32, C.x32, S->s));
+    }
+    while (l > 0) {
+        --l;
+        Level &L = S->lv[l];
+        HZB_TRY(prolong_agg<float>(L.n, L.agg, S->lv[l + 1].x32, L.x32, 1.0f, S->s));
+        HZB_TRY(smooth32(S, l, false, cyc));
+        if (num_lvl[l] < cyc.cycle_type) break;
+        else num_lvl[l] = 0;
+    }
+    if (l > 0) goto forward;
+    return SUCCESS;
+}
+
+int ensure_fp32(hzb_solver *S) {
+    for (int l = 0; l < S->nl; ++l) {
+        Level &L = S->lv[l];
+        if (!L.val32) {
+            HZB_TRY(dalloc(&L.val32, L.nnz));
+            HZB_TRY(csr_val_d2f(L.nnz, L.val, L.val32, S->s));
+        }
+        if (!L.b32) {
+            HZB_TRY(dalloc(&L.b32, L.n));
+            HZB_TRY(dalloc(&L.x32, L.n));
+            HZB_TRY(dalloc(&L.w32, L.n));
+            HZB_TRY(dalloc(&L.t32, L.n));
+        }
+        if (S->amg.smoother == SMOOTHER_GS && l < S->nl - 1 && !L.d_gs32) {
+            if (!L.col.rows) HZB_TRY(multicolor(L.n, L.ia, L.ja, &L.col, S->s));
+            HZB_TRY(dalloc(&L.d_gs32, L.n));
+            HZB_TRY(d2f(L.n, L.d_gs_f, L.d_gs32, S->s));
+        }
+    }
+    HZB_CUDA(cudaStreamSynchronize(S->s));
+    return SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// setup, amg_setup_unsmoothP_unsmoothR (amg_setup_ua.c:1228-1452)
+// ---------------------------------------------------------------------------
+int level_smoother_data(hzb_solver *S, Level &L) {
+    const int sm = S->amg.smoother;
+    const bool gsf = smoother_needs_gs(sm);
+    if (sm == SMOOTHER_JACOBI || gsf || S->bp.precision == HZB_PREC_MIXED) {
+        HZB_TRY(dalloc(&L.d_jac, L.n));
+        HZB_TRY(dalloc(&L.d_gs_f, L.n));
+        HZB_TRY(dalloc(&L.d_gs_b, L.n));
+        HZB_TRY(dalloc(&L.d_sor_f, L.n));
+        HZB_TRY(dalloc(&L.d_sor_b, L.n));
+        HZB_TRY(smoother_diagonals(L.A64(), L.d_jac, L.d_gs_f, L.d_gs_b, L.d_sor_f,
+                                   L.d_sor_b, S->s));
+    }
+    if (gsf) {
+        if (S->bp.gs_schedule == HZB_GS_MULTICOLOR) {
+            HZB_TRY(multicolor(L.n, L.ia, L.ja, &L.col, S->s));
+        } else {
+            HZB_TRY(gs_schedule(L.n, L.ia, L.ja, L.nnz, 0, &L.fwd, S->s));
+            HZB_TRY(gs_schedule(L.n, L.ia, L.ja, L.nnz, 1, &L.bwd, S->s));
+        }
+    }
+    return SUCCESS;
+}
+
+int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
+          const double *d_val, bool copy_in) {
+    for (auto &L : S->lv) L.release();
+    S->lv.clear();
+    dfree(S->Ainv);
+    S->nl = 0;
+    cudaStream_t s = S->s;
+    HZB_CUDA(cudaEventRecord(S->e0, s));
+    S->lv.emplace_back();
+    {
+        Level &L0 = S->lv[0];
+        L0.n = n;
+        L0.nnz = nnz;
+        if (copy_in) {
+            L0.own_A = true;
+            HZB_TRY(dalloc(&L0.ia, n + 1));
+            HZB_TRY(dalloc(&L0.ja, nnz));
+            HZB_TRY(dalloc(&L0.val, nnz));
+            HZB_CUDA(cudaMemcpyAsync(L0.ia, d_ia, sizeof(int) * (n + 1), cudaMemcpyDefault, s));
+            HZB_CUDA(cudaMemcpyAsync(L0.ja, d_ja, sizeof(int) * nnz, cudaMemcpyDefault, s));
+            HZB_CUDA(cudaMemcpyAsync(L0.val, d_val, sizeof(double) * nnz, cudaMemcpyDefault, s));
+        } else {
+            L0.own_A = false;
+            L0.ia = const_cast<int *>(d_ia);
+            L0.ja = const_cast<int *>(d_ja);
+            L0.val = const_cast<double *>(d_val);
+        }
+        HZB_TRY(bundle_capacity(n, L0.ia, s, &L0.bundle_cap));
+    }
+    const short min_cdof = (short)std::max(S->amg.coarse_dof, 1);
+    const int max_levels = std::min<int>(S->amg.max_levels, MAX_AMG_LVL);
+    int lvl = 0;
+    int *tmp = nullptr;
+    HZB_TRY(dalloc(&tmp, scan_tmp_size(n + 2)));
+    int rc = SUCCESS;
+    while (S->lv[lvl].n > min_cdof && lvl < max_levels - 1) {
+        Level &L = S->lv[lvl];
+        const int m = L.n;
+        int *nia = nullptr, *nja = nullptr, *agg = nullptr, *work = nullptr;
+        double *nval = nullptr;
+        int nnnz = 0, nagg = 0;
+        const bool par = S->bp.matching == HZB_MATCH_PARALLEL ||
+                         S->amg.aggregation_type == HEC;
+        if ((rc = dalloc(&nia, m + 1)) || (rc = dalloc(&nja, L.nnz)) ||
+            (rc = dalloc(&nval, L.nnz)) || (rc = dalloc(&agg, m)) ||
+            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8 : (size_t)m))) {
+            dfree(nia); dfree(nja); dfree(nval); dfree(agg); dfree(work);
+            break;
+        }
+        rc = strength_graph(L.A64(), S->amg.strong_coupled, nia, nja, nval, &nnnz, tmp, s);
+        if (!rc) {
+            if (par) rc = hem_parallel(m, nia, nja, nval, agg, &nagg, work, s);
+            else rc = hem_exact(m, nia, nja, nval, agg, &nagg, work, s);
+        }
+        dfree(nia); dfree(nja); dfree(nval); dfree(work);
+        if (rc) { dfree(agg); break; }
+        // adaptive threshold (amg_setup_ua.c:1325-1328), caller's param too
+        if (nagg * 4 > m) S->amg.strong_coupled /= 2;
+        else if (nagg * 1.25 < m) S->amg.strong_coupled *= 2;
+        if (S->caller_amg) S->caller_amg->strong_coupled = S->amg.strong_coupled;
+        if (nagg < MIN_CDOF) { dfree(agg); break; }
+        L.nc = nagg;
+        L.agg = agg;
+        if ((rc = dalloc(&L.ria, nagg + 1)) || (rc = dalloc(&L.rja, m))) break;
+        if ((rc = restriction_pattern(m, nagg, agg, L.ria, L.rja, tmp, s))) break;
+        int *cia = nullptr, *cja = nullptr, cnnz = 0;
+        double *cval = nullptr;
+        if ((rc = rap_agg(L.A64(), nagg, agg, L.ria, L.rja, &cia, &cja, &cval, &cnnz, s)))
+            break;
+        S->lv.emplace_back();
+        Level &C = S->lv.back();
+        C.n = nagg; C.nnz = cnnz; C.ia = cia; C.ja = cja; C.val = cval; C.own_A = true;
+        if ((rc = bundle_capacity(C.n, C.ia, s, &C.bundle_cap))) break;
+        ++lvl;
+    }
+    dfree(tmp);
+    if (rc) return rc;
+    S->nl = lvl + 1;
+    // coarsest level: dense inverse (coarse_solver 32, and always for the
+    // FP32 cycle)
+    if (S->amg.coarse_solver == SOLVER_UMFPACK || S->bp.precision == HZB_PREC_MIXED) {
+        // amg_setup_ua.c:1392-1401: the coarsest matrix is transposed (columns
+        // ascending) and that transpose is factored
+        Level &C = S->lv[S->nl - 1];
+        HZB_TRY(transpose_csr(C.A64(), &C.tia, &C.tja, &C.tval, s));
+        HZB_TRY(dense_inverse(C.AT64(), &S->Ainv, s));
+    }
+    for (int l = 0; l < S->nl; ++l) {
+        Level &L = S->lv[l];
+        HZB_TRY(dalloc(&L.b, L.n));
+        HZB_TRY(dalloc(&L.x, L.n));
+        HZB_TRY(dalloc(&L.w, L.n));
+        HZB_TRY(dalloc(&L.t, L.n));
+        if (l < S->nl - 1) HZB_TRY(level_smoother_data(S, L));
+    }
+    HZB_TRY(S->kw.alloc(n));
+    if (S->amg.coarse_solver != SOLVER_UMFPACK)
+        HZB_TRY(S->kwc.alloc(S->lv[S->nl - 1].n));
+    if (S->bp.precision == HZB_PREC_MIXED) HZB_TRY(ensure_fp32(S));
+    HZB_CUDA(cudaEventRecord(S->e1, s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S->e0, S->e1);
+    S->st.setup_seconds = ms * 1e-3;
+    S->st.num_levels = S->nl;
+    for (int l = 0; l < S->nl && l < MAX_AMG_LVL; ++l) {
+        S->st.rows[l] = S->lv[l].n;
+        S->st.nnz[l] = S->lv[l].nnz;
+    }
+    S->st.strong_coupled = S->amg.strong_coupled;
+    return SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// condition estimate of dcsr_pcg_w_cond_est (krylov.c:400-740): extreme
+// eigenvalues of the Lanczos tridiagonal built from alpha/beta, here by
+// Sturm-sequence bisection instead of LAPACK dsterf.
+// ---------------------------------------------------------------------------
+static int sturm_count(const std::vector<double> &d, const std::vector<double> &e,
+                       double x) {
+    int cnt = 0;
+    double q = d[0] - x;
+    if (q < 0) ++cnt;
+    for (size_t i = 1; i < d.size(); ++i) {
+        double qq = (q == 0.0) ? 1e-300 : q;
+        q = d[i] - x - e[i - 1] * e[i - 1] / qq;
+        if (q < 0) ++cnt;
+    }
+    return cnt;
+}
+static double tri_eig(const std::vector<double> &d, const std::vector<double> &e,
+                      int k) {
+    double lo = d[0], hi = d[0];
+    for (size_t i = 0; i < d.size(); ++i) {
+        double r = (i > 0 ? fabs(e[i - 1]) : 0) + (i + 1 < d.size() ? fabs(e[i]) : 0);
+        lo = std::min(lo, d[i] - r);
+        hi = std::max(hi, d[i] + r);
+    }
+    for (int it = 0; it < 200; ++it) {
+        double mid = 0.5 * (lo + hi);
+        if (sturm_count(d, e, mid) > k) hi = mid; else lo = mid;
+    }
+    return 0.5 * (lo + hi);
+}
+static double cond_estimate(const std::vector<double> &al,
+                            const std::vector<double> &be, int m) {
+    if (m < 1) return 0.0;
+    std::vector<double> d(m), e(m > 1 ? m - 1 : 0);
+    d[0] = 1.0 / al[0];
+    for (int i = 0; i < m - 1; ++i) {
+        d[i + 1] = 1.0 / al[i + 1] + be[i] / al[i];
+        e[i] = sqrt(be[i]) / al[i];
+    }
+    if (m == 1) return 1.0;
+    const double lmin = tri_eig(d, e, 0), lmax = tri_eig(d, e, m - 1);
+    return lmax / lmin;
+}
+
+// ---------------------------------------------------------------------------
+// PCG, dcsr_pcg (krylov.c:122-398)
+// ---------------------------------------------------------------------------
+static void print_info(int prt, int stop_type, int iter, double rel, double abs,
+                       double factor) {
+    if (prt < PRINT_SOME) return;
+    if (iter > 0) {
+        printf("%6lld | %13.6e   | %13.6e  | %10.4f\n", (long long)iter, rel, abs, factor);
+    } else {
+        printf("-----------------------------------------------------------\n");
+        if (stop_type == STOP_REL_RES)
+            printf("It Num |   ||r||/||b||   |     ||r||      |  Conv. Factor\n");
+        else if (stop_type == STOP_REL_PRECRES)
+            printf("It Num | ||r||_B/||b||_B |    ||r||_B     |  Conv. Factor\n");
+        else
+            printf("It Num |   ||r||/||x||   |     ||r||      |  Conv. Factor\n");
+        printf("-----------------------------------------------------------\n");
+        printf("%6lld | %13.6e   | %13.6e  |     -.-- \n", (long long)iter, rel, abs);
+    }
+    fflush(stdout);
+}
+
+static int apply_pc(hzb_solver *S, int kind, HostPrecond *hp, int n,
+                    const double *r, double *z) {
+    if (kind == PC_AMG) return precond64(S, r, z, S->pc_cyc);
+    if (kind == PC_HOST) {
+        HZB_CUDA(cudaMemcpyAsync(hp->h_r, r, sizeof(double) * n, cudaMemcpyDeviceToHost, S->s));
+        HZB_CUDA(cudaStreamSynchronize(S->s));
+        hp->fct(hp->h_r, hp->h_z, hp->data);
+        HZB_CUDA(cudaMemcpyAsync(z, hp->h_z, sizeof(double) * n, cudaMemcpyHostToDevice, S->s));
+        return SUCCESS;
+    }
+    return vcopy<double>(n, r, z, S->s);
+}
+
+// residual measure for the stopping type (krylov.c:157-170, 211-227)
+static int measure(hzb_solver *S, KrylovWork &w, int kind, HostPrecond *hp,
+                   int stop_type, double *absres) {
+    const int n = w.n;
+    if (stop_type == STOP_REL_PRECRES) {
+        HZB_TRY(apply_pc(S, kind, hp, n, w.r, w.z));
+        HZB_TRY(dot(n, w.z, w.r, w.part, w.sc + SC_X, S->s));
+        HZB_TRY(fetch(S, w));
+        *absres = sqrt(fabs(w.h_sc[SC_X]));
+    } else {
+        HZB_TRY(norm2sq(S, w, n, w.r, SC_X));
+        HZB_TRY(fetch(S, w));
+        *absres = sqrt(w.h_sc[SC_X]);
+    }
+    return SUCCESS;
+}
+
+int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
+        int kind, HostPrecond *hp, double tol, int MaxIt, int stop_type,
+        int prtlvl, KrylovWork &w, double *relres_out, double *condest) {
+    const int MaxStag = MAX_STAG, MaxRestartStep = MAX_RESTART;
+    const int m = A.n;
+    const double maxdiff = tol * STAG_RATIO;
+    const double sol_inf_tol = SMALLREAL;
+    cudaStream_t s = S->s;
+    int iter = 0, stag = 1, more_step = 1, restart_step = 1;
+    double absres0 = BIGREAL, absres = BIGREAL, relres = BIGREAL;
+    double normu = BIGREAL, normr0 = BIGREAL;
+    double reldiff, factor, infnormu, alpha, temp1 = 0.0, temp2;
+    std::vector<double> al, be;
+    int iter_condest = 0;
+    const int G = reduce_blocks(m);
+    double *part4 = w.part, *partd = w.part + 4 * G;
+    if (w.n != m) HZB_TRY(w.alloc(m));
+
+    // r = b - A u ; z = B r
+    HZB_TRY(spmv<double>(A, SPMV_RES, u, b, w.r, 1.0, nullptr, s));
+    HZB_TRY(apply_pc(S, kind, hp, m, w.r, w.z));
+    switch (stop_type) {
+    case STOP_REL_RES:
+        HZB_TRY(measure(S, w, kind, hp, STOP_REL_RES, &absres0));
+        normr0 = std::max(SMALLREAL, absres0);
+        relres = absres0 / normr0;
+        break;
+    case STOP_REL_PRECRES:
+        HZB_TRY(dot(m, w.r, w.z, w.part, w.sc + SC_X, s));
+        HZB_TRY(fetch(S, w));
+        absres0 = sqrt(w.h_sc[SC_X]);
+        normr0 = std::max(SMALLREAL, absres0);
+        relres = absres0 / normr0;
+        break;
+    case STOP_MOD_REL_RES:
+        HZB_TRY(measure(S, w, kind, hp, STOP_REL_RES, &absres0));
+        HZB_TRY(norm2sq(S, w, m, u, SC_X));
+        HZB_TRY(fetch(S, w));
+        normu = std::max(SMALLREAL, sqrt(w.h_sc[SC_X]));
+        relres = absres0 / normu;
+        break;
+    default:
+        printf("### ERROR: Unrecognised stopping type for %s!\n", __FUNCTION__);
+        goto finished;
+    }
+    if (relres < tol || absres0 < 1e-3 * tol) goto finished;
+    print_info(prtlvl, stop_type, iter, relres, absres0, 0.0);
+
+    HZB_TRY(vcopy<double>(m, w.z, w.p, s));
+    HZB_TRY(dot(m, w.z, w.r, w.part, w.sc + SC_T1, s));
+
+    while (iter++ < MaxIt) {
+        // t = A p ; temp2 = (t, p) ; alpha = temp1 / temp2 (device)
+        HZB_TRY(spmv<double>(A, SPMV_Y_DOT, w.p, nullptr, w.t, 1.0, partd, s));
+        HZB_TRY(reduce_final(partd, spmv_blocks(m), w.sc + SC_T2, s));
+        // u += alpha p ; r -= alpha t ; norms for checks I and II
+        HZB_TRY(pcg_update(m, w.sc + SC_T1, w.sc + SC_T2, u, w.r, w.p, w.t, part4, s));
+        HZB_TRY(reduce_final(part4, G, w.sc + SC_RR, s));
+        HZB_TRY(reduce_final_max(part4 + G, G, w.sc + SC_UM, s));
+        HZB_TRY(reduce_final(part4 + 2 * G, G, w.sc + SC_UU, s));
+        HZB_TRY(reduce_final(part4 + 3 * G, G, w.sc + SC_PP, s));
+        HZB_TRY(fetch(S, w));
+        if (condest && iter > 1) be.push_back(w.h_sc[SC_T1] / temp1);   // beta_{k-1}
+        temp1 = w.h_sc[SC_T1];
+        temp2 = w.h_sc[SC_T2];
+        alpha = temp1 / temp2;
+        if (condest) al.push_back(alpha);
+        switch (stop_type) {
+        case STOP_REL_RES:
+            absres = sqrt(w.h_sc[SC_RR]);
+            relres = absres / normr0;
+            break;
+        case STOP_REL_PRECRES:
+            HZB_TRY(measure(S, w, kind, hp, STOP_REL_PRECRES, &absres));
+            relres = absres / normr0;
+            break;
+        case STOP_MOD_REL_RES:
+            absres = sqrt(w.h_sc[SC_RR]);
+            relres = absres / normu;
+            break;
+        }
+        factor = absres / absres0;
+        print_info(prtlvl, stop_type, iter, relres, absres, factor);
+
+        // Check I: solution close to zero
+        infnormu = w.h_sc[SC_UM];
+        if (infnormu <= sol_inf_tol) {
+            if (prtlvl > PRINT_MIN)
+                printf("### HAZMATH WARNING: Iteration stopped due to the solution is almost zero! %s : %lld\n",
+                       __FUNCTION__, (long long)__LINE__);
+            iter = ERROR_SOLVER_SOLSTAG;
+            break;
+        }
+        // Check II: stagnation
+        normu = sqrt(w.h_sc[SC_UU]);
+        reldiff = fabs(alpha) * sqrt(w.h_sc[SC_PP]) / normu;
+        if ((stag <= MaxStag) & (reldiff < maxdiff)) {
+            if (prtlvl >= PRINT_MORE) {
+                printf("||u-u'|| = %e and the comp. rel. res. = %e.\n", reldiff, relres);
+                printf("### HAZMATH WARNING: Iteration restarted due to stagnation! %s : %lld\n",
+                       __FUNCTION__, (long long)__LINE__);
+            }
+            if (stag == 1 && restart_step == 1) iter_condest = iter;
+            HZB_TRY(spmv<double>(A, SPMV_RES, u, b, w.r, 1.0, nullptr, s));
+            HZB_TRY(measure(S, w, kind, hp, stop_type == STOP_REL_PRECRES ? STOP_REL_PRECRES : STOP_REL_RES, &absres));
+            relres = absres / (stop_type == STOP_MOD_REL_RES ? normu : normr0);
+            if (prtlvl >= PRINT_MORE)
+                printf("### HAZMATH WARNING: The actual relative residual = %e!\n", relres);
+            if (relres < tol) break;
+            if (stag >= MaxStag) {
+                if (prtlvl > PRINT_MIN)
+                    printf("### HAZMATH WARNING: Iteration stopped due to staggnation! %s : %lld\n",
+                           __FUNCTION__, (long long)__LINE__);
+                iter = ERROR_SOLVER_STAG;
+                break;
+            }
+            HZB_TRY(vzero<double>(m, w.p, s));
+            ++stag;
+            ++restart_step;
+        }
+        // Check III: false convergence
+        if (relres < tol) {
+            const double computed = relres;
+            if (stag == 1 && restart_step == 1) iter_condest = iter;
+            HZB_TRY(spmv<double>(A, SPMV_RES, u, b, w.r, 1.0, nullptr, s));
+            HZB_TRY(measure(S, w, kind, hp, stop_type == STOP_REL_PRECRES ? STOP_REL_PRECRES : STOP_REL_RES, &absres));
+            relres = absres / (stop_type == STOP_MOD_REL_RES ? normu : normr0);
+            if (relres < tol) break;
+            if (prtlvl >= PRINT_MORE) {
+                printf("### HAZMATH WARNING: The computed relative residual = %e!\n", computed);
+                printf("### HAZMATH WARNING: The actual relative residual = %e!\n", relres);
+            }
+            if (more_step >= MaxRestartStep) {
+                if (prtlvl > PRINT_MIN)
+                    printf("### HAZMATH WARNING: The tolerence might be too small! %s : %lld\n",
+                           __FUNCTION__, (long long)__LINE__);
+                iter = ERROR_SOLVER_TOLSMALL;
+                break;
+            }
+            HZB_TRY(vzero<double>(m, w.p, s));
+            ++more_step;
+            ++restart_step;
+        }
+        absres0 = absres;
+        if (stop_type != STOP_REL_PRECRES) HZB_TRY(apply_pc(S, kind, hp, m, w.r, w.z));
+        // beta = (z, r)_new / temp1 ; p = z + beta p ; temp1 = (z, r)_new
+        HZB_TRY(dot(m, w.z, w.r, w.part, w.sc + SC_T3, s));
+        HZB_TRY(pcg_axpby(m, w.sc + SC_T3, w.sc + SC_T1, w.z, w.p, s));
+        k_copy_scalar<<<1, 1, 0, s>>>(w.sc + SC_T3, w.sc + SC_T1);
+        count_launch();
+    }
+finished:
+    if (prtlvl > PRINT_NONE) {
+        if (iter > MaxIt)
+            printf("### HAZMATH WARNING: Max iter %lld reached with rel. resid. %e.\n",
+                   (long long)MaxIt, relres);
+        else if (iter >= 0)
+            printf("Num_iter(krylov.c) = %lld with relative residual %e.\n",
+                   (long long)iter, relres);
+        fflush(stdout);
+    }
+    if (relres_out) *relres_out = relres;
+    if (condest) {
+        if (stag == 1 && restart_step == 1) iter_condest = std::max(0, std::min(iter, MaxIt));
+        const int mm = std::min<int>(iter_condest, (int)al.size());
+        *condest = cond_estimate(al, be, std::min<int>(mm, (int)be.size() + 1));
+    }
+    if (iter > MaxIt) return ERROR_SOLVER_MAXIT;
+    return iter;
+}
+
+// ---------------------------------------------------------------------------
+// flexible CG with the FP32 cycle (mixed precision; no reference counterpart
+// beyond dcsr_pgcg's flexible idea, krylov.c:2309)
+// ---------------------------------------------------------------------------
+static int apply_pc32(hzb_solver *S, const double *r, double *z) {
+    Level &L0 = S->lv[0];
+    AMG_param cyc = S->amg;
+    HZB_TRY(d2f(L0.n, r, L0.b32, S->s));
+    HZB_TRY(vzero<float>(L0.n, L0.x32, S->s));
+    for (int i = 0; i < std::max<int>(1, cyc.maxit); ++i) HZB_TRY(cycle32(S, cyc));
+    return f2d(L0.n, L0.x32, z, S->s);
+}
+
+int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
+              int prtlvl, double *relres_out) {
+    KrylovWork &w = S->kw;
+    const DCsr<double> A = S->lv[0].A64();
+    const int m = A.n;
+    cudaStream_t s = S->s;
+    const int G = reduce_blocks(m);
+    double *part4 = w.part, *partd = w.part + 4 * G;
+    double normr0, relres, absres, absres0;
+    int iter = 0;
+    HZB_TRY(spmv<double>(A, SPMV_RES, x, b, w.r, 1.0, nullptr, s));
+    HZB_TRY(norm2sq(S, w, m, w.r, SC_X));
+    HZB_TRY(fetch(S, w));
+    absres0 = sqrt(w.h_sc[SC_X]);
+    normr0 = std::max(SMALLREAL, absres0);
+    relres = absres0 / normr0;
+    if (relres < tol || absres0 < 1e-3 * tol) {
+        if (relres_out) *relres_out = relres;
+        return 0;
+    }
+    print_info(prtlvl, STOP_REL_RES, 0, relres, absres0, 0.0);
+    HZB_TRY(apply_pc32(S, w.r, w.z));
+    HZB_TRY(vcopy<double>(m, w.z, w.p, s));
+    HZB_TRY(dot(m, w.z, w.r, w.part, w.sc + SC_T1, s));
+    while (iter++ < maxit) {
+        HZB_TRY(spmv<double>(A, SPMV_Y_DOT, w.p, nullptr, w.t, 1.0, partd, s));
+        HZB_TRY(reduce_final(partd, spmv_blocks(m), w.sc + SC_T2, s));
+        HZB_TRY(pcg_update(m, w.sc + SC_T1, w.sc + SC_T2, x, w.r, w.p, w.t, part4, s));
+        HZB_TRY(reduce_final(part4, G, w.sc + SC_RR, s));
+        HZB_TRY(fetch(S, w));
+        absres = sqrt(w.h_sc[SC_RR]);
+        relres = absres / normr0;
+        print_info(prtlvl, STOP_REL_RES, iter, relres, absres, absres / absres0);
+        absres0 = absres;
+        if (relres < tol) {
+            // recompute the true FP64 residual before accepting
+            HZB_TRY(spmv<double>(A, SPMV_RES, x, b, w.r, 1.0, nullptr, s));
+            HZB_TRY(norm2sq(S, w, m, w.r, SC_X));
+            HZB_TRY(fetch(S, w));
+            relres = sqrt(w.h_sc[SC_X]) / normr0;
+            if (relres < tol) break;
+        }
+        HZB_TRY(apply_pc32(S, w.r, w.z));
+        k_dot2_partial<<<G, 256, 0, s>>>(m, w.z, w.t, w.r, part4);
+        count_launch();
+        HZB_TRY(reduce_final(part4, G, w.sc + SC_ZT, s));
+        HZB_TRY(reduce_final(part4 + G, G, w.sc + SC_T3, s));
+        k_fcg_p<<<grid_for(m), 256, 0, s>>>(m, w.sc + SC_ZT, w.sc + SC_T2, w.z, w.p);
+        k_copy_scalar<<<1, 1, 0, s>>>(w.sc + SC_T3, w.sc + SC_T1);
+        count_launch(2);
+        HZB_LAUNCH_CHECK();
+    }
+    if (prtlvl > PRINT_NONE) {
+        printf("Num_iter(fcg) = %lld with relative residual %e.\n", (long long)iter, relres);
+        fflush(stdout);
+    }
+    if (relres_out) *relres_out = relres;
+    return iter > maxit ? ERROR_SOLVER_MAXIT : iter;
+}
+
+void destroy(hzb_solver *S) {
+    for (auto &L : S->lv) L.release();
+    S->lv.clear();
+    dfree(S->Ainv);
+    dfree(S->omega);
+    dfree(S->pr);
+    dfree(S->pz);
+    S->kw.release();
+    S->kwc.release();
+}
+
+}  // namespace hzb

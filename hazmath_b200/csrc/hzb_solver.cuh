@@ -1,0 +1,114 @@
+// hzb_solver.cuh -- the device-resident UA-AMG hierarchy and its solvers.
+#pragma once
+#include <vector>
+#include "hzb_setup.cuh"
+
+struct hzb_solver;
+
+namespace hzb {
+
+struct Level {
+    int n = 0, nnz = 0;
+    int *ia = nullptr, *ja = nullptr;
+    double *val = nullptr;
+    float *val32 = nullptr;
+    bool own_A = true;
+    int bundle_cap = 0;
+    // transfer to level + 1 (P = agg map, R = P^T with ascending rows)
+    int nc = 0;
+    int *agg = nullptr, *ria = nullptr, *rja = nullptr;
+    // cycle vectors
+    double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr;
+    float *b32 = nullptr, *x32 = nullptr, *w32 = nullptr, *t32 = nullptr;
+    // smoother data
+    double *d_jac = nullptr, *d_gs_f = nullptr, *d_gs_b = nullptr;
+    double *d_sor_f = nullptr, *d_sor_b = nullptr;
+    float *d_gs32 = nullptr;
+    Schedule fwd, bwd, col;
+    // coarsest level with the direct solver: the transposed matrix the
+    // reference factors (and leaves in mgl[nl-1].A)
+    int *tia = nullptr, *tja = nullptr;
+    double *tval = nullptr;
+    DCsr<double> AT64() const {
+        DCsr<double> m;
+        m.n = n; m.nnz = nnz; m.ia = tia; m.ja = tja; m.val = tval;
+        return m;
+    }
+    DCsr<double> A64() const {
+        DCsr<double> m;
+        m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val; m.bundle_cap = bundle_cap;
+        return m;
+    }
+    DCsr<float> A32() const {
+        DCsr<float> m;
+        m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val32; m.bundle_cap = bundle_cap;
+        return m;
+    }
+    void release();
+};
+
+// Scratch of one Krylov loop on an n-vector system.
+struct KrylovWork {
+    int n = 0;
+    double *p = nullptr, *z = nullptr, *r = nullptr, *t = nullptr;
+    double *part = nullptr;   // 4 * reduce_blocks(n) + spmv_blocks(n)
+    double *sc = nullptr;     // device scalars
+    double *h_sc = nullptr;   // pinned host mirror
+    int alloc(int n);
+    void release();
+};
+
+// Host-side preconditioner callback used when a foreign pc->fct is given.
+struct HostPrecond {
+    void (*fct)(double *, double *, void *) = nullptr;
+    void *data = nullptr;
+    double *h_r = nullptr, *h_z = nullptr;
+};
+
+}  // namespace hzb
+
+struct hzb_solver {
+    AMG_param amg;
+    linear_itsolver_param it;
+    hzb_param bp;
+    AMG_param *caller_amg = nullptr;   // receives the strong_coupled update
+    AMG_param pc_cyc;                  // cycle parameters of precond_amg
+    double *pr = nullptr, *pz = nullptr;   // host-pointer precond staging
+    cudaStream_t s = nullptr;
+    std::vector<hzb::Level> lv;
+    int nl = 0;
+    double *Ainv = nullptr;           // coarsest-level inverse (coarse_solver 32)
+    hzb::KrylovWork kw;               // outer Krylov loop
+    hzb::KrylovWork kwc;              // coarse-level CG (coarse_solver != 32)
+    float *omega = nullptr;           // learned fine-level weights (device)
+    bool omega_active = false;
+    hzb_stats st{};
+    const int *host_ia = nullptr;     // host matrix given to setup, if any
+    const int *host_ja = nullptr;
+    const double *host_val = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+namespace hzb {
+int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
+          const double *d_val, bool copy_in);
+// z = B r with B = maxit V/W cycles of the FP64 hierarchy (precond_amg)
+int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc);
+// one cycle on level-0 b/x already in place (mgcycle)
+int cycle64(hzb_solver *S, const AMG_param &cyc);
+int cycle32(hzb_solver *S, const AMG_param &cyc);
+// reference PCG on level-0 operator
+int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
+        int pc_kind, HostPrecond *hp, double tol, int maxit, int stop_type,
+        int prtlvl, KrylovWork &w, double *relres_out, double *condest);
+enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2 };
+// FP32-cycle flexible CG (mixed precision)
+int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
+              int prtlvl, double *relres_out);
+int ensure_fp32(hzb_solver *S);
+// smoothing of level l as mgcycle's pre (pre = true) / post smoothing calls
+int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc);
+// diagonals and sweep schedules the configured smoother needs on level L
+int level_smoother_data(hzb_solver *S, Level &L);
+void destroy(hzb_solver *S);
+}  // namespace hzb

@@ -1,0 +1,442 @@
+/*
+ * hazmath_b200.h -- C ABI of the B200-native UA-AMG preconditioned Krylov solve.
+ *
+ * The library (hazmath_b200/libhazb200.so) drops in for HAZmath's
+ * unsmoothed-aggregation AMG + CG path.  The data structures below are
+ * layout-compatible with HAZmath's own (include/sparse.h, include/vec.h,
+ * include/param.h, include/solver.h of the reference), the constants keep
+ * HAZmath's values (include/macro.h), and every entry point in section 3 keeps
+ * the signature and the meaning of the reference function it replaces (cited
+ * file:line within the HAZmath project).  All numeric work runs in CUDA
+ * kernels on an sm_100a GPU; host pointers are accepted wherever the
+ * reference takes them and are copied to and from device memory internally.
+ *
+ * Section 4 adds what the reference has no counterpart for: options for the
+ * mixed-precision and learned-smoother forms, a persistent solver handle that
+ * works on device-resident arrays, the batched solver and the kernel-level
+ * entry points used by the parity tests.
+ */
+#ifndef HAZMATH_B200_H
+#define HAZMATH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------
+ * 1. Scalar types and constants (values as in the reference's include/macro.h)
+ * ------------------------------------------------------------------------- */
+#ifndef INT
+#define INT   int
+#endif
+#ifndef SHORT
+#define SHORT short
+#endif
+#ifndef REAL
+#define REAL  double
+#endif
+
+#define SMALLREAL  1e-20
+#define BIGREAL    1e+20
+#define MAX_AMG_LVL 20
+#define MIN_CDOF   1
+#define STAG_RATIO 1e-4
+#define MAX_STAG   20
+#define MAX_RESTART 20
+
+#define SUCCESS                 0
+#define ERROR_INPUT_PAR       -13
+#define ERROR_MAT_SIZE        -15
+#define ERROR_MISC            -19
+#define ERROR_ALLOC_MEM       -20
+#define ERROR_DATA_STRUCTURE  -21
+#define ERROR_DATA_ZERODIAG   -22
+#define ERROR_AMG_SMOOTH_TYPE -31
+#define ERROR_AMG_AGG_TYPE    -32
+#define ERROR_AMG_COARSEING   -33
+#define ERROR_SOLVER_TYPE     -40
+#define ERROR_SOLVER_PRECTYPE -41
+#define ERROR_SOLVER_STAG     -42
+#define ERROR_SOLVER_SOLSTAG  -43
+#define ERROR_SOLVER_TOLSMALL -44
+#define ERROR_SOLVER_MISC     -47
+#define ERROR_SOLVER_MAXIT    -48
+#define ERROR_SOLVER_EXIT     -49
+#define ERROR_UNKNOWN         -99
+
+#define PRINT_NONE 0
+#define PRINT_MIN  1
+#define PRINT_SOME 2
+#define PRINT_MORE 4
+
+#define SOLVER_DEFAULT  0
+#define SOLVER_CG       1
+#define SOLVER_MinRes   2
+#define SOLVER_VGMRES   3
+#define SOLVER_VFGMRES  4
+#define SOLVER_GCG      5
+#define SOLVER_AMG     21
+#define SOLVER_UMFPACK 32
+
+#define STOP_REL_RES     1
+#define STOP_REL_PRECRES 2
+#define STOP_MOD_REL_RES 3
+
+#define PREC_NULL 0
+#define PREC_DIAG 1
+#define PREC_AMG  2
+
+#define UA_AMG 1
+#define SA_AMG 2
+
+#define VMB 1
+#define HEC 4
+#define HEM 5
+
+#define V_CYCLE 1
+#define W_CYCLE 2
+
+#define SMOOTHER_JACOBI  1
+#define SMOOTHER_GS      2
+#define SMOOTHER_SGS     3
+#define SMOOTHER_SOR     5
+#define SMOOTHER_SSOR    6
+#define SMOOTHER_GSOR    7
+#define SMOOTHER_SGSOR   8
+#define SMOOTHER_L1DIAG 10
+
+#define UNPT -1
+#ifndef ON
+#define ON  1
+#define OFF 0
+#endif
+
+/* ---------------------------------------------------------------------------
+ * 2. Data structures, layout-identical to the reference's
+ * ------------------------------------------------------------------------- */
+
+/* include/sparse.h:25-45 */
+typedef struct dCSRmat {
+    INT row;    /* rows m */
+    INT col;    /* columns n */
+    INT nnz;    /* stored entries */
+    INT *IA;    /* row pointers, m+1, 0-based */
+    INT *JA;    /* column indices, nnz */
+    REAL *val;  /* values, nnz */
+} dCSRmat;
+
+/* include/vec.h:20-28 */
+typedef struct dvector {
+    INT row;
+    REAL *val;
+} dvector;
+
+/* include/vec.h:34-42 */
+typedef struct ivector {
+    INT row;
+    INT *val;
+} ivector;
+
+/* include/param.h:138-156 */
+typedef struct {
+    SHORT linear_itsolver_type;
+    SHORT linear_precond_type;
+    SHORT linear_stop_type;
+    INT   linear_maxit;
+    REAL  linear_tol;
+    INT   linear_restart;
+    SHORT linear_print_level;
+    SHORT HX_smooth_iter;
+    REAL  AL_scaling_param;
+} linear_itsolver_param;
+
+/* include/param.h:164-266 */
+typedef struct {
+    SHORT AMG_type;
+    SHORT print_level;
+    INT   maxit;
+    REAL  tol;
+    SHORT max_levels;
+    INT   coarse_dof;
+    SHORT cycle_type;
+    SHORT smoother;
+    SHORT presmooth_iter;
+    SHORT postsmooth_iter;
+    REAL  relaxation;
+    SHORT polynomial_degree;
+    SHORT coarse_solver;
+    SHORT coarse_scaling;
+    SHORT amli_degree;
+    REAL *amli_coef;
+    SHORT nl_amli_krylov_type;
+    SHORT aggregation_type;
+    REAL  strong_coupled;
+    INT   max_aggregation;
+    SHORT smooth_filter;
+    REAL  tentative_smooth;
+    INT   Schwarz_levels;
+    INT   Schwarz_mmsize;
+    INT   Schwarz_maxlvl;
+    INT   Schwarz_type;
+    INT   Schwarz_blksolver;
+    char *HAZDIR;
+    INT  *Schwarz_on_blk;
+    INT  *Schwarz_patch_type;
+    REAL  damping_param;
+    REAL  BSR_alpha;
+    REAL  BSR_omega;
+    REAL  fpwr;
+    void *smoother_function;
+} AMG_param;
+
+/* include/solver.h:25-36 */
+typedef struct {
+    void *data;
+    void (*fct)(REAL *, REAL *, void *);
+    REAL setup_time;
+} precond;
+
+/* include/solver.h:46-104; only carried inside AMG_data (Schwarz smoothing
+ * is not part of this path, the fields keep the layout).                    */
+typedef struct {
+    dCSRmat A;
+    INT nblk;
+    INT *iblock;
+    INT *jblock;
+    dvector rhsloc1;
+    dvector xloc1;
+    SHORT Schwarz_type;
+    INT blk_solver;
+    INT memt;
+    INT *mask;
+    INT maxbs;
+    INT maxbnnz;
+    dCSRmat *blk_data;
+    void **numeric;
+    void *swzparam;
+} Schwarz_data;
+
+/* include/solver.h:110-164.  The B200 hierarchy hangs off mgl[0].wdata. */
+typedef struct {
+    SHORT max_levels;
+    SHORT num_levels;
+    dCSRmat A;
+    dCSRmat R;
+    dCSRmat P;
+    dvector b;
+    dvector x;
+    dCSRmat M;
+    void *Numeric;
+    INT near_kernel_dim;
+    REAL **near_kernel_basis;
+    INT Schwarz_levels;
+    Schwarz_data Schwarz;
+    dvector w;
+    INT cycle_type;
+    void *wdata;
+} AMG_data;
+
+/* include/solver.h:472-559 */
+typedef struct {
+    SHORT AMG_type;
+    SHORT print_level;
+    INT   maxit;
+    SHORT max_levels;
+    REAL  tol;
+    SHORT cycle_type;
+    SHORT smoother;
+    SHORT presmooth_iter;
+    SHORT postsmooth_iter;
+    REAL  relaxation;
+    SHORT polynomial_degree;
+    SHORT coarse_solver;
+    SHORT coarse_scaling;
+    SHORT amli_degree;
+    SHORT nl_amli_krylov_type;
+    REAL *amli_coef;
+    AMG_data *mgl_data;
+    REAL  fpwr;
+    dCSRmat *A;
+    dCSRmat *A_nk;
+    dCSRmat *P_nk;
+    dCSRmat *R_nk;
+    dvector *r;
+    REAL *w;
+} precond_data;
+
+/* ---------------------------------------------------------------------------
+ * 3. Drop-in entry points (same names, arguments and return conventions as
+ *    the reference).  Return >= 0: iteration count; < 0: an ERROR_* code.
+ *    The library never calls exit(); a device failure returns
+ *    ERROR_ALLOC_MEM (allocation) or ERROR_SOLVER_MISC (CUDA error).
+ * ------------------------------------------------------------------------- */
+
+/* src/solver/itsolver.c:846-931.  Copies A to the GPU, runs the UA setup,
+ * builds the AMG preconditioner and calls the Krylov method selected by
+ * itparam->linear_itsolver_type (1 = CG).  x: initial guess in, solution
+ * out. */
+INT linear_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
+                                  linear_itsolver_param *itparam,
+                                  AMG_param *amgparam);
+
+/* src/solver/itsolver.c:524-630: AMG as a stand-alone iterative solver
+ * (amg_solve, src/solver/amg_solve.c:109). */
+INT linear_solver_amg(dCSRmat *A, dvector *b, dvector *x, AMG_param *param);
+
+/* src/solver/itsolver.c:135-229: Krylov switch on a host preconditioner. */
+INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
+                                precond *pc, linear_itsolver_param *itparam);
+
+/* src/solver/amg_setup_ua.c:53 (amg_setup_unsmoothP_unsmoothR :1228-1452).
+ * mgl[0].A must hold the fine matrix.  Fills mgl[l].A/P/R (host copies) and
+ * num_levels, mutates param->strong_coupled as the reference does, and keeps
+ * the device hierarchy in mgl[0].wdata (released by amg_data_free). */
+SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param);
+
+/* src/solver/mgcycle.c:245-415: one V/W cycle on mgl[0].b, mgl[0].x. */
+void mgcycle(AMG_data *mgl, AMG_param *param);
+
+/* src/solver/precond.c:164-184: z = B r with host arrays r, z. */
+void precond_amg(REAL *r, REAL *z, void *data);
+
+/* src/solver/krylov.c:122-398.  pc == NULL: plain CG; pc->fct ==
+ * precond_amg with a B200 hierarchy: the whole loop runs on the device;
+ * any other pc->fct is called on host arrays every iteration. */
+INT dcsr_pcg(dCSRmat *A, dvector *b, dvector *u, precond *pc,
+             const REAL tol, const INT MaxIt, const SHORT stop_type,
+             const SHORT prtlvl);
+
+/* src/utilities/wrapper.c:36-99.  The reference reads ./input.dat; this one
+ * uses the UA-AMG defaults of the HAZmath examples (V-cycle, GS 1/1, HEM,
+ * coarse direct solve) unless ./input.dat exists, in which case the AMG and
+ * solver keys of that file are honoured. */
+void python_wrapper_krylov_amg(INT *n, INT *nnz, INT *ia, INT *ja, REAL *a,
+                               REAL *b, REAL *u, REAL *tol, INT *maxit,
+                               INT *print_lvl);
+
+/* src/utilities/data.c:66-91, :96-140, :22-55 */
+AMG_data *amg_data_create(SHORT max_levels);
+void amg_data_free(AMG_data *mgl, AMG_param *param);
+void precond_data_null(precond_data *pcdata);
+
+/* src/utilities/parameters.c:158-205, :238-250, :604-640, :649-680 */
+void param_amg_init(AMG_param *amgparam);
+void param_linear_solver_init(linear_itsolver_param *itsparam);
+void param_amg_to_prec(precond_data *pcdata, AMG_param *amgparam);
+void param_prec_to_amg(AMG_param *amgparam, precond_data *pcdata);
+
+/* ---------------------------------------------------------------------------
+ * 4. B200 extensions (no counterpart in the reference)
+ * ------------------------------------------------------------------------- */
+
+/* precision of the V-cycle */
+#define HZB_PREC_FP64  0   /* the drop-in: everything in FP64, reference order */
+#define HZB_PREC_MIXED 1   /* FP32 V-cycle, FP64 flexible CG outer loop       */
+
+/* Gauss-Seidel schedule */
+#define HZB_GS_EXACT      0 /* lexicographic, level-scheduled: bit-exact      */
+#define HZB_GS_MULTICOLOR 1 /* multicolour ordering: parallel, not bit-exact  */
+
+/* heavy edge matching */
+#define HZB_MATCH_EXACT    0 /* the reference's sequential visiting order     */
+#define HZB_MATCH_PARALLEL 1 /* deterministic parallel rounds: not bit-exact  */
+
+typedef struct {
+    SHORT precision;      /* HZB_PREC_*                                        */
+    SHORT gs_schedule;    /* HZB_GS_*                                          */
+    SHORT matching;       /* HZB_MATCH_*                                       */
+    SHORT export_hierarchy;/* amg_setup_ua: copy levels back into mgl[l]      */
+    SHORT use_omega;      /* 1: fine-level l1-Jacobi uses per-row weights      */
+    const float *omega;   /* host array (n) of weights in (0,2), or NULL       */
+    INT   device;         /* CUDA device ordinal                               */
+    SHORT fallback_check; /* 1: measure the learned cycle's contraction and    */
+                          /*    drop omega if it is worse than plain weights   */
+    SHORT use_graph;      /* 1: replay the V-cycle from a captured CUDA graph  */
+    SHORT reserved[6];
+} hzb_param;
+
+void hzb_param_init(hzb_param *p);
+
+/* The drop-in with explicit B200 options (linear_solver_dcsr_krylov_amg is
+ * this call with hzb_param_init defaults). */
+INT hzb_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
+                               linear_itsolver_param *itparam,
+                               AMG_param *amgparam, const hzb_param *bp);
+
+/* Persistent handle on device-resident data. */
+typedef struct hzb_solver hzb_solver;
+
+typedef struct {
+    INT   num_levels;
+    INT   rows[MAX_AMG_LVL];
+    INT   nnz[MAX_AMG_LVL];
+    INT   iterations;
+    REAL  final_relres;
+    REAL  setup_seconds;   /* device time of the last setup                  */
+    REAL  solve_seconds;   /* device time of the last solve                  */
+    REAL  strong_coupled;  /* threshold after the adaptive updates          */
+    REAL  condest;         /* CG condition estimate (0 if not computed)      */
+    REAL  omega_contraction[2]; /* measured contraction: plain, learned     */
+    INT   omega_used;      /* 1 if learned weights were kept                 */
+    INT   launches;        /* kernels launched by the last solve             */
+} hzb_stats;
+
+INT  hzb_create(hzb_solver **s, const AMG_param *amg,
+                const linear_itsolver_param *it, const hzb_param *bp);
+/* setup from device arrays (int32 CSR, FP64 values) */
+INT  hzb_setup_device(hzb_solver *s, INT n, INT nnz, const INT *d_ia,
+                      const INT *d_ja, const REAL *d_val);
+/* setup from a host matrix (copied in) */
+INT  hzb_setup_host(hzb_solver *s, const dCSRmat *A);
+/* solve with device vectors; x holds the initial guess */
+INT  hzb_solve_device(hzb_solver *s, const REAL *d_b, REAL *d_x);
+/* solve with host vectors (H2D/D2H copies included) */
+INT  hzb_solve_host(hzb_solver *s, const REAL *b, REAL *x);
+/* one preconditioner application z = B r on device vectors */
+INT  hzb_precond_device(hzb_solver *s, const REAL *d_r, REAL *d_z);
+/* per-row l1-Jacobi weights for the fine level (device array, n) */
+INT  hzb_set_omega_device(hzb_solver *s, const float *d_omega);
+INT  hzb_get_stats(const hzb_solver *s, hzb_stats *st);
+/* level l of the device hierarchy copied to host arrays sized from stats;
+ * agg (rows of level l) is the aggregate map, -1 for an empty row of P.   */
+INT  hzb_level_copy(const hzb_solver *s, INT l, INT *ia, INT *ja, REAL *val,
+                    INT *agg);
+void hzb_destroy(hzb_solver *s);
+/* last CUDA error message of this thread ("" if none) */
+const char *hzb_last_error(void);
+
+/* Kernel-level entry points on device arrays, one stream-ordered launch
+ * sequence each, used by the parity tests.  Each returns SUCCESS or
+ * ERROR_SOLVER_MISC and synchronises before returning. */
+INT hzb_dcsr_mxv_device(INT n, INT nnz, const INT *ia, const INT *ja,
+                        const REAL *val, const REAL *x, REAL *y);
+INT hzb_dcsr_aAxpy_device(REAL alpha, INT n, INT nnz, const INT *ia,
+                          const INT *ja, const REAL *val, const REAL *x,
+                          REAL *y);
+/* smoother as called by mgcycle's pre (forward=1) or post (forward=0)
+ * smoothing, SMOOTHER_* types JACOBI, GS, SGS, SOR, L1DIAG */
+INT hzb_smoother_device(SHORT smoother, SHORT forward, INT sweeps, REAL relax,
+                        INT n, INT nnz, const INT *ia, const INT *ja,
+                        const REAL *val, const REAL *b, REAL *x);
+/* strength graph + heavy edge matching: agg (n) and the aggregate count */
+INT hzb_aggregation_hem_device(INT n, INT nnz, const INT *ia, const INT *ja,
+                               const REAL *val, REAL strong_coupled,
+                               INT *agg, INT *num_aggregates);
+/* Galerkin product for an aggregate map; the device pattern (int32) and the
+ * values are written to freshly allocated device arrays returned through
+ * rap_*; free them with hzb_free_device. */
+INT hzb_rap_agg_device(INT n, INT nnz, const INT *ia, const INT *ja,
+                       const REAL *val, INT nc, const INT *agg,
+                       INT *rap_nnz, INT **rap_ia, INT **rap_ja,
+                       REAL **rap_val);
+void hzb_free_device(void *p);
+/* copy bytes from device memory returned above into host memory */
+INT hzb_copy_to_host(void *dst, const void *src_device, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HAZMATH_B200_H */

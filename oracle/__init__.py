@@ -1,0 +1,267 @@
+"""CPU oracle for the UA-AMG-PCG path -- TEST INFRASTRUCTURE ONLY.
+
+Two interchangeable back ends with one Python interface:
+
+* ``port`` -- ``libhzoracle.so``, the plain-C restatement of HAZmath's
+  algorithm (oracle/hzoracle.c), available wherever gcc built it;
+* ``ref``  -- ``_ref/libhazref.so``, the reference HAZmath library compiled
+  from its own sources (oracle/build_ref.sh) plus a thin harness
+  (oracle/ref_harness.c).  It exists where the reference sources were present
+  at build time and travels with the repository snapshot as a built file.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package; the product (hazmath_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "libhzoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhazref.so")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle (and the reference harness when its sources exist)."""
+    target = "all" if ref else "libhzoracle.so"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+@dataclass
+class AMGParams:
+    """The AMG_param fields this path reads (include/param.h of the reference),
+    with the survey configuration's values as defaults: UA, HEM, theta = 0,
+    V(1,1) Gauss-Seidel, coarse direct solve below 2000 rows."""
+
+    max_levels: int = 20
+    coarse_dof: int = 2000
+    cycle_type: int = 1
+    smoother: int = 2
+    presmooth_iter: int = 1
+    postsmooth_iter: int = 1
+    coarse_solver: int = 32
+    aggregation_type: int = 5
+    max_aggregation: int = 20
+    coarse_scaling: int = 0
+    print_level: int = 0
+    maxit: int = 1
+    strong_coupled: float = 0.0
+    relaxation: float = 1.0
+    tol: float = 1e-6
+
+    def arrays(self):
+        ip = (ctypes.c_int * 12)(
+            self.max_levels, self.coarse_dof, self.cycle_type, self.smoother,
+            self.presmooth_iter, self.postsmooth_iter, self.coarse_solver,
+            self.aggregation_type, self.max_aggregation, self.coarse_scaling,
+            self.print_level, self.maxit)
+        dp = (ctypes.c_double * 3)(self.strong_coupled, self.relaxation, self.tol)
+        return ip, dp
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Backend:
+    prefix = ""
+
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path}")
+        self.lib = ctypes.CDLL(path)
+        self._keep = None
+        pre = self.prefix
+        self._f = lambda name: getattr(self.lib, pre + name)
+        self._f("pcg").restype = ctypes.c_int
+        self._f("strong_coupled").restype = ctypes.c_double
+
+    # -- hierarchy ---------------------------------------------------------
+    def setup(self, ia, ja, val, params: AMGParams | None = None) -> int:
+        params = params or AMGParams()
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        self._keep = (ia, ja, val)   # the reference keeps pointers to A
+        ip, dp = params.arrays()
+        n = len(ia) - 1
+        return self._f("setup")(n, int(ia[-1]), _p(ia), _p(ja), _p(val), ip, dp)
+
+    def num_levels(self) -> int:
+        return self._f("num_levels")()
+
+    def strong_coupled(self) -> float:
+        return self._f("strong_coupled")()
+
+    def level_info(self, l: int):
+        out = (ctypes.c_int * 5)()
+        self._f("level_info")(l, out)
+        return list(out)
+
+    def level_A(self, l: int):
+        n, nnz = self.level_info(l)[:2]
+        ia = np.empty(n + 1, np.int32)
+        ja = np.empty(nnz, np.int32)
+        val = np.empty(nnz, np.float64)
+        self._f("level_A")(l, _p(ia), _p(ja), _p(val))
+        return ia, ja, val
+
+    def level_agg(self, l: int):
+        n = self.level_info(l)[0]
+        agg = np.empty(n, np.int32)
+        self._f("level_agg")(l, _p(agg))
+        return agg
+
+    def precond(self, r):
+        r = np.ascontiguousarray(r, np.float64).copy()
+        z = np.zeros_like(r)
+        self._f("precond")(_p(r), _p(z))
+        return z
+
+    def pcg(self, b, x0=None, tol=1e-8, maxit=500, stop_type=1, hist_cap=1024):
+        b = np.ascontiguousarray(b, np.float64).copy()
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        hist = np.zeros(hist_cap)
+        nh = ctypes.c_int()
+        it = self._pcg_call(b, x, tol, maxit, stop_type, hist, hist_cap, nh)
+        return it, x, hist[: min(nh.value, hist_cap)].copy()
+
+
+class Port(_Backend):
+    """The C restatement."""
+
+    prefix = "or_"
+
+    def __init__(self):
+        super().__init__(PORT_SO)
+        self.lib.or_hem_agg.restype = ctypes.c_int
+        self.lib.or_rap.restype = ctypes.c_int
+
+    def _pcg_call(self, b, x, tol, maxit, stop_type, hist, cap, nh):
+        return self.lib.or_pcg(_p(b), _p(x), ctypes.c_double(tol), maxit,
+                               stop_type, _p(hist), cap, ctypes.byref(nh))
+
+    def level_info(self, l: int):
+        out = (ctypes.c_int * 3)()
+        self.lib.or_level_info(l, out)
+        return list(out)
+
+    def set_omega(self, omega):
+        self._omega = None if omega is None else np.ascontiguousarray(omega, np.float32)
+        self.lib.or_set_omega(None if omega is None else _p(self._omega))
+
+    def free(self):
+        self.lib.or_free()
+
+    # -- kernels -----------------------------------------------------------
+    def mxv(self, ia, ja, val, x):
+        y = np.empty(len(ia) - 1)
+        self.lib.or_mxv(len(ia) - 1, _p(ia), _p(ja), _p(val), _p(x), _p(y))
+        return y
+
+    def aAxpy(self, alpha, ia, ja, val, x, y):
+        y = np.array(y, np.float64)
+        self.lib.or_aAxpy(ctypes.c_double(alpha), len(ia) - 1, _p(ia), _p(ja),
+                          _p(val), _p(x), _p(y))
+        return y
+
+    def smooth(self, smoother, pre, sweeps, ia, ja, val, b, x, relax=1.0, omega=None):
+        x = np.array(x, np.float64)
+        om = None if omega is None else np.ascontiguousarray(omega, np.float32)
+        rc = self.lib.or_smooth(smoother, int(pre), sweeps, ctypes.c_double(relax),
+                                len(ia) - 1, _p(ia), _p(ja), _p(val), _p(b), _p(x),
+                                None if om is None else _p(om))
+        if rc:
+            raise ValueError(f"smoother {smoother}: {rc}")
+        return x
+
+    def hem(self, ia, ja, val, theta=0.0):
+        n = len(ia) - 1
+        agg = np.empty(n, np.int32)
+        nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
+        return nc, agg
+
+    def rap(self, ia, ja, val, nc, agg):
+        n = len(ia) - 1
+        agg = np.ascontiguousarray(agg, np.int32)
+        cia = np.empty(nc + 1, np.int32)
+        nnz = self.lib.or_rap(n, _p(ia), _p(ja), _p(val), nc, _p(agg), _p(cia), None, None)
+        cja = np.empty(nnz, np.int32)
+        cv = np.empty(nnz)
+        self.lib.or_rap(n, _p(ia), _p(ja), _p(val), nc, _p(agg), _p(cia), _p(cja), _p(cv))
+        return cia, cja, cv
+
+
+class Ref(_Backend):
+    """The reference library compiled from its sources."""
+
+    prefix = "ref_"
+
+    def __init__(self):
+        super().__init__(REF_SO)
+        self.lib.ref_rap_agg.restype = ctypes.c_int
+        self.lib.ref_setup_seconds.restype = ctypes.c_double
+        self.lib.ref_solve_seconds.restype = ctypes.c_double
+
+    def _pcg_call(self, b, x, tol, maxit, stop_type, hist, cap, nh):
+        return self.lib.ref_pcg(_p(b), _p(x), ctypes.c_double(tol), maxit,
+                                stop_type, 0, _p(hist), cap, ctypes.byref(nh))
+
+    def timings(self):
+        return self.lib.ref_setup_seconds(), self.lib.ref_solve_seconds()
+
+    def free(self):
+        self.lib.ref_free()
+
+    def mxv(self, ia, ja, val, x):
+        n = len(ia) - 1
+        y = np.empty(n)
+        self.lib.ref_mxv(n, int(ia[-1]), _p(ia), _p(ja), _p(val), _p(x), _p(y))
+        return y
+
+    def aAxpy(self, alpha, ia, ja, val, x, y):
+        y = np.array(y, np.float64)
+        n = len(ia) - 1
+        self.lib.ref_aAxpy(ctypes.c_double(alpha), n, int(ia[-1]), _p(ia), _p(ja),
+                           _p(val), _p(x), _p(y))
+        return y
+
+    def smooth(self, smoother, pre, sweeps, ia, ja, val, b, x, relax=1.0, omega=None):
+        assert omega is None
+        x = np.array(x, np.float64)
+        n = len(ia) - 1
+        self.lib.ref_smooth(smoother, int(pre), sweeps, ctypes.c_double(relax), n,
+                            int(ia[-1]), _p(ia), _p(ja), _p(val), _p(b), _p(x))
+        return x
+
+    def rap(self, ia, ja, val, nc, agg):
+        n = len(ia) - 1
+        agg = np.ascontiguousarray(agg, np.int32)
+        cia = np.empty(nc + 1, np.int32)
+        nnz = self.lib.ref_rap_agg(n, int(ia[-1]), _p(ia), _p(ja), _p(val), nc,
+                                   _p(agg), _p(cia), None, None)
+        cja = np.empty(nnz, np.int32)
+        cv = np.empty(nnz)
+        self.lib.ref_rap_agg(n, int(ia[-1]), _p(ia), _p(ja), _p(val), nc, _p(agg),
+                             _p(cia), _p(cja), _p(cv))
+        return cia, cja, cv
+
+
+def port() -> Port:
+    return Port()
+
+
+def ref() -> Ref:
+    return Ref()
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)

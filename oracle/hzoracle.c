@@ -1,0 +1,808 @@
+/*
+ * hzoracle.c -- TEST INFRASTRUCTURE ONLY: the CPU oracle.
+ *
+ * A plain-C restatement of HAZmath's UA-AMG preconditioned CG path, written
+ * from the reference's behaviour (each function cites the reference
+ * file:line it follows).  It is the checker for the CUDA library: only the
+ * tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ * It is pinned against the reference itself (oracle/_ref, built by
+ * oracle/build_ref.sh) through the golden fixtures in tests/golden/.
+ *
+ * Build: see oracle/Makefile (gcc -O3 -ffp-contract=off, no FMA), so that
+ * every sum and product is rounded separately, in the reference's order.
+ *
+ * One deliberate difference: the coarsest level is solved by a dense
+ * Cholesky factorisation (the product's method) instead of the reference's
+ * sparse LDL^T with identity permutation (src/solver/hazmath_direct.c:633);
+ * both are direct solves and agree to rounding.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define SMALLREAL 1e-20
+#define BIGREAL 1e20
+#define UNPT (-1)
+
+typedef struct {
+    int n, m, nnz;
+    int *ia, *ja;
+    double *val;
+} ocsr;
+
+static void ocsr_free(ocsr *A)
+{
+    free(A->ia); free(A->ja); free(A->val);
+    memset(A, 0, sizeof(*A));
+}
+
+/* ---------------------------------------------------------------------------
+ * Sparse kernels (src/utilities/sparse.c)
+ * ------------------------------------------------------------------------- */
+
+/* dcsr_mxv sparse.c:1456-1590: y_i = sum_k a_k x_{ja_k}, starting at 0.0,
+ * CSR order (the unrolled cases keep that order). */
+void or_mxv(int n, const int *ia, const int *ja, const double *a,
+            const double *x, double *y)
+{
+    for (int i = 0; i < n; ++i) {
+        double t = 0.0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) t += a[k] * x[ja[k]];
+        y[i] = t;
+    }
+}
+
+/* dcsr_aAxpy sparse.c:1693-1735: y += alpha A x with the alpha = +-1 cases
+ * adding/subtracting the row sum directly. */
+void or_aAxpy(double alpha, int n, const int *ia, const int *ja,
+              const double *a, const double *x, double *y)
+{
+    for (int i = 0; i < n; ++i) {
+        double t = 0.0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) t += a[k] * x[ja[k]];
+        if (alpha == 1.0) y[i] += t;
+        else if (alpha == -1.0) y[i] -= t;
+        else y[i] += t * alpha;
+    }
+}
+
+/* dcsr_mxv_agg sparse.c:1663-1678 applied to R: y_c = sum of x over the
+ * fine rows of the aggregate, in R's (ascending) order, from 0.0 */
+static void or_restrict(int nc, const int *ria, const int *rja,
+                        const double *x, double *y)
+{
+    for (int c = 0; c < nc; ++c) {
+        double t = 0.0;
+        for (int k = ria[c]; k < ria[c + 1]; ++k) t += x[rja[k]];
+        y[c] = t;
+    }
+}
+
+/* dcsr_aAxpy_agg sparse.c:1748-1785 applied to P (one unit entry per
+ * non-empty row, agg[i] < 0 for an empty row) */
+static void or_prolong(double alpha, int n, const int *agg, const double *xc,
+                       double *x)
+{
+    for (int i = 0; i < n; ++i) {
+        double t = 0.0;
+        if (agg[i] >= 0) t += xc[agg[i]];
+        if (alpha == 1.0) x[i] += t;
+        else if (alpha == -1.0) x[i] -= t;
+        else x[i] += t * alpha;
+    }
+}
+
+/* dcsr_getdiag sparse.c:2168-2188: first diagonal entry of each row (0.0 if
+ * none: the reference's dvec_alloc leaves calloc'd zeros) */
+static void or_getdiag(int n, const int *ia, const int *ja, const double *a,
+                       double *d)
+{
+    for (int i = 0; i < n; ++i) {
+        d[i] = 0.0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+            if (ja[k] == i) { d[i] = a[k]; break; }
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Aggregation (src/solver/amg_setup_ua.c)
+ * ------------------------------------------------------------------------- */
+
+/* construct_strongly_coupled amg_setup_ua.c:375-455: keep a_ij if j == i, or
+ * a_ij^2 >= theta^2 |a_ii a_jj| and a_ij < 0; input column order. */
+int or_strength(int n, const int *ia, const int *ja, const double *a,
+                double theta, int *nia, int *nja, double *nval)
+{
+    double *d = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+    or_getdiag(n, ia, ja, a, d);
+    const double th2 = theta * theta;
+    int idx = 0;
+    for (int i = 0; i < n; ++i) {
+        nia[i] = idx;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            int j = ja[k];
+            double v = a[k];
+            if (j == i || ((v * v) >= th2 * fabs(d[i] * d[j]) && v < 0.0)) {
+                nja[idx] = j; nval[idx] = v; ++idx;
+            }
+        }
+    }
+    nia[n] = idx;
+    free(d);
+    return idx;
+}
+
+/* heavy_edg amg_setup_ua.c:864-893: start at position n0, walk to n1, keep
+ * the first strictly larger weight seen. */
+static int or_heavy(const double *w, const int *id, int n0, int n1)
+{
+    int step = (n0 > n1) ? -1 : 1;
+    int best = id[n0];
+    double bw = w[n0];
+    for (int j = n0; j != n1 + step; j += step)
+        if (w[j] > bw && id[j] >= 0) { bw = w[j]; best = id[j]; }
+    return best;
+}
+
+/* aggregation_hem amg_setup_ua.c:913-1050 on the strength graph.
+ * Returns the number of aggregates, or -1 for the "isolated point on the
+ * second pass" case where the reference calls exit(17). */
+int or_hem(int n, const int *ia, const int *ja, const double *a, int *mask)
+{
+    int maxdeg = 1;
+    for (int k = 0; k < n; ++k) {
+        int l = ia[k + 1] - ia[k];
+        if (l > maxdeg) maxdeg = l;
+        mask[k] = (l > 1) ? -1 : -2;      /* pass 0: only a diagonal -> -2 */
+    }
+    double *w = (double *)malloc(sizeof(double) * maxdeg);
+    int *iw = (int *)malloc(sizeof(int) * maxdeg);
+    int *cnt = (int *)calloc(n > 0 ? n : 1, sizeof(int));
+    int nc = 0;
+    for (int k = 0; k < n; ++k) {         /* pass 1: heavy edge matching */
+        if (mask[k] != -1) continue;
+        int iz = 0;
+        for (int p = ia[k]; p < ia[k + 1]; ++p) {
+            int j = ja[p];
+            if (mask[j] < 0 && j != k) { w[iz] = fabs(a[p]); iw[iz] = j; ++iz; }
+        }
+        if (iz) {
+            int pick = or_heavy(w, iw, iz - 1, 0);
+            mask[k] = nc; mask[pick] = nc; cnt[nc] += 2; ++nc;
+        }
+    }
+    int status = nc;
+    for (int k = 0; k < n; ++k) {         /* pass 2: attach leftovers */
+        if (mask[k] != -1) continue;
+        int iz = 0;
+        for (int p = ia[k]; p < ia[k + 1]; ++p) {
+            int kc = mask[ja[p]];
+            if (kc >= 0) { w[iz] = (double)(-cnt[kc]); iw[iz] = kc; ++iz; }
+        }
+        if (!iz) { status = -1; break; }
+        int kc = or_heavy(w, iw, 0, iz - 1);
+        mask[k] = kc; cnt[kc]++;
+    }
+    for (int k = 0; k < n; ++k)           /* pass 3 */
+        if (mask[k] < 0) mask[k] = UNPT;
+    free(w); free(iw); free(cnt);
+    return status;
+}
+
+/* dcsr_trans sparse.c:770-862 on P: R rows list fine indices ascending */
+static void or_trans_agg(int n, int nc, const int *agg, int *ria, int *rja)
+{
+    memset(ria, 0, sizeof(int) * (nc + 1));
+    for (int i = 0; i < n; ++i) if (agg[i] >= 0) ria[agg[i] + 1]++;
+    for (int c = 0; c < nc; ++c) ria[c + 1] += ria[c];
+    int *pos = (int *)malloc(sizeof(int) * (nc > 0 ? nc : 1));
+    memcpy(pos, ria, sizeof(int) * nc);
+    for (int i = 0; i < n; ++i) if (agg[i] >= 0) rja[pos[agg[i]]++] = i;
+    free(pos);
+}
+
+/* dcsr_rap_agg sparse.c:2557-2690.  Row c of A_c: slot 0 is the diagonal
+ * (starting at 0.0 and accumulated), further columns in first-encounter
+ * order over (fine row i in R row c, ascending) x (A row i, CSR order) x
+ * (P row of the column); a new column takes the entry's value, a known one
+ * adds it.  Rows of P with agg < 0 contribute nothing. */
+int or_rap_agg(int n, const int *ia, const int *ja, const double *a, int nc,
+               const int *agg, const int *ria, const int *rja, ocsr *Ac)
+{
+    int *slot = (int *)malloc(sizeof(int) * (nc > 0 ? nc : 1));
+    for (int c = 0; c < nc; ++c) slot[c] = -1;
+    /* symbolic */
+    int *cia = (int *)malloc(sizeof(int) * (nc + 1));
+    int cnt = 0;
+    for (int c = 0; c < nc; ++c) {
+        int rb = cnt;
+        cia[c] = rb;
+        slot[c] = cnt++;
+        for (int q = ria[c]; q < ria[c + 1]; ++q) {
+            int i = rja[q];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                int cc = agg[ja[k]];
+                if (cc < 0) continue;
+                if (slot[cc] < rb) slot[cc] = cnt++;
+            }
+        }
+    }
+    cia[nc] = cnt;
+    int *cja = (int *)malloc(sizeof(int) * (cnt > 0 ? cnt : 1));
+    double *cv = (double *)malloc(sizeof(double) * (cnt > 0 ? cnt : 1));
+    for (int c = 0; c < nc; ++c) slot[c] = -1;
+    cnt = 0;
+    for (int c = 0; c < nc; ++c) {
+        int rb = cnt;
+        slot[c] = cnt;
+        cja[cnt] = c; cv[cnt] = 0.0; ++cnt;
+        for (int q = ria[c]; q < ria[c + 1]; ++q) {
+            int i = rja[q];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                int cc = agg[ja[k]];
+                if (cc < 0) continue;
+                if (slot[cc] < rb) {
+                    slot[cc] = cnt; cja[cnt] = cc; cv[cnt] = a[k]; ++cnt;
+                } else {
+                    cv[slot[cc]] += a[k];
+                }
+            }
+        }
+    }
+    free(slot);
+    Ac->n = Ac->m = nc; Ac->nnz = cnt; Ac->ia = cia; Ac->ja = cja; Ac->val = cv;
+    return cnt;
+}
+
+/* ---------------------------------------------------------------------------
+ * Smoothers (src/solver/smoother.c) and their mgcycle dispatch
+ * ------------------------------------------------------------------------- */
+
+/* smoother_dcsr_jacobi smoother.c:35-100 (w = 1, t from old u) */
+static void or_jacobi(int n, const int *ia, const int *ja, const double *a,
+                      const double *b, double *u, int sweeps, double *t,
+                      double *d)
+{
+    const double w = 1.0;
+    for (int i = 0; i < n; ++i) d[i] = 0.0;
+    while (sweeps--) {
+        for (int i = 0; i < n; ++i) {
+            t[i] = b[i];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                if (ja[k] != i) t[i] -= a[k] * u[ja[k]];
+                else d[i] = a[k];
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            if (fabs(d[i]) > SMALLREAL) u[i] = (1 - w) * u[i] + w * t[i] / d[i];
+    }
+}
+
+/* smoother_dcsr_gs smoother.c:109-190: in place, d = 1/a_ii kept from the
+ * last row that had a usable diagonal */
+static void or_gs(int n, const int *ia, const int *ja, const double *a,
+                  const double *b, double *u, int sweeps, int forward)
+{
+    double d = 0.0;
+    while (sweeps--) {
+        for (int s = 0; s < n; ++s) {
+            int i = forward ? s : n - 1 - s;
+            double t = b[i];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                if (ja[k] != i) t -= a[k] * u[ja[k]];
+                else if (fabs(a[k]) > SMALLREAL) d = 1.e+0 / a[k];
+            }
+            u[i] = t * d;
+        }
+    }
+}
+
+/* smoother_dcsr_sgs smoother.c:196-250 (backward sweep from n-2) */
+static void or_sgs(int n, const int *ia, const int *ja, const double *a,
+                   const double *b, double *u, int sweeps)
+{
+    double d = 0.0;
+    while (sweeps--) {
+        for (int i = 0; i < n; ++i) {
+            double t = b[i];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                if (ja[k] != i) t -= a[k] * u[ja[k]];
+                else d = a[k];
+            }
+            if (fabs(d) > SMALLREAL) u[i] = t / d;
+        }
+        for (int i = n - 2; i >= 0; --i) {
+            double t = b[i];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                if (ja[k] != i) t -= a[k] * u[ja[k]];
+                else d = a[k];
+            }
+            if (fabs(d) > SMALLREAL) u[i] = t / d;
+        }
+    }
+}
+
+/* smoother_dcsr_sor smoother.c:257-318 */
+static void or_sor(int n, const int *ia, const int *ja, const double *a,
+                   const double *b, double *u, int sweeps, int forward,
+                   double w)
+{
+    double d = 0.0;
+    while (sweeps--) {
+        for (int s = 0; s < n; ++s) {
+            int i = forward ? s : n - 1 - s;
+            double t = b[i];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                if (ja[k] != i) t -= a[k] * u[ja[k]];
+                else d = a[k];
+            }
+            if (fabs(d) > SMALLREAL) u[i] = w * (t / d) + (1 - w) * u[i];
+        }
+    }
+}
+
+/* smoother_dcsr_L1diag smoother.c:324-390; omega (may be NULL) scales the
+ * update for the learned form: u_i += omega_i * t_i / d_i, which is the
+ * reference for omega == NULL. */
+static void or_l1(int n, const int *ia, const int *ja, const double *a,
+                  const double *b, double *u, int sweeps, double *t,
+                  double *d, const float *omega)
+{
+    while (sweeps--) {
+        for (int i = 0; i < n; ++i) {
+            t[i] = b[i]; d[i] = 0.0;
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                t[i] -= a[k] * u[ja[k]];
+                d[i] += fabs(a[k]);
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            if (fabs(d[i]) > SMALLREAL) {
+                if (omega) u[i] += (double)omega[i] * (t[i] / d[i]);
+                else u[i] += t[i] / d[i];
+            }
+    }
+}
+
+/* smoother ids as in include/macro.h */
+enum { S_JACOBI = 1, S_GS = 2, S_SGS = 3, S_SOR = 5, S_SSOR = 6, S_GSOR = 7,
+       S_SGSOR = 8, S_L1 = 10 };
+
+/* dcsr_presmoothing / dcsr_postsmoothing mgcycle.c:76-240 */
+int or_smooth(int smoother, int pre, int sweeps, double relax, int n,
+              const int *ia, const int *ja, const double *a, const double *b,
+              double *u, const float *omega)
+{
+    double *t = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+    double *d = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+    int fw = pre ? 1 : 0;
+    int rc = 0;
+    switch (smoother) {
+    case S_JACOBI: or_jacobi(n, ia, ja, a, b, u, sweeps, t, d); break;
+    case S_GS: or_gs(n, ia, ja, a, b, u, sweeps, fw); break;
+    case S_SGS: or_sgs(n, ia, ja, a, b, u, sweeps); break;
+    case S_SOR: or_sor(n, ia, ja, a, b, u, sweeps, fw, relax); break;
+    case S_SSOR:
+        or_sor(n, ia, ja, a, b, u, sweeps, fw, relax);
+        or_sor(n, ia, ja, a, b, u, sweeps, !fw, relax);
+        break;
+    case S_GSOR:
+        if (pre) { or_gs(n, ia, ja, a, b, u, sweeps, 1); or_sor(n, ia, ja, a, b, u, sweeps, 0, relax); }
+        else { or_sor(n, ia, ja, a, b, u, sweeps, 1, relax); or_gs(n, ia, ja, a, b, u, sweeps, 0); }
+        break;
+    case S_SGSOR:
+        if (pre) {
+            or_gs(n, ia, ja, a, b, u, sweeps, 1); or_gs(n, ia, ja, a, b, u, sweeps, 0);
+            or_sor(n, ia, ja, a, b, u, sweeps, 1, relax); or_sor(n, ia, ja, a, b, u, sweeps, 0, relax);
+        } else {
+            or_sor(n, ia, ja, a, b, u, sweeps, 1, relax); or_sor(n, ia, ja, a, b, u, sweeps, 0, relax);
+            or_gs(n, ia, ja, a, b, u, sweeps, 1); or_gs(n, ia, ja, a, b, u, sweeps, 0);
+        }
+        break;
+    case S_L1: or_l1(n, ia, ja, a, b, u, sweeps, t, d, omega); break;
+    default: rc = -31;
+    }
+    free(t); free(d);
+    return rc;
+}
+
+/* ---------------------------------------------------------------------------
+ * Dense Cholesky for the coarsest level
+ * ------------------------------------------------------------------------- */
+static int or_chol(int n, double *L)  /* lower factor in place, row-major */
+{
+    for (int j = 0; j < n; ++j) {
+        double s = L[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) s -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+        if (!(s > 0.0)) return -22;
+        s = sqrt(s);
+        L[(size_t)j * n + j] = s;
+        for (int i = j + 1; i < n; ++i) {
+            double t = L[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) t -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+            L[(size_t)i * n + j] = t / s;
+        }
+    }
+    return 0;
+}
+
+static void or_chol_solve(int n, const double *L, const double *b, double *x)
+{
+    for (int i = 0; i < n; ++i) {
+        double t = b[i];
+        for (int k = 0; k < i; ++k) t -= L[(size_t)i * n + k] * x[k];
+        x[i] = t / L[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double t = x[i];
+        for (int k = i + 1; k < n; ++k) t -= L[(size_t)k * n + i] * x[k];
+        x[i] = t / L[(size_t)i * n + i];
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Hierarchy, setup and cycle
+ * ------------------------------------------------------------------------- */
+#define OR_MAXLVL 20
+
+typedef struct {
+    /* parameters (AMG_param subset) */
+    int max_levels, coarse_dof, cycle_type, smoother, pre, post;
+    int coarse_solver, aggregation_type, coarse_scaling, amg_maxit;
+    double strong_coupled, relaxation;
+    /* hierarchy */
+    int nl;
+    ocsr A[OR_MAXLVL];
+    int *agg[OR_MAXLVL];
+    int nc[OR_MAXLVL];
+    int *ria[OR_MAXLVL], *rja[OR_MAXLVL];
+    double *b[OR_MAXLVL], *x[OR_MAXLVL], *w[OR_MAXLVL];
+    double *Lc;      /* dense Cholesky factor of the coarsest level */
+    const float *omega; /* learned fine-level weights (NULL: plain) */
+} or_amg;
+
+static or_amg g_or;
+
+void or_free(void)
+{
+    for (int l = 0; l < g_or.nl; ++l) {
+        ocsr_free(&g_or.A[l]);
+        free(g_or.agg[l]); free(g_or.ria[l]); free(g_or.rja[l]);
+        free(g_or.b[l]); free(g_or.x[l]); free(g_or.w[l]);
+    }
+    free(g_or.Lc);
+    memset(&g_or, 0, sizeof(g_or));
+}
+
+/* same parameter vectors as the reference harness (oracle/ref_harness.c) */
+int or_setup(int n, int nnz, const int *ia, const int *ja, const double *val,
+             const int *ip, const double *dp)
+{
+    or_free();
+    or_amg *G = &g_or;
+    G->max_levels = ip[0]; G->coarse_dof = ip[1]; G->cycle_type = ip[2];
+    G->smoother = ip[3]; G->pre = ip[4]; G->post = ip[5];
+    G->coarse_solver = ip[6]; G->aggregation_type = ip[7];
+    G->coarse_scaling = ip[9]; G->amg_maxit = ip[11];
+    G->strong_coupled = dp[0]; G->relaxation = dp[1];
+    if (G->aggregation_type != 5) return -32;   /* HEM only in the oracle */
+    ocsr *A0 = &G->A[0];
+    A0->n = A0->m = n; A0->nnz = nnz;
+    A0->ia = (int *)malloc(sizeof(int) * (n + 1));
+    A0->ja = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    A0->val = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    memcpy(A0->ia, ia, sizeof(int) * (n + 1));
+    memcpy(A0->ja, ja, sizeof(int) * nnz);
+    memcpy(A0->val, val, sizeof(double) * nnz);
+    /* amg_setup_ua.c:1233 min_cdof is a SHORT */
+    const short min_cdof = (short)(G->coarse_dof > 1 ? G->coarse_dof : 1);
+    int lvl = 0;
+    while (G->A[lvl].n > min_cdof && lvl < G->max_levels - 1) {
+        ocsr *A = &G->A[lvl];
+        int m = A->n;
+        int *nia = (int *)malloc(sizeof(int) * (m + 1));
+        int *nja = (int *)malloc(sizeof(int) * (A->nnz > 0 ? A->nnz : 1));
+        double *nv = (double *)malloc(sizeof(double) * (A->nnz > 0 ? A->nnz : 1));
+        or_strength(m, A->ia, A->ja, A->val, G->strong_coupled, nia, nja, nv);
+        int *agg = (int *)malloc(sizeof(int) * (m > 0 ? m : 1));
+        int nagg = or_hem(m, nia, nja, nv, agg);
+        free(nia); free(nja); free(nv);
+        if (nagg < 0) { free(agg); return -33; }
+        /* adaptive threshold, amg_setup_ua.c:1325-1328 */
+        if (nagg * 4 > m) G->strong_coupled /= 2;
+        else if (nagg * 1.25 < m) G->strong_coupled *= 2;
+        if (nagg < 1) { free(agg); break; }       /* P.col < MIN_CDOF */
+        G->agg[lvl] = agg;
+        G->nc[lvl] = nagg;
+        G->ria[lvl] = (int *)malloc(sizeof(int) * (nagg + 1));
+        G->rja[lvl] = (int *)malloc(sizeof(int) * (m > 0 ? m : 1));
+        or_trans_agg(m, nagg, agg, G->ria[lvl], G->rja[lvl]);
+        or_rap_agg(m, A->ia, A->ja, A->val, nagg, agg, G->ria[lvl], G->rja[lvl],
+                   &G->A[lvl + 1]);
+        ++lvl;
+    }
+    G->nl = lvl + 1;
+    for (int l = 0; l < G->nl; ++l) {
+        int m = G->A[l].n > 0 ? G->A[l].n : 1;
+        G->b[l] = (double *)calloc(m, sizeof(double));
+        G->x[l] = (double *)calloc(m, sizeof(double));
+        G->w[l] = (double *)calloc(m, sizeof(double));
+    }
+    /* coarsest: dense factorisation (coarse_solver 32) */
+    if (G->coarse_solver == 32) {
+        ocsr *C = &G->A[G->nl - 1];
+        /* amg_setup_ua.c:1392-1398: the coarsest matrix is replaced by its
+         * transpose with ascending column indices (dcsr_transz, p = NULL)
+         * before the factorisation */
+        {
+            int m = C->n, nz = C->nnz;
+            int *tia = (int *)calloc(m + 1, sizeof(int));
+            int *tja = (int *)malloc(sizeof(int) * (nz > 0 ? nz : 1));
+            double *tv = (double *)malloc(sizeof(double) * (nz > 0 ? nz : 1));
+            for (int k = 0; k < nz; ++k) tia[C->ja[k] + 1]++;
+            for (int i = 0; i < m; ++i) tia[i + 1] += tia[i];
+            int *pos = (int *)malloc(sizeof(int) * (m > 0 ? m : 1));
+            memcpy(pos, tia, sizeof(int) * m);
+            for (int i = 0; i < m; ++i)
+                for (int k = C->ia[i]; k < C->ia[i + 1]; ++k) {
+                    int q = pos[C->ja[k]]++;
+                    tja[q] = i; tv[q] = C->val[k];
+                }
+            free(pos);
+            free(C->ia); free(C->ja); free(C->val);
+            C->ia = tia; C->ja = tja; C->val = tv;
+        }
+        int m = C->n;
+        G->Lc = (double *)calloc((size_t)m * m > 0 ? (size_t)m * m : 1, sizeof(double));
+        for (int i = 0; i < m; ++i)
+            for (int k = C->ia[i]; k < C->ia[i + 1]; ++k)
+                G->Lc[(size_t)i * m + C->ja[k]] += C->val[k];
+        if (or_chol(m, G->Lc)) return -22;
+    }
+    return 0;
+}
+
+int or_num_levels(void) { return g_or.nl; }
+double or_strong_coupled(void) { return g_or.strong_coupled; }
+void or_level_info(int l, int *out)
+{
+    out[0] = g_or.A[l].n; out[1] = g_or.A[l].nnz;
+    out[2] = (l < g_or.nl - 1) ? g_or.nc[l] : 0;
+}
+void or_level_A(int l, int *ia, int *ja, double *val)
+{
+    ocsr *A = &g_or.A[l];
+    memcpy(ia, A->ia, sizeof(int) * (A->n + 1));
+    memcpy(ja, A->ja, sizeof(int) * A->nnz);
+    memcpy(val, A->val, sizeof(double) * A->nnz);
+}
+void or_level_agg(int l, int *agg)
+{
+    memcpy(agg, g_or.agg[l], sizeof(int) * g_or.A[l].n);
+}
+void or_set_omega(const float *omega) { g_or.omega = omega; }
+
+static int or_pcg_core(const ocsr *A, const double *b, double *u, int use_pc,
+                       double tol, int maxit, int stop_type, double *hist,
+                       int hist_cap, int *nhist);
+
+/* coarse_itsolver mgcycle.c:34-52: unpreconditioned CG to ctol, maxit 20n */
+static void or_coarse_cg(const ocsr *A, const double *b, double *x, double ctol)
+{
+    or_pcg_core(A, b, x, 0, ctol, 20 * A->n, 1, NULL, 0, NULL);
+}
+
+/* mgcycle mgcycle.c:245-415 (V and W cycles; precond_amg passes tol=1e-6,
+ * so the coarse CG runs to 1e-8) */
+void or_mgcycle(void)
+{
+    or_amg *G = &g_or;
+    const int nl = G->nl;
+    int num_lvl[OR_MAXLVL] = {0};
+    int l = 0;
+    double alpha = 1.0;
+    const double ctol = 1e-6 * 1e-2;
+forward:
+    while (l < nl - 1) {
+        ocsr *A = &G->A[l];
+        num_lvl[l]++;
+        or_smooth(G->smoother, 1, G->pre, G->relaxation, A->n, A->ia, A->ja,
+                  A->val, G->b[l], G->x[l], l == 0 ? G->omega : NULL);
+        memcpy(G->w[l], G->b[l], sizeof(double) * A->n);
+        or_aAxpy(-1.0, A->n, A->ia, A->ja, A->val, G->x[l], G->w[l]);
+        or_restrict(G->nc[l], G->ria[l], G->rja[l], G->w[l], G->b[l + 1]);
+        ++l;
+        memset(G->x[l], 0, sizeof(double) * G->A[l].n);
+    }
+    {
+        ocsr *C = &G->A[nl - 1];
+        if (G->coarse_solver == 32) or_chol_solve(C->n, G->Lc, G->b[nl - 1], G->x[nl - 1]);
+        else or_coarse_cg(C, G->b[nl - 1], G->x[nl - 1], ctol);
+    }
+    while (l > 0) {
+        --l;
+        ocsr *A = &G->A[l];
+        if (G->coarse_scaling == 1) {
+            ocsr *Ac = &G->A[l + 1];
+            double num = 0.0, den = 0.0;
+            for (int i = 0; i < Ac->n; ++i) num += G->x[l + 1][i] * G->b[l + 1][i];
+            /* dcsr_vmv sparse.c:1797-1815 */
+            for (int i = 0; i < Ac->n; ++i) {
+                double t = 0.0;
+                for (int k = Ac->ia[i]; k < Ac->ia[i + 1]; ++k)
+                    t += Ac->val[k] * G->x[l + 1][Ac->ja[k]];
+                den += G->x[l + 1][i] * t;
+            }
+            alpha = num / den;
+            if (alpha > 2.0) alpha = 2.0;
+        }
+        or_prolong(alpha, A->n, G->agg[l], G->x[l + 1], G->x[l]);
+        or_smooth(G->smoother, 0, G->post, G->relaxation, A->n, A->ia, A->ja,
+                  A->val, G->b[l], G->x[l], l == 0 ? G->omega : NULL);
+        if (num_lvl[l] < G->cycle_type) break;
+        else num_lvl[l] = 0;
+    }
+    if (l > 0) goto forward;
+}
+
+/* precond_amg precond.c:164-184 */
+void or_precond(const double *r, double *z)
+{
+    int m = g_or.A[0].n;
+    memcpy(g_or.b[0], r, sizeof(double) * m);
+    memset(g_or.x[0], 0, sizeof(double) * m);
+    for (int i = 0; i < g_or.amg_maxit; ++i) or_mgcycle();
+    memcpy(z, g_or.x[0], sizeof(double) * m);
+}
+
+/* array_norm2 / array_dotprod / array_norminf array.c:448-541 */
+static double or_dot(int n, const double *x, const double *y)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += x[i] * y[i];
+    return s;
+}
+static double or_norm2(int n, const double *x) { return sqrt(or_dot(n, x, x)); }
+static double or_norminf(int n, const double *x)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) { double v = fabs(x[i]); if (v > s) s = v; }
+    return s;
+}
+
+/* residual measure for the three stopping types (krylov.c:157-170 etc.) */
+static double or_resid(int stop_type, int n, const double *r, double *z,
+                       int use_pc, double *absres)
+{
+    (void)z;
+    if (stop_type == 2) {
+        if (use_pc) or_precond(r, z); else memcpy(z, r, sizeof(double) * n);
+        *absres = sqrt(fabs(or_dot(n, z, r)));
+    } else {
+        *absres = or_norm2(n, r);
+    }
+    return *absres;
+}
+
+/* dcsr_pcg krylov.c:122-398, including checks I-III and the restarts */
+static int or_pcg_core(const ocsr *A, const double *b, double *u, int use_pc,
+                       double tol, int maxit, int stop_type, double *hist,
+                       int hist_cap, int *nhist)
+{
+    const int n = A->n;
+    const double maxdiff = tol * 1e-4;
+    int iter = 0, stag = 1, more_step = 1;
+    double absres0 = BIGREAL, absres = BIGREAL, relres = BIGREAL;
+    double normu = BIGREAL, normr0 = BIGREAL;
+    double alpha, beta, temp1, temp2;
+    int nh = 0;
+    double *p = (double *)calloc(4 * (size_t)(n > 0 ? n : 1), sizeof(double));
+    double *z = p + n, *r = z + n, *t = r + n;
+#define PC_APPLY() do { \
+        if (hist && nh < hist_cap) hist[nh] = or_norm2(n, r); \
+        ++nh; \
+        if (use_pc) or_precond(r, z); else memcpy(z, r, sizeof(double) * n); \
+    } while (0)
+
+    memcpy(r, b, sizeof(double) * n);
+    or_aAxpy(-1.0, n, A->ia, A->ja, A->val, u, r);
+    PC_APPLY();
+    switch (stop_type) {
+    case 1: absres0 = or_norm2(n, r); normr0 = absres0 > SMALLREAL ? absres0 : SMALLREAL;
+        relres = absres0 / normr0; break;
+    case 2: absres0 = sqrt(or_dot(n, r, z)); normr0 = absres0 > SMALLREAL ? absres0 : SMALLREAL;
+        relres = absres0 / normr0; break;
+    case 3: absres0 = or_norm2(n, r); normu = or_norm2(n, u);
+        if (normu < SMALLREAL) normu = SMALLREAL;
+        relres = absres0 / normu; break;
+    default: goto done;
+    }
+    if (relres < tol || absres0 < 1e-3 * tol) goto done;
+    memcpy(p, z, sizeof(double) * n);
+    temp1 = or_dot(n, z, r);
+    while (iter++ < maxit) {
+        or_mxv(n, A->ia, A->ja, A->val, p, t);
+        temp2 = or_dot(n, t, p);
+        alpha = temp1 / temp2;
+        for (int i = 0; i < n; ++i) u[i] += alpha * p[i];
+        for (int i = 0; i < n; ++i) r[i] += (-alpha) * t[i];
+        or_resid(stop_type, n, r, z, use_pc, &absres);
+        relres = absres / (stop_type == 3 ? normu : normr0);
+        if (or_norminf(n, u) <= SMALLREAL) { iter = -43; break; }
+        normu = or_norm2(n, u);
+        double reldiff = fabs(alpha) * or_norm2(n, p) / normu;
+        if ((stag <= 20) & (reldiff < maxdiff)) {
+            memcpy(r, b, sizeof(double) * n);
+            or_aAxpy(-1.0, n, A->ia, A->ja, A->val, u, r);
+            or_resid(stop_type, n, r, z, use_pc, &absres);
+            relres = absres / (stop_type == 3 ? normu : normr0);
+            if (relres < tol) break;
+            if (stag >= 20) { iter = -42; break; }
+            memset(p, 0, sizeof(double) * n);
+            ++stag;
+        }
+        if (relres < tol) {
+            memcpy(r, b, sizeof(double) * n);
+            or_aAxpy(-1.0, n, A->ia, A->ja, A->val, u, r);
+            or_resid(stop_type, n, r, z, use_pc, &absres);
+            relres = absres / (stop_type == 3 ? normu : normr0);
+            if (relres < tol) break;
+            if (more_step >= 20) { iter = -44; break; }
+            memset(p, 0, sizeof(double) * n);
+            ++more_step;
+        }
+        absres0 = absres;
+        if (stop_type != 2) PC_APPLY();
+        temp2 = or_dot(n, z, r);
+        beta = temp2 / temp1;
+        temp1 = temp2;
+        for (int i = 0; i < n; ++i) p[i] = 1.0 * z[i] + beta * p[i];
+    }
+done:
+    free(p);
+    if (nhist) *nhist = nh;
+#undef PC_APPLY
+    if (iter > maxit) return -48;
+    return iter;
+}
+
+int or_pcg(const double *b, double *x, double tol, int maxit, int stop_type,
+           double *hist, int hist_cap, int *nhist)
+{
+    return or_pcg_core(&g_or.A[0], b, x, 1, tol, maxit, stop_type, hist,
+                       hist_cap, nhist);
+}
+
+/* ---- kernel-level wrappers for the parity tests ------------------------ */
+int or_hem_agg(int n, const int *ia, const int *ja, const double *a,
+               double theta, int *agg)
+{
+    int nnz = ia[n];
+    int *nia = (int *)malloc(sizeof(int) * (n + 1));
+    int *nja = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    double *nv = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    or_strength(n, ia, ja, a, theta, nia, nja, nv);
+    int nc = or_hem(n, nia, nja, nv, agg);
+    free(nia); free(nja); free(nv);
+    return nc;
+}
+
+static ocsr g_rap;
+int or_rap(int n, const int *ia, const int *ja, const double *a, int nc,
+           const int *agg, int *rap_ia, int *rap_ja, double *rap_val)
+{
+    if (!rap_ja) {
+        int *ria = (int *)malloc(sizeof(int) * (nc + 1));
+        int *rja = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+        or_trans_agg(n, nc, agg, ria, rja);
+        ocsr_free(&g_rap);
+        or_rap_agg(n, ia, ja, a, nc, agg, ria, rja, &g_rap);
+        free(ria); free(rja);
+        memcpy(rap_ia, g_rap.ia, sizeof(int) * (nc + 1));
+        return g_rap.nnz;
+    }
+    memcpy(rap_ja, g_rap.ja, sizeof(int) * g_rap.nnz);
+    memcpy(rap_val, g_rap.val, sizeof(double) * g_rap.nnz);
+    return g_rap.nnz;
+}

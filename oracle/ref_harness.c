@@ -1,0 +1,231 @@
+/*
+ * ref_harness.c -- test infrastructure only.
+ *
+ * A thin ctypes-facing shim over the reference HAZmath library compiled from
+ * its own sources by oracle/build_ref.sh.  It is the checker that pins the C
+ * restatement (oracle/hzoracle.c) and produces the golden fixtures under
+ * tests/golden/.  Nothing in the product links or loads it.
+ *
+ * The UA-AMG-PCG path is driven the way linear_solver_dcsr_krylov_amg
+ * (src/solver/itsolver.c:846-931) drives it, except that dcsr_pcg
+ * (src/solver/krylov.c:122) is called directly instead of
+ * dcsr_pcg_w_cond_est: without LAPACK the latter exits the process with
+ * status 252 after a converged solve (krylov.c:704, message.c:295); its
+ * iterates are the same.
+ */
+#include "hazmath.h"
+#include <time.h>
+
+static AMG_data *g_mgl = NULL;
+static AMG_param g_amg;
+static dCSRmat g_A;            /* caller's matrix, wrapped (not owned) */
+static precond_data g_pcdata;
+static precond g_pc;
+static double *g_hist = NULL;  /* ||r|| seen by each preconditioner call */
+static int g_hist_cap = 0, g_hist_n = 0;
+static double g_setup_s = 0.0, g_solve_s = 0.0;
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* iparam: [0] max_levels [1] coarse_dof [2] cycle_type [3] smoother
+ *         [4] presmooth [5] postsmooth [6] coarse_solver [7] aggregation_type
+ *         [8] max_aggregation [9] coarse_scaling [10] print_level [11] amg maxit
+ * dparam: [0] strong_coupled [1] relaxation [2] amg tol                      */
+static void fill_param(AMG_param *p, const int *ip, const double *dp)
+{
+    param_amg_init(p);
+    p->AMG_type = UA_AMG;
+    p->max_levels = (SHORT)ip[0];
+    p->coarse_dof = ip[1];
+    p->cycle_type = (SHORT)ip[2];
+    p->smoother = (SHORT)ip[3];
+    p->presmooth_iter = (SHORT)ip[4];
+    p->postsmooth_iter = (SHORT)ip[5];
+    p->coarse_solver = (SHORT)ip[6];
+    p->aggregation_type = (SHORT)ip[7];
+    p->max_aggregation = ip[8];
+    p->coarse_scaling = (SHORT)ip[9];
+    p->print_level = (SHORT)ip[10];
+    p->maxit = ip[11];
+    p->strong_coupled = dp[0];
+    p->relaxation = dp[1];
+    p->tol = dp[2];
+}
+
+void ref_free(void)
+{
+    if (g_mgl) {
+        amg_data_free(g_mgl, &g_amg);
+        free(g_mgl);
+        g_mgl = NULL;
+    }
+}
+
+int ref_setup(int n, int nnz, int *ia, int *ja, double *val,
+              const int *iparam, const double *dparam)
+{
+    ref_free();
+    fill_param(&g_amg, iparam, dparam);
+    g_A.row = n; g_A.col = n; g_A.nnz = nnz;
+    g_A.IA = ia; g_A.JA = ja; g_A.val = val;
+    g_mgl = amg_data_create(g_amg.max_levels);
+    g_mgl[0].A = dcsr_create(n, n, nnz);
+    dcsr_cp(&g_A, &g_mgl[0].A);
+    g_mgl[0].b = dvec_create(n);
+    g_mgl[0].x = dvec_create(n);
+    double t0 = now_s();
+    SHORT status = amg_setup_ua(g_mgl, &g_amg);
+    g_setup_s = now_s() - t0;
+    precond_data_null(&g_pcdata);
+    param_amg_to_prec(&g_pcdata, &g_amg);
+    g_pcdata.max_levels = g_mgl[0].num_levels;
+    g_pcdata.mgl_data = g_mgl;
+    g_pc.data = &g_pcdata;
+    g_pc.fct = precond_amg;
+    return status;
+}
+
+double ref_setup_seconds(void) { return g_setup_s; }
+double ref_solve_seconds(void) { return g_solve_s; }
+double ref_strong_coupled(void) { return g_amg.strong_coupled; }
+int ref_num_levels(void) { return g_mgl ? g_mgl[0].num_levels : 0; }
+
+/* out: [0] rows [1] nnz of A_l [2] columns of P_l (0 on the coarsest)
+ *      [3] nnz of P_l [4] nnz of R_l                                        */
+void ref_level_info(int l, int *out)
+{
+    dCSRmat *A = &g_mgl[l].A, *P = &g_mgl[l].P, *R = &g_mgl[l].R;
+    out[0] = A->row; out[1] = A->nnz;
+    out[2] = P->IA ? P->col : 0; out[3] = P->IA ? P->nnz : 0;
+    out[4] = R->IA ? R->nnz : 0;
+}
+
+void ref_level_A(int l, int *ia, int *ja, double *val)
+{
+    dCSRmat *A = &g_mgl[l].A;
+    memcpy(ia, A->IA, sizeof(int) * (A->row + 1));
+    memcpy(ja, A->JA, sizeof(int) * A->nnz);
+    memcpy(val, A->val, sizeof(double) * A->nnz);
+}
+
+/* aggregate map recovered from P: P(i, agg[i]) = 1, or -1 for an empty row */
+void ref_level_agg(int l, int *agg)
+{
+    dCSRmat *P = &g_mgl[l].P;
+    for (int i = 0; i < P->row; ++i)
+        agg[i] = (P->IA[i + 1] > P->IA[i]) ? P->JA[P->IA[i]] : -1;
+}
+
+void ref_level_R(int l, int *ia, int *ja)
+{
+    dCSRmat *R = &g_mgl[l].R;
+    memcpy(ia, R->IA, sizeof(int) * (R->row + 1));
+    memcpy(ja, R->JA, sizeof(int) * R->nnz);
+}
+
+/* one application of the AMG preconditioner, precond_amg (precond.c:164) */
+void ref_precond(double *r, double *z) { precond_amg(r, z, &g_pcdata); }
+
+static void hist_precond(REAL *r, REAL *z, void *data)
+{
+    if (g_hist_n < g_hist_cap) {
+        REAL s = 0.0;
+        for (int i = 0; i < g_mgl[0].A.row; ++i) s += r[i] * r[i];
+        g_hist[g_hist_n] = sqrt(s);
+    }
+    g_hist_n++;
+    precond_amg(r, z, data);
+}
+
+/* PCG with the AMG preconditioner; hist receives ||r|| at every
+ * preconditioner call (r_0, r_1, ...), nhist the number of calls.          */
+int ref_pcg(double *b, double *x, double tol, int maxit, int stop_type,
+            int print_level, double *hist, int hist_cap, int *nhist)
+{
+    dvector bb, xx;
+    bb.row = g_A.row; bb.val = b;
+    xx.row = g_A.row; xx.val = x;
+    g_hist = hist; g_hist_cap = hist ? hist_cap : 0; g_hist_n = 0;
+    precond pc = g_pc;
+    pc.fct = hist ? hist_precond : precond_amg;
+    double t0 = now_s();
+    int it = dcsr_pcg(&g_A, &bb, &xx, &pc, tol, maxit, (SHORT)stop_type,
+                      (SHORT)print_level);
+    g_solve_s = now_s() - t0;
+    if (nhist) *nhist = g_hist_n;
+    g_hist = NULL; g_hist_cap = 0;
+    return it;
+}
+
+/* ---- kernel-level entry points on caller arrays -------------------------- */
+static dCSRmat wrap(int n, int m, int nnz, int *ia, int *ja, double *val)
+{
+    dCSRmat A;
+    A.row = n; A.col = m; A.nnz = nnz; A.IA = ia; A.JA = ja; A.val = val;
+    return A;
+}
+
+void ref_mxv(int n, int nnz, int *ia, int *ja, double *val, double *x, double *y)
+{
+    dCSRmat A = wrap(n, n, nnz, ia, ja, val);
+    dcsr_mxv(&A, x, y);
+}
+
+void ref_aAxpy(double alpha, int n, int nnz, int *ia, int *ja, double *val,
+               double *x, double *y)
+{
+    dCSRmat A = wrap(n, n, nnz, ia, ja, val);
+    dcsr_aAxpy(alpha, &A, x, y);
+}
+
+/* forward != 0: the pre-smoothing call of mgcycle (mgcycle.c:289);
+ * forward == 0: the post-smoothing call (mgcycle.c:397).                   */
+void ref_smooth(int smoother, int forward, int sweeps, double relax, int n,
+                int nnz, int *ia, int *ja, double *val, double *b, double *x)
+{
+    dCSRmat A = wrap(n, n, nnz, ia, ja, val);
+    dvector bb, xx;
+    bb.row = n; bb.val = b; xx.row = n; xx.val = x;
+    int i0 = forward ? 0 : n - 1, i1 = forward ? n - 1 : 0, s = forward ? 1 : -1;
+    switch (smoother) {
+    case SMOOTHER_JACOBI: smoother_dcsr_jacobi(&xx, i0, i1, s, &A, &bb, sweeps); break;
+    case SMOOTHER_GS: smoother_dcsr_gs(&xx, i0, i1, s, &A, &bb, sweeps); break;
+    case SMOOTHER_SGS: smoother_dcsr_sgs(&xx, &A, &bb, sweeps); break;
+    case SMOOTHER_SOR: smoother_dcsr_sor(&xx, i0, i1, s, &A, &bb, sweeps, relax); break;
+    case SMOOTHER_L1DIAG: smoother_dcsr_L1diag(&xx, i0, i1, s, &A, &bb, sweeps); break;
+    default: break;
+    }
+}
+
+/* Galerkin product for aggregation, dcsr_rap_agg (sparse.c:2557); two calls:
+ * first with ia_out only (sizes), then with all outputs.                     */
+static dCSRmat g_rap = {0};
+int ref_rap_agg(int n, int nnz, int *ia, int *ja, double *val, int nc,
+                const int *agg, int *rap_ia, int *rap_ja, double *rap_val)
+{
+    if (!rap_ja) {
+        dCSRmat A = wrap(n, n, nnz, ia, ja, val), P, R;
+        int np = 0;
+        for (int i = 0; i < n; ++i) np += agg[i] >= 0;
+        P = dcsr_create(n, nc, np);
+        for (int i = 0, k = 0; i < n; ++i) {
+            P.IA[i] = k;
+            if (agg[i] >= 0) { P.JA[k] = agg[i]; P.val[k] = 1.0; ++k; }
+        }
+        P.IA[n] = np;
+        dcsr_trans(&P, &R);
+        if (g_rap.IA) dcsr_free(&g_rap);
+        dcsr_rap_agg(&R, &A, &P, &g_rap);
+        dcsr_free(&P); dcsr_free(&R);
+        memcpy(rap_ia, g_rap.IA, sizeof(int) * (nc + 1));
+        return g_rap.nnz;
+    }
+    memcpy(rap_ja, g_rap.JA, sizeof(int) * g_rap.nnz);
+    memcpy(rap_val, g_rap.val, sizeof(double) * g_rap.nnz);
+    return g_rap.nnz;
+}

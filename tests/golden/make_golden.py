@@ -1,0 +1,201 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py [REFERENCE_DIR]
+
+Runs the reference HAZmath library compiled from its own sources
+(oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
+and on the reference's only shipped known-answer case for this path
+(examples/solvers/A.dat + b.dat: 128x128 5-point Laplacian), and stores its
+outputs: hierarchy sizes, aggregate maps, coarse operators (full arrays for
+small cases, SHA-256 digests for large ones), PCG iteration counts, residual
+histories and solutions, smoother outputs, the RAP product, and the struct
+layout of the reference headers.  The fixtures let the CPU tests pin the
+C restatement (oracle/hzoracle.c) without the reference present, and the GPU
+tests compare the CUDA path against the same numbers.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from hazmath_b200 import problems as P  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HAZ_REF", "/root/reference")
+
+
+def sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def hierarchy(R, ia, ja, val, params, full: bool):
+    st = R.setup(ia, ja, val, params)
+    assert st == 0, st
+    nl = R.num_levels()
+    info = np.array([R.level_info(l)[:3] for l in range(nl)], np.int64)
+    out = {"info": info, "theta_after": np.float64(R.strong_coupled())}
+    for l in range(nl):
+        A = R.level_A(l)
+        if full:
+            out[f"A{l}_ia"], out[f"A{l}_ja"], out[f"A{l}_val"] = A
+        else:
+            out[f"A{l}_sha"] = np.array([sha(A[0]), sha(A[1]), sha(A[2])])
+        if l < nl - 1:
+            out[f"agg{l}"] = R.level_agg(l)
+    return out
+
+
+def solve(R, b, tol=1e-8, maxit=500):
+    it, x, hist = R.pcg(b, None, tol, maxit, 1)
+    return {"iters": np.int64(it), "x": x, "hist": hist}
+
+
+def layout() -> dict:
+    """sizeof/offsetof of the drop-in structures, from the reference headers."""
+    src = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "hazmath.h"
+#define S(T) printf("\"sizeof(" #T ")\": %zu,\n", sizeof(T));
+#define O(T,f) printf("\"" #T "." #f "\": %zu,\n", offsetof(T,f));
+int main(){S(dCSRmat)S(dvector)S(ivector)S(linear_itsolver_param)S(AMG_param)
+S(precond)S(Schwarz_data)S(AMG_data)S(precond_data)
+O(dCSRmat,IA)O(dCSRmat,val)O(linear_itsolver_param,linear_tol)
+O(linear_itsolver_param,AL_scaling_param)O(AMG_param,tol)O(AMG_param,coarse_dof)
+O(AMG_param,relaxation)O(AMG_param,amli_coef)O(AMG_param,strong_coupled)
+O(AMG_param,max_aggregation)O(AMG_param,tentative_smooth)O(AMG_param,HAZDIR)
+O(AMG_param,damping_param)O(AMG_param,fpwr)O(AMG_param,smoother_function)
+O(precond,fct)O(precond,setup_time)O(AMG_data,A)O(AMG_data,R)O(AMG_data,P)
+O(AMG_data,b)O(AMG_data,x)O(AMG_data,Numeric)O(AMG_data,near_kernel_dim)
+O(AMG_data,Schwarz)O(AMG_data,w)O(AMG_data,cycle_type)O(AMG_data,wdata)
+O(precond_data,tol)O(precond_data,amli_coef)O(precond_data,mgl_data)
+O(precond_data,fpwr)O(precond_data,A)O(precond_data,w)
+printf("\"end\": 0\n");return 0;}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "lay.c")
+        exe = os.path.join(d, "lay")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-w", "-I", os.path.join(ROOT, "oracle", "_ref", "include"),
+                        "-I", os.path.join(REF, "include"), c, "-o", exe], check=True)
+        txt = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    d = json.loads("{" + txt + "}")
+    d.pop("end")
+    return d
+
+
+def main():
+    if not oracle.ref_available():
+        oracle.build(ref=True)
+    R = oracle.ref()
+    rng = np.random.default_rng(20261203)
+    base = oracle.AMGParams()
+
+    # 1. struct layouts
+    with open(os.path.join(HERE, "layout.json"), "w") as f:
+        json.dump(layout(), f, indent=1, sort_keys=True)
+
+    # 2. the reference's known-answer case: examples/solvers A.dat / b.dat
+    ia, ja, val = P.read_coo(os.path.join(REF, "examples", "solvers", "A.dat"))
+    gia, gja, gval = P.poisson2d_5pt(128)
+    assert np.array_equal(ia, gia) and np.array_equal(ja, gja) and np.array_equal(val, gval)
+    b = np.loadtxt(os.path.join(REF, "examples", "solvers", "b.dat"), skiprows=1)
+    g = hierarchy(R, ia, ja, val, base, full=False)
+    g.update(solve(R, b))
+    g["b"] = b
+    g["A_sha"] = np.array([sha(ia), sha(ja), sha(val)])
+    np.savez_compressed(os.path.join(HERE, "fixture128.npz"), **g)
+    print("fixture128: levels", g["info"][:, 0], "iters", g["iters"])
+
+    # 3. C1: 255^2 interior 5-point, b ~ U[-1,1] seed 1
+    ia, ja, val = P.poisson2d_5pt(255)
+    b = P.rhs_uniform(len(ia) - 1, 1)
+    g = hierarchy(R, ia, ja, val, base, full=False)
+    g.update(solve(R, b))
+    g["x_sha"] = np.array([sha(g["x"])])
+    g["x_head"] = g.pop("x")[:64]
+    np.savez_compressed(os.path.join(HERE, "c1_poisson255.npz"), **g)
+    print("C1: levels", g["info"][:, 0], "iters", g["iters"])
+
+    # 4. small cases: full hierarchies, one preconditioner application, PCG
+    small = {}
+    cases = {
+        "p2d_40": (P.poisson2d_5pt(40), base),
+        "aniso2d_31": (P.aniso2d_p1(31, 0.02, 0.7), oracle.AMGParams(coarse_dof=60)),
+        "kuhn_12": (P.kuhn3d_p1(12, P.lognormal_field(12, 1.0, 3.0, 2)),
+                    oracle.AMGParams(coarse_dof=100)),
+        "p2d_40_l1": (P.poisson2d_5pt(40), oracle.AMGParams(smoother=10, presmooth_iter=2,
+                                                           postsmooth_iter=2, coarse_dof=80)),
+        "p2d_40_sgs_w": (P.poisson2d_5pt(40), oracle.AMGParams(smoother=3, cycle_type=2,
+                                                              coarse_dof=80)),
+        "p2d_40_sor_cs": (P.poisson2d_5pt(40), oracle.AMGParams(smoother=5, relaxation=1.3,
+                                                               coarse_scaling=1,
+                                                               coarse_dof=80)),
+        "p2d_40_jac_cg": (P.poisson2d_5pt(40), oracle.AMGParams(smoother=1, presmooth_iter=2,
+                                                               postsmooth_iter=2,
+                                                               coarse_solver=0,
+                                                               coarse_dof=80)),
+        "theta_p2d_40": (P.poisson2d_5pt(40), oracle.AMGParams(strong_coupled=0.25,
+                                                              coarse_dof=50)),
+    }
+    for name, ((ia, ja, val), prm) in cases.items():
+        n = len(ia) - 1
+        g = hierarchy(R, ia, ja, val, prm, full=True)
+        r = rng.uniform(-1, 1, n)
+        z = R.precond(r)
+        b = rng.uniform(-1, 1, n)
+        s = solve(R, b)
+        for k, v in g.items():
+            small[f"{name}/{k}"] = v
+        small[f"{name}/A_ia"], small[f"{name}/A_ja"], small[f"{name}/A_val"] = ia, ja, val
+        small[f"{name}/params"] = np.array(
+            [prm.max_levels, prm.coarse_dof, prm.cycle_type, prm.smoother, prm.presmooth_iter,
+             prm.postsmooth_iter, prm.coarse_solver, prm.aggregation_type,
+             prm.max_aggregation, prm.coarse_scaling, prm.print_level, prm.maxit], np.int64)
+        small[f"{name}/dparams"] = np.array([prm.strong_coupled, prm.relaxation, prm.tol])
+        small[f"{name}/r"], small[f"{name}/z"] = r, z
+        small[f"{name}/b"] = b
+        small[f"{name}/iters"], small[f"{name}/x"], small[f"{name}/hist"] = (
+            s["iters"], s["x"], s["hist"])
+        print(name, "levels", g["info"][:, 0], "iters", s["iters"])
+    np.savez_compressed(os.path.join(HERE, "small_cases.npz"), **small)
+
+    # 5. smoothers (pre = mgcycle's forward call, post = backward call)
+    ia, ja, val = P.aniso2d_p1(19, 0.05, 1.1)
+    n = len(ia) - 1
+    b = rng.uniform(-1, 1, n)
+    x0 = rng.uniform(-1, 1, n)
+    sm = {"ia": ia, "ja": ja, "val": val, "b": b, "x0": x0}
+    for s_id in (1, 2, 3, 5, 10):
+        for pre in (1, 0):
+            sm[f"s{s_id}_pre{pre}"] = R.smooth(s_id, pre, 2, ia, ja, val, b, x0, relax=1.2)
+    sm["mxv"] = R.mxv(ia, ja, val, x0)
+    sm["aAxpy_m1"] = R.aAxpy(-1.0, ia, ja, val, x0, b)
+    sm["aAxpy_07"] = R.aAxpy(0.7, ia, ja, val, x0, b)
+    np.savez_compressed(os.path.join(HERE, "smoothers.npz"), **sm)
+
+    # 6. RAP on a 3D anisotropic Kuhn matrix with a seeded aggregate map
+    ia, ja, val = P.aniso3d_p1(7, 0.1, 0.8, (1.0, 2.0, 0.5))
+    n = len(ia) - 1
+    nc = n // 3
+    agg = rng.integers(-1, nc, n).astype(np.int32)
+    agg[:nc] = np.arange(nc)          # every aggregate non-empty
+    cia, cja, cval = R.rap(ia, ja, val, nc, agg)
+    np.savez_compressed(os.path.join(HERE, "rap.npz"), ia=ia, ja=ja, val=val, agg=agg,
+                        nc=np.int64(nc), cia=cia, cja=cja, cval=cval)
+    R.free()
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
