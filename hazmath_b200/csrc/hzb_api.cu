@@ -305,6 +305,48 @@ extern "C" INT hzb_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z) {
     return SUCCESS;
 }
 
+extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
+                               REAL *ms_per_launch, REAL *bytes_per_launch) {
+    if (!S || level < 0 || level >= S->nl || reps < 1) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    Level &L = S->lv[level];
+    const bool f32 = which == HZB_K_SPMV32 || which == HZB_K_L1_32;
+    if (f32 && !L.val32) HZB_TRY(ensure_fp32(S));
+    const double vb = f32 ? 4.0 : 8.0;
+    const double n = L.n, nnz = L.nnz;
+    double bytes = nnz * (vb + 4.0) + 4.0 * (n + 1);
+    switch (which) {
+    case HZB_K_SPMV64: case HZB_K_SPMV32: bytes += 2 * vb * n; break;     // x, y
+    case HZB_K_RES64: bytes += 3 * vb * n; break;                        // x, b, w
+    case HZB_K_L1_32: case HZB_K_L1_64: bytes += 3 * vb * n; break;      // x, b, xn
+    default: return ERROR_INPUT_PAR;
+    }
+    auto launch = [&]() -> int {
+        switch (which) {
+        case HZB_K_SPMV64:
+            return spmv<double>(L.A64(), SPMV_Y, L.x, nullptr, L.w, 1.0, nullptr, S->s);
+        case HZB_K_SPMV32:
+            return spmv<float>(L.A32(), SPMV_Y, L.x32, nullptr, L.w32, 1.0f, nullptr, S->s);
+        case HZB_K_RES64:
+            return spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, S->s);
+        case HZB_K_L1_32:
+            return l1_sweep<float>(L.A32(), L.b32, L.x32, L.t32, nullptr, S->s);
+        default:
+            return l1_sweep<double>(L.A64(), L.b, L.x, L.t, nullptr, S->s);
+        }
+    };
+    HZB_TRY(launch());
+    HZB_CUDA(cudaEventRecord(S->e0, S->s));
+    for (int r = 0; r < reps; ++r) HZB_TRY(launch());
+    HZB_CUDA(cudaEventRecord(S->e1, S->s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    HZB_CUDA(cudaEventElapsedTime(&ms, S->e0, S->e1));
+    *ms_per_launch = ms / reps;
+    *bytes_per_launch = bytes;
+    return SUCCESS;
+}
+
 extern "C" INT hzb_get_stats(const hzb_solver *S, hzb_stats *st) {
     if (!S || !st) return ERROR_INPUT_PAR;
     *st = S->st;

@@ -408,6 +408,22 @@ void hzb_destroy(hzb_solver *s);
 /* last CUDA error message of this thread ("" if none) */
 const char *hzb_last_error(void);
 
+/* Time `reps` back-to-back launches of one cycle kernel on level `level` of
+ * the handle's hierarchy, on the handle's stream with CUDA events, after a
+ * warm-up launch.  Returns the mean device time per launch and the
+ * algorithmic bytes one launch must move (FP64 value 8 B or FP32 4 B + int32
+ * index per entry, row pointers, and each vector once).  which:
+ *   HZB_K_SPMV64  y = A x, FP64        HZB_K_SPMV32  y = A x, FP32
+ *   HZB_K_RES64   w = b - A x, FP64    HZB_K_L1_32   l1-Jacobi sweep, FP32
+ *   HZB_K_L1_64   l1-Jacobi sweep, FP64                                    */
+#define HZB_K_SPMV64 0
+#define HZB_K_SPMV32 1
+#define HZB_K_RES64  2
+#define HZB_K_L1_32  3
+#define HZB_K_L1_64  4
+INT hzb_time_kernel(hzb_solver *s, INT which, INT level, INT reps,
+                    REAL *ms_per_launch, REAL *bytes_per_launch);
+
 /* Kernel-level entry points on device arrays, one stream-ordered launch
  * sequence each, used by the parity tests.  Each returns SUCCESS or
  * ERROR_SOLVER_MISC and synchronises before returning. */

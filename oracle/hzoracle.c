@@ -383,9 +383,9 @@ int or_smooth(int smoother, int pre, int sweeps, double relax, int n,
     case S_GS: or_gs(n, ia, ja, a, b, u, sweeps, fw); break;
     case S_SGS: or_sgs(n, ia, ja, a, b, u, sweeps); break;
     case S_SOR: or_sor(n, ia, ja, a, b, u, sweeps, fw, relax); break;
-    case S_SSOR:
-        or_sor(n, ia, ja, a, b, u, sweeps, fw, relax);
-        or_sor(n, ia, ja, a, b, u, sweeps, !fw, relax);
+    case S_SSOR:   /* forward then backward in both calls (mgcycle.c:100, :187) */
+        or_sor(n, ia, ja, a, b, u, sweeps, 1, relax);
+        or_sor(n, ia, ja, a, b, u, sweeps, 0, relax);
         break;
     case S_GSOR:
         if (pre) { or_gs(n, ia, ja, a, b, u, sweeps, 1); or_sor(n, ia, ja, a, b, u, sweeps, 0, relax); }

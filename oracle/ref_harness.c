@@ -192,12 +192,46 @@ void ref_smooth(int smoother, int forward, int sweeps, double relax, int n,
     dvector bb, xx;
     bb.row = n; bb.val = b; xx.row = n; xx.val = x;
     int i0 = forward ? 0 : n - 1, i1 = forward ? n - 1 : 0, s = forward ? 1 : -1;
+    /* the argument pattern of dcsr_presmoothing / dcsr_postsmoothing,
+     * with istart = 0, iend = n-1, istep = +1 (pre) or -1 (post) */
+    const int is = 0, ie = n - 1, st = forward ? 1 : -1;
     switch (smoother) {
     case SMOOTHER_JACOBI: smoother_dcsr_jacobi(&xx, i0, i1, s, &A, &bb, sweeps); break;
     case SMOOTHER_GS: smoother_dcsr_gs(&xx, i0, i1, s, &A, &bb, sweeps); break;
     case SMOOTHER_SGS: smoother_dcsr_sgs(&xx, &A, &bb, sweeps); break;
     case SMOOTHER_SOR: smoother_dcsr_sor(&xx, i0, i1, s, &A, &bb, sweeps, relax); break;
     case SMOOTHER_L1DIAG: smoother_dcsr_L1diag(&xx, i0, i1, s, &A, &bb, sweeps); break;
+    case SMOOTHER_SSOR:
+        if (forward) {
+            smoother_dcsr_sor(&xx, is, ie, st, &A, &bb, sweeps, relax);
+            smoother_dcsr_sor(&xx, ie, is, -st, &A, &bb, sweeps, relax);
+        } else {
+            smoother_dcsr_sor(&xx, is, ie, -st, &A, &bb, sweeps, relax);
+            smoother_dcsr_sor(&xx, ie, is, st, &A, &bb, sweeps, relax);
+        }
+        break;
+    case SMOOTHER_GSOR:
+        if (forward) {
+            smoother_dcsr_gs(&xx, is, ie, st, &A, &bb, sweeps);
+            smoother_dcsr_sor(&xx, ie, is, -st, &A, &bb, sweeps, relax);
+        } else {
+            smoother_dcsr_sor(&xx, is, ie, -st, &A, &bb, sweeps, relax);
+            smoother_dcsr_gs(&xx, ie, is, st, &A, &bb, sweeps);
+        }
+        break;
+    case SMOOTHER_SGSOR:
+        if (forward) {
+            smoother_dcsr_gs(&xx, is, ie, st, &A, &bb, sweeps);
+            smoother_dcsr_gs(&xx, ie, is, -st, &A, &bb, sweeps);
+            smoother_dcsr_sor(&xx, is, ie, st, &A, &bb, sweeps, relax);
+            smoother_dcsr_sor(&xx, ie, is, -st, &A, &bb, sweeps, relax);
+        } else {
+            smoother_dcsr_sor(&xx, is, ie, -st, &A, &bb, sweeps, relax);
+            smoother_dcsr_sor(&xx, ie, is, st, &A, &bb, sweeps, relax);
+            smoother_dcsr_gs(&xx, is, ie, -st, &A, &bb, sweeps);
+            smoother_dcsr_gs(&xx, ie, is, st, &A, &bb, sweeps);
+        }
+        break;
     default: break;
     }
 }

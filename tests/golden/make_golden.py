@@ -176,7 +176,7 @@ def main():
     b = rng.uniform(-1, 1, n)
     x0 = rng.uniform(-1, 1, n)
     sm = {"ia": ia, "ja": ja, "val": val, "b": b, "x0": x0}
-    for s_id in (1, 2, 3, 5, 10):
+    for s_id in (1, 2, 3, 5, 6, 7, 8, 10):
         for pre in (1, 0):
             sm[f"s{s_id}_pre{pre}"] = R.smooth(s_id, pre, 2, ia, ja, val, b, x0, relax=1.2)
     sm["mxv"] = R.mxv(ia, ja, val, x0)

@@ -38,7 +38,7 @@ def test_mxv_kuhn_vs_oracle(port, N):
     assert np.array_equal(host(y), port.mxv(ia, ja, val, x))
 
 
-@pytest.mark.parametrize("sm", [1, 2, 3, 5, 10])
+@pytest.mark.parametrize("sm", [1, 2, 3, 5, 6, 7, 8, 10])
 @pytest.mark.parametrize("pre", [1, 0])
 def test_smoothers_bit_exact(golden, sm, pre):
     """GS/SGS/SOR through the level-scheduled exact sweep; Jacobi and
