@@ -298,6 +298,17 @@ __global__ void k_pm_init(int n, const int *__restrict__ ia, int *state) {
         state[k] = (ia[k + 1] - ia[k] > 1) ? -1 : -2;   // -1 free, -2 isolated
 }
 
+__device__ __forceinline__ unsigned edge_hash(int i, int j) {
+    unsigned lo = (unsigned)min(i, j), hi = (unsigned)max(i, j);
+    unsigned x = lo * 0x9e3779b1u ^ (hi + 0x7f4a7c15u + (lo << 6) + (lo >> 2));
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return x;
+}
+
+// Every free vertex points at the free neighbour with the largest edge key
+// (|a_ij| rounded to FP32, then a hash of the unordered pair): the key is
+// symmetric, so the heaviest free-free edge is always mutual and every round
+// matches at least one pair while free-free edges remain.
 __global__ void k_pm_point(int n, const int *__restrict__ ia,
                            const int *__restrict__ ja, const double *__restrict__ a,
                            const int *__restrict__ state, int *ptr) {
@@ -305,13 +316,17 @@ __global__ void k_pm_point(int n, const int *__restrict__ ia,
          k += gridDim.x * blockDim.x) {
         int best = -1;
         if (state[k] == -1) {
-            double bw = 0.0;
-            int bp = -1;
+            float bw = -1.0f;
+            unsigned bh = 0u;
             for (int p = ia[k]; p < ia[k + 1]; ++p) {
                 const int j = ja[p];
-                if (j != k && state[j] == -1) better_last(bw, bp, fabs(a[p]), p);
+                if (j == k || state[j] != -1) continue;
+                const float w = (float)fabs(a[p]);
+                const unsigned h = edge_hash(k, j);
+                if (best < 0 || w > bw || (w == bw && (h > bh || (h == bh && j > best)))) {
+                    best = j; bw = w; bh = h;
+                }
             }
-            if (bp >= 0) best = ja[bp];
         }
         ptr[k] = best;
     }
@@ -347,24 +362,36 @@ __global__ void k_pm_sizes(int n, const int *__restrict__ state, int *size) {
         if (state[k] >= 0) atomicAdd(size + state[k], 1);
 }
 
+// Leftover free vertices join the adjacent aggregate with the fewest members
+// (sizes counted before this pass; the first such neighbour on ties).  A
+// free vertex without an aggregated neighbour becomes its own aggregate:
+// flag[k] = 1, numbered after the pairs through a scan.
 __global__ void k_pm_leftover(int n, const int *__restrict__ ia,
                               const int *__restrict__ ja,
                               const int *__restrict__ state,
-                              const int *__restrict__ size, int *out, int *bad) {
+                              const int *__restrict__ size, int *out, int *flag) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += gridDim.x * blockDim.x) {
-        int st = state[k];
+        int st = state[k], f = 0;
         if (st == -1) {
             int bc = -1, bs = 0;
             for (int p = ia[k]; p < ia[k + 1]; ++p) {
                 const int c = state[ja[p]];
                 if (c >= 0 && (bc < 0 || size[c] < bs)) { bc = c; bs = size[c]; }
             }
-            if (bc < 0) *bad = 1;
             st = bc;
+            f = bc < 0;
         }
         out[k] = st < 0 ? UNPT : st;
+        flag[k] = f;
     }
+}
+
+__global__ void k_pm_singletons(int n, const int *__restrict__ flag,
+                                const int *__restrict__ pos, int base, int *out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x)
+        if (flag[k]) out[k] = base + pos[k];
 }
 
 int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
@@ -396,17 +423,22 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
         nc += cnt;
     }
     cudaMemsetAsync(size, 0, sizeof(int) * (nc > 0 ? nc : 1), s);
-    cudaMemsetAsync(dflag + 1, 0, sizeof(int), s);
     k_pm_sizes<<<g, 256, 0, s>>>(n, state, size);
-    k_pm_leftover<<<g, 256, 0, s>>>(n, nia, nja, state, size, agg, dflag + 1);
+    k_pm_leftover<<<g, 256, 0, s>>>(n, nia, nja, state, size, agg, flag);
     count_launch(2);
-    int bad = 0;
-    cudaMemcpyAsync(&bad, dflag + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    int rc = scan_exclusive(flag, pos, n, tmp, s);
+    int extra = 0;
+    if (!rc) {
+        k_pm_singletons<<<g, 256, 0, s>>>(n, flag, pos, nc, agg);
+        count_launch();
+        cudaMemcpyAsync(&extra, pos + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+    }
     cudaError_t e = cudaStreamSynchronize(s);
     dfree(dflag);
+    if (rc) return rc;
     if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
-    *nagg = nc;
-    return bad ? ERROR_AMG_COARSEING : SUCCESS;
+    *nagg = nc + extra;
+    return SUCCESS;
 }
 
 // ---------------------------------------------------------------------------

@@ -90,7 +90,7 @@ def lognormal_field(N: int, sigma: float, corr: float, seed: int):
     kz, ky, kx = np.meshgrid(f, f, np.fft.rfftfreq(N), indexing="ij")
     # Gaussian kernel exp(-r^2 / (2 corr^2)) in Fourier space
     filt = np.exp(-2.0 * (np.pi * corr) ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))
-    g = np.fft.irfftn(np.fft.rfftn(w) * filt, s=(N, N, N))
+    g = np.fft.irfftn(np.fft.rfftn(w) * filt, s=(N, N, N), axes=(0, 1, 2))
     g -= g.mean()
     g /= g.std()
     return np.exp(sigma * g)
