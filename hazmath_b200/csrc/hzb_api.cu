@@ -146,7 +146,7 @@ extern "C" void hzb_param_init(hzb_param *p) {
     p->omega = NULL;
     p->device = 0;
     p->fallback_check = 0;
-    p->use_graph = 0;
+    p->use_graph = 1;
 }
 
 extern "C" const char *hzb_last_error(void) { return hzb::last_error(); }

@@ -331,6 +331,53 @@ template int l1_sweep<double>(const DCsr<double> &, const double *, const double
 template int l1_sweep<float>(const DCsr<float> &, const float *, const float *,
                              float *, const float *, cudaStream_t);
 
+template <typename T>
+__global__ void k_l1_norms(int n, const int *__restrict__ ia, const T *__restrict__ a,
+                           T *__restrict__ d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        T s = T(0);
+        for (int k = ia[i]; k < ia[i + 1]; ++k) s += fabs(a[k]);
+        d[i] = s;
+    }
+}
+
+template <typename T>
+__global__ void k_l1_first(int n, const T *__restrict__ b, const T *__restrict__ d,
+                           T *__restrict__ xn, const float *__restrict__ omega) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const T di = d[i];
+        T xi = T(0);
+        if (fabs(di) > T(SMALLREAL)) xi += (omega ? T(omega[i]) : T(1)) * (b[i] / di);
+        xn[i] = xi;
+    }
+}
+
+template <typename T>
+int l1_norms(const DCsr<T> &A, T *d, cudaStream_t s) {
+    if (A.n <= 0) return SUCCESS;
+    k_l1_norms<T><<<grid_for(A.n), 256, 0, s>>>(A.n, A.ia, A.val, d);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template <typename T>
+int l1_first_sweep(int n, const T *b, const T *d, T *xn, const float *omega,
+                   cudaStream_t s) {
+    if (n <= 0) return SUCCESS;
+    k_l1_first<T><<<grid_for(n), 256, 0, s>>>(n, b, d, xn, omega);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+template int l1_norms<float>(const DCsr<float> &, float *, cudaStream_t);
+template int l1_norms<double>(const DCsr<double> &, double *, cudaStream_t);
+template int l1_first_sweep<float>(int, const float *, const float *, float *,
+                                   const float *, cudaStream_t);
+template int l1_first_sweep<double>(int, const double *, const double *, double *,
+                                    const float *, cudaStream_t);
+
 // Gauss-Seidel family on independent rows.  x is read with plain loads:
 // in gs_run earlier sets of the same CTA wrote it.
 // Row `skip` is left untouched: the backward sweep of smoother_dcsr_sgs starts

@@ -52,6 +52,13 @@ int jacobi_sweep(const DCsr<double> &A, const double *dj, const double *b,
 template <typename T>
 int l1_sweep(const DCsr<T> &A, const T *b, const T *x, T *xn,
              const float *omega, cudaStream_t s);
+// l1 row norms d_i = sum_j |a_ij| (CSR order), and the first l1-Jacobi sweep
+// from x = 0, which needs no matrix: xn_i = omega_i * (b_i / d_i).
+template <typename T>
+int l1_norms(const DCsr<T> &A, T *d, cudaStream_t s);
+template <typename T>
+int l1_first_sweep(int n, const T *b, const T *d, T *xn, const float *omega,
+                   cudaStream_t s);
 // Gauss-Seidel family on a list of independent rows (one level set / colour).
 //   kind 0: x_i = t * d_i            (GS, d_i = 1/a_ii)
 //   kind 1: x_i = w (t/d_i) + (1-w) x_i  if |d_i| > 1e-20   (SOR)

@@ -298,6 +298,11 @@ __global__ void k_pm_init(int n, const int *__restrict__ ia, int *state) {
         state[k] = (ia[k + 1] - ia[k] > 1) ? -1 : -2;   // -1 free, -2 isolated
 }
 
+__device__ __forceinline__ unsigned hash_u32(unsigned x) {
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return x;
+}
+
 __device__ __forceinline__ unsigned edge_hash(int i, int j) {
     unsigned lo = (unsigned)min(i, j), hi = (unsigned)max(i, j);
     unsigned x = lo * 0x9e3779b1u ^ (hi + 0x7f4a7c15u + (lo << 6) + (lo >> 2));
@@ -305,54 +310,78 @@ __device__ __forceinline__ unsigned edge_hash(int i, int j) {
     return x;
 }
 
-// Every free vertex points at the free neighbour with the largest edge key
-// (|a_ij| rounded to FP32, then a hash of the unordered pair): the key is
-// symmetric, so the heaviest free-free edge is always mutual and every round
-// matches at least one pair while free-free edges remain.
-__global__ void k_pm_point(int n, const int *__restrict__ ia,
-                           const int *__restrict__ ja, const double *__restrict__ a,
-                           const int *__restrict__ state, int *ptr) {
+// Red/blue handshake (one round): a hashed coin splits the free vertices;
+// every free red vertex proposes to its heaviest free blue neighbour (edge
+// key: |a_ij| in FP32, then a hash of the unordered pair), every blue vertex
+// accepts its heaviest proposer.  Accepted pairs are disjoint, and a constant
+// fraction of the free vertices pairs up per round whatever the weights look
+// like (heaviest-neighbour pointers alone form long chains on smooth
+// coefficient fields).
+__device__ __forceinline__ bool pm_red(int k, int round) {
+    return (hash_u32((unsigned)k * 2654435761u + (unsigned)round * 0x632be5abu) >> 7) & 1u;
+}
+
+__device__ __forceinline__ bool pm_better(float w, unsigned h, int j, float bw,
+                                          unsigned bh, int best) {
+    return best < 0 || w > bw || (w == bw && (h > bh || (h == bh && j > best)));
+}
+
+__global__ void k_pm_propose(int n, int round, const int *__restrict__ ia,
+                             const int *__restrict__ ja, const double *__restrict__ a,
+                             const int *__restrict__ state, int *ptr) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += gridDim.x * blockDim.x) {
         int best = -1;
-        if (state[k] == -1) {
+        if (state[k] == -1 && pm_red(k, round)) {
             float bw = -1.0f;
             unsigned bh = 0u;
             for (int p = ia[k]; p < ia[k + 1]; ++p) {
                 const int j = ja[p];
-                if (j == k || state[j] != -1) continue;
+                if (j == k || state[j] != -1 || pm_red(j, round)) continue;
                 const float w = (float)fabs(a[p]);
                 const unsigned h = edge_hash(k, j);
-                if (best < 0 || w > bw || (w == bw && (h > bh || (h == bh && j > best)))) {
-                    best = j; bw = w; bh = h;
-                }
+                if (pm_better(w, h, j, bw, bh, best)) { best = j; bw = w; bh = h; }
             }
         }
         ptr[k] = best;
     }
 }
 
-// flag[k] = 1 if k is the lower end of a mutual pair
-__global__ void k_pm_mutual(int n, const int *__restrict__ ptr, int *flag,
-                            int *any) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += gridDim.x * blockDim.x) {
-        const int j = ptr[k];
-        int f = (j >= 0 && ptr[j] == k && k < j) ? 1 : 0;
-        flag[k] = f;
-        if (f) *any = 1;
+// blue j: acc[j] = heaviest red neighbour proposing to j (or -1); flag marks
+// accepted pairs, numbered by their blue end
+__global__ void k_pm_accept(int n, int round, const int *__restrict__ ia,
+                            const int *__restrict__ ja, const double *__restrict__ a,
+                            const int *__restrict__ state, const int *__restrict__ ptr,
+                            int *acc, int *flag, int *any) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += gridDim.x * blockDim.x) {
+        int best = -1;
+        if (state[j] == -1 && !pm_red(j, round)) {
+            float bw = -1.0f;
+            unsigned bh = 0u;
+            for (int p = ia[j]; p < ia[j + 1]; ++p) {
+                const int i = ja[p];
+                if (i == j || ptr[i] != j) continue;
+                const float w = (float)fabs(a[p]);
+                const unsigned h = edge_hash(i, j);
+                if (pm_better(w, h, i, bw, bh, best)) { best = i; bw = w; bh = h; }
+            }
+        }
+        acc[j] = best;
+        flag[j] = best >= 0;
+        if (best >= 0) *any = 1;
     }
 }
 
-__global__ void k_pm_assign(int n, const int *__restrict__ ptr,
+__global__ void k_pm_assign(int n, const int *__restrict__ acc,
                             const int *__restrict__ flag,
                             const int *__restrict__ pos, int base, int *state) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += gridDim.x * blockDim.x)
-        if (flag[k]) {
-            const int c = base + pos[k];
-            state[k] = c;
-            state[ptr[k]] = c;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += gridDim.x * blockDim.x)
+        if (flag[j]) {
+            const int c = base + pos[j];
+            state[j] = c;
+            state[acc[j]] = c;
         }
 }
 
@@ -405,10 +434,11 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
     k_pm_init<<<g, 256, 0, s>>>(n, nia, state);
     count_launch();
     int nc = 0;
-    for (int round = 0; round < 64; ++round) {
+    int *acc = size;   // free during the rounds
+    for (int round = 0, idle = 0; round < 96 && idle < 4; ++round) {
         cudaMemsetAsync(dflag, 0, sizeof(int), s);
-        k_pm_point<<<g, 256, 0, s>>>(n, nia, nja, nval, state, ptr);
-        k_pm_mutual<<<g, 256, 0, s>>>(n, ptr, flag, dflag);
+        k_pm_propose<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr);
+        k_pm_accept<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr, acc, flag, dflag);
         count_launch(2);
         int any = 0, cnt = 0;
         int rc = scan_exclusive(flag, pos, n, tmp, s);
@@ -417,8 +447,10 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
         cudaMemcpyAsync(&cnt, pos + n, sizeof(int), cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { dfree(dflag); set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
-        if (!any) break;
-        k_pm_assign<<<g, 256, 0, s>>>(n, ptr, flag, pos, nc, state);
+        // stop after a few rounds in a row without a new pair
+        if (!any) { ++idle; continue; }
+        idle = 0;
+        k_pm_assign<<<g, 256, 0, s>>>(n, acc, flag, pos, nc, state);
         count_launch();
         nc += cnt;
     }
@@ -907,10 +939,6 @@ done:
 // ---------------------------------------------------------------------------
 // multicolouring (Jones-Plassmann, hashed priorities, smallest free colour)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned hash_u32(unsigned x) {
-    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
-    return x;
-}
 
 __global__ void k_jp_round(int n, const int *__restrict__ ia, const int *__restrict__ ja,
                            const int *__restrict__ col_in, int *col_out, int *left) {

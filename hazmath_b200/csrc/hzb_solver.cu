@@ -55,6 +55,7 @@ void Level::release() {
     dfree(b32); dfree(x32); dfree(w32); dfree(t32);
     dfree(d_jac); dfree(d_gs_f); dfree(d_gs_b); dfree(d_sor_f); dfree(d_sor_b);
     dfree(d_gs32);
+    dfree(l1_32);
     dfree(tia); dfree(tja); dfree(tval);
     fwd.release(); bwd.release(); col.release();
 }
@@ -253,7 +254,8 @@ forward:
 }
 
 // precond_amg (precond.c:164-184)
-int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
+static int precond64_body(hzb_solver *S, const double *r, double *z,
+                          const AMG_param &cyc) {
     Level &L0 = S->lv[0];
     double *sb = L0.b, *sx = L0.x;
     L0.b = const_cast<double *>(r);
@@ -269,7 +271,9 @@ int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
 // FP32 cycle (mixed precision): same structure, single-precision vectors and
 // matrix values, FP32 accumulation; the coarse solve reads the FP64 inverse.
 // ---------------------------------------------------------------------------
-static int smooth32(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
+// xzero: x32 holds zeros on entry (first visit of the level in this cycle);
+// the first sweep then needs no matrix and nothing has to zero x32 first.
+static int smooth32(hzb_solver *S, int l, bool pre, const AMG_param &cyc, bool xzero) {
     Level &L = S->lv[l];
     const int sweeps = pre ? cyc.presmooth_iter : cyc.postsmooth_iter;
     const DCsr<float> A = L.A32();
@@ -277,18 +281,33 @@ static int smooth32(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
     case SMOOTHER_L1DIAG:
     case SMOOTHER_JACOBI: {
         const float *om = (l == 0 && S->omega_active) ? S->omega : nullptr;
-        for (int k = 0; k < sweeps; ++k) {
-            // ping-pong x <-> t; an odd count ends with a copy back to x
-            const bool odd = (k & 1) == 0;
-            HZB_TRY(l1_sweep<float>(A, L.b32, odd ? L.x32 : L.t32, odd ? L.t32 : L.x32,
-                                    om, S->s));
+        if (sweeps == 0) return xzero ? vzero<float>(L.n, L.x32, S->s) : SUCCESS;
+        if (!xzero && (sweeps & 1)) {
+            // odd count from a nonzero x: ping-pong, copy back at the end
+            for (int k = 0; k < sweeps; ++k) {
+                const bool fwd = (k & 1) == 0;
+                HZB_TRY(l1_sweep<float>(A, L.b32, fwd ? L.x32 : L.t32, fwd ? L.t32 : L.x32,
+                                        om, S->s));
+            }
+            return vcopy<float>(L.n, L.t32, L.x32, S->s);
         }
-        if (sweeps & 1) HZB_TRY(vcopy<float>(L.n, L.t32, L.x32, S->s));
+        // sweep j writes x32 when (sweeps-1-j) is even, t32 otherwise, so the
+        // last one lands in x32 without a copy
+        float *prev = L.x32;
+        for (int j = 0; j < sweeps; ++j) {
+            float *dst = ((sweeps - 1 - j) & 1) ? L.t32 : L.x32;
+            if (j == 0 && xzero)
+                HZB_TRY(l1_first_sweep<float>(L.n, L.b32, L.l1_32, dst, om, S->s));
+            else
+                HZB_TRY(l1_sweep<float>(A, L.b32, prev, dst, om, S->s));
+            prev = dst;
+        }
         return SUCCESS;
     }
     case SMOOTHER_GS: {
         const Schedule &sc = L.col;
         const int ns = (int)sc.h_ptr.size() - 1;
+        if (xzero) HZB_TRY(vzero<float>(L.n, L.x32, S->s));
         for (int k = 0; k < sweeps; ++k)
             for (int q = 0; q < ns; ++q) {
                 const int c = pre ? q : ns - 1 - q;
@@ -303,19 +322,23 @@ static int smooth32(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
     return ERROR_AMG_SMOOTH_TYPE;
 }
 
-int cycle32(hzb_solver *S, const AMG_param &cyc) {
+// level0_zero: the caller left x32 of level 0 at zero
+int cycle32(hzb_solver *S, const AMG_param &cyc, bool level0_zero) {
     const int nl = S->nl;
     int num_lvl[MAX_AMG_LVL] = {0};
+    bool zero[MAX_AMG_LVL] = {false};
+    zero[0] = level0_zero;
     int l = 0;
 forward:
     while (l < nl - 1) {
         Level &L = S->lv[l];
         num_lvl[l]++;
-        HZB_TRY(smooth32(S, l, true, cyc));
+        HZB_TRY(smooth32(S, l, true, cyc, zero[l]));
+        zero[l] = false;
         HZB_TRY(spmv<float>(L.A32(), SPMV_RES, L.x32, L.b32, L.w32, 1.0f, nullptr, S->s));
         HZB_TRY(restrict_agg<float>(L.nc, L.ria, L.rja, L.w32, S->lv[l + 1].b32, S->s));
         ++l;
-        HZB_TRY(vzero<float>(S->lv[l].n, S->lv[l].x32, S->s));
+        if (l < nl - 1) zero[l] = true;   // x_l = 0, folded into its first sweep
     }
     {
         Level &C = S->lv[nl - 1];
@@ -325,7 +348,7 @@ forward:
         --l;
         Level &L = S->lv[l];
         HZB_TRY(prolong_agg<float>(L.n, L.agg, S->lv[l + 1].x32, L.x32, 1.0f, S->s));
-        HZB_TRY(smooth32(S, l, false, cyc));
+        HZB_TRY(smooth32(S, l, false, cyc, false));
         if (num_lvl[l] < cyc.cycle_type) break;
         else num_lvl[l] = 0;
     }
@@ -345,6 +368,10 @@ int ensure_fp32(hzb_solver *S) {
             HZB_TRY(dalloc(&L.x32, L.n));
             HZB_TRY(dalloc(&L.w32, L.n));
             HZB_TRY(dalloc(&L.t32, L.n));
+        }
+        if (!L.l1_32) {
+            HZB_TRY(dalloc(&L.l1_32, L.n));
+            HZB_TRY(l1_norms<float>(L.A32(), L.l1_32, S->s));
         }
         if (S->amg.smoother == SMOOTHER_GS && l < S->nl - 1 && !L.d_gs32) {
             if (!L.col.rows) HZB_TRY(multicolor(L.n, L.ia, L.ja, &L.col, S->s));
@@ -384,6 +411,8 @@ int level_smoother_data(hzb_solver *S, Level &L) {
 
 int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
           const double *d_val, bool copy_in) {
+    S->g64.release();
+    S->g32.release();
     for (auto &L : S->lv) L.release();
     S->lv.clear();
     dfree(S->Ainv);
@@ -767,13 +796,70 @@ finished:
 // flexible CG with the FP32 cycle (mixed precision; no reference counterpart
 // beyond dcsr_pgcg's flexible idea, krylov.c:2309)
 // ---------------------------------------------------------------------------
-static int apply_pc32(hzb_solver *S, const double *r, double *z) {
+static int apply_pc32_body(hzb_solver *S, const double *r, double *z) {
     Level &L0 = S->lv[0];
     AMG_param cyc = S->amg;
     HZB_TRY(d2f(L0.n, r, L0.b32, S->s));
-    HZB_TRY(vzero<float>(L0.n, L0.x32, S->s));
-    for (int i = 0; i < std::max<int>(1, cyc.maxit); ++i) HZB_TRY(cycle32(S, cyc));
+    for (int i = 0; i < std::max<int>(1, cyc.maxit); ++i) HZB_TRY(cycle32(S, cyc, i == 0));
     return f2d(L0.n, L0.x32, z, S->s);
+}
+
+// Replays `body` from a CUDA graph captured on the solver's stream; the
+// capture is redone whenever the key (vector pointers, tag) changes.
+template <typename F>
+static int with_graph(hzb_solver *S, GraphCache &G, const void *k0, const void *k1,
+                      long long tag, F body) {
+    if (!S->bp.use_graph) return body();
+    if (!G.exec || G.k0 != k0 || G.k1 != k1 || G.tag != tag) {
+        G.release();
+        const long long before = launch_count();
+        HZB_CUDA(cudaStreamBeginCapture(S->s, cudaStreamCaptureModeThreadLocal));
+        int rc = body();
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(S->s, &g);
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) set_error(e, __FILE__, __LINE__);
+            return rc ? rc : ERROR_SOLVER_MISC;
+        }
+        e = cudaGraphInstantiate(&G.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            G.exec = nullptr;
+            set_error(e, __FILE__, __LINE__);
+            return ERROR_SOLVER_MISC;
+        }
+        G.k0 = k0;
+        G.k1 = k1;
+        G.tag = tag;
+        G.kernels = launch_count() - before;   // counted once by the capture
+    } else {
+        count_launch((int)G.kernels);
+    }
+    HZB_CUDA(cudaGraphLaunch(G.exec, S->s));
+    return SUCCESS;
+}
+
+static long long cycle_tag(const hzb_solver *S, const AMG_param &c) {
+    return (long long)c.maxit | ((long long)c.cycle_type << 8) |
+           ((long long)c.smoother << 12) | ((long long)c.presmooth_iter << 20) |
+           ((long long)c.postsmooth_iter << 26) | ((long long)S->omega_active << 32) |
+           ((long long)c.coarse_solver << 34) | ((long long)(c.relaxation * 1e6) << 42);
+}
+
+static int apply_pc32(hzb_solver *S, const double *r, double *z) {
+    return with_graph(S, S->g32, r, z, cycle_tag(S, S->amg),
+                      [&]() { return apply_pc32_body(S, r, z); });
+}
+
+// The FP64 preconditioner is replayed from a graph unless a branch of the
+// cycle reads a device value on the host (coarse scaling, coarse CG).
+int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
+    const bool capturable = cyc.coarse_solver == SOLVER_UMFPACK && S->Ainv &&
+                            cyc.coarse_scaling != ON;
+    if (!capturable) return precond64_body(S, r, z, cyc);
+    return with_graph(S, S->g64, r, z, cycle_tag(S, cyc),
+                      [&]() { return precond64_body(S, r, z, cyc); });
 }
 
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
@@ -837,6 +923,8 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
 }
 
 void destroy(hzb_solver *S) {
+    S->g64.release();
+    S->g32.release();
     for (auto &L : S->lv) L.release();
     S->lv.clear();
     dfree(S->Ainv);

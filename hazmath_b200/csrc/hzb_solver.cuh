@@ -24,6 +24,7 @@ struct Level {
     double *d_jac = nullptr, *d_gs_f = nullptr, *d_gs_b = nullptr;
     double *d_sor_f = nullptr, *d_sor_b = nullptr;
     float *d_gs32 = nullptr;
+    float *l1_32 = nullptr;           // l1 row norms for the FP32 first sweep
     Schedule fwd, bwd, col;
     // coarsest level with the direct solver: the transposed matrix the
     // reference factors (and leaves in mgl[nl-1].A)
@@ -58,6 +59,19 @@ struct KrylovWork {
     void release();
 };
 
+// A captured preconditioner application, replayed while its key matches.
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    const void *k0 = nullptr, *k1 = nullptr;
+    long long tag = -1;
+    long long kernels = 0;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        tag = -1;
+    }
+};
+
 // Host-side preconditioner callback used when a foreign pc->fct is given.
 struct HostPrecond {
     void (*fct)(double *, double *, void *) = nullptr;
@@ -80,6 +94,7 @@ struct hzb_solver {
     double *Ainv = nullptr;           // coarsest-level inverse (coarse_solver 32)
     hzb::KrylovWork kw;               // outer Krylov loop
     hzb::KrylovWork kwc;              // coarse-level CG (coarse_solver != 32)
+    hzb::GraphCache g64, g32;         // captured FP64 / FP32 preconditioners
     float *omega = nullptr;           // learned fine-level weights (device)
     bool omega_active = false;
     hzb_stats st{};
@@ -96,7 +111,7 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
 int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc);
 // one cycle on level-0 b/x already in place (mgcycle)
 int cycle64(hzb_solver *S, const AMG_param &cyc);
-int cycle32(hzb_solver *S, const AMG_param &cyc);
+int cycle32(hzb_solver *S, const AMG_param &cyc, bool level0_zero);
 // reference PCG on level-0 operator
 int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
         int pc_kind, HostPrecond *hp, double tol, int maxit, int stop_type,
