@@ -175,6 +175,11 @@ def lib() -> C.CDLL:
         L.hzb_rap_agg_device.argtypes = [INT, INT, C.c_void_p, C.c_void_p, C.c_void_p, INT,
                                          C.c_void_p, P(INT), P(C.c_void_p), P(C.c_void_p),
                                          P(C.c_void_p)]
+        L.hzb_rap_agg_device_noalloc.argtypes = [INT, INT, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, INT, C.c_void_p, INT,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, P(INT)]
+        L.hzb_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        L.hzb_free_device.argtypes = [C.c_void_p]
         L.dcsr_pcg.argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL, INT,
                                SHORT, SHORT]
         L.python_wrapper_krylov_amg.argtypes = [P(INT), P(INT), C.c_void_p, C.c_void_p,

@@ -3,6 +3,7 @@
 // rounded in the reference's order.
 #include "hzb_setup.cuh"
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 namespace hzb {
@@ -1037,4 +1038,106 @@ done:
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// Galerkin product without device allocation.
+//
+// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is
+// being captured into a graph, processes whose device memory is reserved up
+// front by their own allocator, and library code that must not trigger the
+// implicit device synchronisation of cudaMalloc/cudaFree.  For them the
+// product's scratch (restriction pattern, per-row bounds, slot lists, scan
+// partials) lives in one file-scope device array of fixed size, held by every
+// device that loads this library until the process exits.  Its size bounds
+// the problem: n <= HZB_NOALLOC_MAX_ROWS fine rows and nnz <=
+// HZB_NOALLOC_MAX_NNZ stored entries.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t NA_ROWS = HZB_NOALLOC_MAX_ROWS;
+constexpr size_t NA_NNZ = HZB_NOALLOC_MAX_NNZ;
+constexpr size_t NA_TMP = (NA_ROWS + 1 + 2047) / 2048 + 8;
+// int words: cnt, ria, rja, ub, off, rowcnt, scan tmp, scol
+constexpr size_t NA_INTS = 6 * (NA_ROWS + 1) + NA_TMP + (NA_NNZ + NA_ROWS);
+constexpr size_t NA_INT_WORDS = (NA_INTS + 1) / 2;   // in 8-byte words
+constexpr size_t NA_WORDS = NA_INT_WORDS + (NA_NNZ + NA_ROWS);   // + sval
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_scratch[NA_WORDS];
+
+// Device address of g_noalloc_scratch for each device, resolved once with
+// that device current (in host code the symbol is only a host stand-in).
+static void *g_noalloc_addr[64];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(double **p) {
+    int dev = 0;
+    HZB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) { set_error_msg("device ordinal out of range"); return ERROR_MISC; }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *a = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+        g_noalloc_addr[dev] = a;
+    }
+    *p = (double *)g_noalloc_addr[dev];
+    return SUCCESS;
+}
+
 }  // namespace hzb
+
+// The same kernels, in the same order, as hzb_rap_agg_device, so the result
+// is identical bit for bit; only the scratch comes from the static array and
+// the outputs from the caller.
+extern "C" INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const INT *ja,
+                                          const REAL *val, INT nc, const INT *agg,
+                                          INT cap_nnz, INT *rap_ia, INT *rap_ja,
+                                          REAL *rap_val, INT *rap_nnz) {
+    using namespace hzb;
+    if (n < 1 || nnz < 0 || nc < 1 || nc > n || (size_t)n > NA_ROWS || (size_t)nnz > NA_NNZ) {
+        set_error_msg("hzb_rap_agg_device_noalloc: sizes beyond HZB_NOALLOC_MAX_ROWS / "
+                      "HZB_NOALLOC_MAX_NNZ");
+        return ERROR_MAT_SIZE;
+    }
+    double *base = nullptr;
+    HZB_TRY(noalloc_scratch(&base));
+    int *ip = (int *)base;
+    int *cnt = ip;                       ip += NA_ROWS + 1;
+    int *ria = ip;                       ip += NA_ROWS + 1;
+    int *rja = ip;                       ip += NA_ROWS + 1;
+    int *ub = ip;                        ip += NA_ROWS + 1;
+    int *off = ip;                       ip += NA_ROWS + 1;
+    int *rowcnt = ip;                    ip += NA_ROWS + 1;
+    int *tmp = ip;                       ip += NA_TMP;
+    int *scol = ip;
+    double *sval = base + NA_INT_WORDS;
+    cudaStream_t s = 0;
+    const int gn = grid_for(n), gc = grid_for(nc);
+    // R = P^T (counts start at zero: the array keeps the previous call's data)
+    HZB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * nc, s));
+    k_agg_count<<<gn, 256, 0, s>>>(n, agg, cnt);
+    count_launch();
+    HZB_TRY(scan_exclusive(cnt, ria, nc, tmp, s));
+    HZB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * nc, s));
+    k_agg_fill<<<gn, 256, 0, s>>>(n, agg, ria, cnt, rja);
+    k_sort_rows<<<gc, 256, 0, s>>>(nc, ria, rja);
+    // slot lists per coarse row, then the compacted product
+    k_rap_bound<<<gc, 256, 0, s>>>(nc, ria, rja, ia, ub);
+    count_launch(3);
+    HZB_TRY(scan_exclusive(ub, off, nc, tmp, s));
+    k_rap_build<<<gc, 128, 0, s>>>(nc, ria, rja, ia, ja, val, agg, off, scol, sval, rowcnt);
+    count_launch();
+    HZB_TRY(scan_exclusive(rowcnt, rap_ia, nc, tmp, s));
+    int total = 0;
+    HZB_CUDA(cudaMemcpyAsync(&total, rap_ia + nc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HZB_CUDA(cudaStreamSynchronize(s));
+    *rap_nnz = total;
+    if (total > cap_nnz) {
+        set_error_msg("hzb_rap_agg_device_noalloc: output capacity too small (*rap_nnz "
+                      "holds the size needed)");
+        return ERROR_INPUT_PAR;
+    }
+    k_rap_compact<<<gc, 256, 0, s>>>(nc, off, rap_ia, scol, sval, rap_ja, rap_val);
+    count_launch();
+    HZB_CUDA(cudaStreamSynchronize(s));
+    return SUCCESS;
+}

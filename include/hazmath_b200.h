@@ -452,6 +452,32 @@ void hzb_free_device(void *p);
 /* copy bytes from device memory returned above into host memory */
 INT hzb_copy_to_host(void *dst, const void *src_device, size_t bytes);
 
+/* Galerkin product that allocates nothing.  No counterpart in the
+ * reference.  It serves callers that cannot call cudaMalloc: code running
+ * while a stream is captured into a CUDA graph, processes whose device
+ * memory is reserved up front by their own allocator, and library code that
+ * must not trigger the implicit device synchronisation of cudaMalloc or
+ * cudaFree.  The result equals hzb_rap_agg_device's bit for bit.
+ *  - Inputs and outputs are the caller's device arrays: rap_ia (nc+1 ints),
+ *    rap_ja (cap_nnz ints) and rap_val (cap_nnz doubles); *rap_nnz receives
+ *    the product's entry count, also when it exceeds cap_nnz (then the call
+ *    returns ERROR_INPUT_PAR and fills only rap_ia).
+ *  - Scratch is one file-scope device array of about 15 MB, held by every
+ *    device that loads the library until the process exits.  It limits the
+ *    fine matrix to n <= HZB_NOALLOC_MAX_ROWS rows and nnz <=
+ *    HZB_NOALLOC_MAX_NNZ entries; larger sizes return ERROR_MAT_SIZE.
+ *  - The first call on a device looks up the array's device address (with
+ *    that device current); make that first call before any stream capture.
+ *  - Every call shares the array: calls that overlap on the GPU (several
+ *    host threads or streams at once) race.  Runs on the legacy default
+ *    stream and synchronises before returning. */
+#define HZB_NOALLOC_MAX_ROWS 65536
+#define HZB_NOALLOC_MAX_NNZ  1048576
+INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const INT *ja,
+                               const REAL *val, INT nc, const INT *agg,
+                               INT cap_nnz, INT *rap_ia, INT *rap_ja,
+                               REAL *rap_val, INT *rap_nnz);
+
 #ifdef __cplusplus
 }
 #endif
