@@ -194,6 +194,7 @@ extern "C" INT hzb_create(hzb_solver **out, const AMG_param *amg,
 extern "C" void hzb_destroy(hzb_solver *S) {
     if (!S) return;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     if (S->s) cudaStreamSynchronize(S->s);
     hzb::destroy(S);
     if (S->e0) cudaEventDestroy(S->e0);
@@ -222,6 +223,7 @@ extern "C" INT hzb_setup_device(hzb_solver *S, INT n, INT nnz, const INT *d_ia,
                                 const INT *d_ja, const REAL *d_val) {
     if (!S || n <= 0 || nnz <= 0) return ERROR_MAT_SIZE;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     S->host_ia = nullptr; S->host_ja = nullptr; S->host_val = nullptr;
     HZB_TRY(hzb::setup(S, n, nnz, d_ia, d_ja, d_val, false));
     return upload_omega(S);
@@ -232,6 +234,7 @@ extern "C" INT hzb_setup_host(hzb_solver *S, const dCSRmat *A) {
     if (A->row != A->col) return ERROR_MAT_SIZE;
     HZB_TRY(check_csr_host(A->row, A->nnz, A->IA));
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     HZB_TRY(hzb::setup(S, A->row, A->nnz, A->IA, A->JA, A->val, true));
     S->host_ia = A->IA; S->host_ja = A->JA; S->host_val = A->val;
     return upload_omega(S);
@@ -240,6 +243,7 @@ extern "C" INT hzb_setup_host(hzb_solver *S, const dCSRmat *A) {
 extern "C" INT hzb_set_omega_device(hzb_solver *S, const float *d_omega) {
     if (!S || S->nl == 0) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     if (!d_omega) { S->omega_active = false; return SUCCESS; }
     const int n = S->lv[0].n;
     if (!S->omega) HZB_TRY(dalloc(&S->omega, n));
@@ -252,6 +256,7 @@ extern "C" INT hzb_set_omega_device(hzb_solver *S, const float *d_omega) {
 extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
     if (!S || S->nl == 0) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     const long long l0 = hzb::launch_count();
     HZB_CUDA(cudaEventRecord(S->e0, S->s));
     double rel = 0.0, cond = 0.0;
@@ -281,6 +286,7 @@ extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
 extern "C" INT hzb_solve_host(hzb_solver *S, const REAL *b, REAL *x) {
     if (!S || S->nl == 0) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     const int n = S->lv[0].n;
     double *db = nullptr, *dx = nullptr;
     HZB_TRY(dalloc(&db, n));
@@ -300,6 +306,7 @@ extern "C" INT hzb_solve_host(hzb_solver *S, const REAL *b, REAL *x) {
 extern "C" INT hzb_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z) {
     if (!S || S->nl == 0) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     HZB_TRY(precond64(S, d_r, d_z, S->pc_cyc));
     HZB_CUDA(cudaStreamSynchronize(S->s));
     return SUCCESS;
@@ -309,6 +316,7 @@ extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
                                REAL *ms_per_launch, REAL *bytes_per_launch) {
     if (!S || level < 0 || level >= S->nl || reps < 1) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     Level &L = S->lv[level];
     const bool f32 = which == HZB_K_SPMV32 || which == HZB_K_L1_32;
     if (f32 && !L.val32) HZB_TRY(ensure_fp32(S));
@@ -357,6 +365,7 @@ extern "C" INT hzb_level_copy(const hzb_solver *S, INT l, INT *ia, INT *ja,
                               REAL *val, INT *agg) {
     if (!S || l < 0 || l >= S->nl) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     const Level &L = S->lv[l];
     // the coarsest level is reported as the reference leaves it: transposed
     // when the direct coarse solver is used
@@ -545,6 +554,7 @@ extern "C" void mgcycle(AMG_data *mgl, AMG_param *param) {
     hzb_solver *S = handle_of(mgl);
     if (!S || !param) return;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     Level &L0 = S->lv[0];
     cudaMemcpyAsync(L0.b, mgl[0].b.val, sizeof(double) * L0.n, cudaMemcpyHostToDevice, S->s);
     cudaMemcpyAsync(L0.x, mgl[0].x.val, sizeof(double) * L0.n, cudaMemcpyHostToDevice, S->s);
@@ -559,6 +569,7 @@ extern "C" void precond_amg(REAL *r, REAL *z, void *data) {
     hzb_solver *S = pcdata ? handle_of(pcdata->mgl_data) : nullptr;
     if (!S) return;
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     const int n = S->lv[0].n;
     if (!S->pr) {
         if (dalloc(&S->pr, n) || dalloc(&S->pz, n)) return;
@@ -624,6 +635,7 @@ static INT pcg_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol,
         }
     }
     cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
     int rc = SUCCESS;
     DCsr<double> D;
     TmpCsr T;
@@ -938,6 +950,8 @@ extern "C" INT hzb_smoother_device(SHORT smoother, SHORT forward, INT sweeps,
     amg.relaxation = relax;
     HZB_TRY(hzb_create(&S, &amg, NULL, NULL));
     int rc = SUCCESS;
+    {
+    StreamScope scope_(S->s);
     S->lv.emplace_back();
     Level &L = S->lv[0];
     L.n = n; L.nnz = nnz; L.own_A = false;
@@ -953,6 +967,7 @@ extern "C" INT hzb_smoother_device(SHORT smoother, SHORT forward, INT sweeps,
     if (!rc && cudaStreamSynchronize(S->s) != cudaSuccess) rc = ERROR_SOLVER_MISC;
     L.b = nullptr;   // not owned
     L.x = nullptr;
+    }
     hzb_destroy(S);
     return rc;
 }

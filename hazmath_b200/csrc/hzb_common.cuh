@@ -44,12 +44,26 @@ inline int grid_for(long long n, int block = 256) {
     return (int)g;
 }
 
+// Device allocations are stream-ordered (cudaMallocAsync / cudaFreeAsync on
+// the calling solver's stream, from the device's default pool with its
+// release threshold raised so freed blocks stay cached): rebuilding a
+// hierarchy does not pay cudaMalloc/cudaFree and their device-wide syncs.
+// The stream is a thread-local set by StreamScope at each entry point
+// (legacy default stream otherwise).
+cudaStream_t &cur_stream();
+void ensure_pool();
+struct StreamScope {
+    cudaStream_t prev;
+    explicit StreamScope(cudaStream_t s) : prev(cur_stream()) { cur_stream() = s; ensure_pool(); }
+    ~StreamScope() { cur_stream() = prev; }
+};
+
 // Device allocation helpers (return ERROR_ALLOC_MEM on failure).
 template <typename T>
 int dalloc(T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), cur_stream());
     if (e != cudaSuccess) {
         set_error(e, __FILE__, __LINE__);
         *p = nullptr;
@@ -59,7 +73,7 @@ int dalloc(T **p, size_t count) {
 }
 template <typename T>
 void dfree(T *&p) {
-    if (p) cudaFree((void *)p);
+    if (p) cudaFreeAsync((void *)p, cur_stream());
     p = nullptr;
 }
 

@@ -26,6 +26,26 @@ const char *last_error() { return g_err.c_str(); }
 void count_launch(int k) { g_launches += k; }
 long long launch_count() { return g_launches; }
 
+cudaStream_t &cur_stream() {
+    static thread_local cudaStream_t s = 0;
+    return s;
+}
+
+void ensure_pool() {
+    static std::mutex mu;
+    static bool done[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;   // process-local pool attribute
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done[dev] = true;
+}
+
 int sm_count() {
     static int cached = 0;
     if (!cached) {
