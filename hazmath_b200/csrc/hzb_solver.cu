@@ -215,10 +215,12 @@ static int coarse_solve64(hzb_solver *S, const AMG_param &cyc) {
     return it == ERROR_SOLVER_MISC ? it : SUCCESS;
 }
 
-int cycle64(hzb_solver *S, const AMG_param &cyc) {
+// l0 > 0 runs the same cycle on the sub-hierarchy below level l0 (the
+// coarse-grid operator B_c used by the learned-weight training).
+int cycle64(hzb_solver *S, const AMG_param &cyc, int l0) {
     const int nl = S->nl;
     int num_lvl[MAX_AMG_LVL] = {0};
-    int l = 0;
+    int l = l0;
     double alpha = 1.0;
 forward:
     while (l < nl - 1) {
@@ -231,7 +233,7 @@ forward:
         HZB_TRY(vzero<double>(S->lv[l].n, S->lv[l].x, S->s));
     }
     HZB_TRY(coarse_solve64(S, cyc));
-    while (l > 0) {
+    while (l > l0) {
         --l;
         Level &L = S->lv[l];
         if (cyc.coarse_scaling == ON) {
@@ -249,7 +251,7 @@ forward:
         if (num_lvl[l] < cyc.cycle_type) break;
         else num_lvl[l] = 0;
     }
-    if (l > 0) goto forward;
+    if (l > l0) goto forward;
     return SUCCESS;
 }
 

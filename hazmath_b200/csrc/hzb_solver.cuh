@@ -110,7 +110,7 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
 // z = B r with B = maxit V/W cycles of the FP64 hierarchy (precond_amg)
 int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc);
 // one cycle on level-0 b/x already in place (mgcycle)
-int cycle64(hzb_solver *S, const AMG_param &cyc);
+int cycle64(hzb_solver *S, const AMG_param &cyc, int l0 = 0);
 int cycle32(hzb_solver *S, const AMG_param &cyc, bool level0_zero);
 // reference PCG on level-0 operator
 int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
@@ -121,6 +121,10 @@ enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2 };
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out);
 int ensure_fp32(hzb_solver *S);
+// learned-weight loss (hzb_learn.cu)
+int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E);
+int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
+                    double *loss, float *domega);
 // smoothing of level l as mgcycle's pre (pre = true) / post smoothing calls
 int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc);
 // diagonals and sweep schedules the configured smoother needs on level L

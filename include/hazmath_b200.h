@@ -408,6 +408,41 @@ void hzb_destroy(hzb_solver *s);
 /* last CUDA error message of this thread ("" if none) */
 const char *hzb_last_error(void);
 
+/* Learned l1-Jacobi weights (no counterpart in the reference).
+ * A 3-layer message-passing network over the fine-level matrix graph (width
+ * 32, BF16 weights, FP32 accumulation; tensor-core dense layers) maps
+ * scale-invariant node/edge features of A to omega_i in (0,2).  An untrained
+ * network returns omega = 1 (the reference's l1-Jacobi).  Training uses the
+ * method's own error vectors and the two-cycle A-norm contraction as loss. */
+typedef struct hzb_gnn hzb_gnn;
+INT  hzb_gnn_num_params(void);
+INT  hzb_gnn_create(hzb_gnn **g, unsigned long long seed, INT device);
+void hzb_gnn_destroy(hzb_gnn *g);
+INT  hzb_gnn_get_params(const hzb_gnn *g, float *host);   /* FP32 master copy */
+INT  hzb_gnn_set_params(hzb_gnn *g, const float *host);
+INT  hzb_gnn_get_grads(const hzb_gnn *g, float *host);
+INT  hzb_gnn_zero_grad(hzb_gnn *g);
+INT  hzb_gnn_adam_step(hzb_gnn *g, REAL lr);
+/* omega (device array, n) for level 0 of the solver's hierarchy; keeps the
+ * activations for hzb_gnn_backward */
+INT  hzb_gnn_infer(hzb_gnn *g, hzb_solver *s, float *d_omega);
+/* accumulate parameter gradients for dL/domega (device array, n) */
+INT  hzb_gnn_backward(hzb_gnn *g, hzb_solver *s, const float *d_domega);
+/* ns training error vectors (device, n x ns, FP64): seeded random vectors
+ * after three plain l1 sweeps and two plain V-cycles, unit A-norm */
+INT  hzb_learn_errors(hzb_solver *s, INT ns, unsigned long long seed, REAL *d_E);
+/* mean over the ns vectors of ||E(omega)^2 e||_A^2 / ||e||_A^2 for the V(2,2)
+ * l1-Jacobi cycle with fine-level weights omega, and its gradient */
+INT  hzb_learn_loss_grad(hzb_solver *s, const float *d_omega, INT ns,
+                         const REAL *d_E, REAL *loss, float *d_domega);
+/* Set up the learned weights on a solver with fallback: infer omega, measure
+ * the per-cycle contraction with and without it on ns method-generated
+ * error vectors, keep omega only if it contracts better.  Both contractions
+ * are returned and recorded in hzb_stats (omega_contraction, omega_used). */
+INT  hzb_learn_select_omega(hzb_solver *s, hzb_gnn *g, INT ns,
+                            unsigned long long seed, REAL *rho_plain,
+                            REAL *rho_learned);
+
 /* Time `reps` back-to-back launches of one cycle kernel on level `level` of
  * the handle's hierarchy, on the handle's stream with CUDA events, after a
  * warm-up launch.  Returns the mean device time per launch and the

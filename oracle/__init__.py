@@ -15,6 +15,7 @@ this package; the product (hazmath_b200) never does.
 from __future__ import annotations
 
 import ctypes
+import ctypes as C
 import os
 import subprocess
 from dataclasses import dataclass
@@ -160,6 +161,41 @@ class Port(_Backend):
 
     def free(self):
         self.lib.or_free()
+
+    # -- learned weights ---------------------------------------------------
+    def gnn_num_params(self):
+        return self.lib.or_gnn_num_params()
+
+    def gnn_forward(self, ia, ja, val, params, rounding=True):
+        self.lib.or_gnn_set_rounding(1 if rounding else 0)
+        self._gnn_keep = (np.ascontiguousarray(ia, np.int32), np.ascontiguousarray(ja, np.int32),
+                          np.ascontiguousarray(val, np.float64))
+        ia, ja, val = self._gnn_keep
+        prm = np.ascontiguousarray(params, np.float32)
+        om = np.empty(len(ia) - 1, np.float32)
+        self.lib.or_gnn_forward(len(ia) - 1, _p(ia), _p(ja), _p(val), _p(prm), _p(om))
+        return om
+
+    def gnn_backward(self, params, domega):
+        prm = np.ascontiguousarray(params, np.float32)
+        d = np.ascontiguousarray(domega, np.float32)
+        g = np.empty(self.gnn_num_params(), np.float32)
+        self.lib.or_gnn_backward(_p(prm), _p(d), _p(g))
+        return g
+
+    def learn_errors(self, ns, seed):
+        n = self.level_info(0)[0]
+        E = np.empty((ns, n))
+        self.lib.or_learn_errors(ns, C.c_ulonglong(seed), _p(E))
+        return E
+
+    def learn_loss_grad(self, omega, E):
+        om = np.ascontiguousarray(omega, np.float32)
+        E = np.ascontiguousarray(E, np.float64)
+        d = np.empty(E.shape[1])
+        self.lib.or_learn_loss_grad.restype = C.c_double
+        loss = self.lib.or_learn_loss_grad(_p(om), E.shape[0], _p(E), _p(d))
+        return loss, d
 
     # -- kernels -----------------------------------------------------------
     def mxv(self, ia, ja, val, x):

@@ -595,12 +595,12 @@ static void or_coarse_cg(const ocsr *A, const double *b, double *x, double ctol)
 
 /* mgcycle mgcycle.c:245-415 (V and W cycles; precond_amg passes tol=1e-6,
  * so the coarse CG runs to 1e-8) */
-void or_mgcycle(void)
+static void or_mgcycle_from(int l0)
 {
     or_amg *G = &g_or;
     const int nl = G->nl;
     int num_lvl[OR_MAXLVL] = {0};
-    int l = 0;
+    int l = l0;
     double alpha = 1.0;
     const double ctol = 1e-6 * 1e-2;
 forward:
@@ -620,7 +620,7 @@ forward:
         if (G->coarse_solver == 32) or_chol_solve(C->n, G->Lc, G->b[nl - 1], G->x[nl - 1]);
         else or_coarse_cg(C, G->b[nl - 1], G->x[nl - 1], ctol);
     }
-    while (l > 0) {
+    while (l > l0) {
         --l;
         ocsr *A = &G->A[l];
         if (G->coarse_scaling == 1) {
@@ -643,7 +643,34 @@ forward:
         if (num_lvl[l] < G->cycle_type) break;
         else num_lvl[l] = 0;
     }
-    if (l > 0) goto forward;
+    if (l > l0) goto forward;
+}
+
+void or_mgcycle(void) { or_mgcycle_from(0); }
+
+/* the cycle on the levels from l0 down (x_l0 = 0, b_l0 = b) */
+void or_cycle_from(int l0, const double *b, double *x)
+{
+    int m = g_or.A[l0].n;
+    memcpy(g_or.b[l0], b, sizeof(double) * m);
+    memset(g_or.x[l0], 0, sizeof(double) * m);
+    if (l0 == g_or.nl - 1) {
+        ocsr *C = &g_or.A[l0];
+        if (g_or.coarse_solver == 32) or_chol_solve(C->n, g_or.Lc, g_or.b[l0], g_or.x[l0]);
+        else or_coarse_cg(C, g_or.b[l0], g_or.x[l0], 1e-8);
+    } else {
+        or_mgcycle_from(l0);
+    }
+    memcpy(x, g_or.x[l0], sizeof(double) * m);
+}
+
+int or_hier_level(int l, int *n, const int **ia, const int **ja, const double **a,
+                  const int **agg, const int **ria, const int **rja, int *nc)
+{
+    if (l < 0 || l >= g_or.nl) return -1;
+    *n = g_or.A[l].n; *ia = g_or.A[l].ia; *ja = g_or.A[l].ja; *a = g_or.A[l].val;
+    *agg = g_or.agg[l]; *ria = g_or.ria[l]; *rja = g_or.rja[l]; *nc = g_or.nc[l];
+    return 0;
 }
 
 /* precond_amg precond.c:164-184 */
