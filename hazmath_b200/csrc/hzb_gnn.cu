@@ -298,6 +298,7 @@ __global__ void k_gnn_output(int n, const bf16 *__restrict__ h3, const float *__
     const float wo = prm[OFF_WO + lane], bo = prm[OFF_BO];
     for (int i = warp; i < n; i += nw) {
         float z = warp_sum(wo * __bfloat162float(h3[(size_t)i * 32 + lane])) + bo;
+        z = fminf(12.f, fmaxf(-12.f, z));   // omega stays strictly inside (0, 2)
         if (lane == 0) omega[i] = 2.0f / (1.0f + expf(-z));
     }
 }
@@ -738,11 +739,12 @@ extern "C" INT hzb_gnn_backward(hzb_gnn *G, hzb_solver *S, const float *d_domega
     return SUCCESS;
 }
 
-extern "C" INT hzb_learn_errors(hzb_solver *S, INT ns, unsigned long long seed, REAL *d_E) {
+extern "C" INT hzb_learn_errors(hzb_solver *S, INT ns, unsigned long long seed, REAL *d_E,
+                                const float *d_omega) {
     if (!S) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
-    return learn_errors(S, ns, seed, d_E);
+    return learn_errors(S, ns, seed, d_E, d_omega);
 }
 
 extern "C" INT hzb_learn_loss_grad(hzb_solver *S, const float *d_omega, INT ns,
@@ -775,9 +777,11 @@ extern "C" INT hzb_learn_select_omega(hzb_solver *S, hzb_gnn *G, INT ns,
     float *dom = nullptr;
     HZB_TRY(dalloc(&E, (size_t)n * ns));
     int rc = dalloc(&dom, n);
+    // each cycle is measured on the errors it leaves itself (its slowest modes)
     double lp = 0.0, ll = 0.0;
-    if (!rc) rc = learn_errors(S, ns, seed, E);
+    if (!rc) rc = learn_errors(S, ns, seed, E, nullptr);
     if (!rc) rc = learn_loss_grad(S, nullptr, ns, E, &lp, dom);
+    if (!rc) rc = learn_errors(S, ns, seed, E, S->omega);
     if (!rc) rc = learn_loss_grad(S, S->omega, ns, E, &ll, dom);
     dfree(E);
     dfree(dom);

@@ -154,7 +154,10 @@ static int need_levels(hzb_solver *S) {
     return SUCCESS;
 }
 
-int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E) {
+// omega == nullptr: errors of the plain cycle; otherwise the two V-cycles
+// use omega on the fine level (the errors the learned cycle leaves).
+int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
+                 const float *omega) {
     HZB_TRY(need_levels(S));
     Level &L0 = S->lv[0];
     const int n = L0.n;
@@ -163,7 +166,11 @@ int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E) {
     HZB_TRY(w.alloc(n));
     HZB_TRY(l1_norms<double>(L0.A64(), w.l1, s));
     const bool was = S->omega_active;
-    S->omega_active = false;
+    float *was_om = S->omega;
+    const short was_graph = S->bp.use_graph;
+    S->bp.use_graph = 0;   // omega's address is not part of a captured cycle
+    S->omega = const_cast<float *>(omega);
+    S->omega_active = omega != nullptr;
     const AMG_param cyc = plain_cycle(S);
     int rc = SUCCESS;
     const int g = grid_for(n);
@@ -191,6 +198,8 @@ int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E) {
         }
     }
     S->omega_active = was;
+    S->omega = was_om;
+    S->bp.use_graph = was_graph;
     if (!rc) HZB_CUDA(cudaStreamSynchronize(s));
     return rc;
 }

@@ -122,7 +122,8 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out);
 int ensure_fp32(hzb_solver *S);
 // learned-weight loss (hzb_learn.cu)
-int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E);
+int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
+                 const float *omega);
 int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
                     double *loss, float *domega);
 // smoothing of level l as mgcycle's pre (pre = true) / post smoothing calls

@@ -429,8 +429,10 @@ INT  hzb_gnn_infer(hzb_gnn *g, hzb_solver *s, float *d_omega);
 /* accumulate parameter gradients for dL/domega (device array, n) */
 INT  hzb_gnn_backward(hzb_gnn *g, hzb_solver *s, const float *d_domega);
 /* ns training error vectors (device, n x ns, FP64): seeded random vectors
- * after three plain l1 sweeps and two plain V-cycles, unit A-norm */
-INT  hzb_learn_errors(hzb_solver *s, INT ns, unsigned long long seed, REAL *d_E);
+ * after three plain l1 sweeps and two V-cycles, unit A-norm; the cycles use
+ * the fine-level weights d_omega (device, n) or plain weights if NULL */
+INT  hzb_learn_errors(hzb_solver *s, INT ns, unsigned long long seed, REAL *d_E,
+                      const float *d_omega);
 /* mean over the ns vectors of ||E(omega)^2 e||_A^2 / ||e||_A^2 for the V(2,2)
  * l1-Jacobi cycle with fine-level weights omega, and its gradient */
 INT  hzb_learn_loss_grad(hzb_solver *s, const float *d_omega, INT ns,

@@ -183,10 +183,12 @@ class Port(_Backend):
         self.lib.or_gnn_backward(_p(prm), _p(d), _p(g))
         return g
 
-    def learn_errors(self, ns, seed):
+    def learn_errors(self, ns, seed, omega=None):
         n = self.level_info(0)[0]
         E = np.empty((ns, n))
-        self.lib.or_learn_errors(ns, C.c_ulonglong(seed), _p(E))
+        om = None if omega is None else np.ascontiguousarray(omega, np.float32)
+        self.lib.or_learn_errors(ns, C.c_ulonglong(seed), _p(E),
+                                 None if om is None else _p(om))
         return E
 
     def learn_loss_grad(self, omega, E):

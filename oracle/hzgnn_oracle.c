@@ -158,6 +158,7 @@ void or_gnn_forward(int n, const int *ia, const int *ja, const double *a,
     for (int i = 0; i < n; ++i) {
         float z = prm[OFF_BO];
         for (int f = 0; f < H; ++f) z += prm[OFF_WO + f] * g_h[3][i * H + f];
+        z = z > 12.f ? 12.f : (z < -12.f ? -12.f : z);
         g_om[i] = 2.0f / (1.0f + expf(-z));
         omega[i] = g_om[i];
     }
@@ -303,8 +304,13 @@ static void l1n(int n, const int *ia, const double *a, double *l1)
     }
 }
 
-void or_learn_errors(int ns, unsigned long long seed, double *E)
+void or_set_omega(const float *omega);
+
+/* omega == NULL: the plain cycle's errors; otherwise the two cycles use
+ * omega on the fine level */
+void or_learn_errors(int ns, unsigned long long seed, double *E, const float *omega)
 {
+    or_set_omega(omega);
     int n, nc;
     const int *ia, *ja, *agg, *ria, *rja;
     const double *a;
@@ -329,6 +335,7 @@ void or_learn_errors(int ns, unsigned long long seed, double *E)
         double s2 = 1.0 / sqrt(dotp(n, e, r));
         for (int i = 0; i < n; ++i) e[i] *= s2;
     }
+    or_set_omega(NULL);
     free(l1); free(r); free(t);
 }
 
