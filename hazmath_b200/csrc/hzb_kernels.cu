@@ -59,32 +59,87 @@ int sm_count() {
 
 // ---------------------------------------------------------------------------
 // SpMV: row bundles staged in shared memory
+//
+// A CTA owns ROWS consecutive rows (ROWS = 64, 128 or 256, picked per level
+// by autotune_bundle).  Their entries form one contiguous range of val/ja;
+// it is copied to shared memory with 16-byte streaming loads (ld.global.cs:
+// the matrix is read once per pass and should not evict x from L2), then
+// every thread sums its own row sequentially in CSR order, gathering x
+// through the read-only path.
 // ---------------------------------------------------------------------------
-__global__ void k_bundle_cap(int n, const int *__restrict__ ia, int *cap) {
+__global__ void k_bundle_cap(int n, int rows, const int *__restrict__ ia, int *cap) {
     __shared__ int sh[32];
     int best = 0;
-    const int nb = (n + SPMV_ROWS - 1) / SPMV_ROWS;
+    const int nb = (n + rows - 1) / rows;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb;
          b += gridDim.x * blockDim.x) {
-        int r0 = b * SPMV_ROWS, r1 = min(r0 + SPMV_ROWS, n);
+        int r0 = b * rows, r1 = min(r0 + rows, n);
         best = max(best, ia[r1] - ia[r0]);
     }
     best = block_max(best, sh);
     if (threadIdx.x == 0) atomicMax(cap, best);
 }
 
-int bundle_capacity(int n, const int *ia, cudaStream_t s, int *cap) {
+int bundle_capacity_rows(int n, int rows, const int *ia, cudaStream_t s, int *cap) {
     int *d = nullptr;
     HZB_TRY(dalloc(&d, 1));
     cudaMemsetAsync(d, 0, sizeof(int), s);
-    const int nb = div_up(n, SPMV_ROWS);
-    k_bundle_cap<<<grid_for(nb), 256, 0, s>>>(n, ia, d);
+    const int nb = div_up(n, rows);
+    k_bundle_cap<<<grid_for(nb), 256, 0, s>>>(n, rows, ia, d);
     count_launch();
     cudaError_t e = cudaMemcpyAsync(cap, d, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d);
+    dfree(d);
     if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
     return SUCCESS;
+}
+
+int bundle_capacity(int n, const int *ia, cudaStream_t s, int *cap) {
+    return bundle_capacity_rows(n, SPMV_ROWS, ia, s, cap);
+}
+
+// shared-memory words needed for a bundle of cap entries (4 elements of
+// alignment slack in front, one vector of slack at the end)
+template <typename T>
+__host__ __device__ inline size_t bundle_sc_offset(int cap) {
+    return (((size_t)cap + 8) * sizeof(T) + 15) & ~(size_t)15;   // 16-byte aligned
+}
+template <typename T>
+__host__ __device__ inline size_t bundle_smem(int cap) {
+    return bundle_sc_offset<T>(cap) + ((size_t)cap + 8) * sizeof(int);
+}
+// the staged kernels load val/ja with 16-byte vectors: both bases must be
+// 16-byte aligned (device allocations are; arbitrary caller views may not be)
+template <typename T>
+inline bool bundle_aligned(const DCsr<T> &A) {
+    return ((reinterpret_cast<uintptr_t>(A.val) | reinterpret_cast<uintptr_t>(A.ja)) & 15) == 0;
+}
+
+// Stage entries [s, e) into sv/sc at offsets k - s0, s0 = s rounded down to
+// a multiple of 4 (so that both T and int loads are 16-byte aligned).
+template <typename T, int NT>
+__device__ __forceinline__ int stage_bundle(const T *__restrict__ val, const int *__restrict__ ja,
+                                            int s, int e, T *sv, int *sc) {
+    const int s0 = s & ~3;
+    const int ev = e & ~3;               // end of the vector part
+    const int nvec = ev > s0 ? (ev - s0) >> 2 : 0;
+    if (sizeof(T) == 8) {
+        const double2 *v2 = reinterpret_cast<const double2 *>(val + s0);
+        double2 *d2 = reinterpret_cast<double2 *>(sv);
+        for (int q = threadIdx.x; q < 2 * nvec; q += NT) d2[q] = __ldcs(v2 + q);
+    } else {
+        const float4 *v4 = reinterpret_cast<const float4 *>(val + s0);
+        float4 *d4 = reinterpret_cast<float4 *>(sv);
+        for (int q = threadIdx.x; q < nvec; q += NT) d4[q] = __ldcs(v4 + q);
+    }
+    const int4 *j4 = reinterpret_cast<const int4 *>(ja + s0);
+    int4 *c4 = reinterpret_cast<int4 *>(sc);
+    for (int q = threadIdx.x; q < nvec; q += NT) c4[q] = __ldcs(j4 + q);
+    for (int k = max(ev, s0) + threadIdx.x; k < e; k += NT) {
+        sv[k - s0] = val[k];
+        sc[k - s0] = ja[k];
+    }
+    return s0;
 }
 
 template <typename T, int MODE>
@@ -100,28 +155,24 @@ __device__ __forceinline__ void spmv_store(int row, T t, const T *b, T *y, T alp
     }
 }
 
-template <typename T, int MODE>
-__global__ void __launch_bounds__(SPMV_ROWS)
+template <typename T, int MODE, int ROWS>
+__global__ void __launch_bounds__(ROWS)
 k_spmv_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
               const T *__restrict__ val, const T *__restrict__ x,
               const T *__restrict__ b, T *__restrict__ y, T alpha,
               T *__restrict__ part, int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sv = reinterpret_cast<T *>(smem_raw);
-    int *sc = reinterpret_cast<int *>(sv + ((cap + 1) & ~1));
-    const int r0 = blockIdx.x * SPMV_ROWS;
-    const int r1 = min(r0 + SPMV_ROWS, n);
+    int *sc = reinterpret_cast<int *>(smem_raw + bundle_sc_offset<T>(cap));
+    const int r0 = blockIdx.x * ROWS;
+    const int r1 = min(r0 + ROWS, n);
     const int s = __ldg(ia + r0), e = __ldg(ia + r1);
-    const int cnt = e - s;
-    for (int k = threadIdx.x; k < cnt; k += SPMV_ROWS) {
-        sv[k] = __ldg(val + s + k);
-        sc[k] = __ldg(ja + s + k);
-    }
+    const int s0 = stage_bundle<T, ROWS>(val, ja, s, e, sv, sc);
     __syncthreads();
     const int row = r0 + threadIdx.x;
     T t = T(0), prod = T(0);
     if (row < r1) {
-        const int b0 = __ldg(ia + row) - s, b1 = __ldg(ia + row + 1) - s;
+        const int b0 = __ldg(ia + row) - s0, b1 = __ldg(ia + row + 1) - s0;
         for (int k = b0; k < b1; ++k) t += sv[k] * __ldg(x + sc[k]);
         spmv_store<T, MODE>(row, t, b, y, alpha);
         if (MODE == SPMV_Y_DOT) prod = t * __ldg(x + row);
@@ -134,13 +185,13 @@ k_spmv_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
 }
 
 // Rows too long for the staged bundle: one thread per row from global memory.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(SPMV_ROWS)
+template <typename T, int MODE, int ROWS>
+__global__ void __launch_bounds__(ROWS)
 k_spmv_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
             const T *__restrict__ val, const T *__restrict__ x,
             const T *__restrict__ b, T *__restrict__ y, T alpha,
             T *__restrict__ part) {
-    const int row = blockIdx.x * SPMV_ROWS + threadIdx.x;
+    const int row = blockIdx.x * ROWS + threadIdx.x;
     T t = T(0), prod = T(0);
     if (row < n) {
         const int b0 = ia[row], b1 = ia[row + 1];
@@ -156,28 +207,42 @@ k_spmv_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
 }
 
 int spmv_blocks(int n) { return div_up(n > 0 ? n : 1, SPMV_ROWS); }
+int spmv_blocks_rows(int n, int rows) { return div_up(n > 0 ? n : 1, rows > 0 ? rows : SPMV_ROWS); }
 
-template <typename T, int MODE>
-static int spmv_mode(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha,
-                     T *part, cudaStream_t s) {
-    if (A.n <= 0) return SUCCESS;
-    const int grid = spmv_blocks(A.n);
-    const size_t smem = (size_t)((A.bundle_cap + 1) & ~1) * sizeof(T) +
-                        (size_t)A.bundle_cap * sizeof(int);
-    if (A.bundle_cap > 0 && smem <= SPMV_SMEM_MAX) {
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(k_spmv_bundle<T, MODE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        k_spmv_bundle<T, MODE><<<grid, SPMV_ROWS, smem, s>>>(
-            A.n, A.ia, A.ja, A.val, x, b, y, alpha, part, A.bundle_cap);
+template <typename T, int MODE, int ROWS>
+static int spmv_launch(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, T *part,
+                       cudaStream_t s) {
+    const int grid = div_up(A.n, ROWS);
+    const size_t smem = bundle_smem<T>(A.bundle_cap);
+    if (A.bundle_cap > 0 && smem <= SPMV_SMEM_MAX && bundle_aligned(A)) {
+        if (smem > 48 * 1024) {
+            static bool done = false;   // per instantiation: raise the limit once
+            if (!done) {
+                cudaFuncSetAttribute(k_spmv_bundle<T, MODE, ROWS>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
+                done = true;
+            }
+        }
+        k_spmv_bundle<T, MODE, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, x, b,
+                                                              y, alpha, part, A.bundle_cap);
     } else {
-        k_spmv_rows<T, MODE><<<grid, SPMV_ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val,
-                                                       x, b, y, alpha, part);
+        k_spmv_rows<T, MODE, ROWS><<<grid, ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y,
+                                                         alpha, part);
     }
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
+}
+
+template <typename T, int MODE>
+static int spmv_mode(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, T *part,
+                     cudaStream_t s) {
+    if (A.n <= 0) return SUCCESS;
+    switch (A.bundle_rows) {
+    case 64: return spmv_launch<T, MODE, 64>(A, x, b, y, alpha, part, s);
+    case 256: return spmv_launch<T, MODE, 256>(A, x, b, y, alpha, part, s);
+    default: return spmv_launch<T, MODE, 128>(A, x, b, y, alpha, part, s);
+    }
 }
 
 template <typename T>
@@ -195,6 +260,36 @@ template int spmv<double>(const DCsr<double> &, int, const double *, const doubl
                           double *, double, double *, cudaStream_t);
 template int spmv<float>(const DCsr<float> &, int, const float *, const float *,
                          float *, float, float *, cudaStream_t);
+
+// Autotuner of the bundle size: times each candidate on this level's SpMV
+// (y = A x with the level's own buffers) and keeps the fastest.
+int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s) {
+    const int cands[3] = {64, 128, 256};
+    cudaEvent_t e0, e1;
+    HZB_CUDA(cudaEventCreate(&e0));
+    HZB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_rows = SPMV_ROWS, best_cap = A.bundle_cap;
+    for (int c : cands) {
+        DCsr<double> B = A;
+        B.bundle_rows = c;
+        HZB_TRY(bundle_capacity_rows(A.n, c, A.ia, s, &B.bundle_cap));
+        if (bundle_smem<double>(B.bundle_cap) > SPMV_SMEM_MAX) continue;
+        HZB_TRY(spmv<double>(B, SPMV_Y, x, nullptr, y, 1.0, nullptr, s));   // warm
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; ++r) HZB_TRY(spmv<double>(B, SPMV_Y, x, nullptr, y, 1.0, nullptr, s));
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; best_rows = c; best_cap = B.bundle_cap; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    A.bundle_rows = best_rows;
+    A.bundle_cap = best_cap;
+    return SUCCESS;
+}
 
 // ---------------------------------------------------------------------------
 // Transfers (P = aggregate map, R = P^T with ascending fine rows)
@@ -283,24 +378,21 @@ int jacobi_sweep(const DCsr<double> &A, const double *dj, const double *b,
 
 // l1-Jacobi: t = b_i - sum_j a_ij x_j, d = sum_j |a_ij| (both in CSR order);
 // x_i += omega_i * (t / d).  Rows are staged per bundle like the SpMV.
-template <typename T>
-__global__ void __launch_bounds__(SPMV_ROWS)
+template <typename T, int ROWS>
+__global__ void __launch_bounds__(ROWS)
 k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
             const T *__restrict__ a, const T *__restrict__ b,
             const T *__restrict__ x, T *__restrict__ xn,
             const float *__restrict__ omega, int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sv = reinterpret_cast<T *>(smem_raw);
-    int *sc = reinterpret_cast<int *>(sv + ((cap + 1) & ~1));
-    const int r0 = blockIdx.x * SPMV_ROWS;
-    const int r1 = min(r0 + SPMV_ROWS, n);
+    int *sc = reinterpret_cast<int *>(smem_raw + bundle_sc_offset<T>(cap));
+    const int r0 = blockIdx.x * ROWS;
+    const int r1 = min(r0 + ROWS, n);
     const int s = __ldg(ia + r0), e = __ldg(ia + r1);
-    const int cnt = e - s;
+    int s0 = s;
     if (cap > 0) {
-        for (int k = threadIdx.x; k < cnt; k += SPMV_ROWS) {
-            sv[k] = __ldg(a + s + k);
-            sc[k] = __ldg(ja + s + k);
-        }
+        s0 = stage_bundle<T, ROWS>(a, ja, s, e, sv, sc);
         __syncthreads();
     }
     const int i = r0 + threadIdx.x;
@@ -308,7 +400,7 @@ k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
     T t = b[i], d = T(0);
     const int b0 = __ldg(ia + i), b1 = __ldg(ia + i + 1);
     if (cap > 0) {
-        for (int k = b0 - s; k < b1 - s; ++k) {
+        for (int k = b0 - s0; k < b1 - s0; ++k) {
             const T v = sv[k];
             t -= v * __ldg(x + sc[k]);
             d += fabs(v);
@@ -328,23 +420,36 @@ k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
     xn[i] = xi;
 }
 
+template <typename T, int ROWS>
+static int l1_launch(const DCsr<T> &A, const T *b, const T *x, T *xn, const float *omega,
+                     cudaStream_t s) {
+    const int grid = div_up(A.n, ROWS);
+    size_t smem = bundle_smem<T>(A.bundle_cap);
+    int cap = A.bundle_cap;
+    if (cap <= 0 || smem > SPMV_SMEM_MAX || !bundle_aligned(A)) { cap = 0; smem = 0; }
+    if (smem > 48 * 1024) {
+        static bool done = false;
+        if (!done) {
+            cudaFuncSetAttribute(k_l1_bundle<T, ROWS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
+            done = true;
+        }
+    }
+    k_l1_bundle<T, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega, cap);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
 template <typename T>
 int l1_sweep(const DCsr<T> &A, const T *b, const T *x, T *xn,
              const float *omega, cudaStream_t s) {
     if (A.n <= 0) return SUCCESS;
-    const int grid = spmv_blocks(A.n);
-    size_t smem = (size_t)((A.bundle_cap + 1) & ~1) * sizeof(T) +
-                  (size_t)A.bundle_cap * sizeof(int);
-    int cap = A.bundle_cap;
-    if (cap <= 0 || smem > SPMV_SMEM_MAX) { cap = 0; smem = 0; }
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_l1_bundle<T>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_l1_bundle<T><<<grid, SPMV_ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn,
-                                                 omega, cap);
-    count_launch();
-    HZB_LAUNCH_CHECK();
-    return SUCCESS;
+    switch (A.bundle_rows) {
+    case 64: return l1_launch<T, 64>(A, b, x, xn, omega, s);
+    case 256: return l1_launch<T, 256>(A, b, x, xn, omega, s);
+    default: return l1_launch<T, 128>(A, b, x, xn, omega, s);
+    }
 }
 template int l1_sweep<double>(const DCsr<double> &, const double *, const double *,
                               double *, const float *, cudaStream_t);

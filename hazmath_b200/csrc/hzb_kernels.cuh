@@ -15,7 +15,8 @@ struct DCsr {
     int n = 0, nnz = 0;
     const int *ia = nullptr, *ja = nullptr;
     const T *val = nullptr;
-    int bundle_cap = 0;   // max entries in any SPMV_ROWS-row bundle (0: none)
+    int bundle_cap = 0;   // max entries in any bundle of bundle_rows rows (0: none)
+    int bundle_rows = 128;   // rows per CTA of the staged kernels: 64, 128 or 256
 };
 
 constexpr int SPMV_ROWS = 128;          // rows per CTA in the row-bundle SpMV
@@ -23,8 +24,12 @@ constexpr int SPMV_SMEM_MAX = 160 * 1024;
 
 enum SpmvMode { SPMV_Y = 0, SPMV_RES = 1, SPMV_AXPY = 2, SPMV_Y_DOT = 3 };
 
-// Largest number of stored entries in any SPMV_ROWS-row bundle of A.
+// Largest number of stored entries in any SPMV_ROWS-row (rows-row) bundle.
 int bundle_capacity(int n, const int *ia, cudaStream_t s, int *cap);
+int bundle_capacity_rows(int n, int rows, const int *ia, cudaStream_t s, int *cap);
+// Picks the bundle size (64/128/256 rows) of A by timing its SpMV on x -> y.
+int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s);
+int spmv_blocks_rows(int n, int rows);
 
 // y = A x (SPMV_Y); y = b - A x (SPMV_RES); y += alpha A x with the
 // reference's +-1 special cases (SPMV_AXPY); y = A x and partial dot(y, x)

@@ -68,7 +68,7 @@ int KrylovWork::alloc(int nn) {
     release();
     n = nn;
     const int G = reduce_blocks(n);
-    const int np = 4 * G + spmv_blocks(n) + 8;
+    const int np = 4 * G + spmv_blocks_rows(n, 64) + 8;   // smallest bundle
     HZB_TRY(dalloc(&p, n));
     HZB_TRY(dalloc(&z, n));
     HZB_TRY(dalloc(&r, n));
@@ -507,6 +507,13 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
         HZB_TRY(dalloc(&L.w, L.n));
         HZB_TRY(dalloc(&L.t, L.n));
         if (l < S->nl - 1) HZB_TRY(level_smoother_data(S, L));
+        if (L.n >= 32768) {   // large levels: time the bundle sizes once
+            HZB_TRY(vzero<double>(L.n, L.x, s));
+            DCsr<double> A = L.A64();
+            HZB_TRY(autotune_bundle(A, L.x, L.w, s));
+            L.bundle_rows = A.bundle_rows;
+            L.bundle_cap = A.bundle_cap;
+        }
     }
     HZB_TRY(S->kw.alloc(n));
     if (S->amg.coarse_solver != SOLVER_UMFPACK)
@@ -677,7 +684,7 @@ int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
     while (iter++ < MaxIt) {
         // t = A p ; temp2 = (t, p) ; alpha = temp1 / temp2 (device)
         HZB_TRY(spmv<double>(A, SPMV_Y_DOT, w.p, nullptr, w.t, 1.0, partd, s));
-        HZB_TRY(reduce_final(partd, spmv_blocks(m), w.sc + SC_T2, s));
+        HZB_TRY(reduce_final(partd, spmv_blocks_rows(m, A.bundle_rows), w.sc + SC_T2, s));
         // u += alpha p ; r -= alpha t ; norms for checks I and II
         HZB_TRY(pcg_update(m, w.sc + SC_T1, w.sc + SC_T2, u, w.r, w.p, w.t, part4, s));
         HZB_TRY(reduce_final(part4, G, w.sc + SC_RR, s));
@@ -890,7 +897,7 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
     HZB_TRY(dot(m, w.z, w.r, w.part, w.sc + SC_T1, s));
     while (iter++ < maxit) {
         HZB_TRY(spmv<double>(A, SPMV_Y_DOT, w.p, nullptr, w.t, 1.0, partd, s));
-        HZB_TRY(reduce_final(partd, spmv_blocks(m), w.sc + SC_T2, s));
+        HZB_TRY(reduce_final(partd, spmv_blocks_rows(m, A.bundle_rows), w.sc + SC_T2, s));
         HZB_TRY(pcg_update(m, w.sc + SC_T1, w.sc + SC_T2, x, w.r, w.p, w.t, part4, s));
         HZB_TRY(reduce_final(part4, G, w.sc + SC_RR, s));
         HZB_TRY(fetch(S, w));

@@ -14,6 +14,7 @@ struct Level {
     float *val32 = nullptr;
     bool own_A = true;
     int bundle_cap = 0;
+    int bundle_rows = 128;            // picked by autotune_bundle
     // transfer to level + 1 (P = agg map, R = P^T with ascending rows)
     int nc = 0;
     int *agg = nullptr, *ria = nullptr, *rja = nullptr;
@@ -38,11 +39,13 @@ struct Level {
     DCsr<double> A64() const {
         DCsr<double> m;
         m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val; m.bundle_cap = bundle_cap;
+        m.bundle_rows = bundle_rows;
         return m;
     }
     DCsr<float> A32() const {
         DCsr<float> m;
         m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val32; m.bundle_cap = bundle_cap;
+        m.bundle_rows = bundle_rows;
         return m;
     }
     void release();
