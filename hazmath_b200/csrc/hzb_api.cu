@@ -321,7 +321,8 @@ extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
     const bool f32 = which == HZB_K_SPMV32 || which == HZB_K_L1_32;
     if (f32 && !L.val32) HZB_TRY(ensure_fp32(S));
     const double vb = f32 ? 4.0 : 8.0;
-    const double n = L.n, nnz = L.nnz;
+    // the FP32 kernels read the zero-free copy
+    const double n = L.n, nnz = f32 ? L.nnz32 : L.nnz;
     double bytes = nnz * (vb + 4.0) + 4.0 * (n + 1);
     switch (which) {
     case HZB_K_SPMV64: case HZB_K_SPMV32: bytes += 2 * vb * n; break;     // x, y

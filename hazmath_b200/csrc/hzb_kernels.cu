@@ -773,6 +773,40 @@ int f2d(int n, const float *x, double *y, cudaStream_t s) {
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
+// FP32 copy of a CSR matrix without its exactly-zero entries (row order kept)
+__global__ void k_nz_count(int n, const int *__restrict__ ia, const double *__restrict__ a,
+                           int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        int c = 0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) c += a[k] != 0.0;
+        cnt[i] = c;
+    }
+}
+__global__ void k_nz_fill(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                          const double *__restrict__ a, const int *__restrict__ ia32,
+                          int *ja32, float *a32) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        int p = ia32[i];
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+            if (a[k] != 0.0) { ja32[p] = ja[k]; a32[p] = (float)a[k]; ++p; }
+    }
+}
+int csr_nonzero_count(int n, const int *ia, const double *a, int *cnt, cudaStream_t s) {
+    k_nz_count<<<grid_for(n), 256, 0, s>>>(n, ia, a, cnt);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+int csr_nonzero_fill(int n, const int *ia, const int *ja, const double *a, const int *ia32,
+                     int *ja32, float *a32, cudaStream_t s) {
+    k_nz_fill<<<grid_for(n), 256, 0, s>>>(n, ia, ja, a, ia32, ja32, a32);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
 int csr_val_d2f(int nnz, const double *x, float *y, cudaStream_t s) {
     return d2f(nnz, x, y, s);
 }

@@ -50,6 +50,9 @@ void Level::release() {
     if (own_A) { dfree(ia); dfree(ja); dfree(val); }
     ia = ja = nullptr; val = nullptr;
     dfree(val32);
+    if (own32) { dfree(ia32); dfree(ja32); }
+    ia32 = ja32 = nullptr;
+    own32 = false;
     dfree(agg); dfree(ria); dfree(rja);
     dfree(b); dfree(x); dfree(w); dfree(t);
     dfree(b32); dfree(x32); dfree(w32); dfree(t32);
@@ -362,8 +365,34 @@ int ensure_fp32(hzb_solver *S) {
     for (int l = 0; l < S->nl; ++l) {
         Level &L = S->lv[l];
         if (!L.val32) {
-            HZB_TRY(dalloc(&L.val32, L.nnz));
-            HZB_TRY(csr_val_d2f(L.nnz, L.val, L.val32, S->s));
+            // drop the stored exact zeros: they add nothing to a row sum
+            int *cnt = nullptr, *ia32 = nullptr, *tmp = nullptr;
+            HZB_TRY(dalloc(&cnt, L.n));
+            HZB_TRY(dalloc(&ia32, L.n + 1));
+            HZB_TRY(dalloc(&tmp, scan_tmp_size(L.n + 1)));
+            HZB_TRY(csr_nonzero_count(L.n, L.ia, L.val, cnt, S->s));
+            HZB_TRY(scan_exclusive(cnt, ia32, L.n, tmp, S->s));
+            int nz = 0;
+            HZB_CUDA(cudaMemcpyAsync(&nz, ia32 + L.n, sizeof(int), cudaMemcpyDeviceToHost, S->s));
+            HZB_CUDA(cudaStreamSynchronize(S->s));
+            dfree(cnt);
+            dfree(tmp);
+            if (nz == L.nnz) {   // nothing to drop: share the pattern
+                dfree(ia32);
+                HZB_TRY(dalloc(&L.val32, L.nnz));
+                HZB_TRY(csr_val_d2f(L.nnz, L.val, L.val32, S->s));
+                L.ia32 = L.ia;
+                L.ja32 = L.ja;
+                L.own32 = false;
+            } else {
+                L.ia32 = ia32;
+                HZB_TRY(dalloc(&L.ja32, nz));
+                HZB_TRY(dalloc(&L.val32, nz));
+                HZB_TRY(csr_nonzero_fill(L.n, L.ia, L.ja, L.val, L.ia32, L.ja32, L.val32, S->s));
+                L.own32 = true;
+            }
+            L.nnz32 = nz;
+            HZB_TRY(bundle_capacity_rows(L.n, L.bundle_rows, L.ia32, S->s, &L.bundle_cap32));
         }
         if (!L.b32) {
             HZB_TRY(dalloc(&L.b32, L.n));

@@ -11,10 +11,15 @@ struct Level {
     int n = 0, nnz = 0;
     int *ia = nullptr, *ja = nullptr;
     double *val = nullptr;
-    float *val32 = nullptr;
     bool own_A = true;
     int bundle_cap = 0;
     int bundle_rows = 128;            // picked by autotune_bundle
+    // FP32 copy for the mixed cycle without the stored exact zeros (a zero
+    // entry adds nothing to a row sum); aliases ia/ja when there are none
+    int nnz32 = 0, bundle_cap32 = 0;
+    int *ia32 = nullptr, *ja32 = nullptr;
+    float *val32 = nullptr;
+    bool own32 = false;
     // transfer to level + 1 (P = agg map, R = P^T with ascending rows)
     int nc = 0;
     int *agg = nullptr, *ria = nullptr, *rja = nullptr;
@@ -44,7 +49,8 @@ struct Level {
     }
     DCsr<float> A32() const {
         DCsr<float> m;
-        m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val32; m.bundle_cap = bundle_cap;
+        m.n = n; m.nnz = nnz32; m.ia = ia32; m.ja = ja32; m.val = val32;
+        m.bundle_cap = bundle_cap32;
         m.bundle_rows = bundle_rows;
         return m;
     }
