@@ -270,16 +270,199 @@ k_hem_seq(int n, const int *__restrict__ ia, const int *__restrict__ ja,
     if (lane == 0) { out[0] = nc; out[1] = status; }
 }
 
+// --- the same matching with the pass-1 state in shared memory -------------
+// Pass 1 only asks "is j already matched?".  While every neighbour index is
+// within B of its row (B = the graph's bandwidth), the vertices in play at
+// step k lie in [k - B, k + B], so one bit per vertex in a ring of RING bits
+// (RING > 2B) indexed by v mod RING holds that state; the slot of vertex
+// k + B is cleared when step k begins (its previous owner, k + B - RING,
+// finished long ago).  Pass 2 then visits only the vertices left unmatched.
+constexpr int HEM_RING_BITS = 1 << 20;                 // 128 KB of shared memory
+constexpr int HEM_RING_WORDS = HEM_RING_BITS / 32;
+
+__global__ void k_graph_bandwidth(int n, const int *__restrict__ ia,
+                                  const int *__restrict__ ja, int *bw) {
+    __shared__ int sh[32];
+    int b = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) b = max(b, abs(ja[k] - i));
+    b = block_max(b, sh);
+    if (threadIdx.x == 0) atomicMax(bw, b);
+}
+
+__global__ void k_hem_init(int n, const int *__restrict__ ia, int *mask, int *cnt) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x) {
+        mask[k] = (ia[k + 1] - ia[k] > 1) ? -1 : -2;   // pass 0
+        cnt[k] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(32)
+k_hem_pass1_ring(int n, int bw, const int *__restrict__ ia, const int *__restrict__ ja,
+                 const double *__restrict__ a, int *mask, int *cnt, int *out) {
+    extern __shared__ unsigned ring[];
+    const int lane = threadIdx.x;
+    for (int w = lane; w < HEM_RING_WORDS; w += 32) ring[w] = 0u;
+    __syncwarp();
+    constexpr unsigned RM = HEM_RING_BITS - 1;
+    int nc = 0;
+    for (int k = 0; k < n; ++k) {
+        if (lane == 0) {
+            const unsigned v = (unsigned)(k + bw) & RM;   // entering the window
+            ring[v >> 5] &= ~(1u << (v & 31));
+        }
+        __syncwarp();
+        const unsigned vk = (unsigned)k & RM;
+        const bool matched = (ring[vk >> 5] >> (vk & 31)) & 1u;
+        const int b0 = __ldg(ia + k), b1 = __ldg(ia + k + 1);
+        if (matched || b1 - b0 <= 1) continue;   // already paired / pass-0 isolated
+        double bwgt = 0.0;
+        int bp = -1;
+        for (int p = b0 + lane; p < b1; p += 32) {
+            const int j = __ldg(ja + p);
+            const unsigned vj = (unsigned)j & RM;
+            const bool mj = (ring[vj >> 5] >> (vj & 31)) & 1u;
+            if (j != k && !mj) better_last(bwgt, bp, fabs(__ldg(a + p)), p);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w2 = __shfl_xor_sync(0xffffffffu, bwgt, o);
+            int p2 = __shfl_xor_sync(0xffffffffu, bp, o);
+            better_last(bwgt, bp, w2, p2);
+        }
+        if (bp >= 0) {
+            if (lane == 0) {
+                const int pick = __ldg(ja + bp);
+                const unsigned vp = (unsigned)pick & RM;
+                ring[vk >> 5] |= 1u << (vk & 31);
+                ring[vp >> 5] |= 1u << (vp & 31);
+                mask[k] = nc;
+                mask[pick] = nc;
+                cnt[nc] = 2;
+            }
+            ++nc;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) out[0] = nc;
+}
+
+__global__ void k_flag_eq(int n, const int *__restrict__ v, int val, int *flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        flag[i] = v[i] == val;
+}
+__global__ void k_compact(int n, const int *__restrict__ flag, const int *__restrict__ pos,
+                          int *list) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        if (flag[i]) list[pos[i]] = i;
+}
+
+// pass 2 over the leftover list (ascending), one warp, reference semantics
+__global__ void __launch_bounds__(32)
+k_hem_pass2_list(int m, const int *__restrict__ list, const int *__restrict__ ia,
+                 const int *__restrict__ ja, int *mask_, int *cnt_, int *out) {
+    volatile int *mask = mask_;
+    volatile int *cnt = cnt_;
+    const int lane = threadIdx.x;
+    int status = 0;
+    for (int q = 0; q < m; ++q) {
+        const int k = list[q];
+        const int b0 = ia[k], b1 = ia[k + 1];
+        double bwgt = 0.0;
+        int bp = -1, bc = -1;
+        for (int p = b0 + lane; p < b1; p += 32) {
+            const int kc = mask[ja[p]];
+            if (kc >= 0) {
+                double w2 = (double)(-cnt[kc]);
+                int oldp = bp;
+                better_first(bwgt, bp, w2, p);
+                if (bp != oldp) bc = kc;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w2 = __shfl_xor_sync(0xffffffffu, bwgt, o);
+            int p2 = __shfl_xor_sync(0xffffffffu, bp, o);
+            int c2 = __shfl_xor_sync(0xffffffffu, bc, o);
+            int oldp = bp;
+            better_first(bwgt, bp, w2, p2);
+            if (bp != oldp) bc = c2;
+        }
+        if (bp < 0) { status = -1; break; }
+        if (lane == 0) {
+            mask[k] = bc;
+            cnt[bc] = cnt[bc] + 1;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) out[1] = status;
+}
+
+__global__ void k_hem_final(int n, int *mask) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += gridDim.x * blockDim.x)
+        if (mask[k] < 0) mask[k] = UNPT;
+}
+
 int hem_exact(int n, const int *nia, const int *nja, const double *nval,
               int *agg, int *nagg, int *work_n, cudaStream_t s) {
     int *out = nullptr;
-    HZB_TRY(dalloc(&out, 2));
-    k_hem_seq<<<1, 32, 0, s>>>(n, nia, nja, nval, agg, work_n, out);
+    HZB_TRY(dalloc(&out, 3));
+    HZB_CUDA(cudaMemsetAsync(out, 0, 3 * sizeof(int), s));
+    k_graph_bandwidth<<<grid_for(n), 256, 0, s>>>(n, nia, nja, out + 2);
     count_launch();
+    int bw = 0;
+    HZB_CUDA(cudaMemcpyAsync(&bw, out + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HZB_CUDA(cudaStreamSynchronize(s));
+    int rc = SUCCESS;
+    if (2 * bw + 2 < HEM_RING_BITS) {
+        int *flag = nullptr, *pos = nullptr, *list = nullptr, *tmp = nullptr;
+        const int g = grid_for(n);
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_hem_pass1_ring, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 HEM_RING_WORDS * 4);
+            attr = true;
+        }
+        k_hem_init<<<g, 256, 0, s>>>(n, nia, agg, work_n);
+        k_hem_pass1_ring<<<1, 32, HEM_RING_WORDS * 4, s>>>(n, bw, nia, nja, nval, agg,
+                                                          work_n, out);
+        count_launch(2);
+        if ((rc = dalloc(&flag, n)) || (rc = dalloc(&pos, n + 1)) || (rc = dalloc(&list, n)) ||
+            (rc = dalloc(&tmp, scan_tmp_size(n + 1)))) {
+            dfree(flag); dfree(pos); dfree(list); dfree(tmp); dfree(out);
+            return rc;
+        }
+        k_flag_eq<<<g, 256, 0, s>>>(n, agg, -1, flag);
+        count_launch();
+        rc = scan_exclusive(flag, pos, n, tmp, s);
+        int m = 0;
+        if (!rc) {
+            k_compact<<<g, 256, 0, s>>>(n, flag, pos, list);
+            count_launch();
+            cudaMemcpyAsync(&m, pos + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
+            if (m > 0) {
+                k_hem_pass2_list<<<1, 32, 0, s>>>(m, list, nia, nja, agg, work_n, out);
+                count_launch();
+            }
+            k_hem_final<<<g, 256, 0, s>>>(n, agg);
+            count_launch();
+        }
+        dfree(flag); dfree(pos); dfree(list); dfree(tmp);
+    } else {   // wide graph: the whole state in global memory
+        k_hem_seq<<<1, 32, 0, s>>>(n, nia, nja, nval, agg, work_n, out);
+        count_launch();
+    }
     int h[2] = {0, 0};
     cudaError_t e = cudaMemcpyAsync(h, out, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(out);
+    dfree(out);
+    if (rc) return rc;
     if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
     *nagg = h[0];
     return h[1] < 0 ? ERROR_AMG_COARSEING : SUCCESS;
