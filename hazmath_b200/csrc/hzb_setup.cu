@@ -3,6 +3,7 @@
 // rounded in the reference's order.
 #include "hzb_setup.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -280,15 +281,19 @@ k_hem_seq(int n, const int *__restrict__ ia, const int *__restrict__ ja,
 constexpr int HEM_RING_BITS = 1 << 20;                 // 128 KB of shared memory
 constexpr int HEM_RING_WORDS = HEM_RING_BITS / 32;
 
+// bw[0] = max |j - i| over the stored entries, bw[1] = longest row
 __global__ void k_graph_bandwidth(int n, const int *__restrict__ ia,
                                   const int *__restrict__ ja, int *bw) {
     __shared__ int sh[32];
-    int b = 0;
+    int b = 0, len = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += gridDim.x * blockDim.x)
+         i += gridDim.x * blockDim.x) {
         for (int k = ia[i]; k < ia[i + 1]; ++k) b = max(b, abs(ja[k] - i));
+        len = max(len, ia[i + 1] - ia[i]);
+    }
     b = block_max(b, sh);
-    if (threadIdx.x == 0) atomicMax(bw, b);
+    len = block_max(len, sh);
+    if (threadIdx.x == 0) { atomicMax(bw, b); atomicMax(bw + 1, len); }
 }
 
 __global__ void k_hem_init(int n, const int *__restrict__ ia, int *mask, int *cnt) {
@@ -347,6 +352,255 @@ k_hem_pass1_ring(int n, int bw, const int *__restrict__ ia, const int *__restric
         __syncwarp();
     }
     if (lane == 0) out[0] = nc;
+}
+
+// --- pass 1 with pre-ranked candidate lists ---------------------------------
+// Pass 1 of vertex k takes, among the unmatched neighbours j != k, the entry
+// of largest |a_kj|, ties to the later position.  That order does not depend
+// on the matching state, so a parallel kernel first writes every row's
+// neighbours in that order (self entries as -1 at the end), and the
+// sequential walk only looks for the first unmatched entry of the list.
+// The walk streams the lists through shared memory in tiles of 32 rows with
+// cp.async, HEM_PIPE tiles ahead of the tile it works on, so no global load
+// latency sits on its critical path.
+constexpr int HEM_PIPE = 4;                 // tiles in flight ahead of the walk
+constexpr int HEM_TILE_CAP = 3072;          // staged candidates per tile
+constexpr int HEM_RANK_MAXLEN = 4096;       // longest row the ranking accepts
+// slots: the tiles in flight plus the one being walked
+constexpr int HEM_IA_SLOTS = 2 * HEM_PIPE + 2, HEM_IA_STRIDE = 36;
+constexpr int HEM_C_SLOTS = HEM_PIPE + 2;
+constexpr int HEM_MISC_WORDS = 32 * 2 + 32 + 2 * 32 + 2;   // info, Pm, picks, accepted
+constexpr size_t HEM_STAGED_SMEM =
+    (size_t)HEM_RING_WORDS * 4 + (size_t)HEM_C_SLOTS * HEM_TILE_CAP * 4 +
+    (size_t)HEM_IA_SLOTS * HEM_IA_STRIDE * 4 + (size_t)HEM_MISC_WORDS * 4;
+
+// one warp per row: rank of entry p = number of entries that come before it
+__global__ void k_hem_rank(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                           const double *__restrict__ a, int *__restrict__ cand) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
+        const int b0 = ia[k], b1 = ia[k + 1];
+        int nself = 0;
+        for (int p = b0 + lane; p < b1; p += 32) nself += ja[p] == k;
+        for (int o = 16; o > 0; o >>= 1) nself += __shfl_xor_sync(0xffffffffu, nself, o);
+        const int nother = b1 - b0 - nself;
+        for (int p = b0 + lane; p < b1; p += 32) {
+            const int j = ja[p];
+            int r = 0;
+            if (j != k) {
+                const double w = fabs(a[p]);
+                for (int q = b0; q < b1; ++q) {
+                    if (ja[q] == k) continue;
+                    const double w2 = fabs(a[q]);
+                    r += (w2 > w) || (w2 == w && q > p);
+                }
+                cand[b0 + r] = j;
+            } else {
+                for (int q = b0; q < p; ++q) r += ja[q] == k;
+                cand[b0 + nother + r] = -1;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The matched state of the vertices in play lives in a ring of shared memory:
+// one byte per vertex (BYTES, 2^17 vertices, plain stores) while the window
+// fits, else one bit per vertex (2^20 vertices, atomicOr).  Both rings take
+// 128 KB.  Ring size > 2 bw + 64: the 32 slots entering the window are
+// cleared when a tile begins (vertices >= r0 + bw cannot be matched before
+// tile r0 starts, and the slot's previous owner lies below r0 - bw).
+template <bool BYTES>
+struct HemRing {
+    static constexpr unsigned SIZE = BYTES ? (1u << 17) : (1u << 20);
+    static constexpr unsigned RM = SIZE - 1;
+    void *mem;
+    __device__ __forceinline__ bool get(int v) const {
+        const unsigned u = (unsigned)v & RM;
+        if (BYTES) return ((const volatile unsigned char *)mem)[u] != 0;
+        return (((const volatile unsigned *)mem)[u >> 5] >> (u & 31)) & 1u;
+    }
+    __device__ __forceinline__ void set(int v) {
+        const unsigned u = (unsigned)v & RM;
+        if (BYTES) ((volatile unsigned char *)mem)[u] = 1;
+        else atomicOr((unsigned *)mem + (u >> 5), 1u << (u & 31));
+    }
+    // vertices v0 .. v0 + 31, by the whole warp
+    __device__ __forceinline__ void clear32(int v0, int lane) {
+        if (BYTES) {
+            ((unsigned char *)mem)[((unsigned)v0 + lane) & RM] = 0;
+        } else {
+            const unsigned u = (unsigned)v0 & RM, sh = u & 31u, w0 = u >> 5;
+            unsigned *w = (unsigned *)mem;
+            if (lane == 0) w[w0] &= ~(0xffffffffu << sh);
+            if (lane == 1 && sh) w[(w0 + 1) & (SIZE / 32 - 1)] &= ~((1u << sh) - 1u);
+        }
+    }
+};
+
+// Two warps.  Warp 1 streams row pointers and ranked lists into shared
+// memory (cp.async, HEM_PIPE tiles ahead) and writes the pairs of finished
+// tiles to mask/cnt; warp 0 walks the tiles.  Within a tile of 32 rows every
+// row first takes its best candidate unmatched when the tile starts; rows are
+// then settled in order.  A row keeps that choice unless an earlier row of
+// the tile took it or matched the row's choice (vertices only ever become
+// matched, so the entries ranked above it stay ineligible); such a row scans
+// its list again.  For a row that keeps its choice the effect on the rows
+// after it is known in advance: the row it picks leaves the walk (rm) and the
+// rows that wanted the same vertex or this row go stale (st).
+template <bool BYTES>
+__global__ void __launch_bounds__(64)
+k_hem_pass1_staged(int n, int bw, const int *__restrict__ ia, const int *__restrict__ cand,
+                   int *mask, int *cnt, int *out) {
+    extern __shared__ unsigned hem_smem[];
+    HemRing<BYTES> ring{hem_smem};
+    int *cbuf = (int *)(hem_smem + HEM_RING_WORDS);
+    int *iabuf = cbuf + HEM_C_SLOTS * HEM_TILE_CAP;
+    uint2 *info = (uint2 *)(iabuf + HEM_IA_SLOTS * HEM_IA_STRIDE);
+    unsigned *pm = (unsigned *)(info + 32);
+    int *picks = (int *)(pm + 32);              // [2][32], by tile parity
+    unsigned *accepted = (unsigned *)(picks + 64);   // [2]
+    const int lane = threadIdx.x & 31;
+    const int ntiles = (n + 31) >> 5;
+
+    if (threadIdx.x >= 32) {   // ---- warp 1: staging and output
+        int nc = 0;
+        auto emit = [&](int u) {
+            const unsigned acc = accepted[u & 1];
+            if ((acc >> lane) & 1u) {
+                const int id = nc + __popc(acc & ((1u << lane) - 1u));
+                const int q = picks[(u & 1) * 32 + lane];
+                mask[(u << 5) + lane] = id;
+                mask[q] = id;
+                cnt[id] = 2;
+            }
+            nc += __popc(acc);
+        };
+        for (int j = -2 * HEM_PIPE; j < ntiles; ++j) {
+            if (j >= 2) emit(j - 2);
+            const int ui = j + 2 * HEM_PIPE;   // row pointers of tile j + 2 PIPE
+            if (ui < ntiles) {
+                const int r0 = ui << 5, rows = min(32, n - r0);
+                int *dst = iabuf + (ui % HEM_IA_SLOTS) * HEM_IA_STRIDE;
+                cp_async4(dst + lane, ia + r0 + min(lane, rows));
+                if (lane == 0) cp_async4(dst + 32, ia + r0 + rows);
+            }
+            cp_async_wait<HEM_PIPE - 1>();   // ia(j + PIPE) and cand(j) have landed
+            __syncwarp();
+            const int uc = j + HEM_PIPE;     // ranked lists of tile j + PIPE
+            if (uc >= 0 && uc < ntiles) {
+                const int *iu = iabuf + (uc % HEM_IA_SLOTS) * HEM_IA_STRIDE;
+                const int rows = min(32, n - (uc << 5));
+                const int e0 = iu[0], m = iu[rows] - e0;
+                if (m <= HEM_TILE_CAP) {
+                    int *dst = cbuf + (uc % HEM_C_SLOTS) * HEM_TILE_CAP;
+                    for (int e = lane; e < m; e += 32) cp_async4(dst + e, cand + e0 + e);
+                }
+            }
+            cp_async_commit();
+            if (j >= 0) __syncthreads();   // tile j is ready; tile j - 1 is walked
+        }
+        cp_async_wait<0>();
+        __syncthreads();                    // the last tile is walked
+        if (ntiles >= 2) emit(ntiles - 2);
+        if (ntiles >= 1) emit(ntiles - 1);
+        if (lane == 0) out[0] = nc;
+        return;
+    }
+
+    // ---- warp 0: the walk
+    for (int w = lane; w < HEM_RING_WORDS; w += 32) hem_smem[w] = 0u;
+    __syncthreads();
+    for (int t = 0; t < ntiles; ++t) {
+        const int r0 = t << 5, rows = min(32, n - r0);
+        ring.clear32(r0 + bw, lane);
+        __syncwarp();
+        const int *it = iabuf + (t % HEM_IA_SLOTS) * HEM_IA_STRIDE;
+        const int e0 = it[0];
+        const bool staged = it[rows] - e0 <= HEM_TILE_CAP;
+        const int *ct = staged ? cbuf + (t % HEM_C_SLOTS) * HEM_TILE_CAP : cand;
+        const int off = staged ? e0 : 0;
+        int *pk = picks + (t & 1) * 32;
+        // rows of the tile still unmatched and not isolated (pass 0)
+        const bool act = lane < rows && it[lane + 1] - it[lane] > 1 && !ring.get(r0 + lane);
+        unsigned todo = __ballot_sync(0xffffffffu, act);
+        int p = -1;
+        if (act) {
+            const int b1 = it[lane + 1];
+            for (int e = it[lane]; e < b1; e += 2) {
+                const int c0 = ct[e - off];
+                const int c1 = e + 1 < b1 ? ct[e + 1 - off] : -1;
+                const bool ok0 = c0 >= 0 && !ring.get(c0);
+                const bool ok1 = c1 >= 0 && !ring.get(c1);
+                if (ok0) { p = c0; break; }
+                if (ok1) { p = c1; break; }
+            }
+        }
+        const unsigned tl = (unsigned)(p - r0);   // < 32: the pick is a row of this tile
+        pm[lane] = 0u;
+        __syncwarp();
+        if (p >= 0 && tl < 32u) atomicOr(pm + tl, 1u << lane);
+        const unsigned same = __match_any_sync(0xffffffffu, p);
+        const unsigned has = __ballot_sync(0xffffffffu, p >= 0);
+        __syncwarp();
+        if (p >= 0) info[lane] = make_uint2(tl < 32u ? 1u << tl : 0u, same | pm[lane]);
+        else info[lane] = make_uint2(0u, 0u);
+        pk[lane] = p;
+        __syncwarp();
+        unsigned stale = 0u, done = 0u, racc = 0u, written = 0u;
+        while (todo) {
+            const int i = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            if ((stale >> i) & 1u) {
+                // the ring takes every pick of the tile so far, then row i scans again
+                const unsigned w = done & has & ~written;
+                if ((w >> lane) & 1u) { ring.set(r0 + lane); ring.set(p); }
+                written |= w;
+                __syncwarp();
+                const int b0 = it[i], b1 = it[i + 1];
+                int q = -1;
+                for (int e = b0; e < b1; e += 32) {
+                    const int c = e + lane < b1 ? ct[e + lane - off] : -1;
+                    const bool ok = c >= 0 && !ring.get(c);
+                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                    if (bal) {
+                        q = __shfl_sync(0xffffffffu, c, __ffs(bal) - 1);
+                        break;
+                    }
+                }
+                if (q >= 0) {
+                    if (lane == 0) { ring.set(r0 + i); ring.set(q); pk[i] = q; }
+                    racc |= 1u << i;
+                    const unsigned d = (unsigned)(q - r0);
+                    if (d < 32u) todo &= ~(1u << d);
+                    stale |= __ballot_sync(0xffffffffu, p == q || p == r0 + i);
+                }
+                __syncwarp();
+                continue;
+            }
+            const uint2 f = info[i];
+            done |= 1u << i;
+            todo &= ~f.x;
+            stale |= f.y;
+        }
+        const unsigned acc = (done & has) | racc;
+        const unsigned w = done & has & ~written;
+        if ((w >> lane) & 1u) { ring.set(r0 + lane); ring.set(p); }
+        if (lane == 0) accepted[t & 1] = acc;
+        __syncthreads();   // tile t walked; tile t + 1 staged
+    }
 }
 
 __global__ void k_flag_eq(int n, const int *__restrict__ v, int val, int *flag) {
@@ -411,15 +665,29 @@ __global__ void k_hem_final(int n, int *mask) {
 int hem_exact(int n, const int *nia, const int *nja, const double *nval,
               int *agg, int *nagg, int *work_n, cudaStream_t s) {
     int *out = nullptr;
-    HZB_TRY(dalloc(&out, 3));
-    HZB_CUDA(cudaMemsetAsync(out, 0, 3 * sizeof(int), s));
+    HZB_TRY(dalloc(&out, 4));
+    HZB_CUDA(cudaMemsetAsync(out, 0, 4 * sizeof(int), s));
     k_graph_bandwidth<<<grid_for(n), 256, 0, s>>>(n, nia, nja, out + 2);
     count_launch();
-    int bw = 0;
-    HZB_CUDA(cudaMemcpyAsync(&bw, out + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int gb[3] = {0, 0, 0};
+    HZB_CUDA(cudaMemcpyAsync(gb, out + 2, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    HZB_CUDA(cudaMemcpyAsync(gb + 2, nia + n, sizeof(int), cudaMemcpyDeviceToHost, s));
     HZB_CUDA(cudaStreamSynchronize(s));
+    const int bw = gb[0], maxlen = gb[1], gnnz = gb[2];
+    // Four implementations with the same decisions, the fastest that the
+    // graph allows: 1 ranked lists + byte ring, 2 ranked lists + bit ring,
+    // 3 bit ring over the raw rows, 4 state in global memory.  HZB_HEM_PATH
+    // names one (if the graph allows it) for tests of the others.
+    int path = 4;
+    if (2 * bw + 64 < (int)HemRing<true>::SIZE && maxlen <= HEM_RANK_MAXLEN) path = 1;
+    else if (2 * bw + 64 < HEM_RING_BITS && maxlen <= HEM_RANK_MAXLEN) path = 2;
+    else if (2 * bw + 2 < HEM_RING_BITS) path = 3;
+    if (const char *f = getenv("HZB_HEM_PATH")) {
+        const int want = atoi(f);
+        if (want >= path && want <= 4) path = want;
+    }
     int rc = SUCCESS;
-    if (2 * bw + 2 < HEM_RING_BITS) {
+    if (path <= 3) {
         int *flag = nullptr, *pos = nullptr, *list = nullptr, *tmp = nullptr;
         const int g = grid_for(n);
         static bool attr = false;
@@ -428,14 +696,38 @@ int hem_exact(int n, const int *nia, const int *nja, const double *nval,
                                  HEM_RING_WORDS * 4);
             attr = true;
         }
-        k_hem_init<<<g, 256, 0, s>>>(n, nia, agg, work_n);
-        k_hem_pass1_ring<<<1, 32, HEM_RING_WORDS * 4, s>>>(n, bw, nia, nja, nval, agg,
-                                                          work_n, out);
-        count_launch(2);
         if ((rc = dalloc(&flag, n)) || (rc = dalloc(&pos, n + 1)) || (rc = dalloc(&list, n)) ||
             (rc = dalloc(&tmp, scan_tmp_size(n + 1)))) {
             dfree(flag); dfree(pos); dfree(list); dfree(tmp); dfree(out);
             return rc;
+        }
+        k_hem_init<<<g, 256, 0, s>>>(n, nia, agg, work_n);
+        count_launch();
+        int *cand = nullptr;
+        if (path <= 2 && dalloc(&cand, std::max(1, gnnz)) == SUCCESS) {
+            static bool attr2 = false;
+            if (!attr2) {
+                cudaFuncSetAttribute(k_hem_pass1_staged<true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)HEM_STAGED_SMEM);
+                cudaFuncSetAttribute(k_hem_pass1_staged<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)HEM_STAGED_SMEM);
+                attr2 = true;
+            }
+            k_hem_rank<<<std::min(div_up(n, 8), 148 * 64), 256, 0, s>>>(n, nia, nja, nval, cand);
+            if (path == 1)
+                k_hem_pass1_staged<true><<<1, 64, HEM_STAGED_SMEM, s>>>(n, bw, nia, cand, agg,
+                                                                        work_n, out);
+            else
+                k_hem_pass1_staged<false><<<1, 64, HEM_STAGED_SMEM, s>>>(n, bw, nia, cand, agg,
+                                                                         work_n, out);
+            count_launch(2);
+            dfree(cand);
+        } else {
+            k_hem_pass1_ring<<<1, 32, HEM_RING_WORDS * 4, s>>>(n, bw, nia, nja, nval, agg,
+                                                              work_n, out);
+            count_launch();
         }
         k_flag_eq<<<g, 256, 0, s>>>(n, agg, -1, flag);
         count_launch();

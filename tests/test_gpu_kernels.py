@@ -92,6 +92,26 @@ def test_hem_random_vs_oracle(port, seed):
     assert nc == nc_o and np.array_equal(agg, agg_o)
 
 
+@pytest.mark.parametrize("path", [1, 2, 3, 4])
+def test_hem_implementations_agree(golden, port, monkeypatch, path):
+    # ranked lists + byte ring, ranked lists + bit ring, bit ring over the raw
+    # rows, state in global memory: the same aggregates as the reference
+    monkeypatch.setenv("HZB_HEM_PATH", str(path))
+    z = golden("small_cases.npz")
+    for case in ["aniso2d_31", "kuhn_12", "theta_p2d_40"]:
+        theta = float(z[f"{case}/dparams"][0])
+        nc, agg = _hem(z[f"{case}/A_ia"], z[f"{case}/A_ja"], z[f"{case}/A_val"], theta)
+        assert np.array_equal(agg, z[f"{case}/agg0"]), case
+        assert nc == int(z[f"{case}/info"][0][2])
+    k = P.lognormal_field(14, 1.0, 3.0, 7)
+    ia, ja, val = P.kuhn3d_p1(14, k)
+    rows = np.repeat(np.arange(len(ia) - 1), np.diff(ia))
+    val = val * (1.0 + 0.01 * ((rows + ja + path) % 3))   # symmetric ties and near-ties
+    nc, agg = _hem(ia, ja, val, 0.05)
+    nc_o, agg_o = port.hem(ia, ja, val, 0.05)
+    assert nc == nc_o and np.array_equal(agg, agg_o)
+
+
 def test_rap_bit_exact(golden):
     g = golden("rap.npz")
     A = DevCSR(g["ia"], g["ja"], g["val"])

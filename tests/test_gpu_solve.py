@@ -91,6 +91,17 @@ def test_fixture128_hierarchy_and_history(golden):
     S.close()
 
 
+@pytest.mark.parametrize("path", [2, 4])
+def test_c1_hierarchy_other_hem_paths(golden, monkeypatch, path):
+    monkeypatch.setenv("HZB_HEM_PATH", str(path))
+    g = golden("c1_poisson255.npz")
+    ia, ja, val = P.poisson2d_5pt(255)
+    S = hz.Solver()
+    assert S.setup_host(ia, ja, val) == 0, hz.last_error()
+    check_levels(S, g, full=False)
+    S.close()
+
+
 def test_c1_poisson255(golden):
     g = golden("c1_poisson255.npz")
     ia, ja, val = P.poisson2d_5pt(255)
