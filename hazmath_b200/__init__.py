@@ -166,6 +166,10 @@ def lib() -> C.CDLL:
                                      C.c_void_p]
         L.hzb_get_stats.argtypes = [C.c_void_p, P(hzb_stats)]
         L.hzb_destroy.argtypes = [C.c_void_p]
+        L.hzb_batch_setup_device.argtypes = [C.c_void_p, INT, P(INT), INT, INT, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
+        L.hzb_batch_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, P(INT),
+                                             P(REAL), P(REAL)]
         L.hzb_dcsr_aAxpy_device.argtypes = [REAL, INT, INT, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p]
         L.hzb_smoother_device.argtypes = [SHORT, SHORT, INT, REAL, INT, INT, C.c_void_p,
@@ -394,6 +398,28 @@ class Solver:
 
     def precond_device(self, r_ptr, z_ptr) -> int:
         return lib().hzb_precond_device(self.h, r_ptr, z_ptr)
+
+    def batch_setup_device(self, off, nnz, ia_ptr, ja_ptr, val_ptr) -> int:
+        """Hierarchy of the block-diagonal union of len(off) - 1 systems
+        (rows of system k: off[k] .. off[k+1]-1)."""
+        self._off = np.ascontiguousarray(off, np.int32)
+        ns = len(self._off) - 1
+        return lib().hzb_batch_setup_device(self.h, ns, self._off.ctypes.data_as(
+            C.POINTER(INT)), int(self._off[-1]), nnz, ia_ptr, ja_ptr, val_ptr)
+
+    def batch_solve_device(self, b_ptr, x_ptr):
+        """Per-system flexible CG: (return code, iterations, relative
+        residuals, seconds from the solve's start to each system's
+        convergence)."""
+        ns = len(self._off) - 1
+        its = np.zeros(ns, np.int32)
+        rel = np.zeros(ns)
+        sec = np.zeros(ns)
+        rc = lib().hzb_batch_solve_device(self.h, b_ptr, x_ptr,
+                                          its.ctypes.data_as(C.POINTER(INT)),
+                                          rel.ctypes.data_as(C.POINTER(REAL)),
+                                          sec.ctypes.data_as(C.POINTER(REAL)))
+        return rc, its, rel, sec
 
     def set_omega_device(self, omega_ptr) -> int:
         return lib().hzb_set_omega_device(self.h, omega_ptr)

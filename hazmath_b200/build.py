@@ -27,6 +27,7 @@ SOURCES = [
     ("hzb_setup.cu", False),
     ("hzb_dense.cu", True),
     ("hzb_solver.cu", False),
+    ("hzb_batch.cu", False),
     ("hzb_learn.cu", False),
     ("hzb_gnn.cu", True),
     ("hzb_api.cu", False),

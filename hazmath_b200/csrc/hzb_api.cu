@@ -283,6 +283,42 @@ extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
     return it;
 }
 
+extern "C" INT hzb_batch_setup_device(hzb_solver *S, INT nsys, const INT *off, INT n,
+                                      INT nnz, const INT *d_ia, const INT *d_ja,
+                                      const REAL *d_val) {
+    if (!S || n <= 0 || nnz <= 0) return ERROR_MAT_SIZE;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    S->host_ia = nullptr; S->host_ja = nullptr; S->host_val = nullptr;
+    HZB_CUDA(cudaEventRecord(S->e0, S->s));
+    HZB_TRY(hzb::batch_setup(S, nsys, off, n, nnz, d_ia, d_ja, d_val));
+    HZB_CUDA(cudaEventRecord(S->e1, S->s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S->e0, S->e1);
+    S->st.setup_seconds = ms * 1e-3;
+    return upload_omega(S);
+}
+
+extern "C" INT hzb_batch_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x,
+                                      INT *iters, REAL *relres, REAL *seconds) {
+    if (!S || S->nl == 0 || !S->batch) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    const long long l0 = hzb::launch_count();
+    HZB_CUDA(cudaEventRecord(S->e0, S->s));
+    const int it = hzb::batch_solve(S, d_b, d_x, S->it.linear_tol, S->it.linear_maxit, iters,
+                                    relres, seconds);
+    HZB_CUDA(cudaEventRecord(S->e1, S->s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S->e0, S->e1);
+    S->st.solve_seconds = ms * 1e-3;
+    S->st.iterations = it;
+    S->st.launches = (INT)(hzb::launch_count() - l0);
+    return it;
+}
+
 extern "C" INT hzb_solve_host(hzb_solver *S, const REAL *b, REAL *x) {
     if (!S || S->nl == 0) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);

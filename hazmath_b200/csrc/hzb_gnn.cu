@@ -740,19 +740,20 @@ extern "C" INT hzb_gnn_backward(hzb_gnn *G, hzb_solver *S, const float *d_domega
 }
 
 extern "C" INT hzb_learn_errors(hzb_solver *S, INT ns, unsigned long long seed, REAL *d_E,
-                                const float *d_omega) {
+                                const float *d_omega, INT ncycles) {
     if (!S) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
-    return learn_errors(S, ns, seed, d_E, d_omega);
+    return learn_errors(S, ns, seed, d_E, d_omega, ncycles);
 }
 
 extern "C" INT hzb_learn_loss_grad(hzb_solver *S, const float *d_omega, INT ns,
-                                   const REAL *d_E, REAL *loss, float *d_domega) {
+                                   const REAL *d_E, INT ncycles, REAL *loss,
+                                   float *d_domega) {
     if (!S) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
-    return learn_loss_grad(S, d_omega, ns, d_E, loss, d_domega);
+    return learn_loss_grad(S, d_omega, ns, d_E, ncycles, loss, d_domega);
 }
 
 // Infer omega for the solver's fine level, measure the two-cycle contraction
@@ -779,10 +780,10 @@ extern "C" INT hzb_learn_select_omega(hzb_solver *S, hzb_gnn *G, INT ns,
     int rc = dalloc(&dom, n);
     // each cycle is measured on the errors it leaves itself (its slowest modes)
     double lp = 0.0, ll = 0.0;
-    if (!rc) rc = learn_errors(S, ns, seed, E, nullptr);
-    if (!rc) rc = learn_loss_grad(S, nullptr, ns, E, &lp, dom);
-    if (!rc) rc = learn_errors(S, ns, seed, E, S->omega);
-    if (!rc) rc = learn_loss_grad(S, S->omega, ns, E, &ll, dom);
+    if (!rc) rc = learn_errors(S, ns, seed, E, nullptr, 2);
+    if (!rc) rc = learn_loss_grad(S, nullptr, ns, E, 2, &lp, dom);
+    if (!rc) rc = learn_errors(S, ns, seed, E, S->omega, 2);
+    if (!rc) rc = learn_loss_grad(S, S->omega, ns, E, 2, &ll, dom);
     dfree(E);
     dfree(dom);
     if (rc) return rc;

@@ -17,6 +17,7 @@
 // Everything runs in FP64 on the solver's stream with the cycle kernels.
 #include <cmath>
 #include "hzb_solver.cuh"
+#include <vector>
 
 namespace hzb {
 
@@ -83,14 +84,18 @@ __global__ void k_to_float(int n, const double *__restrict__ d, double f, float 
         out[i] = (float)(d[i] * f);
 }
 
+constexpr int LEARN_MAX_CYCLES = 16;
+
 struct LearnWork {
     int n = 0;
     double *r = nullptr, *t = nullptr, *g = nullptr, *l1 = nullptr, *e = nullptr;
-    double *dom = nullptr, *Ae[8] = {nullptr}, *sc = nullptr, *part = nullptr;
-    int alloc(int nn) {
+    double *dom = nullptr, *sc = nullptr, *part = nullptr;
+    std::vector<double *> Ae;   // A e before each of the 4 sweeps of every cycle
+    int alloc(int nn, int ncyc = 0) {
         n = nn;
         HZB_TRY(dalloc(&r, n)); HZB_TRY(dalloc(&t, n)); HZB_TRY(dalloc(&g, n));
         HZB_TRY(dalloc(&l1, n)); HZB_TRY(dalloc(&e, n)); HZB_TRY(dalloc(&dom, n));
+        Ae.assign(4 * (size_t)ncyc, nullptr);
         for (auto &p : Ae) HZB_TRY(dalloc(&p, n));
         HZB_TRY(dalloc(&sc, 8));
         HZB_TRY(dalloc(&part, reduce_blocks(n) + 8));
@@ -157,7 +162,8 @@ static int need_levels(hzb_solver *S) {
 // omega == nullptr: errors of the plain cycle; otherwise the two V-cycles
 // use omega on the fine level (the errors the learned cycle leaves).
 int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
-                 const float *omega) {
+                 const float *omega, int ncyc) {
+    if (ncyc < 0 || ncyc > LEARN_MAX_CYCLES) return ERROR_INPUT_PAR;
     HZB_TRY(need_levels(S));
     Level &L0 = S->lv[0];
     const int n = L0.n;
@@ -183,7 +189,7 @@ int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
             k_err_sweep<<<g, 256, 0, s>>>(n, nullptr, w.l1, w.r, e);
             count_launch();
         }
-        for (int it = 0; it < 2 && !rc; ++it) {   // two plain cycles: e <- e - B A e
+        for (int it = 0; it < ncyc && !rc; ++it) {   // cycles: e <- e - B A e
             rc = spmv<double>(L0.A64(), SPMV_Y, e, nullptr, w.g, 1.0, nullptr, s);
             if (!rc) rc = precond64(S, w.g, w.t, cyc);
             if (!rc) {
@@ -204,8 +210,9 @@ int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
     return rc;
 }
 
-int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
+int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, int ncyc,
                     double *loss, float *domega) {
+    if (ncyc < 1 || ncyc > LEARN_MAX_CYCLES) return ERROR_INPUT_PAR;
     HZB_TRY(need_levels(S));
     Level &L0 = S->lv[0];
     const int n = L0.n;
@@ -213,7 +220,7 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
     cudaStream_t s = S->s;
     const int g = grid_for(n);
     LearnWork w;
-    HZB_TRY(w.alloc(n));
+    HZB_TRY(w.alloc(n, ncyc));
     HZB_TRY(l1_norms<double>(A, w.l1, s));
     HZB_TRY(vzero<double>(n, w.dom, s));
     double total = 0.0;
@@ -221,7 +228,7 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
         HZB_TRY(vcopy<double>(n, E + (size_t)k * n, w.e, s));
         HZB_TRY(anorm2(S, w, w.e, w.sc + 0));          // ||e||_A^2
         int q = 0;
-        for (int cyc = 0; cyc < 2; ++cyc) {            // forward, storing A e_in
+        for (int cyc = 0; cyc < ncyc; ++cyc) {         // forward, storing A e_in
             for (int j = 0; j < 2; ++j, ++q) {
                 HZB_TRY(spmv<double>(A, SPMV_Y, w.e, nullptr, w.Ae[q], 1.0, nullptr, s));
                 k_err_sweep<<<g, 256, 0, s>>>(n, omega, w.l1, w.Ae[q], w.e);
@@ -234,11 +241,11 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
                 count_launch();
             }
         }
-        HZB_TRY(anorm2(S, w, w.e, w.sc + 1));          // ||E^2 e||_A^2, A e in w.r
+        HZB_TRY(anorm2(S, w, w.e, w.sc + 1));          // ||E^k e||_A^2, A e in w.r
         HZB_TRY(vcopy<double>(n, w.r, w.g, s));        // g = 2 A e / ||e0||_A^2
         k_scale_by<<<g, 256, 0, s>>>(n, w.sc + 0, 2.0, w.g);
         count_launch();
-        for (int cyc = 1; cyc >= 0; --cyc) {           // backward
+        for (int cyc = ncyc - 1; cyc >= 0; --cyc) {    // backward
             for (int j = 0; j < 2; ++j) {
                 --q;
                 k_err_sweep_adj<<<g, 256, 0, s>>>(n, omega, w.l1, w.Ae[q], w.g, w.t, w.dom);

@@ -961,6 +961,7 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
 }
 
 void destroy(hzb_solver *S) {
+    batch_release(S);
     S->g64.release();
     S->g32.release();
     for (auto &L : S->lv) L.release();

@@ -81,6 +81,8 @@ struct GraphCache {
     }
 };
 
+struct Batch;   // packed independent systems (hzb_batch.cu)
+
 // Host-side preconditioner callback used when a foreign pc->fct is given.
 struct HostPrecond {
     void (*fct)(double *, double *, void *) = nullptr;
@@ -111,6 +113,7 @@ struct hzb_solver {
     const int *host_ja = nullptr;
     const double *host_val = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    hzb::Batch *batch = nullptr;      // set by batch_setup
 };
 
 namespace hzb {
@@ -132,12 +135,18 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
 int ensure_fp32(hzb_solver *S);
 // learned-weight loss (hzb_learn.cu)
 int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
-                 const float *omega);
-int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E,
+                 const float *omega, int ncyc);
+int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, int ncyc,
                     double *loss, float *domega);
 // smoothing of level l as mgcycle's pre (pre = true) / post smoothing calls
 int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc);
 // diagonals and sweep schedules the configured smoother needs on level L
 int level_smoother_data(hzb_solver *S, Level &L);
 void destroy(hzb_solver *S);
+// batched independent systems (hzb_batch.cu): off[nsys + 1] host row offsets
+int batch_setup(hzb_solver *S, int nsys, const int *off, int n, int nnz, const int *d_ia,
+                const int *d_ja, const double *d_val);
+int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit,
+                int *h_iters, double *h_relres, double *h_seconds);
+void batch_release(hzb_solver *S);
 }  // namespace hzb

@@ -214,3 +214,44 @@ def read_coo(path: str):
     ia = np.zeros(m + 1, np.int64)
     np.add.at(ia, i + 1, 1)
     return np.cumsum(ia).astype(np.int32), j[order].copy(), v[order].copy()
+
+
+def batch_anisotropic(nsys: int = 512, seed: int = 11, dof_lo: int = 1000,
+                      dof_hi: int = 200000):
+    """nsys independent SPD systems: 2D or 3D (equal odds) P1 anisotropic
+    diffusion on structured meshes, epsilon uniform in [1e-3, 1], angle
+    uniform in [0, pi) (3D: about a random axis), dofs log-uniform in
+    [dof_lo, dof_hi], one uniform random right-hand side each.  Returns the
+    list of (ia, ja, val, b) and their block-diagonal union
+    (off, ia, ja, val, b), off[k] the first row of system k."""
+    rng = np.random.default_rng(seed)
+    systems = []
+    for _ in range(nsys):
+        d = float(np.exp(rng.uniform(np.log(dof_lo), np.log(dof_hi))))
+        eps = float(rng.uniform(1e-3, 1.0))
+        theta = float(rng.uniform(0.0, np.pi))
+        if rng.uniform() < 0.5:
+            ia, ja, val = aniso2d_p1(max(2, int(round(np.sqrt(d)))), eps, theta)
+        else:
+            axis = rng.normal(size=3)
+            ia, ja, val = aniso3d_p1(max(2, int(round(np.cbrt(d)))), eps, theta, axis)
+        b = rng.uniform(-1.0, 1.0, len(ia) - 1)
+        systems.append((ia, ja, val, b))
+    off = np.zeros(nsys + 1, np.int64)
+    eo = np.zeros(nsys + 1, np.int64)
+    for k, (ia, ja, val, b) in enumerate(systems):
+        off[k + 1] = off[k] + len(ia) - 1
+        eo[k + 1] = eo[k] + ia[-1]
+    n, nnz = int(off[-1]), int(eo[-1])
+    uia = np.empty(n + 1, np.int64)
+    uja = np.empty(nnz, np.int32)
+    uval = np.empty(nnz)
+    ub = np.empty(n)
+    for k, (ia, ja, val, b) in enumerate(systems):
+        r0, r1, e0, e1 = off[k], off[k + 1], eo[k], eo[k + 1]
+        uia[r0:r1] = ia[:-1] + e0
+        uja[e0:e1] = ja + r0
+        uval[e0:e1] = val
+        ub[r0:r1] = b
+    uia[n] = nnz
+    return systems, (off.astype(np.int32), uia.astype(np.int32), uja, uval, ub)

@@ -397,6 +397,26 @@ INT  hzb_solve_device(hzb_solver *s, const REAL *d_b, REAL *d_x);
 INT  hzb_solve_host(hzb_solver *s, const REAL *b, REAL *x);
 /* one preconditioner application z = B r on device vectors */
 INT  hzb_precond_device(hzb_solver *s, const REAL *d_r, REAL *d_z);
+/* Batched independent systems (no counterpart in the reference, whose
+ * solvers take one system per call).  The device CSR (n rows, nnz entries)
+ * holds nsys SPD systems on its diagonal blocks: rows and columns of system
+ * k are [off[k], off[k+1]) (host array, off[0] = 0, off[nsys] = n); an entry
+ * outside its row's block is rejected (ERROR_INPUT_PAR).  One hierarchy is
+ * built on the union -- aggregates never cross systems, so each system's
+ * block of every level is a hierarchy of that system -- and one V-cycle
+ * pass serves all systems.  The handle's hzb_param.precision picks the
+ * cycle (HZB_PREC_MIXED: FP32).                                            */
+INT  hzb_batch_setup_device(hzb_solver *s, INT nsys, const INT *off, INT n, INT nnz,
+                            const INT *d_ia, const INT *d_ja, const REAL *d_val);
+/* Flexible CG per system to the handle's linear_tol (relative residual,
+ * the true FP64 residual checked before a system is retired) and
+ * linear_maxit.  Per system (host arrays of nsys, any may be NULL): the
+ * iterations (ERROR_SOLVER_MAXIT if not converged), the final relative
+ * residual, and the device time in seconds from the solve's start until the
+ * system converged.  Returns the largest iteration count, or
+ * ERROR_SOLVER_MAXIT if a system did not converge.                        */
+INT  hzb_batch_solve_device(hzb_solver *s, const REAL *d_b, REAL *d_x, INT *iters,
+                            REAL *relres, REAL *seconds);
 /* per-row l1-Jacobi weights for the fine level (device array, n) */
 INT  hzb_set_omega_device(hzb_solver *s, const float *d_omega);
 INT  hzb_get_stats(const hzb_solver *s, hzb_stats *st);
@@ -429,14 +449,18 @@ INT  hzb_gnn_infer(hzb_gnn *g, hzb_solver *s, float *d_omega);
 /* accumulate parameter gradients for dL/domega (device array, n) */
 INT  hzb_gnn_backward(hzb_gnn *g, hzb_solver *s, const float *d_domega);
 /* ns training error vectors (device, n x ns, FP64): seeded random vectors
- * after three plain l1 sweeps and two V-cycles, unit A-norm; the cycles use
- * the fine-level weights d_omega (device, n) or plain weights if NULL */
+ * after three plain l1 sweeps and ncycles (0..16) V-cycles, unit A-norm; the
+ * cycles use the fine-level weights d_omega (device, n) or plain weights if
+ * NULL.  ncycles = 0 gives vectors that do not depend on omega.            */
 INT  hzb_learn_errors(hzb_solver *s, INT ns, unsigned long long seed, REAL *d_E,
-                      const float *d_omega);
-/* mean over the ns vectors of ||E(omega)^2 e||_A^2 / ||e||_A^2 for the V(2,2)
- * l1-Jacobi cycle with fine-level weights omega, and its gradient */
+                      const float *d_omega, INT ncycles);
+/* mean over the ns vectors of ||E(omega)^k e||_A^2 / ||e||_A^2, k = ncycles
+ * (1..16), for the V(2,2) l1-Jacobi cycle with fine-level weights omega, and
+ * its gradient (adjoint cycles).  Training minimises the two-cycle
+ * contraction of the errors the current cycle leaves, (||E^4 z||/||E^2 z||)^2
+ * for omega-independent z, through the k = 4 and k = 2 gradients.          */
 INT  hzb_learn_loss_grad(hzb_solver *s, const float *d_omega, INT ns,
-                         const REAL *d_E, REAL *loss, float *d_domega);
+                         const REAL *d_E, INT ncycles, REAL *loss, float *d_domega);
 /* Set up the learned weights on a solver with fallback: infer omega, measure
  * the per-cycle contraction with and without it on ns method-generated
  * error vectors, keep omega only if it contracts better.  Both contractions

@@ -183,20 +183,20 @@ class Port(_Backend):
         self.lib.or_gnn_backward(_p(prm), _p(d), _p(g))
         return g
 
-    def learn_errors(self, ns, seed, omega=None):
+    def learn_errors(self, ns, seed, omega=None, ncycles=2):
         n = self.level_info(0)[0]
         E = np.empty((ns, n))
         om = None if omega is None else np.ascontiguousarray(omega, np.float32)
         self.lib.or_learn_errors(ns, C.c_ulonglong(seed), _p(E),
-                                 None if om is None else _p(om))
+                                 None if om is None else _p(om), ncycles)
         return E
 
-    def learn_loss_grad(self, omega, E):
+    def learn_loss_grad(self, omega, E, ncycles=2):
         om = np.ascontiguousarray(omega, np.float32)
         E = np.ascontiguousarray(E, np.float64)
         d = np.empty(E.shape[1])
         self.lib.or_learn_loss_grad.restype = C.c_double
-        loss = self.lib.or_learn_loss_grad(_p(om), E.shape[0], _p(E), _p(d))
+        loss = self.lib.or_learn_loss_grad(_p(om), E.shape[0], _p(E), ncycles, _p(d))
         return loss, d
 
     # -- kernels -----------------------------------------------------------

@@ -6,7 +6,7 @@
  *    CUDA library, restated sequentially in FP32 with BF16 rounding at the
  *    same points (stored activations, dense-layer inputs and weights);
  *  - or_learn_errors / or_learn_loss_grad: the method-generated training
- *    errors and the two-cycle A-norm contraction loss with its adjoint
+ *    errors and the ncyc-cycle A-norm contraction loss with its adjoint
  *    gradient, in FP64 on the oracle hierarchy built by or_setup (l1-Jacobi
  *    smoother), so the GPU gradients can be checked here and by finite
  *    differences.
@@ -306,9 +306,11 @@ static void l1n(int n, const int *ia, const double *a, double *l1)
 
 void or_set_omega(const float *omega);
 
-/* omega == NULL: the plain cycle's errors; otherwise the two cycles use
- * omega on the fine level */
-void or_learn_errors(int ns, unsigned long long seed, double *E, const float *omega)
+/* seeded random vectors after three plain l1 sweeps and ncyc V-cycles, unit
+ * A-norm; the cycles use omega on the fine level (NULL: plain weights).
+ * ncyc = 0 gives vectors that do not depend on omega. */
+void or_learn_errors(int ns, unsigned long long seed, double *E, const float *omega,
+                     int ncyc)
 {
     or_set_omega(omega);
     int n, nc;
@@ -326,7 +328,7 @@ void or_learn_errors(int ns, unsigned long long seed, double *E, const float *om
             mxv(n, ia, ja, a, e, r);
             for (int i = 0; i < n; ++i) e[i] -= (1.0 / l1[i]) * r[i];
         }
-        for (int it = 0; it < 2; ++it) {
+        for (int it = 0; it < ncyc; ++it) {
             mxv(n, ia, ja, a, e, r);
             or_precond(r, t);
             for (int i = 0; i < n; ++i) e[i] -= t[i];
@@ -339,7 +341,8 @@ void or_learn_errors(int ns, unsigned long long seed, double *E, const float *om
     free(l1); free(r); free(t);
 }
 
-double or_learn_loss_grad(const float *omega, int ns, const double *E, double *domega)
+double or_learn_loss_grad(const float *omega, int ns, const double *E, int ncyc,
+                          double *domega)
 {
     int n, nc;
     const int *ia, *ja, *agg, *ria, *rja;
@@ -350,7 +353,7 @@ double or_learn_loss_grad(const float *omega, int ns, const double *E, double *d
     double *r = (double *)malloc(sizeof(double) * n);
     double *g = (double *)malloc(sizeof(double) * n);
     double *t = (double *)malloc(sizeof(double) * n);
-    double *Ae = (double *)malloc(sizeof(double) * 8 * (size_t)n);
+    double *Ae = (double *)malloc(sizeof(double) * 4 * (size_t)ncyc * (size_t)n);
     l1n(n, ia, a, l1);
     memset(domega, 0, sizeof(double) * n);
     double total = 0.0;
@@ -359,7 +362,7 @@ double or_learn_loss_grad(const float *omega, int ns, const double *E, double *d
         mxv(n, ia, ja, a, e, r);
         double n0 = dotp(n, e, r);
         int q = 0;
-        for (int c = 0; c < 2; ++c) {
+        for (int c = 0; c < ncyc; ++c) {
             for (int j = 0; j < 2; ++j, ++q) {
                 mxv(n, ia, ja, a, e, Ae + (size_t)q * n);
                 for (int i = 0; i < n; ++i) e[i] -= ((double)omega[i] / l1[i]) * Ae[(size_t)q * n + i];
@@ -375,7 +378,7 @@ double or_learn_loss_grad(const float *omega, int ns, const double *E, double *d
         double n1 = dotp(n, e, r);
         total += n1 / n0;
         for (int i = 0; i < n; ++i) g[i] = r[i] * (2.0 / n0);
-        for (int c = 1; c >= 0; --c) {
+        for (int c = ncyc - 1; c >= 0; --c) {
             for (int j = 0; j < 2; ++j) {
                 --q;
                 for (int i = 0; i < n; ++i) {

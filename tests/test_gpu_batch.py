@@ -1,0 +1,119 @@
+"""Batched independent systems (hzb_batch_setup_device / hzb_batch_solve_device):
+every system reaches its own tolerance on its own true FP64 residual, each
+system's answer is the one an independent solve gives, one system alone
+takes the single-system path's iterations, and an entry that couples two
+systems is rejected."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import hazmath_b200 as hz
+from hazmath_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _amg():
+    return hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+
+
+def _it(tol=1e-8):
+    return hz.itsolver_param(linear_itsolver_type=hz.SOLVER_CG, linear_precond_type=hz.PREC_AMG,
+                             linear_tol=tol, linear_maxit=400, linear_stop_type=hz.STOP_REL_RES)
+
+
+def _solver(prec=None):
+    prec = hz.HZB_PREC_MIXED if prec is None else prec
+    return hz.Solver(_amg(), _it(), hz.b200_param(precision=prec,
+                                                  matching=hz.HZB_MATCH_PARALLEL))
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _batch_solve(union, prec=None):
+    off, ia, ja, val, b = union
+    S = _solver(prec)
+    dia, dja, dval, db = _dev(ia), _dev(ja), _dev(val), _dev(b)
+    rc = S.batch_setup_device(off, int(ia[-1]), dia.data_ptr(), dja.data_ptr(), dval.data_ptr())
+    assert rc == 0, hz.last_error()
+    dx = torch.zeros_like(db)
+    rc, its, rel, sec = S.batch_solve_device(db.data_ptr(), dx.data_ptr())
+    st = S.stats()
+    S.close()
+    return rc, its, rel, sec, dx.cpu().numpy(), st
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_batch_each_system_converges(prec):
+    systems, union = P.batch_anisotropic(24, seed=3, dof_lo=500, dof_hi=30000)
+    p = hz.HZB_PREC_MIXED if prec == "mixed" else hz.HZB_PREC_FP64
+    rc, its, rel, sec, x, st = _batch_solve(union, p)
+    assert rc == its.max() > 0, (rc, hz.last_error())
+    off = union[0]
+    for k, (ia, ja, val, b) in enumerate(systems):
+        A = sp.csr_matrix((val, ja, ia))
+        xk = x[off[k]:off[k + 1]]
+        true_rel = np.linalg.norm(b - A @ xk) / np.linalg.norm(b)
+        assert true_rel < 1e-8, (k, true_rel)
+        assert rel[k] == pytest.approx(true_rel, rel=1e-3, abs=1e-14)
+        assert 0 < its[k] <= its.max()
+    assert np.all(sec > 0) and sec.max() <= st.solve_seconds * 1.01
+    # a system that needs more iterations finishes no earlier
+    order = np.argsort(its, kind="stable")
+    assert sec[order[-1]] >= sec[order[0]]
+
+
+def test_batch_matches_independent_solves():
+    systems, union = P.batch_anisotropic(6, seed=5, dof_lo=2000, dof_hi=20000)
+    rc, its, rel, sec, x, _ = _batch_solve(union)
+    assert rc > 0, hz.last_error()
+    off = union[0]
+    for k, (ia, ja, val, b) in enumerate(systems):
+        S = _solver()
+        xs = np.zeros(len(b))
+        assert S.setup_host(ia, ja, val) == 0
+        it1 = S.solve_host(b, xs)
+        S.close()
+        assert it1 > 0
+        A = sp.csr_matrix((val, ja, ia))
+        xk = x[off[k]:off[k + 1]]
+        # both are 1e-8 residual solutions of the same system
+        err = np.linalg.norm(xk - xs) / np.linalg.norm(xs)
+        assert err < 1e-5, (k, err)
+        # the union's hierarchy is deeper for a small system (coarsening runs
+        # until the whole union is small), which costs iterations, not accuracy
+        assert its[k] <= 2 * it1 + 10, (k, its[k], it1)
+
+
+def test_single_system_batch_is_the_single_system_solve():
+    k = P.lognormal_field(24, 1.0, 4.0, 9)
+    ia, ja, val = P.kuhn3d_p1(24, k)
+    b = P.rhs_uniform(len(ia) - 1, 4)
+    off = np.array([0, len(b)], np.int32)
+    rc, its, rel, sec, x, _ = _batch_solve((off, ia, ja, val, b))
+    S = _solver()
+    xs = np.zeros(len(b))
+    assert S.setup_host(ia, ja, val) == 0
+    it1 = S.solve_host(b, xs)
+    S.close()
+    # same hierarchy and cycle; only the inner-product summation order differs
+    assert abs(int(its[0]) - it1) <= 1
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-6
+
+
+def test_batch_rejects_coupled_systems():
+    systems, union = P.batch_anisotropic(3, seed=7, dof_lo=500, dof_hi=2000)
+    off, ia, ja, val, b = union
+    ja = ja.copy()
+    r = off[1]                       # first row of system 1 points into system 0
+    ja[ia[r]] = 0
+    S = _solver()
+    dia, dja, dval = _dev(ia), _dev(ja), _dev(val)
+    rc = S.batch_setup_device(off, int(ia[-1]), dia.data_ptr(), dja.data_ptr(),
+                              dval.data_ptr())
+    S.close()
+    assert rc == hz.ERROR_INPUT_PAR

@@ -80,20 +80,21 @@ def test_untrained_network_is_plain_l1(problem):
     S.close()
 
 
-def test_errors_and_loss_gradient_vs_oracle(problem):
+@pytest.mark.parametrize("cyc_err,cyc_loss", [(2, 2), (0, 4), (0, 1)])
+def test_errors_and_loss_gradient_vs_oracle(problem, cyc_err, cyc_loss):
     ia, ja, val = problem
     n = len(ia) - 1
     S = solver_for(ia, ja, val)
     port = oracle_for(ia, ja, val)
     ns = 3
     E = dev(np.zeros((ns, n)))
-    learn.errors(S, ns, 11, E.data_ptr())
-    Eo = port.learn_errors(ns, 11)
+    learn.errors(S, ns, 11, E.data_ptr(), None, cyc_err)
+    Eo = port.learn_errors(ns, 11, None, cyc_err)
     assert np.linalg.norm(host(E) - Eo) / np.linalg.norm(Eo) < 1e-8
     om = (1.0 + 0.3 * np.random.default_rng(7).uniform(-1, 1, n)).astype(np.float32)
     dom = dev(np.zeros(n, np.float32))
-    loss = learn.loss_grad(S, dev(om).data_ptr(), E.data_ptr(), ns, dom.data_ptr())
-    lo, do = port.learn_loss_grad(om, host(E))
+    loss = learn.loss_grad(S, dev(om).data_ptr(), E.data_ptr(), ns, dom.data_ptr(), cyc_loss)
+    lo, do = port.learn_loss_grad(om, host(E), cyc_loss)
     assert abs(loss - lo) <= 1e-8 * lo
     d = host(dom).astype(np.float64)
     assert np.linalg.norm(d - do) / np.linalg.norm(do) < 1e-6   # FP32 output of FP64 sums
