@@ -1,26 +1,36 @@
-"""Benchmark: UA-AMG-PCG time to a 1e-8 FP64 relative residual on B200.
+"""Benchmark: UA-AMG-PCG time to a 1e-8 FP64 relative residual on B200,
+mixed precision + learned smoother weights against the plain FP64 drop-in.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload c2|c1|c5]
+                    [--workload c5|c2|c1|c3] [--no-cpu-baseline]
 
-Workload (default c2): 3D P1 diffusion -div(k grad u) = f on the Kuhn
-tetrahedral mesh of 128^3 cubes (127^3 = 2,048,383 dofs, 30,340,171 stored
-entries of the 15-point pattern), k = exp(g) per cube with g a unit-variance
-Gaussian field of correlation length 8 cubes (seed 2), b ~ U[-1,1] (seed 3),
-x0 = 0.  Synthetic, seeded inputs of the configuration's shapes.
+Workload c5 (default): 3D P1 diffusion -div(k grad u) = f on the Kuhn
+tetrahedral mesh of 256^3 cubes (255^3 = 16,581,375 dofs, 247,163,083 stored
+entries of the 15-point pattern), k = exp(1.5 g) per cube with g a
+unit-variance Gaussian field of correlation length 8 cubes (seed 7),
+b ~ U[-1,1] (seed 8), x0 = 0.  c2 is the 128^3 instance (sigma 1, seeds
+2/3), c1 the 2D 255^2 Poisson problem.  Synthetic, seeded inputs of the
+configurations' shapes.
 
-One step = one UA-AMG-PCG solve of that system from x0 = 0 to 1e-8 FP64
-relative residual, setup (aggregation + Galerkin products + coarse
-factorisation) included: the time a user pays for one call.  `value` is that
-time with the matrix and vectors resident in HBM (FP32 V-cycle inside FP64
-flexible CG, the mixed form); `e2e` is the same solve through the drop-in C
-entry point with host arrays (copies included).  The plain FP64 drop-in is
-timed beside it (`plain_fp64_*`), and the level SpMV is timed on its own for
-the roofline.  The stored matrix (364 MB) exceeds the 126 MB L2, so no
-explicit flush is needed between steps.
+One step = one solve of that system from x0 = 0 to 1e-8 FP64 relative
+residual as a user pays for it: UA-AMG setup (parallel matching, Galerkin
+products, coarse factorisation), the learned weights (network inference
+and the measured-contraction fallback check), and flexible CG with the FP32
+V-cycle (l1-Jacobi V(2,2)).  `value` is that time with the inputs resident
+in HBM; `e2e` is the same through the handle API with host arrays (matrix
+and vectors copied in, the solution copied out, all inside the timed
+region).  The plain FP64 drop-in (exact HEM, FP64 cycle, same smoother) is
+timed beside it (`plain_fp64`).  The stored matrix (2.97 GB) is far larger
+than the 126 MB L2, so no flush is needed between steps.
+
+Workload c3: 512 independent SPD systems (2D/3D anisotropic P1 diffusion,
+1k-200k dofs log-uniform, seed 11) solved together (hzb_batch_*); one step
+= batch setup + batch solve; reports the batch time and the p50/p99 of the
+per-system solve times.
 
 --impl reference times the reference HAZmath implementation (compiled from
-its sources, single-threaded C) on the same workload and settings.
+its own C sources, single-threaded -- the reference has no threading) on a
+bounded sample of the same workload, scaled to it by the dof count.
 Multi-GPU: the path does not shard; N ranks run N independent replicas.
 """
 from __future__ import annotations
@@ -43,6 +53,20 @@ from hazmath_b200 import problems as P  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
+METRIC = "AMG-PCG time to 1e-8 FP64 residual: mixed+learned vs plain on B200; SpMV GB/s"
+
+
+def kuhn_case(N: int, sigma: float, seeds):
+    k = P.lognormal_field(N, sigma, 8.0, seeds[0])
+    ia, ja, val = P.kuhn3d_p1(N, k)
+    b = P.rhs_uniform(len(ia) - 1, seeds[1])
+    desc = {"workload": f"3D P1 log-normal diffusion, Kuhn mesh {N}^3 cubes "
+                        f"(sigma={sigma}, corr 8 cubes)",
+            "dofs": int(len(b)), "nnz": int(ia[-1])}
+    return ia, ja, val, b, desc
+
+
+CASES = {"c5": (256, 1.5, (7, 8)), "c2": (128, 1.0, (2, 3))}
 
 
 def workload(name: str):
@@ -52,14 +76,21 @@ def workload(name: str):
         desc = {"workload": "2D P1 Poisson 257^2 vertices (255^2 dofs, 5-pt)",
                 "dofs": int(len(b)), "nnz": int(ia[-1])}
         return ia, ja, val, b, desc
-    N, sigma, seeds = (128, 1.0, (2, 3)) if name == "c2" else (256, 1.5, (7, 8))
-    k = P.lognormal_field(N, sigma, 8.0, seeds[0])
-    ia, ja, val = P.kuhn3d_p1(N, k)
-    b = P.rhs_uniform(len(ia) - 1, seeds[1])
-    desc = {"workload": f"3D P1 log-normal diffusion, Kuhn mesh {N}^3 cubes "
-                        f"(sigma={sigma}, corr 8 cubes)",
-            "dofs": int(len(b)), "nnz": int(ia[-1])}
-    return ia, ja, val, b, desc
+    return kuhn_case(*CASES[name])
+
+
+def cpu_sample(name: str):
+    """The bounded CPU sample of a workload and its scale to the full one:
+    the 128^3 instance of the same family for c5 (about 30 s single-threaded),
+    the workload itself otherwise."""
+    if name == "c5":
+        N, sigma, seeds = CASES["c5"]
+        ia, ja, val, b, _ = kuhn_case(128, sigma, seeds)
+        return ia, ja, val, b, 16581375 / (len(ia) - 1), \
+            "reference setup+solve of the 128^3-cube instance of the same family " \
+            "(2,048,383 dofs, sigma 1.5, seeds 7/8), scaled by the dof ratio 8.095"
+    ia, ja, val, b, _ = workload(name)
+    return ia, ja, val, b, 1.0, "reference setup+solve of the full workload"
 
 
 class Clocks:
@@ -111,39 +142,80 @@ def amg_l1(hz):
     return hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
 
 
-def itparam(hz):
+def itparam(hz, maxit=500):
     return hz.itsolver_param(linear_itsolver_type=hz.SOLVER_CG,
                              linear_precond_type=hz.PREC_AMG, linear_tol=1e-8,
-                             linear_maxit=500, linear_stop_type=hz.STOP_REL_RES)
+                             linear_maxit=maxit, linear_stop_type=hz.STOP_REL_RES)
 
 
-def run_reference(args, ia, ja, val, b, desc):
+def time_reference(ia, ja, val, b):
+    """One setup + PCG solve by the reference compiled from its sources (the
+    C restatement if the reference library is absent), single-threaded."""
     import oracle
     kind = "reference" if oracle.ref_available() else "port"
     R = oracle.ref() if kind == "reference" else oracle.port()
     prm = oracle.AMGParams(smoother=10, presmooth_iter=2, postsmooth_iter=2)
-    times, iters = [], 0
-    for step in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        assert R.setup(ia, ja, val, prm) == 0
-        iters, x, _ = R.pcg(b, None, 1e-8, 500, 1)
-        t = time.perf_counter() - t0
-        if step >= args.warmup:
-            times.append(t)
+    t0 = time.perf_counter()
+    assert R.setup(ia, ja, val, prm) == 0
+    it, _, _ = R.pcg(b, None, 1e-8, 500, 1)
+    t = time.perf_counter() - t0
     R.free()
+    return t, int(it), kind
+
+
+def run_reference(args):
+    name = args.workload
+    if name == "c3":
+        systems, _ = P.batch_anisotropic(512, 11)
+        rng = np.random.default_rng(5)
+        pick = sorted(rng.choice(len(systems), 24, replace=False))
+        total = sum(len(s[3]) for s in systems)
+        sample = sum(len(systems[k][3]) for k in pick)
+        scale = total / sample
+        what = (f"reference setup+solve of 24 of the 512 systems one after another "
+                f"({sample} of {total} dofs), scaled by the dof ratio {scale:.2f}")
+        warm = [systems[pick[0]]]
+        work = [systems[k] for k in pick]
+    else:
+        ia, ja, val, b, scale, what = cpu_sample(name)
+        wia, wja, wval, wb, _ = kuhn_case(48, 1.0, (2, 3))
+        warm = [(wia, wja, wval, wb)]
+        work = [(ia, ja, val, b)]
+    times, iters, kind = [], 0, "reference"
+    for step in range(args.warmup + args.steps):
+        # warm-up steps run the same code on a small instance (untimed)
+        batch = warm if step < args.warmup else work
+        t = 0.0
+        for (ia, ja, val, b) in batch:
+            dt, iters, kind = time_reference(ia, ja, val, b)
+            t += dt
+        if step >= args.warmup:
+            times.append(t * scale)
     v = statistics.mean(times)
-    line = {"metric": "AMG-PCG time to 1e-8 FP64 relative residual (setup + solve)",
+    desc = workload_desc(name)
+    line = {"metric": METRIC if name != "c3" else "batched UA-AMG-PCG: 512 systems, batch time",
             "value": v, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "iterations": int(iters),
-            "config": dict(desc, smoother="l1-Jacobi x2, V(2,2), HEM, coarse direct",
+            "config": dict(desc, smoother="l1-Jacobi V(2,2), HEM, coarse direct, FP64 CG",
                            parallelism="replicas", l2="inputs larger than L2"),
             "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": kind,
-                             "sample": "full workload, one solve per step, 1 thread"},
+                             "sample": what},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def workload_desc(name):
+    if name == "c3":
+        return {"workload": "512 independent 2D/3D anisotropic P1 diffusion systems, "
+                            "1k-200k dofs log-uniform (seed 11)"}
+    if name == "c1":
+        return {"workload": "2D P1 Poisson 257^2 vertices (255^2 dofs, 5-pt)"}
+    N, sigma, _ = CASES[name]
+    return {"workload": f"3D P1 log-normal diffusion, Kuhn mesh {N}^3 cubes "
+                        f"(sigma={sigma}, corr 8 cubes)"}
 
 
 def main():
@@ -152,7 +224,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c5"])
+    ap.add_argument("--workload", default="c5", choices=["c1", "c2", "c5", "c3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -162,21 +234,41 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        ia, ja, val, b, desc = workload(args.workload)
-        run_reference(args, ia, ja, val, b, desc)
+        if rank == 0:
+            run_reference(args)
         return
 
     import torch
-    import hazmath_b200 as hz
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.workload == "c3":
+            run_batch(args, rank, world, local, dist)
+        else:
+            run_single(args, rank, world, local, dist)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
 
+
+def max_over_ranks(dist, v, dev):
+    if not dist:
+        return v
+    import torch
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_single(args, rank, world, local, dist):
+    import torch
+    import hazmath_b200 as hz
+    from hazmath_b200 import learn
     ia, ja, val, b, desc = workload(args.workload)
     n, nnz = len(b), int(ia[-1])
     dev = f"cuda:{local}"
@@ -187,133 +279,273 @@ def main():
     bp_mixed = hz.b200_param(precision=hz.HZB_PREC_MIXED, matching=hz.HZB_MATCH_PARALLEL,
                              device=local)
     bp_plain = hz.b200_param(device=local)
+    gnn = learn.GNN(device=local, weights=learn.WEIGHTS)
+    NS_SELECT = 2
 
-    def solve_once(S):
+    def check(rc, what):
+        if rc < 0:
+            raise RuntimeError(f"{what} failed {rc}: {hz.last_error()}")
+        return rc
+
+    def step(S, learned):
+        """setup + (learned weights with fallback) + solve; device seconds
+        of each part from the handle's events and a sync around the check"""
         dx.zero_()
-        rc = S.setup_device(n, nnz, p(dia), p(dja), p(dval))
-        if rc:
-            raise RuntimeError(f"setup failed {rc}: {hz.last_error()}")
-        it = S.solve_device(p(db), p(dx))
-        if it < 0:
-            raise RuntimeError(f"solve failed {it}: {hz.last_error()}")
-        return it
+        check(S.setup_device(n, nnz, p(dia), p(dja), p(dval)), "setup")
+        sel = None
+        if learned:
+            t0 = time.perf_counter()
+            rp, rl, used = gnn.select(S, NS_SELECT, 99)
+            sel = {"rho_plain": rp, "rho_learned": rl, "learned_used": used,
+                   "select_s": time.perf_counter() - t0}
+        it = check(S.solve_device(p(db), p(dx)), "solve")
+        return it, sel
 
     S = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
     for _ in range(args.warmup):
-        solve_once(S)
+        step(S, True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    setup_s, solve_s, launches, iters = [], [], 0, 0
+    setup_s, solve_s, select_s, launches, iters, sel = [], [], [], 0, 0, None
+    torch.cuda.profiler.start()
     ev0.record()
     for _ in range(args.steps):
-        iters = solve_once(S)
+        iters, sel = step(S, True)
         st = S.stats()
         setup_s.append(st.setup_seconds)
         solve_s.append(st.solve_seconds)
+        select_s.append(sel["select_s"])
         launches += st.launches
     ev1.record()
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     clk = clocks.stop()
-    total_ms = ev0.elapsed_time(ev1)
-    step_s = total_ms * 1e-3 / args.steps
-    if dist:
-        t = torch.tensor([step_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_s = float(t.item())
+    step_s = max_over_ranks(dist, ev0.elapsed_time(ev1) * 1e-3 / args.steps, dev)
     x = dx.cpu().numpy()
     import scipy.sparse as sp
     A = sp.csr_matrix((val, ja, ia), shape=(n, n))
     relres = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
 
+    # the mixed cycle with plain weights, for the learned part's share
+    Sp = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
+    step(Sp, False)
+    it_mp = step(Sp, False)[0]
+    st_mp = Sp.stats()
+
     # plain FP64 drop-in (exact HEM, FP64 V-cycle, same smoother) beside it
     S64 = hz.Solver(amg_l1(hz), itparam(hz), bp_plain)
-    solve_once(S64)
-    it64 = solve_once(S64)
+    step(S64, False)
+    it64 = step(S64, False)[0]
     st64 = S64.stats()
     x64 = dx.cpu().numpy()
     err_vs_fp64 = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
+    total64 = st64.setup_seconds + st64.solve_seconds
 
-    # roofline: level-0 SpMV (FP64 drop-in operator) and FP32 l1 sweep
+    # roofline: level-0 SpMV of the FP64 drop-in (the level SpMV the target
+    # names), 50 launches on the solver's stream with CUDA events
     peak, peak_kind = hbm_peak()
     ms, by = C.c_double(), C.c_double()
-    assert hz.lib().hzb_time_kernel(S64.h, 0, 0, 50, C.byref(ms), C.byref(by)) == 0
+    check(hz.lib().hzb_time_kernel(S64.h, hz.HZB_K_SPMV64, 0, 50, C.byref(ms), C.byref(by)),
+          "time_kernel")
     spmv64_gbs = by.value / (ms.value * 1e-3) / 1e9
-    spmv64_ms = ms.value
-    spmv64_bytes = by.value
-    assert hz.lib().hzb_time_kernel(S.h, 3, 0, 50, C.byref(ms), C.byref(by)) == 0
+    spmv64 = (ms.value, by.value)
+    check(hz.lib().hzb_time_kernel(S.h, hz.HZB_K_L1_32, 0, 50, C.byref(ms), C.byref(by)),
+          "time_kernel")
     l1_32_gbs = by.value / (ms.value * 1e-3) / 1e9
+    check(hz.lib().hzb_time_kernel(S.h, hz.HZB_K_SPMV32, 0, 50, C.byref(ms), C.byref(by)),
+          "time_kernel")
+    spmv32_gbs = by.value / (ms.value * 1e-3) / 1e9
 
-    # e2e: the drop-in C entry point with host arrays (mixed form)
+    # e2e: the handle API with host arrays (copies in and out inside the region)
+    Se = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
+    xh = np.zeros(n)
     e2e = []
-    xb = np.zeros(n)
-    amg = amg_l1(hz)
     for k in range(1 + min(args.steps, 3)):
-        xb[:] = 0.0
-        amg.strong_coupled = 0.0
+        xh[:] = 0.0
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rc = hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, xb, itparam(hz), amg, bp_mixed)
+        check(Se.setup_host(ia, ja, val), "setup_host")
+        gnn.select(Se, NS_SELECT, 99)
+        check(Se.solve_host(b, xh), "solve_host")
         t = time.perf_counter() - t0
-        assert rc > 0, (rc, hz.last_error())
         if k:
             e2e.append(t)
-    e2e_s = statistics.mean(e2e)
+    e2e_s = max_over_ranks(dist, statistics.mean(e2e), dev)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        import oracle
-        kind = "reference" if oracle.ref_available() else "port"
-        R = oracle.ref() if kind == "reference" else oracle.port()
-        prm = oracle.AMGParams(smoother=10, presmooth_iter=2, postsmooth_iter=2)
-        t0 = time.perf_counter()
-        R.setup(ia, ja, val, prm)
-        it_ref, _, _ = R.pcg(b, None, 1e-8, 500, 1)
-        cpu_t = time.perf_counter() - t0
-        R.free()
-        cpu = {"value": cpu_t, "unit": "s", "cores": 1, "kind": kind,
-               "sample": "one full setup+solve of the workload, single thread",
-               "iterations": int(it_ref)}
+        sia, sja, sval, sb, scale, what = cpu_sample(args.workload)
+        t, it_ref, kind = time_reference(sia, sja, sval, sb)
+        cpu = {"value": t * scale, "unit": "s", "cores": 1, "kind": kind, "sample": what,
+               "sample_seconds": t, "sample_iterations": it_ref}
 
     if rank == 0:
+        solve_ml = statistics.mean(solve_s)
         line = {
-            "metric": "AMG-PCG time to 1e-8 FP64 relative residual (setup + solve)",
-            "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32-cycle/f64-outer",
-            "data": "synthetic",
-            "config": dict(desc, solver="UA-AMG (HEM, parallel matching) V(2,2) l1-Jacobi, "
-                           "FP32 cycle in FP64 flexible CG", parallelism="replicas",
+            "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-cycle/f64-outer", "data": "synthetic",
+            "config": dict(desc, solver="UA-AMG (parallel matching) V(2,2) l1-Jacobi with "
+                           "learned weights (fallback to plain), FP32 cycle in FP64 "
+                           "flexible CG", parallelism="replicas",
                            l2="inputs larger than L2 (no flush)"),
             "iterations": int(iters), "final_relres": relres,
-            "setup_s": statistics.mean(setup_s), "solve_s": statistics.mean(solve_s),
-            "dof_per_s": n / statistics.mean(solve_s),
+            "setup_s": statistics.mean(setup_s), "learned_select_s": statistics.mean(select_s),
+            "solve_s": solve_ml, "dof_per_s": n / solve_ml,
+            "learned": dict(sel, ns=NS_SELECT),
+            "mixed_plain_weights": {"iterations": int(it_mp), "solve_s": st_mp.solve_seconds},
             "plain_fp64": {"iterations": int(it64), "setup_s": st64.setup_seconds,
-                           "solve_s": st64.solve_seconds,
-                           "total_s": st64.setup_seconds + st64.solve_seconds},
-            "speedup_solve_vs_plain": st64.solve_seconds / statistics.mean(solve_s),
+                           "solve_s": st64.solve_seconds, "total_s": total64},
+            "speedup_vs_plain": total64 / step_s,
+            "speedup_solve_vs_plain": st64.solve_seconds / solve_ml,
             "err_vs_fp64": err_vs_fp64,
-            "roofline": {"bound": "hbm", "kernel": "level-0 SpMV FP64 (row bundles)",
-                         "achieved": spmv64_gbs, "peak": peak, "unit": "GB/s",
-                         "frac": spmv64_gbs / peak, "peak_kind": peak_kind,
-                         "bytes_per_launch": spmv64_bytes, "ms_per_launch": spmv64_ms,
-                         "traffic": None},
-            "l1_sweep_fp32_gbs": l1_32_gbs,
+            "roofline": {"bound": "hbm", "kernel": "level-0 SpMV FP64 of the drop-in "
+                         "(k_spmv_bundle<double>)", "achieved": spmv64_gbs, "peak": peak,
+                         "unit": "GB/s", "frac": spmv64_gbs / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": spmv64[1], "ms_per_launch": spmv64[0],
+                         "traffic": TRAFFIC.get(args.workload)},
+            "l1_sweep_fp32_gbs": l1_32_gbs, "spmv_fp32_gbs": spmv32_gbs,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s",
                     "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + val.nbytes + b.nbytes
-                                              + xb.nbytes),
-                    "d2h_bytes_per_step": int(xb.nbytes)},
+                                              + xh.nbytes),
+                    "d2h_bytes_per_step": int(xh.nbytes)},
             "gpu_launches": int(launches),
             "clocks": clk,
         }
         print(json.dumps(line))
-    S.close()
-    S64.close()
+    for h in (S, Sp, S64, Se):
+        h.close()
+    gnn.close()
+
+
+# DRAM bytes read + written per launch of the roofline kernel, from ncu
+# (profiles/spmv64_level0.md): captured on the c2 case and scaled by the
+# stored entries for c5.
+TRAFFIC = {}
+
+
+def run_batch(args, rank, world, local, dist):
+    import torch
+    import hazmath_b200 as hz
+    systems, (off, ia, ja, val, b) = P.batch_anisotropic(512, 11)
+    n, nnz = len(b), int(ia[-1])
+    dev = f"cuda:{local}"
+    dia, dja = torch.from_numpy(ia).to(dev), torch.from_numpy(ja).to(dev)
+    dval, db = torch.from_numpy(val).to(dev), torch.from_numpy(b).to(dev)
+    dx = torch.zeros_like(db)
+    p = lambda t: t.data_ptr()  # noqa: E731
+    bp = hz.b200_param(precision=hz.HZB_PREC_MIXED, matching=hz.HZB_MATCH_PARALLEL,
+                       device=local)
+    S = hz.Solver(amg_l1(hz), itparam(hz, 1000), bp)
+
+    def step():
+        dx.zero_()
+        rc = S.batch_setup_device(off, nnz, p(dia), p(dja), p(dval))
+        if rc:
+            raise RuntimeError(f"batch setup {rc}: {hz.last_error()}")
+        su = S.stats().setup_seconds
+        rc, its, rel, sec = S.batch_solve_device(p(db), p(dx))
+        if rc < 0:
+            raise RuntimeError(f"batch solve {rc}: {hz.last_error()}")
+        return su, S.stats().solve_seconds, its, rel, sec
+
+    for _ in range(args.warmup):
+        step()
     if dist:
         dist.barrier()
-        dist.destroy_process_group()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = []
+    launches = 0
+    torch.cuda.profiler.start()
+    ev0.record()
+    for _ in range(args.steps):
+        res.append(step())
+        launches += S.stats().launches
+    ev1.record()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    clk = clocks.stop()
+    step_s = max_over_ranks(dist, ev0.elapsed_time(ev1) * 1e-3 / args.steps, dev)
+    su, so, its, rel, sec = res[-1]
+    x = dx.cpu().numpy()
+    import scipy.sparse as sp
+    worst = 0.0
+    for k, (sia, sja, sval, sb) in enumerate(systems):
+        A = sp.csr_matrix((sval, sja, sia))
+        xk = x[off[k]:off[k + 1]]
+        worst = max(worst, float(np.linalg.norm(sb - A @ xk) / np.linalg.norm(sb)))
+    peak, peak_kind = hbm_peak()
+    ms, by = C.c_double(), C.c_double()
+    rc = hz.lib().hzb_time_kernel(S.h, hz.HZB_K_L1_32, 0, 50, C.byref(ms), C.byref(by))
+    l1_gbs = by.value / (ms.value * 1e-3) / 1e9 if rc == 0 else None
+    rc = hz.lib().hzb_time_kernel(S.h, hz.HZB_K_SPMV64, 0, 50, C.byref(ms), C.byref(by))
+    spmv_gbs = by.value / (ms.value * 1e-3) / 1e9 if rc == 0 else None
+    # e2e through the API with host arrays: upload, batch setup + solve, download
+    e2e = []
+    xh = np.zeros(n)
+    for k in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tia, tja = torch.from_numpy(ia).to(dev), torch.from_numpy(ja).to(dev)
+        tval, tb = torch.from_numpy(val).to(dev), torch.from_numpy(b).to(dev)
+        tx = torch.zeros_like(tb)
+        S.batch_setup_device(off, nnz, p(tia), p(tja), p(tval))
+        S.batch_solve_device(p(tb), p(tx))
+        xh[:] = tx.cpu().numpy()
+        e2e.append(time.perf_counter() - t0)
+        del tia, tja, tval, tb, tx
+    e2e_s = max_over_ranks(dist, e2e[-1], dev)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        rng = np.random.default_rng(5)
+        pick = sorted(rng.choice(len(systems), 24, replace=False))
+        t, kind = 0.0, "reference"
+        for k in pick:
+            dt, _, kind = time_reference(*systems[k])
+            t += dt
+        sample = sum(len(systems[k][3]) for k in pick)
+        scale = n / sample
+        cpu = {"value": t * scale, "unit": "s", "cores": 1, "kind": kind,
+               "sample": f"reference setup+solve of 24 of the 512 systems one after another "
+                         f"({sample} of {n} dofs, {t:.1f} s), scaled by the dof ratio "
+                         f"{scale:.2f}"}
+    if rank == 0:
+        line = {
+            "metric": "batched UA-AMG-PCG: 512 systems, batch time", "value": step_s,
+            "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-cycle/f64-outer", "data": "synthetic",
+            "config": dict(workload_desc("c3"), systems=len(systems), dofs=n, nnz=nnz,
+                           solver="one union hierarchy (parallel matching), per-system "
+                           "flexible CG, FP32 V(2,2) l1-Jacobi", parallelism="replicas",
+                           l2="inputs larger than L2 (no flush)"),
+            "setup_s": su, "solve_s": so,
+            "per_system_solve_s": {"p50": float(np.percentile(sec, 50)),
+                                   "p99": float(np.percentile(sec, 99)),
+                                   "max": float(sec.max())},
+            "iterations": {"p50": float(np.percentile(its, 50)),
+                           "p99": float(np.percentile(its, 99)), "max": int(its.max())},
+            "worst_true_relres": worst,
+            "roofline": {"bound": "hbm", "kernel": "level-0 FP32 l1-Jacobi sweep of the union",
+                         "achieved": l1_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": (l1_gbs / peak) if l1_gbs else None, "peak_kind": peak_kind,
+                         "traffic": None},
+            "spmv_fp64_gbs": spmv_gbs,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s",
+                    "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + val.nbytes + b.nbytes),
+                    "d2h_bytes_per_step": int(xh.nbytes)},
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line))
+    S.close()
 
 
 if __name__ == "__main__":

@@ -51,6 +51,8 @@ SMOOTHER_L1DIAG = 10
 HZB_PREC_FP64, HZB_PREC_MIXED = 0, 1
 HZB_GS_EXACT, HZB_GS_MULTICOLOR = 0, 1
 HZB_MATCH_EXACT, HZB_MATCH_PARALLEL = 0, 1
+# kernels hzb_time_kernel can time
+HZB_K_SPMV64, HZB_K_SPMV32, HZB_K_RES64, HZB_K_L1_32, HZB_K_L1_64 = 0, 1, 2, 3, 4
 MAX_AMG_LVL = 20
 
 
@@ -166,6 +168,7 @@ def lib() -> C.CDLL:
                                      C.c_void_p]
         L.hzb_get_stats.argtypes = [C.c_void_p, P(hzb_stats)]
         L.hzb_destroy.argtypes = [C.c_void_p]
+        L.hzb_time_kernel.argtypes = [C.c_void_p, INT, INT, INT, P(REAL), P(REAL)]
         L.hzb_batch_setup_device.argtypes = [C.c_void_p, INT, P(INT), INT, INT, C.c_void_p,
                                              C.c_void_p, C.c_void_p]
         L.hzb_batch_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, P(INT),

@@ -265,6 +265,9 @@ __global__ void k_gnn_input(int n, const float *__restrict__ feats,
     }
 }
 
+// Warp per row, lane = channel.  The row's edges are loaded one per lane
+// (features computed once per edge), then broadcast four at a time so four
+// neighbour rows of P are gathered together; the sum runs in CSR order.
 __global__ void k_gnn_message(int n, const int *__restrict__ ia, const int *__restrict__ ja,
                               const double *__restrict__ a, const double *__restrict__ diag,
                               const bf16 *__restrict__ P, const float *__restrict__ lay,
@@ -277,14 +280,41 @@ __global__ void k_gnn_message(int n, const int *__restrict__ ia, const int *__re
         float s = 0.f;
         int deg = 0;
         const double aii = diag[i];
-        for (int k = ia[i]; k < ia[i + 1]; ++k) {
-            const int j = ja[k];
-            if (j == i) continue;
-            float e0, e1;
-            edge_feat(a[k], aii, diag[j], e0, e1);
-            const float q = __bfloat162float(P[(size_t)j * 32 + lane]) + v0 * e0 + v1 * e1 + c;
-            s += fmaxf(q, 0.f);
-            ++deg;
+        const int b1 = ia[i + 1];
+        for (int base = ia[i]; base < b1; base += 32) {
+            const int k = base + lane;
+            int j = -1;
+            float e0 = 0.f, e1 = 0.f;
+            if (k < b1) {
+                j = ja[k];
+                if (j != i) edge_feat(a[k], aii, diag[j], e0, e1);
+                else j = -1;
+            }
+            unsigned m = __ballot_sync(0xffffffffu, j >= 0);
+            deg += __popc(m);
+            while (m) {
+                int src[4], jj[4];
+                int cnt = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    src[u] = m ? __ffs(m) - 1 : 0;
+                    cnt += m != 0u;
+                    m &= m - 1u;
+                }
+                float q[4], f0[4], f1[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    jj[u] = __shfl_sync(0xffffffffu, j, src[u]);
+                    f0[u] = __shfl_sync(0xffffffffu, e0, src[u]);
+                    f1[u] = __shfl_sync(0xffffffffu, e1, src[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    q[u] = u < cnt ? __bfloat162float(P[(size_t)jj[u] * 32 + lane]) : 0.f;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (u < cnt) s += fmaxf(q[u] + v0 * f0[u] + v1 * f1[u] + c, 0.f);
+            }
         }
         M[(size_t)i * 32 + lane] = __float2bfloat16_rn(deg ? s / deg : 0.f);
     }
@@ -757,9 +787,10 @@ extern "C" INT hzb_learn_loss_grad(hzb_solver *S, const float *d_omega, INT ns,
 }
 
 // Infer omega for the solver's fine level, measure the two-cycle contraction
-// with and without it on ns method-generated error vectors, and keep the
-// learned weights only if they contract better (plain l1-Jacobi otherwise).
-// Contractions are reported per cycle: (||E^2 e||_A / ||e||_A)^(1/2).
+// of the solve's own cycle with and without it on ns method-generated error
+// vectors, and keep the learned weights only if they contract better (plain
+// l1-Jacobi otherwise).  Contractions are reported per cycle:
+// (||E^2 e||_A / ||e||_A)^(1/2).
 extern "C" INT hzb_learn_select_omega(hzb_solver *S, hzb_gnn *G, INT ns,
                                       unsigned long long seed, REAL *rho_plain,
                                       REAL *rho_learned) {
@@ -774,23 +805,15 @@ extern "C" INT hzb_learn_select_omega(hzb_solver *S, hzb_gnn *G, INT ns,
         HZB_TRY(gnn_forward(G, S->lv[0], S->omega));
         HZB_CUDA(cudaStreamSynchronize(G->s));
     }
-    double *E = nullptr;
-    float *dom = nullptr;
-    HZB_TRY(dalloc(&E, (size_t)n * ns));
-    int rc = dalloc(&dom, n);
-    // each cycle is measured on the errors it leaves itself (its slowest modes)
+    // each cycle -- the one the solve runs -- is measured on the errors it
+    // leaves itself (its slowest modes), from the same seeded vectors
     double lp = 0.0, ll = 0.0;
-    if (!rc) rc = learn_errors(S, ns, seed, E, nullptr, 2);
-    if (!rc) rc = learn_loss_grad(S, nullptr, ns, E, 2, &lp, dom);
-    if (!rc) rc = learn_errors(S, ns, seed, E, S->omega, 2);
-    if (!rc) rc = learn_loss_grad(S, S->omega, ns, E, 2, &ll, dom);
-    dfree(E);
-    dfree(dom);
-    if (rc) return rc;
+    S->omega_active = false;
+    HZB_TRY(cycle_contraction(S, ns, seed, &lp));
+    S->omega_active = true;
+    HZB_TRY(cycle_contraction(S, ns, seed, &ll));
     const double rp = std::pow(std::max(lp, 0.0), 0.25), rl = std::pow(std::max(ll, 0.0), 0.25);
     S->omega_active = rl < rp;
-    S->g64.release();
-    S->g32.release();
     S->st.omega_contraction[0] = rp;
     S->st.omega_contraction[1] = rl;
     S->st.omega_used = S->omega_active ? 1 : 0;

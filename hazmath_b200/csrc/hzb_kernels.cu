@@ -5,8 +5,11 @@
 // one thread; coalescing comes from staging each row bundle's entries in
 // shared memory (the CSR-stream schedule), not from splitting rows.
 #include "hzb_kernels.cuh"
+#include <algorithm>
 #include <cstdio>
+#include <map>
 #include <mutex>
+#include <utility>
 
 namespace hzb {
 
@@ -115,31 +118,109 @@ inline bool bundle_aligned(const DCsr<T> &A) {
     return ((reinterpret_cast<uintptr_t>(A.val) | reinterpret_cast<uintptr_t>(A.ja)) & 15) == 0;
 }
 
-// Stage entries [s, e) into sv/sc at offsets k - s0, s0 = s rounded down to
-// a multiple of 4 (so that both T and int loads are 16-byte aligned).
+// One bundle's shared-memory stage: values, column indices and row pointers.
+template <typename T>
+__host__ __device__ inline size_t bundle_stage_bytes(int cap, int rows) {
+    return (bundle_smem<T>(cap) + ((size_t)rows + 4) * sizeof(int) + 15) & ~(size_t)15;
+}
+
+__device__ __forceinline__ void cp_async16(unsigned dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(unsigned dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Issue (without waiting) the copies of a bundle of rows [r0, r1) with
+// entries [s, e) into a stage: values/columns at offsets k - s0, s0 = s
+// rounded down to 4 entries (16 bytes for both), and ia[r0..r1].  The
+// 16-byte body goes as 16-byte copies, the ragged end element by element, so
+// nothing outside the arrays is read (their bases are 16-byte aligned).
 template <typename T, int NT>
-__device__ __forceinline__ int stage_bundle(const T *__restrict__ val, const int *__restrict__ ja,
-                                            int s, int e, T *sv, int *sc) {
+__device__ __forceinline__ int issue_bundle(const int *__restrict__ ia, const T *__restrict__ val,
+                                            const int *__restrict__ ja, int r0, int r1, int s,
+                                            int e, T *sv, int *sc, int *sia) {
     const int s0 = s & ~3;
-    const int ev = e & ~3;               // end of the vector part
+    const int ev = e & ~3;
     const int nvec = ev > s0 ? (ev - s0) >> 2 : 0;
-    if (sizeof(T) == 8) {
-        const double2 *v2 = reinterpret_cast<const double2 *>(val + s0);
-        double2 *d2 = reinterpret_cast<double2 *>(sv);
-        for (int q = threadIdx.x; q < 2 * nvec; q += NT) d2[q] = __ldcs(v2 + q);
-    } else {
-        const float4 *v4 = reinterpret_cast<const float4 *>(val + s0);
-        float4 *d4 = reinterpret_cast<float4 *>(sv);
-        for (int q = threadIdx.x; q < nvec; q += NT) d4[q] = __ldcs(v4 + q);
-    }
-    const int4 *j4 = reinterpret_cast<const int4 *>(ja + s0);
-    int4 *c4 = reinterpret_cast<int4 *>(sc);
-    for (int q = threadIdx.x; q < nvec; q += NT) c4[q] = __ldcs(j4 + q);
+    const unsigned dv = (unsigned)__cvta_generic_to_shared(sv);
+    const unsigned dc = (unsigned)__cvta_generic_to_shared(sc);
+    const unsigned di = (unsigned)__cvta_generic_to_shared(sia);
+    const int nv = sizeof(T) == 8 ? 2 * nvec : nvec;
+    const char *gv = reinterpret_cast<const char *>(val + s0);
+    const char *gc = reinterpret_cast<const char *>(ja + s0);
+    for (int q = threadIdx.x; q < nv; q += NT) cp_async16(dv + 16u * q, gv + 16 * (size_t)q);
+    for (int q = threadIdx.x; q < nvec; q += NT) cp_async16(dc + 16u * q, gc + 16 * (size_t)q);
     for (int k = max(ev, s0) + threadIdx.x; k < e; k += NT) {
-        sv[k - s0] = val[k];
-        sc[k - s0] = ja[k];
+        cp_async_small<sizeof(T)>(dv + (unsigned)((k - s0) * sizeof(T)), val + k);
+        cp_async_small<4>(dc + 4u * (k - s0), ja + k);
     }
+    for (int q = threadIdx.x; q <= r1 - r0; q += NT) cp_async_small<4>(di + 4u * q, ia + r0 + q);
     return s0;
+}
+
+// Persistent bundle loop: CTA c works on bundles c, c + grid, ...; while it
+// computes one bundle the copies of its next are in flight (two stages).
+// body(bundle, r0, r1, s0, sv, sc, sia) runs between two __syncthreads.
+template <typename T, int ROWS, typename F>
+__device__ __forceinline__ void bundle_pipeline(int n, const int *__restrict__ ia,
+                                                const T *__restrict__ val,
+                                                const int *__restrict__ ja, int cap,
+                                                unsigned char *smem, F body) {
+    const int nb = (n + ROWS - 1) / ROWS;
+    const size_t stage = bundle_stage_bytes<T>(cap, ROWS);
+    const size_t off_c = bundle_sc_offset<T>(cap), off_i = bundle_smem<T>(cap);
+    auto SV = [&](int k) { return reinterpret_cast<T *>(smem + k * stage); };
+    auto SC = [&](int k) { return reinterpret_cast<int *>(smem + k * stage + off_c); };
+    auto SI = [&](int k) { return reinterpret_cast<int *>(smem + k * stage + off_i); };
+    int bid = blockIdx.x;
+    if (bid >= nb) return;
+    int r0 = bid * ROWS, r1 = min(r0 + ROWS, n);
+    int s0 = issue_bundle<T, ROWS>(ia, val, ja, r0, r1, __ldg(ia + r0), __ldg(ia + r1), SV(0),
+                                   SC(0), SI(0));
+    cp_async_commit();
+    // entry range of the next bundle, loaded one bundle ahead
+    int nxt = bid + gridDim.x;
+    int ns = 0, ne = 0;
+    if (nxt < nb) {
+        ns = __ldg(ia + nxt * ROWS);
+        ne = __ldg(ia + min(nxt * ROWS + ROWS, n));
+    }
+    for (int it = 0; bid < nb; ++it) {
+        const int st = it & 1;
+        int s0n = 0, r0n = 0, r1n = 0;
+        if (nxt < nb) {
+            r0n = nxt * ROWS;
+            r1n = min(r0n + ROWS, n);
+            s0n = issue_bundle<T, ROWS>(ia, val, ja, r0n, r1n, ns, ne, SV(st ^ 1), SC(st ^ 1),
+                                        SI(st ^ 1));
+        }
+        cp_async_commit();
+        const int after = nxt + gridDim.x;
+        if (after < nb) {
+            ns = __ldg(ia + after * ROWS);
+            ne = __ldg(ia + min(after * ROWS + ROWS, n));
+        }
+        cp_async_wait<1>();   // this bundle's copies have landed
+        __syncthreads();
+        body(bid, r0, r1, s0, SV(st), SC(st), SI(st));
+        __syncthreads();      // the stage is free for the bundle after next
+        bid = nxt;
+        nxt = after;
+        r0 = r0n;
+        r1 = r1n;
+        s0 = s0n;
+    }
+    cp_async_wait<0>();
 }
 
 template <typename T, int MODE>
@@ -162,26 +243,23 @@ k_spmv_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
               const T *__restrict__ b, T *__restrict__ y, T alpha,
               T *__restrict__ part, int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sv = reinterpret_cast<T *>(smem_raw);
-    int *sc = reinterpret_cast<int *>(smem_raw + bundle_sc_offset<T>(cap));
-    const int r0 = blockIdx.x * ROWS;
-    const int r1 = min(r0 + ROWS, n);
-    const int s = __ldg(ia + r0), e = __ldg(ia + r1);
-    const int s0 = stage_bundle<T, ROWS>(val, ja, s, e, sv, sc);
-    __syncthreads();
-    const int row = r0 + threadIdx.x;
-    T t = T(0), prod = T(0);
-    if (row < r1) {
-        const int b0 = __ldg(ia + row) - s0, b1 = __ldg(ia + row + 1) - s0;
-        for (int k = b0; k < b1; ++k) t += sv[k] * __ldg(x + sc[k]);
-        spmv_store<T, MODE>(row, t, b, y, alpha);
-        if (MODE == SPMV_Y_DOT) prod = t * __ldg(x + row);
-    }
-    if (MODE == SPMV_Y_DOT) {
-        __shared__ T sh[32];
-        prod = block_sum(prod, sh);
-        if (threadIdx.x == 0) part[blockIdx.x] = prod;
-    }
+    __shared__ T sh[32];
+    bundle_pipeline<T, ROWS>(n, ia, val, ja, cap, smem_raw,
+                             [&](int bundle, int r0, int r1, int s0, const T *sv, const int *sc,
+                                 const int *sia) {
+        const int row = r0 + threadIdx.x;
+        T t = T(0), prod = T(0);
+        if (row < r1) {
+            const int b0 = sia[threadIdx.x] - s0, b1 = sia[threadIdx.x + 1] - s0;
+            for (int k = b0; k < b1; ++k) t += sv[k] * __ldg(x + sc[k]);
+            spmv_store<T, MODE>(row, t, b, y, alpha);
+            if (MODE == SPMV_Y_DOT) prod = t * __ldg(x + row);
+        }
+        if (MODE == SPMV_Y_DOT) {
+            prod = block_sum(prod, sh);
+            if (threadIdx.x == 0) part[bundle] = prod;
+        }
+    });
 }
 
 // Rows too long for the staged bundle: one thread per row from global memory.
@@ -209,23 +287,48 @@ k_spmv_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
 int spmv_blocks(int n) { return div_up(n > 0 ? n : 1, SPMV_ROWS); }
 int spmv_blocks_rows(int n, int rows) { return div_up(n > 0 ? n : 1, rows > 0 ? rows : SPMV_ROWS); }
 
+// Grid of a persistent bundle kernel: as many CTAs as fit on all SMs at
+// once (at most one per bundle).
+template <typename K>
+static int persistent_grid(K kernel, int threads, size_t smem, int nbundles) {
+    static thread_local std::map<std::pair<const void *, size_t>, int> cache;
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), smem);
+    auto it = cache.find(key);
+    int per_sm = 0;
+    if (it != cache.end()) {
+        per_sm = it->second;
+    } else {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+            cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        cache[key] = per_sm;
+    }
+    return std::max(1, std::min(nbundles, per_sm * sm_count()));
+}
+
+template <typename T>
+static bool staged_ok(const DCsr<T> &A, int rows, size_t *smem) {
+    *smem = 2 * bundle_stage_bytes<T>(A.bundle_cap, rows);
+    return A.bundle_cap > 0 && *smem <= SPMV_SMEM_MAX && bundle_aligned(A);
+}
+
 template <typename T, int MODE, int ROWS>
 static int spmv_launch(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, T *part,
                        cudaStream_t s) {
-    const int grid = div_up(A.n, ROWS);
-    const size_t smem = bundle_smem<T>(A.bundle_cap);
-    if (A.bundle_cap > 0 && smem <= SPMV_SMEM_MAX && bundle_aligned(A)) {
-        if (smem > 48 * 1024) {
-            static bool done = false;   // per instantiation: raise the limit once
-            if (!done) {
-                cudaFuncSetAttribute(k_spmv_bundle<T, MODE, ROWS>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
-                done = true;
-            }
+    const int nb = div_up(A.n, ROWS);
+    size_t smem = 0;
+    if (staged_ok(A, ROWS, &smem)) {
+        static bool done = false;   // per instantiation: raise the limit once
+        if (!done) {
+            cudaFuncSetAttribute(k_spmv_bundle<T, MODE, ROWS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
+            done = true;
         }
+        const int grid = persistent_grid(k_spmv_bundle<T, MODE, ROWS>, ROWS, smem, nb);
         k_spmv_bundle<T, MODE, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, x, b,
                                                               y, alpha, part, A.bundle_cap);
     } else {
+        const int grid = nb;
         k_spmv_rows<T, MODE, ROWS><<<grid, ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y,
                                                          alpha, part);
     }
@@ -274,7 +377,7 @@ int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s)
         DCsr<double> B = A;
         B.bundle_rows = c;
         HZB_TRY(bundle_capacity_rows(A.n, c, A.ia, s, &B.bundle_cap));
-        if (bundle_smem<double>(B.bundle_cap) > SPMV_SMEM_MAX) continue;
+        if (2 * bundle_stage_bytes<double>(B.bundle_cap, c) > SPMV_SMEM_MAX) continue;
         HZB_TRY(spmv<double>(B, SPMV_Y, x, nullptr, y, 1.0, nullptr, s));   // warm
         cudaEventRecord(e0, s);
         for (int r = 0; r < 3; ++r) HZB_TRY(spmv<double>(B, SPMV_Y, x, nullptr, y, 1.0, nullptr, s));
@@ -378,6 +481,17 @@ int jacobi_sweep(const DCsr<double> &A, const double *dj, const double *b,
 
 // l1-Jacobi: t = b_i - sum_j a_ij x_j, d = sum_j |a_ij| (both in CSR order);
 // x_i += omega_i * (t / d).  Rows are staged per bundle like the SpMV.
+template <typename T>
+__device__ __forceinline__ T l1_update(int i, T t, T d, const T *__restrict__ x,
+                                      const float *__restrict__ omega) {
+    T xi = x[i];
+    if (fabs(d) > T(SMALLREAL)) {
+        if (omega) xi += T(omega[i]) * (t / d);
+        else xi += t / d;
+    }
+    return xi;
+}
+
 template <typename T, int ROWS>
 __global__ void __launch_bounds__(ROWS)
 k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
@@ -385,57 +499,57 @@ k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
             const T *__restrict__ x, T *__restrict__ xn,
             const float *__restrict__ omega, int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sv = reinterpret_cast<T *>(smem_raw);
-    int *sc = reinterpret_cast<int *>(smem_raw + bundle_sc_offset<T>(cap));
-    const int r0 = blockIdx.x * ROWS;
-    const int r1 = min(r0 + ROWS, n);
-    const int s = __ldg(ia + r0), e = __ldg(ia + r1);
-    int s0 = s;
-    if (cap > 0) {
-        s0 = stage_bundle<T, ROWS>(a, ja, s, e, sv, sc);
-        __syncthreads();
-    }
-    const int i = r0 + threadIdx.x;
-    if (i >= r1) return;
-    T t = b[i], d = T(0);
-    const int b0 = __ldg(ia + i), b1 = __ldg(ia + i + 1);
-    if (cap > 0) {
-        for (int k = b0 - s0; k < b1 - s0; ++k) {
+    bundle_pipeline<T, ROWS>(n, ia, a, ja, cap, smem_raw,
+                             [&](int, int r0, int r1, int s0, const T *sv, const int *sc,
+                                 const int *sia) {
+        const int i = r0 + threadIdx.x;
+        if (i >= r1) return;
+        T t = b[i], d = T(0);
+        const int b0 = sia[threadIdx.x] - s0, b1 = sia[threadIdx.x + 1] - s0;
+        for (int k = b0; k < b1; ++k) {
             const T v = sv[k];
             t -= v * __ldg(x + sc[k]);
             d += fabs(v);
         }
-    } else {
-        for (int k = b0; k < b1; ++k) {
-            const T v = a[k];
-            t -= v * __ldg(x + ja[k]);
-            d += fabs(v);
-        }
+        xn[i] = l1_update(i, t, d, x, omega);
+    });
+}
+
+// Rows too long for a staged bundle: one thread per row from global memory.
+template <typename T, int ROWS>
+__global__ void __launch_bounds__(ROWS)
+k_l1_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+          const T *__restrict__ a, const T *__restrict__ b, const T *__restrict__ x,
+          T *__restrict__ xn, const float *__restrict__ omega) {
+    const int i = blockIdx.x * ROWS + threadIdx.x;
+    if (i >= n) return;
+    T t = b[i], d = T(0);
+    for (int k = ia[i]; k < ia[i + 1]; ++k) {
+        const T v = a[k];
+        t -= v * __ldg(x + ja[k]);
+        d += fabs(v);
     }
-    T xi = x[i];
-    if (fabs(d) > T(SMALLREAL)) {
-        if (omega) xi += T(omega[i]) * (t / d);
-        else xi += t / d;
-    }
-    xn[i] = xi;
+    xn[i] = l1_update(i, t, d, x, omega);
 }
 
 template <typename T, int ROWS>
 static int l1_launch(const DCsr<T> &A, const T *b, const T *x, T *xn, const float *omega,
                      cudaStream_t s) {
-    const int grid = div_up(A.n, ROWS);
-    size_t smem = bundle_smem<T>(A.bundle_cap);
-    int cap = A.bundle_cap;
-    if (cap <= 0 || smem > SPMV_SMEM_MAX || !bundle_aligned(A)) { cap = 0; smem = 0; }
-    if (smem > 48 * 1024) {
+    const int nb = div_up(A.n, ROWS);
+    size_t smem = 0;
+    if (staged_ok(A, ROWS, &smem)) {
         static bool done = false;
         if (!done) {
             cudaFuncSetAttribute(k_l1_bundle<T, ROWS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
             done = true;
         }
+        const int grid = persistent_grid(k_l1_bundle<T, ROWS>, ROWS, smem, nb);
+        k_l1_bundle<T, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega,
+                                                      A.bundle_cap);
+    } else {
+        k_l1_rows<T, ROWS><<<nb, ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega);
     }
-    k_l1_bundle<T, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega, cap);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;

@@ -219,8 +219,9 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, 
     const DCsr<double> A = L0.A64();
     cudaStream_t s = S->s;
     const int g = grid_for(n);
+    const bool grad = domega != nullptr;   // without it: the loss alone
     LearnWork w;
-    HZB_TRY(w.alloc(n, ncyc));
+    HZB_TRY(w.alloc(n, grad ? ncyc : 0));
     HZB_TRY(l1_norms<double>(A, w.l1, s));
     HZB_TRY(vzero<double>(n, w.dom, s));
     double total = 0.0;
@@ -229,19 +230,24 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, 
         HZB_TRY(anorm2(S, w, w.e, w.sc + 0));          // ||e||_A^2
         int q = 0;
         for (int cyc = 0; cyc < ncyc; ++cyc) {         // forward, storing A e_in
-            for (int j = 0; j < 2; ++j, ++q) {
-                HZB_TRY(spmv<double>(A, SPMV_Y, w.e, nullptr, w.Ae[q], 1.0, nullptr, s));
-                k_err_sweep<<<g, 256, 0, s>>>(n, omega, w.l1, w.Ae[q], w.e);
-                count_launch();
-            }
-            HZB_TRY(coarse_correct(S, w, w.e));
-            for (int j = 0; j < 2; ++j, ++q) {
-                HZB_TRY(spmv<double>(A, SPMV_Y, w.e, nullptr, w.Ae[q], 1.0, nullptr, s));
-                k_err_sweep<<<g, 256, 0, s>>>(n, omega, w.l1, w.Ae[q], w.e);
-                count_launch();
+            for (int half = 0; half < 2; ++half) {
+                if (half) HZB_TRY(coarse_correct(S, w, w.e));
+                for (int j = 0; j < 2; ++j, ++q) {
+                    double *Ae = grad ? w.Ae[q] : w.t;
+                    HZB_TRY(spmv<double>(A, SPMV_Y, w.e, nullptr, Ae, 1.0, nullptr, s));
+                    k_err_sweep<<<g, 256, 0, s>>>(n, omega, w.l1, Ae, w.e);
+                    count_launch();
+                }
             }
         }
         HZB_TRY(anorm2(S, w, w.e, w.sc + 1));          // ||E^k e||_A^2, A e in w.r
+        if (!grad) {
+            double h[2];
+            HZB_CUDA(cudaMemcpyAsync(h, w.sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            HZB_CUDA(cudaStreamSynchronize(s));
+            total += h[1] / h[0];
+            continue;
+        }
         HZB_TRY(vcopy<double>(n, w.r, w.g, s));        // g = 2 A e / ||e0||_A^2
         k_scale_by<<<g, 256, 0, s>>>(n, w.sc + 0, 2.0, w.g);
         count_launch();
@@ -267,15 +273,56 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, 
     }
     // gradient of the mean over samples; the FP64 sum of the per-sample
     // gradients is divided by ns once
-    k_to_float<<<g, 256, 0, s>>>(n, w.dom, 1.0 / ns, domega);
-    count_launch();
-    HZB_CUDA(cudaStreamSynchronize(s));
+    if (grad) {
+        k_to_float<<<g, 256, 0, s>>>(n, w.dom, 1.0 / ns, domega);
+        count_launch();
+        HZB_CUDA(cudaStreamSynchronize(s));
+    }
     *loss = total / ns;
     return SUCCESS;
 }
 
-// The contraction loss above is ||E^2 e||_A^2 / ||e||_A^2, whose gradient
-// dom accumulates d/domega of each sample's ratio: the ratio's derivative
-// with ||e||_A fixed (the errors do not depend on omega).
+int cycle_contraction(hzb_solver *S, int ns, unsigned long long seed, double *loss) {
+    if (ns < 1) return ERROR_INPUT_PAR;
+    HZB_TRY(need_levels(S));
+    Level &L0 = S->lv[0];
+    const int n = L0.n;
+    const DCsr<double> A = L0.A64();
+    cudaStream_t s = S->s;
+    const int g = grid_for(n);
+    KrylovWork &kw = S->kw;   // r, z as the preconditioner's operands (its graph key)
+    if (kw.n != n) HZB_TRY(kw.alloc(n));
+    LearnWork w;
+    HZB_TRY(w.alloc(n));
+    HZB_TRY(l1_norms<double>(A, w.l1, s));
+    double total = 0.0;
+    for (int k = 0; k < ns; ++k) {
+        k_rand<<<g, 256, 0, s>>>(n, seed + 7919ull * (unsigned long long)k, w.e);
+        count_launch();
+        for (int it = 0; it < 3; ++it) {   // plain l1 sweeps
+            HZB_TRY(spmv<double>(A, SPMV_Y, w.e, nullptr, w.t, 1.0, nullptr, s));
+            k_err_sweep<<<g, 256, 0, s>>>(n, nullptr, w.l1, w.t, w.e);
+            count_launch();
+        }
+        for (int it = 0; it < 4; ++it) {   // e <- e - B A e, twice, then twice measured
+            if (it == 2) HZB_TRY(anorm2(S, w, w.e, w.sc + 0));
+            HZB_TRY(spmv<double>(A, SPMV_Y, w.e, nullptr, kw.r, 1.0, nullptr, s));
+            HZB_TRY(solver_precond(S, kw.r, kw.z));
+            k_sub<<<g, 256, 0, s>>>(n, kw.z, w.e);
+            count_launch();
+        }
+        HZB_TRY(anorm2(S, w, w.e, w.sc + 1));
+        double h[2];
+        HZB_CUDA(cudaMemcpyAsync(h, w.sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        HZB_CUDA(cudaStreamSynchronize(s));
+        total += h[1] / h[0];
+    }
+    *loss = total / ns;
+    return SUCCESS;
+}
+
+// The contraction loss above is ||E^k e||_A^2 / ||e||_A^2 with e given, whose
+// gradient dom accumulates d/domega of each sample's ratio with ||e||_A
+// fixed (e does not depend on omega).
 
 }  // namespace hzb

@@ -861,6 +861,27 @@ __global__ void k_pm_assign(int n, const int *__restrict__ acc,
         }
 }
 
+// Renumbering by leader: aggregate ids follow their smallest member vertex,
+// so coarse rows keep the fine ordering's locality (ids were handed out round
+// by round).
+__global__ void k_pm_lead(int n, const int *__restrict__ agg, int *lead) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+         v += gridDim.x * blockDim.x)
+        if (agg[v] >= 0) atomicMin(lead + agg[v], v);
+}
+__global__ void k_pm_leadflag(int n, const int *__restrict__ agg, const int *__restrict__ lead,
+                              int *flag) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+         v += gridDim.x * blockDim.x)
+        flag[v] = agg[v] >= 0 && lead[agg[v]] == v;
+}
+__global__ void k_pm_renumber(int n, const int *__restrict__ lead, const int *__restrict__ pos,
+                              int *agg) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+         v += gridDim.x * blockDim.x)
+        if (agg[v] >= 0) agg[v] = pos[lead[agg[v]]];
+}
+
 __global__ void k_pm_sizes(int n, const int *__restrict__ state, int *size) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += gridDim.x * blockDim.x)
@@ -940,6 +961,18 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
         k_pm_singletons<<<g, 256, 0, s>>>(n, flag, pos, nc, agg);
         count_launch();
         cudaMemcpyAsync(&extra, pos + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+    }
+    if (!rc) {   // ids in the order of each aggregate's smallest vertex
+        int *lead = size;
+        cudaMemsetAsync(lead, 0x7f, sizeof(int) * (size_t)n, s);
+        k_pm_lead<<<g, 256, 0, s>>>(n, agg, lead);
+        k_pm_leadflag<<<g, 256, 0, s>>>(n, agg, lead, flag);
+        count_launch(2);
+        rc = scan_exclusive(flag, pos, n, tmp, s);
+        if (!rc) {
+            k_pm_renumber<<<g, 256, 0, s>>>(n, lead, pos, agg);
+            count_launch();
+        }
     }
     cudaError_t e = cudaStreamSynchronize(s);
     dfree(dflag);

@@ -900,6 +900,11 @@ int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
                       [&]() { return precond64_body(S, r, z, cyc); });
 }
 
+int solver_precond(hzb_solver *S, const double *r, double *z) {
+    if (S->bp.precision == HZB_PREC_MIXED) return apply_pc32(S, r, z);
+    return precond64(S, r, z, S->pc_cyc);
+}
+
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out) {
     KrylovWork &w = S->kw;

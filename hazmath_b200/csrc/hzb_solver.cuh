@@ -133,6 +133,13 @@ enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2 };
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out);
 int ensure_fp32(hzb_solver *S);
+// z = B r with the preconditioner the handle's solve uses (the FP32 cycle in
+// mixed precision, precond_amg's FP64 cycle otherwise)
+int solver_precond(hzb_solver *S, const double *r, double *z);
+// Mean over ns seeded vectors of ||E^2 e||_A^2 / ||e||_A^2 for the solve's
+// own cycle E = I - B A, e the errors two cycles leave (random vectors after
+// three plain l1 sweeps); uses the Krylov scratch vectors r, z.
+int cycle_contraction(hzb_solver *S, int ns, unsigned long long seed, double *loss);
 // learned-weight loss (hzb_learn.cu)
 int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
                  const float *omega, int ncyc);

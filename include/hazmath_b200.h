@@ -456,15 +456,17 @@ INT  hzb_learn_errors(hzb_solver *s, INT ns, unsigned long long seed, REAL *d_E,
                       const float *d_omega, INT ncycles);
 /* mean over the ns vectors of ||E(omega)^k e||_A^2 / ||e||_A^2, k = ncycles
  * (1..16), for the V(2,2) l1-Jacobi cycle with fine-level weights omega, and
- * its gradient (adjoint cycles).  Training minimises the two-cycle
+ * its gradient (adjoint cycles; d_domega NULL: the loss alone).  Training minimises the two-cycle
  * contraction of the errors the current cycle leaves, (||E^4 z||/||E^2 z||)^2
  * for omega-independent z, through the k = 4 and k = 2 gradients.          */
 INT  hzb_learn_loss_grad(hzb_solver *s, const float *d_omega, INT ns,
                          const REAL *d_E, INT ncycles, REAL *loss, float *d_domega);
 /* Set up the learned weights on a solver with fallback: infer omega, measure
- * the per-cycle contraction with and without it on ns method-generated
- * error vectors, keep omega only if it contracts better.  Both contractions
- * are returned and recorded in hzb_stats (omega_contraction, omega_used). */
+ * the per-cycle contraction of the solve's own cycle (the FP32 cycle in
+ * mixed precision) with and without it on ns method-generated error vectors
+ * (the errors two cycles leave), keep omega only if it contracts better.
+ * Both contractions are returned and recorded in hzb_stats
+ * (omega_contraction, omega_used).                                          */
 INT  hzb_learn_select_omega(hzb_solver *s, hzb_gnn *g, INT ns,
                             unsigned long long seed, REAL *rho_plain,
                             REAL *rho_learned);
