@@ -344,20 +344,21 @@ def run_single(args, rank, world, local, dist):
     err_vs_fp64 = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
     total64 = st64.setup_seconds + st64.solve_seconds
 
-    # roofline: level-0 SpMV of the FP64 drop-in (the level SpMV the target
-    # names), 50 launches on the solver's stream with CUDA events
+    # roofline of the step's dominant kernel (the level-0 FP32 l1-Jacobi
+    # sweep, a quarter of the step's device time) and of the drop-in's
+    # level-0 FP64 SpMV (the level SpMV the 70 % target names): each timed as
+    # 50 launches on the solver's stream between CUDA events
     peak, peak_kind = hbm_peak()
-    ms, by = C.c_double(), C.c_double()
-    check(hz.lib().hzb_time_kernel(S64.h, hz.HZB_K_SPMV64, 0, 50, C.byref(ms), C.byref(by)),
-          "time_kernel")
-    spmv64_gbs = by.value / (ms.value * 1e-3) / 1e9
-    spmv64 = (ms.value, by.value)
-    check(hz.lib().hzb_time_kernel(S.h, hz.HZB_K_L1_32, 0, 50, C.byref(ms), C.byref(by)),
-          "time_kernel")
-    l1_32_gbs = by.value / (ms.value * 1e-3) / 1e9
-    check(hz.lib().hzb_time_kernel(S.h, hz.HZB_K_SPMV32, 0, 50, C.byref(ms), C.byref(by)),
-          "time_kernel")
-    spmv32_gbs = by.value / (ms.value * 1e-3) / 1e9
+
+    def kernel(h, which):
+        ms, by = C.c_double(), C.c_double()
+        check(hz.lib().hzb_time_kernel(h, which, 0, 50, C.byref(ms), C.byref(by)),
+              "time_kernel")
+        return ms.value, by.value, by.value / (ms.value * 1e-3) / 1e9
+
+    l1_ms, l1_by, l1_gbs = kernel(S.h, hz.HZB_K_L1_32)
+    sp_ms, sp_by, spmv64_gbs = kernel(S64.h, hz.HZB_K_SPMV64)
+    spmv32_gbs = kernel(S.h, hz.HZB_K_SPMV32)[2]
 
     # e2e: the handle API with host arrays (copies in and out inside the region)
     Se = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
@@ -403,12 +404,20 @@ def run_single(args, rank, world, local, dist):
             "speedup_vs_plain": total64 / step_s,
             "speedup_solve_vs_plain": st64.solve_seconds / solve_ml,
             "err_vs_fp64": err_vs_fp64,
-            "roofline": {"bound": "hbm", "kernel": "level-0 SpMV FP64 of the drop-in "
-                         "(k_spmv_bundle<double>)", "achieved": spmv64_gbs, "peak": peak,
-                         "unit": "GB/s", "frac": spmv64_gbs / peak, "peak_kind": peak_kind,
-                         "bytes_per_launch": spmv64[1], "ms_per_launch": spmv64[0],
-                         "traffic": TRAFFIC.get(args.workload)},
-            "l1_sweep_fp32_gbs": l1_32_gbs, "spmv_fp32_gbs": spmv32_gbs,
+            "roofline": {"bound": "hbm", "kernel": "level-0 FP32 l1-Jacobi sweep of the "
+                         "mixed cycle (k_l1_vec / k_l1_bundle<float>, autotuned)",
+                         "achieved": l1_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": l1_gbs / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": l1_by, "ms_per_launch": l1_ms,
+                         "traffic": TRAFFIC_PER_BYTE["l1_32"] * l1_by,
+                         "traffic_source": "ncu DRAM bytes per algorithmic byte on the "
+                         "128^3 case (profiles/l1_32_level0_c2.md), times this launch's bytes"},
+            "drop_in_spmv64": {"kernel": "level-0 FP64 SpMV of the drop-in "
+                               "(k_spmv_bundle<double>)", "achieved": spmv64_gbs,
+                               "peak": peak, "unit": "GB/s", "frac": spmv64_gbs / peak,
+                               "bytes_per_launch": sp_by, "ms_per_launch": sp_ms,
+                               "traffic": TRAFFIC_PER_BYTE["spmv64"] * sp_by},
+            "spmv_fp32_gbs": spmv32_gbs,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s",
                     "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + val.nbytes + b.nbytes
@@ -423,10 +432,13 @@ def run_single(args, rank, world, local, dist):
     gnn.close()
 
 
-# DRAM bytes read + written per launch of the roofline kernel, from ncu
-# (profiles/spmv64_level0.md): captured on the c2 case and scaled by the
-# stored entries for c5.
-TRAFFIC = {}
+# DRAM bytes (read + written) per algorithmic byte of one launch, measured by
+# ncu on the level-0 kernels of the 128^3 case (dram__bytes_read.sum +
+# dram__bytes_write.sum over the bytes hzb_time_kernel counts): the FP32
+# l1-Jacobi sweep in its lanes-per-row schedule, and the drop-in's FP64 SpMV.
+# The 256^3 launches run the same kernels over 8.1x the entries, and their
+# traffic is this ratio times their algorithmic bytes.
+TRAFFIC_PER_BYTE = {"l1_32": 143.73e6 / 146709388.0, "spmv64": 404.52e6 / 405049716.0}
 
 
 def run_batch(args, rank, world, local, dist):

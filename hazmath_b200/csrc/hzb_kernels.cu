@@ -337,10 +337,81 @@ static int spmv_launch(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, 
     return SUCCESS;
 }
 
+// ---------------------------------------------------------------------------
+// FP32 vector CSR: LPR lanes per row read the row's entries with coalesced
+// loads (no staging), partial sums combined by shuffles.  For the FP32 cycle,
+// whose arithmetic is judged by convergence, not by the reference's order.
+template <int LPR>
+__device__ __forceinline__ float lanes_sum(float v) {
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, LPR);
+    return v;
+}
+
+template <int MODE, int LPR>
+__global__ void __launch_bounds__(256)
+k_spmv_vec(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+           const float *__restrict__ val, const float *__restrict__ x,
+           const float *__restrict__ b, float *__restrict__ y, float alpha) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+    const int lane = threadIdx.x % LPR;
+    const int row = g < n ? g : n - 1;   // whole groups stay in the shuffles
+    float t = 0.f;
+    for (int k = __ldg(ia + row) + lane; k < __ldg(ia + row + 1); k += LPR)
+        t += __ldcs(val + k) * __ldg(x + __ldcs(ja + k));
+    t = lanes_sum<LPR>(t);
+    if (lane == 0 && g < n) spmv_store<float, MODE>(row, t, b, y, alpha);
+}
+
+template <int LPR>
+__global__ void __launch_bounds__(256)
+k_l1_vec(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+         const float *__restrict__ a, const float *__restrict__ b,
+         const float *__restrict__ x, float *__restrict__ xn, const float *__restrict__ omega) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+    const int lane = threadIdx.x % LPR;
+    const int row = g < n ? g : n - 1;
+    float t = 0.f, d = 0.f;
+    for (int k = __ldg(ia + row) + lane; k < __ldg(ia + row + 1); k += LPR) {
+        const float v = __ldcs(a + k);
+        t += v * __ldg(x + __ldcs(ja + k));
+        d += fabsf(v);
+    }
+    t = lanes_sum<LPR>(t);
+    d = lanes_sum<LPR>(d);
+    if (lane == 0 && g < n) {
+        float xi = x[row];
+        if (fabsf(d) > float(SMALLREAL)) {
+            const float r = b[row] - t;
+            xi += omega ? omega[row] * (r / d) : r / d;
+        }
+        xn[row] = xi;
+    }
+}
+
+template <int MODE>
+static int spmv_vec_launch(const DCsr<float> &A, const float *x, const float *b, float *y,
+                           float alpha, cudaStream_t s) {
+    const int L = A.vec_lanes;
+    const int grid = div_up(A.n, 256 / L);
+    switch (L) {
+    case 2: k_spmv_vec<MODE, 2><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
+    case 4: k_spmv_vec<MODE, 4><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
+    case 8: k_spmv_vec<MODE, 8><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
+    default: k_spmv_vec<MODE, 16><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
+    }
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
 template <typename T, int MODE>
 static int spmv_mode(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, T *part,
                      cudaStream_t s) {
     if (A.n <= 0) return SUCCESS;
+    if constexpr (sizeof(T) == 4 && MODE != SPMV_Y_DOT) {
+        if (A.vec_lanes > 0) return spmv_vec_launch<MODE>(A, x, b, y, alpha, s);
+    }
     switch (A.bundle_rows) {
     case 64: return spmv_launch<T, MODE, 64>(A, x, b, y, alpha, part, s);
     case 256: return spmv_launch<T, MODE, 256>(A, x, b, y, alpha, part, s);
@@ -391,6 +462,33 @@ int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s)
     cudaEventDestroy(e1);
     A.bundle_rows = best_rows;
     A.bundle_cap = best_cap;
+    return SUCCESS;
+}
+
+// FP32 schedule of a level: the staged bundles (vec_lanes 0) or 4/8/16 lanes
+// per row, whichever runs this level's l1-Jacobi sweep fastest.
+int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cudaStream_t s) {
+    const int cands[4] = {0, 4, 8, 16};
+    cudaEvent_t e0, e1;
+    HZB_CUDA(cudaEventCreate(&e0));
+    HZB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int pick = 0;
+    for (int c : cands) {
+        DCsr<float> B = A;
+        B.vec_lanes = c;
+        HZB_TRY(l1_sweep<float>(B, b, x, xn, nullptr, s));   // warm
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; ++r) HZB_TRY(l1_sweep<float>(B, b, x, xn, nullptr, s));
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; pick = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    A.vec_lanes = pick;
     return SUCCESS;
 }
 
@@ -555,10 +653,28 @@ static int l1_launch(const DCsr<T> &A, const T *b, const T *x, T *xn, const floa
     return SUCCESS;
 }
 
+static int l1_vec_launch(const DCsr<float> &A, const float *b, const float *x, float *xn,
+                         const float *omega, cudaStream_t s) {
+    const int L = A.vec_lanes;
+    const int grid = div_up(A.n, 256 / L);
+    switch (L) {
+    case 2: k_l1_vec<2><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
+    case 4: k_l1_vec<4><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
+    case 8: k_l1_vec<8><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
+    default: k_l1_vec<16><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
+    }
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
 template <typename T>
 int l1_sweep(const DCsr<T> &A, const T *b, const T *x, T *xn,
              const float *omega, cudaStream_t s) {
     if (A.n <= 0) return SUCCESS;
+    if constexpr (sizeof(T) == 4) {
+        if (A.vec_lanes > 0) return l1_vec_launch(A, b, x, xn, omega, s);
+    }
     switch (A.bundle_rows) {
     case 64: return l1_launch<T, 64>(A, b, x, xn, omega, s);
     case 256: return l1_launch<T, 256>(A, b, x, xn, omega, s);

@@ -17,6 +17,10 @@ struct DCsr {
     const T *val = nullptr;
     int bundle_cap = 0;   // max entries in any bundle of bundle_rows rows (0: none)
     int bundle_rows = 128;   // rows per CTA of the staged kernels: 64, 128 or 256
+    // FP32 only: lanes per row of the vector-CSR kernels (2..16), 0 for the
+    // staged bundles.  A row's partial sums are combined across its lanes,
+    // so this is not the sequential CSR-order sum of the FP64 kernels.
+    int vec_lanes = 0;
 };
 
 constexpr int SPMV_ROWS = 128;          // rows per CTA in the row-bundle SpMV
@@ -29,6 +33,9 @@ int bundle_capacity(int n, const int *ia, cudaStream_t s, int *cap);
 int bundle_capacity_rows(int n, int rows, const int *ia, cudaStream_t s, int *cap);
 // Picks the bundle size (64/128/256 rows) of A by timing its SpMV on x -> y.
 int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s);
+// Picks the FP32 schedule (staged bundles or 4/8/16 lanes per row) by timing
+// the l1-Jacobi sweep of A on b, x -> xn.
+int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cudaStream_t s);
 int spmv_blocks_rows(int n, int rows);
 
 // y = A x (SPMV_Y); y = b - A x (SPMV_RES); y += alpha A x with the

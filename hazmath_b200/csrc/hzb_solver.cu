@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace hzb {
@@ -403,6 +404,19 @@ int ensure_fp32(hzb_solver *S) {
         if (!L.l1_32) {
             HZB_TRY(dalloc(&L.l1_32, L.n));
             HZB_TRY(l1_norms<float>(L.A32(), L.l1_32, S->s));
+            // staged bundles or lanes per row, by timing; HZB_FP32_LANES
+            // (0, 2, 4, 8 or 16) names one for every level instead
+            const char *force = getenv("HZB_FP32_LANES");
+            const int fl = force ? atoi(force) : -1;
+            if (fl == 0 || fl == 2 || fl == 4 || fl == 8 || fl == 16) {
+                L.vec32 = fl;
+            } else if (L.n >= 4096) {
+                HZB_TRY(vzero<float>(L.n, L.b32, S->s));
+                HZB_TRY(vzero<float>(L.n, L.x32, S->s));
+                DCsr<float> A = L.A32();
+                HZB_TRY(autotune_fp32(A, L.b32, L.x32, L.w32, S->s));
+                L.vec32 = A.vec_lanes;
+            }
         }
         if (S->amg.smoother == SMOOTHER_GS && l < S->nl - 1 && !L.d_gs32) {
             if (!L.col.rows) HZB_TRY(multicolor(L.n, L.ia, L.ja, &L.col, S->s));

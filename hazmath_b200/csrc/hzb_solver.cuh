@@ -17,6 +17,7 @@ struct Level {
     // FP32 copy for the mixed cycle without the stored exact zeros (a zero
     // entry adds nothing to a row sum); aliases ia/ja when there are none
     int nnz32 = 0, bundle_cap32 = 0;
+    int vec32 = 0;                    // FP32 schedule: lanes per row, 0 = bundles
     int *ia32 = nullptr, *ja32 = nullptr;
     float *val32 = nullptr;
     bool own32 = false;
@@ -52,6 +53,7 @@ struct Level {
         m.n = n; m.nnz = nnz32; m.ia = ia32; m.ja = ja32; m.val = val32;
         m.bundle_cap = bundle_cap32;
         m.bundle_rows = bundle_rows;
+        m.vec_lanes = vec32;
         return m;
     }
     void release();

@@ -1,0 +1,86 @@
+"""Level-kernel timing on a workload's hierarchy.
+
+    python -m hazmath_b200.kernel_bench [--case c2|c5] [--levels 0,1,2]
+        [--kernels spmv64,spmv32,res64,l1_32,l1_64] [--reps 50]
+        [--precision mixed|fp64] [--matching parallel|exact]
+
+Builds the UA-AMG hierarchy (l1-Jacobi V(2,2) settings) of the 3D P1
+log-normal diffusion problem on the Kuhn mesh of 128^3 (c2, sigma 1) or
+256^3 (c5, sigma 1.5) cubes, then times each requested kernel on each
+requested level with hzb_time_kernel: `reps` back-to-back launches on the
+handle's stream between CUDA events, after one warm-up launch.  Prints
+achieved GB/s from the kernel's algorithmic bytes and the fraction of the
+measured HBM copy bandwidth.  The timed launches are bracketed by
+cudaProfilerStart/Stop, so `ncu --profile-from-start off` sees only them.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+from . import (HZB_K_L1_32, HZB_K_L1_64, HZB_K_RES64, HZB_K_SPMV32, HZB_K_SPMV64,
+               HZB_MATCH_EXACT, HZB_MATCH_PARALLEL, HZB_PREC_FP64, HZB_PREC_MIXED,
+               SMOOTHER_L1DIAG, Solver, b200_param, last_error, lib, survey_amg)
+from . import problems as P
+
+KERNELS = {"spmv64": HZB_K_SPMV64, "spmv32": HZB_K_SPMV32, "res64": HZB_K_RES64,
+           "l1_32": HZB_K_L1_32, "l1_64": HZB_K_L1_64}
+CASES = {"c2": (128, 1.0, 2), "c5": (256, 1.5, 7)}
+PEAKS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                     "MEASURED_PEAKS.json")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="c2", choices=sorted(CASES))
+    ap.add_argument("--levels", default="0,1,2")
+    ap.add_argument("--kernels", default="spmv64,spmv32,res64,l1_32,l1_64")
+    ap.add_argument("--reps", type=int, default=50)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--matching", default="parallel", choices=["parallel", "exact"])
+    a = ap.parse_args()
+    import torch
+    N, sigma, seed = CASES[a.case]
+    ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, sigma, 8.0, seed))
+    n = len(ia) - 1
+    dia, dja, dval = (torch.from_numpy(v).cuda() for v in (ia, ja, val))
+    amg = survey_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    prec = HZB_PREC_MIXED if a.precision == "mixed" else HZB_PREC_FP64
+    match = HZB_MATCH_PARALLEL if a.matching == "parallel" else HZB_MATCH_EXACT
+    S = Solver(amg, None, b200_param(precision=prec, matching=match))
+    rc = S.setup_device(n, len(ja), dia.data_ptr(), dja.data_ptr(), dval.data_ptr())
+    if rc:
+        raise SystemExit(f"setup failed {rc}: {last_error()}")
+    try:
+        peak = float(json.load(open(PEAKS))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        peak = 6650.0
+    st = S.stats()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for lv in (int(x) for x in a.levels.split(",")):
+        if lv >= st.num_levels:
+            continue
+        for name in a.kernels.split(","):
+            ms, by = C.c_double(), C.c_double()
+            rc = lib().hzb_time_kernel(S.h, KERNELS[name], lv, a.reps, C.byref(ms),
+                                       C.byref(by))
+            if rc:
+                print(f"level {lv} {name}: error {rc} {last_error()}")
+                continue
+            gbs = by.value / (ms.value * 1e-3) / 1e9
+            print(json.dumps({"case": a.case, "level": lv, "rows": int(st.rows[lv]),
+                              "nnz": int(st.nnz[lv]), "kernel": name,
+                              "us_per_launch": ms.value * 1e3,
+                              "bytes_per_launch": by.value, "gbs": gbs,
+                              "frac_of_measured_peak": gbs / peak}), flush=True)
+    torch.cuda.profiler.stop()
+    S.close()
+
+
+if __name__ == "__main__":
+    main()
