@@ -46,11 +46,23 @@ struct Batch {
     int *nactive = nullptr;         // device count of active systems
     int *h_nactive = nullptr;       // pinned mirror
     GraphCache g_iter;
+    // per level: the system of every row and the activity of 256-row blocks
+    int nlev = 0, nblk_all = 0;
+    std::vector<int *> sysmap;
+    std::vector<unsigned char *> actv;
+    int **d_sys = nullptr;          // device copies of the per-level pointers
+    unsigned char **d_act = nullptr;
+    int *d_nrows = nullptr, *d_blkoff = nullptr;   // rows, first block per level
     void release() {
         g_iter.release();
         dfree(item_lo); dfree(item_hi); dfree(item_sys); dfree(sys_item);
         dfree(state); dfree(iters); dfree(sc); dfree(part);
         dfree(t_done); dfree(t_start); dfree(queue); dfree(nactive);
+        for (auto p : sysmap) dfree(p);
+        for (auto p : actv) dfree(p);
+        sysmap.clear();
+        actv.clear();
+        dfree(d_sys); dfree(d_act); dfree(d_nrows); dfree(d_blkoff);
         if (h_nactive) cudaFreeHost(h_nactive);
         h_nactive = nullptr;
     }
@@ -225,7 +237,49 @@ __global__ void k_bat_stamp(unsigned long long *t, int nsys, const int *state,
         if (state[s] == BAT_DONE) t_done[s] = now;
 }
 
+// row -> system on level 0 (from the work items) and on the levels below
+// (every member of an aggregate belongs to the aggregate's system)
+__global__ void k_bat_sys0(int nitems, const int *__restrict__ lo, const int *__restrict__ hi,
+                           const int *__restrict__ isys, int *sys) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x)
+        for (int i = lo[it] + threadIdx.x; i < hi[it]; i += blockDim.x) sys[i] = isys[it];
+}
+__global__ void k_bat_sys_down(int n, const int *__restrict__ agg,
+                               const int *__restrict__ sys, int *sys_c) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (agg[i] >= 0) sys_c[agg[i]] = sys[i];
+}
+
+// Activity of every 256-row block of every level: a block is active if a row
+// of it belongs to an active system.  A warp per block checks every row.
+__global__ void k_bat_activity(int nlev, int nblk_all, const int *__restrict__ blkoff,
+                               const int *__restrict__ nrows, int *const *__restrict__ sys,
+                               unsigned char *const *__restrict__ act,
+                               const int *__restrict__ state) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < nblk_all; g += nw) {
+        int l = 0;
+        while (l + 1 < nlev && blkoff[l + 1] <= g) ++l;
+        const int blk = g - blkoff[l], n = nrows[l];
+        const int r0 = blk * ACT_ROWS, r1 = min(r0 + ACT_ROWS, n);
+        bool a = false;
+        for (int r = r0 + lane; r < r1 && !a; r += 32) a = state[sys[l][r]] == BAT_ACTIVE;
+        const unsigned any = __ballot_sync(0xffffffffu, a);
+        if (lane == 0) act[l][blk] = any != 0u;
+    }
+}
+
 static int bat_grid(int nitems) { return std::max(1, std::min(nitems, sm_count() * 8)); }
+
+static int bat_activity(hzb_solver *S, Batch &B) {
+    if (B.nblk_all == 0) return SUCCESS;
+    k_bat_activity<<<grid_for(32LL * B.nblk_all), 256, 0, S->s>>>(
+        B.nlev, B.nblk_all, B.d_blkoff, B.d_nrows, B.d_sys, B.d_act, B.state);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
 
 template <int OP>
 static int bat_vec(hzb_solver *S, Batch &B, unsigned *q, const double *b, double *x,
@@ -267,6 +321,7 @@ static int bat_iteration(hzb_solver *S, Batch &B, const double *b, double *x) {
     HZB_TRY(bat_final<FIN_TRUERES>(S, B));
     HZB_CUDA(cudaMemcpyAsync(B.h_nactive, B.nactive, sizeof(int), cudaMemcpyDeviceToHost,
                              S->s));
+    HZB_TRY(bat_activity(S, B));       // the cycle and the next SpMV skip retired systems
     HZB_TRY(bat_precond(S, w.r, w.z));
     HZB_TRY(bat_vec<OP_ZTR>(S, B, q + 3, b, x, w.r, w.p, w.z, w.t));
     HZB_TRY(bat_final<FIN_ZTR>(S, B));
@@ -279,9 +334,9 @@ static int bat_precond(hzb_solver *S, const double *r, double *z) {
     Level &L0 = S->lv[0];
     AMG_param cyc = S->amg;
     if (S->bp.precision == HZB_PREC_MIXED) {
-        HZB_TRY(d2f(L0.n, r, L0.b32, S->s));
+        HZB_TRY(d2f(L0.n, r, L0.b32, S->s, L0.act));
         for (int i = 0; i < std::max<int>(1, cyc.maxit); ++i) HZB_TRY(cycle32(S, cyc, i == 0));
-        return f2d(L0.n, L0.x32, z, S->s);
+        return f2d(L0.n, L0.x32, z, S->s, L0.act);
     }
     HZB_TRY(vcopy<double>(L0.n, r, L0.b, S->s));
     HZB_TRY(vzero<double>(L0.n, L0.x, S->s));
@@ -365,6 +420,40 @@ int batch_setup(hzb_solver *S, int nsys, const int *off, int n, int nnz, const i
         return rc;
     }
     if (S->bp.precision == HZB_PREC_MIXED) HZB_TRY(ensure_fp32(S));
+    // per-level row -> system maps and activity blocks
+    B->nlev = S->nl;
+    std::vector<int> nrows(S->nl), blkoff(S->nl + 1, 0);
+    B->sysmap.assign(S->nl, nullptr);
+    B->actv.assign(S->nl, nullptr);
+    for (int l = 0; l < S->nl; ++l) {
+        const int nl_rows = S->lv[l].n;
+        nrows[l] = nl_rows;
+        blkoff[l + 1] = blkoff[l] + (nl_rows + ACT_ROWS - 1) / ACT_ROWS;
+        HZB_TRY(dalloc(&B->sysmap[l], std::max(1, nl_rows)));
+        HZB_TRY(dalloc(&B->actv[l], std::max(1, blkoff[l + 1] - blkoff[l])));
+    }
+    B->nblk_all = blkoff[S->nl];
+    k_bat_sys0<<<bat_grid(B->nitems), 256, 0, s>>>(B->nitems, B->item_lo, B->item_hi,
+                                                   B->item_sys, B->sysmap[0]);
+    count_launch();
+    for (int l = 0; l + 1 < S->nl; ++l) {
+        k_bat_sys_down<<<grid_for(S->lv[l].n), 256, 0, s>>>(S->lv[l].n, S->lv[l].agg,
+                                                            B->sysmap[l], B->sysmap[l + 1]);
+        count_launch();
+    }
+    HZB_TRY(dalloc(&B->d_sys, S->nl));
+    HZB_TRY(dalloc(&B->d_act, S->nl));
+    HZB_TRY(dalloc(&B->d_nrows, S->nl));
+    HZB_TRY(dalloc(&B->d_blkoff, S->nl + 1));
+    HZB_CUDA(cudaMemcpyAsync(B->d_sys, B->sysmap.data(), S->nl * sizeof(int *),
+                             cudaMemcpyHostToDevice, s));
+    HZB_CUDA(cudaMemcpyAsync(B->d_act, B->actv.data(), S->nl * sizeof(unsigned char *),
+                             cudaMemcpyHostToDevice, s));
+    HZB_CUDA(cudaMemcpyAsync(B->d_nrows, nrows.data(), S->nl * sizeof(int),
+                             cudaMemcpyHostToDevice, s));
+    HZB_CUDA(cudaMemcpyAsync(B->d_blkoff, blkoff.data(), (S->nl + 1) * sizeof(int),
+                             cudaMemcpyHostToDevice, s));
+    HZB_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
     return SUCCESS;
 }
 
@@ -378,9 +467,16 @@ int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit
     cudaStream_t s = S->s;
     if (w.n != B->n) HZB_TRY(w.alloc(B->n));
     unsigned *q = B->queue;
+    // the level kernels skip converged systems while this solve runs
+    struct ActScope {
+        hzb_solver *S;
+        ~ActScope() { for (auto &L : S->lv) L.act = nullptr; }
+    } act_scope{S};
+    for (int l = 0; l < S->nl; ++l) S->lv[l].act = B->actv[l];
     // r = b - A x0, per-system norms; z = B r, p = z, (z, r)
     HZB_TRY(bat_vec<OP_INIT>(S, *B, q + 5, b, x, w.r, w.p, w.z, w.t));
     HZB_TRY(bat_final<FIN_INIT>(S, *B));
+    HZB_TRY(bat_activity(S, *B));
     k_bat_stamp<<<std::max(1, (B->nsys + 127) / 128), 128, 0, s>>>(B->t_start, B->nsys,
                                                                    B->state, B->t_done);
     count_launch();

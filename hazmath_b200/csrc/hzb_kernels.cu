@@ -171,25 +171,33 @@ __device__ __forceinline__ int issue_bundle(const int *__restrict__ ia, const T 
 // Persistent bundle loop: CTA c works on bundles c, c + grid, ...; while it
 // computes one bundle the copies of its next are in flight (two stages).
 // body(bundle, r0, r1, s0, sv, sc, sia) runs between two __syncthreads.
-template <typename T, int ROWS, typename F>
+template <typename T, int ROWS, bool ACT, typename F>
 __device__ __forceinline__ void bundle_pipeline(int n, const int *__restrict__ ia,
                                                 const T *__restrict__ val,
                                                 const int *__restrict__ ja, int cap,
+                                                const unsigned char *__restrict__ act,
                                                 unsigned char *smem, F body) {
+    static_assert(ACT_ROWS % ROWS == 0, "bundles tile the activity blocks");
     const int nb = (n + ROWS - 1) / ROWS;
+    // ACT: the next bundle of this CTA at or after b that is active
+    auto next_active = [&](int b) {
+        if constexpr (ACT)
+            while (b < nb && !act[(b * ROWS) / ACT_ROWS]) b += gridDim.x;
+        return b;
+    };
     const size_t stage = bundle_stage_bytes<T>(cap, ROWS);
     const size_t off_c = bundle_sc_offset<T>(cap), off_i = bundle_smem<T>(cap);
     auto SV = [&](int k) { return reinterpret_cast<T *>(smem + k * stage); };
     auto SC = [&](int k) { return reinterpret_cast<int *>(smem + k * stage + off_c); };
     auto SI = [&](int k) { return reinterpret_cast<int *>(smem + k * stage + off_i); };
-    int bid = blockIdx.x;
+    int bid = next_active(blockIdx.x);
     if (bid >= nb) return;
     int r0 = bid * ROWS, r1 = min(r0 + ROWS, n);
     int s0 = issue_bundle<T, ROWS>(ia, val, ja, r0, r1, __ldg(ia + r0), __ldg(ia + r1), SV(0),
                                    SC(0), SI(0));
     cp_async_commit();
     // entry range of the next bundle, loaded one bundle ahead
-    int nxt = bid + gridDim.x;
+    int nxt = next_active(bid + gridDim.x);
     int ns = 0, ne = 0;
     if (nxt < nb) {
         ns = __ldg(ia + nxt * ROWS);
@@ -205,7 +213,8 @@ __device__ __forceinline__ void bundle_pipeline(int n, const int *__restrict__ i
                                         SI(st ^ 1));
         }
         cp_async_commit();
-        const int after = nxt + gridDim.x;
+        const int after = ACT ? (nxt < nb ? next_active(nxt + gridDim.x) : nb)
+                              : nxt + gridDim.x;
         if (after < nb) {
             ns = __ldg(ia + after * ROWS);
             ne = __ldg(ia + min(after * ROWS + ROWS, n));
@@ -236,15 +245,15 @@ __device__ __forceinline__ void spmv_store(int row, T t, const T *b, T *y, T alp
     }
 }
 
-template <typename T, int MODE, int ROWS>
+template <typename T, int MODE, int ROWS, bool ACT>
 __global__ void __launch_bounds__(ROWS)
 k_spmv_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
               const T *__restrict__ val, const T *__restrict__ x,
               const T *__restrict__ b, T *__restrict__ y, T alpha,
-              T *__restrict__ part, int cap) {
+              T *__restrict__ part, int cap, const unsigned char *__restrict__ act) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T sh[32];
-    bundle_pipeline<T, ROWS>(n, ia, val, ja, cap, smem_raw,
+    bundle_pipeline<T, ROWS, ACT>(n, ia, val, ja, cap, act, smem_raw,
                              [&](int bundle, int r0, int r1, int s0, const T *sv, const int *sc,
                                  const int *sia) {
         const int row = r0 + threadIdx.x;
@@ -268,10 +277,10 @@ __global__ void __launch_bounds__(ROWS)
 k_spmv_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
             const T *__restrict__ val, const T *__restrict__ x,
             const T *__restrict__ b, T *__restrict__ y, T alpha,
-            T *__restrict__ part) {
+            T *__restrict__ part, const unsigned char *__restrict__ act) {
     const int row = blockIdx.x * ROWS + threadIdx.x;
     T t = T(0), prod = T(0);
-    if (row < n) {
+    if (row < n && (!act || act[row / ACT_ROWS])) {
         const int b0 = ia[row], b1 = ia[row + 1];
         for (int k = b0; k < b1; ++k) t += val[k] * __ldg(x + ja[k]);
         spmv_store<T, MODE>(row, t, b, y, alpha);
@@ -320,17 +329,27 @@ static int spmv_launch(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, 
     if (staged_ok(A, ROWS, &smem)) {
         static bool done = false;   // per instantiation: raise the limit once
         if (!done) {
-            cudaFuncSetAttribute(k_spmv_bundle<T, MODE, ROWS>,
+            cudaFuncSetAttribute(k_spmv_bundle<T, MODE, ROWS, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
+            cudaFuncSetAttribute(k_spmv_bundle<T, MODE, ROWS, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
             done = true;
         }
-        const int grid = persistent_grid(k_spmv_bundle<T, MODE, ROWS>, ROWS, smem, nb);
-        k_spmv_bundle<T, MODE, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, x, b,
-                                                              y, alpha, part, A.bundle_cap);
+        // the activity check is a separate instantiation: ordinary solves
+        // run the kernel without it
+        if (A.act) {
+            const int grid = persistent_grid(k_spmv_bundle<T, MODE, ROWS, true>, ROWS, smem, nb);
+            k_spmv_bundle<T, MODE, ROWS, true><<<grid, ROWS, smem, s>>>(
+                A.n, A.ia, A.ja, A.val, x, b, y, alpha, part, A.bundle_cap, A.act);
+        } else {
+            const int grid = persistent_grid(k_spmv_bundle<T, MODE, ROWS, false>, ROWS, smem, nb);
+            k_spmv_bundle<T, MODE, ROWS, false><<<grid, ROWS, smem, s>>>(
+                A.n, A.ia, A.ja, A.val, x, b, y, alpha, part, A.bundle_cap, nullptr);
+        }
     } else {
         const int grid = nb;
         k_spmv_rows<T, MODE, ROWS><<<grid, ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y,
-                                                         alpha, part);
+                                                         alpha, part, A.act);
     }
     count_launch();
     HZB_LAUNCH_CHECK();
@@ -348,57 +367,95 @@ __device__ __forceinline__ float lanes_sum(float v) {
     return v;
 }
 
-template <int MODE, int LPR>
+// Without an activity array (ACT false) a thread group handles one row of a
+// flat grid.  With one, a CTA takes 256-row blocks in turn, skips inactive
+// blocks, and its 256 / LPR groups cover a block in LPR passes.
+template <int MODE, int LPR, bool ACT>
 __global__ void __launch_bounds__(256)
 k_spmv_vec(int n, const int *__restrict__ ia, const int *__restrict__ ja,
            const float *__restrict__ val, const float *__restrict__ x,
-           const float *__restrict__ b, float *__restrict__ y, float alpha) {
-    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
-    const int lane = threadIdx.x % LPR;
-    const int row = g < n ? g : n - 1;   // whole groups stay in the shuffles
-    float t = 0.f;
-    for (int k = __ldg(ia + row) + lane; k < __ldg(ia + row + 1); k += LPR)
-        t += __ldcs(val + k) * __ldg(x + __ldcs(ja + k));
-    t = lanes_sum<LPR>(t);
-    if (lane == 0 && g < n) spmv_store<float, MODE>(row, t, b, y, alpha);
+           const float *__restrict__ b, float *__restrict__ y, float alpha,
+           const unsigned char *__restrict__ act) {
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR;
+    auto one_row = [&](int g) {
+        const int row = g < n ? g : n - 1;   // whole groups stay in the shuffles
+        float t = 0.f;
+        for (int k = __ldg(ia + row) + lane; k < __ldg(ia + row + 1); k += LPR)
+            t += __ldcs(val + k) * __ldg(x + __ldcs(ja + k));
+        t = lanes_sum<LPR>(t);
+        if (lane == 0 && g < n) spmv_store<float, MODE>(row, t, b, y, alpha);
+    };
+    if constexpr (!ACT) {
+        one_row((blockIdx.x * blockDim.x + threadIdx.x) / LPR);
+    } else {
+        const int nblk = (n + ACT_ROWS - 1) / ACT_ROWS;
+        for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+            if (!act[blk]) continue;
+            for (int pass = 0; pass < LPR; ++pass)
+                one_row(blk * ACT_ROWS + pass * (256 / LPR) + grp);
+        }
+    }
 }
 
-template <int LPR>
+template <int LPR, bool ACT>
 __global__ void __launch_bounds__(256)
 k_l1_vec(int n, const int *__restrict__ ia, const int *__restrict__ ja,
          const float *__restrict__ a, const float *__restrict__ b,
-         const float *__restrict__ x, float *__restrict__ xn, const float *__restrict__ omega) {
-    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPR;
-    const int lane = threadIdx.x % LPR;
-    const int row = g < n ? g : n - 1;
-    float t = 0.f, d = 0.f;
-    for (int k = __ldg(ia + row) + lane; k < __ldg(ia + row + 1); k += LPR) {
-        const float v = __ldcs(a + k);
-        t += v * __ldg(x + __ldcs(ja + k));
-        d += fabsf(v);
-    }
-    t = lanes_sum<LPR>(t);
-    d = lanes_sum<LPR>(d);
-    if (lane == 0 && g < n) {
-        float xi = x[row];
-        if (fabsf(d) > float(SMALLREAL)) {
-            const float r = b[row] - t;
-            xi += omega ? omega[row] * (r / d) : r / d;
+         const float *__restrict__ x, float *__restrict__ xn, const float *__restrict__ omega,
+         const unsigned char *__restrict__ act) {
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR;
+    auto one_row = [&](int g) {
+        const int row = g < n ? g : n - 1;
+        float t = 0.f, d = 0.f;
+        for (int k = __ldg(ia + row) + lane; k < __ldg(ia + row + 1); k += LPR) {
+            const float v = __ldcs(a + k);
+            t += v * __ldg(x + __ldcs(ja + k));
+            d += fabsf(v);
         }
-        xn[row] = xi;
+        t = lanes_sum<LPR>(t);
+        d = lanes_sum<LPR>(d);
+        if (lane == 0 && g < n) {
+            float xi = x[row];
+            if (fabsf(d) > float(SMALLREAL)) {
+                const float r = b[row] - t;
+                xi += omega ? omega[row] * (r / d) : r / d;
+            }
+            xn[row] = xi;
+        }
+    };
+    if constexpr (!ACT) {
+        one_row((blockIdx.x * blockDim.x + threadIdx.x) / LPR);
+    } else {
+        const int nblk = (n + ACT_ROWS - 1) / ACT_ROWS;
+        for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+            if (!act[blk]) continue;
+            for (int pass = 0; pass < LPR; ++pass)
+                one_row(blk * ACT_ROWS + pass * (256 / LPR) + grp);
+        }
     }
+}
+
+// grid of the lane kernels: one row per group, or (with an activity array)
+// the 256-row blocks shared by at most 16 CTAs per SM
+static int vec_grid(int n, int lanes, bool act) {
+    if (!act) return div_up(n, 256 / lanes);
+    return std::max(1, std::min((n + ACT_ROWS - 1) / ACT_ROWS, 16 * sm_count()));
 }
 
 template <int MODE>
 static int spmv_vec_launch(const DCsr<float> &A, const float *x, const float *b, float *y,
                            float alpha, cudaStream_t s) {
     const int L = A.vec_lanes;
-    const int grid = div_up(A.n, 256 / L);
+    const bool act = A.act != nullptr;
+    const int grid = vec_grid(A.n, L, act);
+    auto go = [&](auto kernel) {
+        kernel<<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha, A.act);
+    };
     switch (L) {
-    case 2: k_spmv_vec<MODE, 2><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
-    case 4: k_spmv_vec<MODE, 4><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
-    case 8: k_spmv_vec<MODE, 8><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
-    default: k_spmv_vec<MODE, 16><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, x, b, y, alpha); break;
+    case 2: act ? go(k_spmv_vec<MODE, 2, true>) : go(k_spmv_vec<MODE, 2, false>); break;
+    case 4: act ? go(k_spmv_vec<MODE, 4, true>) : go(k_spmv_vec<MODE, 4, false>); break;
+    case 8: act ? go(k_spmv_vec<MODE, 8, true>) : go(k_spmv_vec<MODE, 8, false>); break;
+    default: act ? go(k_spmv_vec<MODE, 16, true>) : go(k_spmv_vec<MODE, 16, false>); break;
     }
     count_launch();
     HZB_LAUNCH_CHECK();
@@ -435,9 +492,33 @@ template int spmv<double>(const DCsr<double> &, int, const double *, const doubl
 template int spmv<float>(const DCsr<float> &, int, const float *, const float *,
                          float *, float, float *, cudaStream_t);
 
+// Decisions of the autotuners, kept per level shape (rows, stored entries)
+// for the life of the process: a later setup of a level of the same shape
+// reuses them instead of timing the candidates again.
+namespace {
+std::mutex tune_mu;
+std::map<std::pair<int, int>, int> tune_bundle_rows, tune_fp32_lanes;
+bool tune_lookup(std::map<std::pair<int, int>, int> &m, int n, int nnz, int *v) {
+    std::lock_guard<std::mutex> g(tune_mu);
+    auto it = m.find({n, nnz});
+    if (it == m.end()) return false;
+    *v = it->second;
+    return true;
+}
+void tune_store(std::map<std::pair<int, int>, int> &m, int n, int nnz, int v) {
+    std::lock_guard<std::mutex> g(tune_mu);
+    m[{n, nnz}] = v;
+}
+}  // namespace
+
 // Autotuner of the bundle size: times each candidate on this level's SpMV
 // (y = A x with the level's own buffers) and keeps the fastest.
 int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s) {
+    int known = 0;
+    if (tune_lookup(tune_bundle_rows, A.n, A.nnz, &known)) {
+        A.bundle_rows = known;
+        return bundle_capacity_rows(A.n, known, A.ia, s, &A.bundle_cap);
+    }
     const int cands[3] = {64, 128, 256};
     cudaEvent_t e0, e1;
     HZB_CUDA(cudaEventCreate(&e0));
@@ -462,12 +543,18 @@ int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s)
     cudaEventDestroy(e1);
     A.bundle_rows = best_rows;
     A.bundle_cap = best_cap;
+    tune_store(tune_bundle_rows, A.n, A.nnz, best_rows);
     return SUCCESS;
 }
 
 // FP32 schedule of a level: the staged bundles (vec_lanes 0) or 4/8/16 lanes
 // per row, whichever runs this level's l1-Jacobi sweep fastest.
 int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cudaStream_t s) {
+    int known = 0;
+    if (tune_lookup(tune_fp32_lanes, A.n, A.nnz, &known)) {
+        A.vec_lanes = known;
+        return SUCCESS;
+    }
     const int cands[4] = {0, 4, 8, 16};
     cudaEvent_t e0, e1;
     HZB_CUDA(cudaEventCreate(&e0));
@@ -489,6 +576,7 @@ int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cud
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     A.vec_lanes = pick;
+    tune_store(tune_fp32_lanes, A.n, A.nnz, pick);
     return SUCCESS;
 }
 
@@ -498,9 +586,10 @@ int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cud
 template <typename T>
 __global__ void k_restrict(int nc, const int *__restrict__ ria,
                            const int *__restrict__ rja, const T *__restrict__ w,
-                           T *__restrict__ bc) {
+                           T *__restrict__ bc, const unsigned char *__restrict__ act) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc;
          c += gridDim.x * blockDim.x) {
+        if (act && !act[c / ACT_ROWS]) continue;
         T t = T(0);
         for (int k = ria[c]; k < ria[c + 1]; ++k) t += w[rja[k]];
         bc[c] = t;
@@ -509,23 +598,25 @@ __global__ void k_restrict(int nc, const int *__restrict__ ria,
 
 template <typename T>
 int restrict_agg(int nc, const int *ria, const int *rja, const T *w, T *bc,
-                 cudaStream_t s) {
+                 cudaStream_t s, const unsigned char *act_c) {
     if (nc <= 0) return SUCCESS;
-    k_restrict<T><<<grid_for(nc), 256, 0, s>>>(nc, ria, rja, w, bc);
+    k_restrict<T><<<grid_for(nc), 256, 0, s>>>(nc, ria, rja, w, bc, act_c);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
 template int restrict_agg<double>(int, const int *, const int *, const double *,
-                                  double *, cudaStream_t);
+                                  double *, cudaStream_t, const unsigned char *);
 template int restrict_agg<float>(int, const int *, const int *, const float *,
-                                 float *, cudaStream_t);
+                                 float *, cudaStream_t, const unsigned char *);
 
 template <typename T>
 __global__ void k_prolong(int n, const int *__restrict__ agg,
-                          const T *__restrict__ xc, T *__restrict__ x, T alpha) {
+                          const T *__restrict__ xc, T *__restrict__ x, T alpha,
+                          const unsigned char *__restrict__ act) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += gridDim.x * blockDim.x) {
+        if (act && !act[i / ACT_ROWS]) continue;
         T t = T(0);
         const int c = agg[i];
         if (c >= 0) t += xc[c];
@@ -537,17 +628,17 @@ __global__ void k_prolong(int n, const int *__restrict__ agg,
 
 template <typename T>
 int prolong_agg(int n, const int *agg, const T *xc, T *x, T alpha,
-                cudaStream_t s) {
+                cudaStream_t s, const unsigned char *act) {
     if (n <= 0) return SUCCESS;
-    k_prolong<T><<<grid_for(n), 256, 0, s>>>(n, agg, xc, x, alpha);
+    k_prolong<T><<<grid_for(n), 256, 0, s>>>(n, agg, xc, x, alpha, act);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
 template int prolong_agg<double>(int, const int *, const double *, double *,
-                                 double, cudaStream_t);
+                                 double, cudaStream_t, const unsigned char *);
 template int prolong_agg<float>(int, const int *, const float *, float *, float,
-                                cudaStream_t);
+                                cudaStream_t, const unsigned char *);
 
 // ---------------------------------------------------------------------------
 // Point smoothers
@@ -590,14 +681,14 @@ __device__ __forceinline__ T l1_update(int i, T t, T d, const T *__restrict__ x,
     return xi;
 }
 
-template <typename T, int ROWS>
+template <typename T, int ROWS, bool ACT>
 __global__ void __launch_bounds__(ROWS)
 k_l1_bundle(int n, const int *__restrict__ ia, const int *__restrict__ ja,
             const T *__restrict__ a, const T *__restrict__ b,
             const T *__restrict__ x, T *__restrict__ xn,
-            const float *__restrict__ omega, int cap) {
+            const float *__restrict__ omega, int cap, const unsigned char *__restrict__ act) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    bundle_pipeline<T, ROWS>(n, ia, a, ja, cap, smem_raw,
+    bundle_pipeline<T, ROWS, ACT>(n, ia, a, ja, cap, act, smem_raw,
                              [&](int, int r0, int r1, int s0, const T *sv, const int *sc,
                                  const int *sia) {
         const int i = r0 + threadIdx.x;
@@ -618,9 +709,10 @@ template <typename T, int ROWS>
 __global__ void __launch_bounds__(ROWS)
 k_l1_rows(int n, const int *__restrict__ ia, const int *__restrict__ ja,
           const T *__restrict__ a, const T *__restrict__ b, const T *__restrict__ x,
-          T *__restrict__ xn, const float *__restrict__ omega) {
+          T *__restrict__ xn, const float *__restrict__ omega,
+          const unsigned char *__restrict__ act) {
     const int i = blockIdx.x * ROWS + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (act && !act[i / ACT_ROWS])) return;
     T t = b[i], d = T(0);
     for (int k = ia[i]; k < ia[i + 1]; ++k) {
         const T v = a[k];
@@ -638,15 +730,24 @@ static int l1_launch(const DCsr<T> &A, const T *b, const T *x, T *xn, const floa
     if (staged_ok(A, ROWS, &smem)) {
         static bool done = false;
         if (!done) {
-            cudaFuncSetAttribute(k_l1_bundle<T, ROWS>,
+            cudaFuncSetAttribute(k_l1_bundle<T, ROWS, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
+            cudaFuncSetAttribute(k_l1_bundle<T, ROWS, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SPMV_SMEM_MAX);
             done = true;
         }
-        const int grid = persistent_grid(k_l1_bundle<T, ROWS>, ROWS, smem, nb);
-        k_l1_bundle<T, ROWS><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega,
-                                                      A.bundle_cap);
+        if (A.act) {
+            const int grid = persistent_grid(k_l1_bundle<T, ROWS, true>, ROWS, smem, nb);
+            k_l1_bundle<T, ROWS, true><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x,
+                                                                xn, omega, A.bundle_cap, A.act);
+        } else {
+            const int grid = persistent_grid(k_l1_bundle<T, ROWS, false>, ROWS, smem, nb);
+            k_l1_bundle<T, ROWS, false><<<grid, ROWS, smem, s>>>(A.n, A.ia, A.ja, A.val, b, x,
+                                                                 xn, omega, A.bundle_cap,
+                                                                 nullptr);
+        }
     } else {
-        k_l1_rows<T, ROWS><<<nb, ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega);
+        k_l1_rows<T, ROWS><<<nb, ROWS, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega, A.act);
     }
     count_launch();
     HZB_LAUNCH_CHECK();
@@ -656,12 +757,16 @@ static int l1_launch(const DCsr<T> &A, const T *b, const T *x, T *xn, const floa
 static int l1_vec_launch(const DCsr<float> &A, const float *b, const float *x, float *xn,
                          const float *omega, cudaStream_t s) {
     const int L = A.vec_lanes;
-    const int grid = div_up(A.n, 256 / L);
+    const bool act = A.act != nullptr;
+    const int grid = vec_grid(A.n, L, act);
+    auto go = [&](auto kernel) {
+        kernel<<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega, A.act);
+    };
     switch (L) {
-    case 2: k_l1_vec<2><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
-    case 4: k_l1_vec<4><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
-    case 8: k_l1_vec<8><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
-    default: k_l1_vec<16><<<grid, 256, 0, s>>>(A.n, A.ia, A.ja, A.val, b, x, xn, omega); break;
+    case 2: act ? go(k_l1_vec<2, true>) : go(k_l1_vec<2, false>); break;
+    case 4: act ? go(k_l1_vec<4, true>) : go(k_l1_vec<4, false>); break;
+    case 8: act ? go(k_l1_vec<8, true>) : go(k_l1_vec<8, false>); break;
+    default: act ? go(k_l1_vec<16, true>) : go(k_l1_vec<16, false>); break;
     }
     count_launch();
     HZB_LAUNCH_CHECK();
@@ -699,9 +804,11 @@ __global__ void k_l1_norms(int n, const int *__restrict__ ia, const T *__restric
 
 template <typename T>
 __global__ void k_l1_first(int n, const T *__restrict__ b, const T *__restrict__ d,
-                           T *__restrict__ xn, const float *__restrict__ omega) {
+                           T *__restrict__ xn, const float *__restrict__ omega,
+                           const unsigned char *__restrict__ act) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += gridDim.x * blockDim.x) {
+        if (act && !act[i / ACT_ROWS]) continue;
         const T di = d[i];
         T xi = T(0);
         if (fabs(di) > T(SMALLREAL)) xi += (omega ? T(omega[i]) : T(1)) * (b[i] / di);
@@ -719,9 +826,9 @@ int l1_norms(const DCsr<T> &A, T *d, cudaStream_t s) {
 }
 template <typename T>
 int l1_first_sweep(int n, const T *b, const T *d, T *xn, const float *omega,
-                   cudaStream_t s) {
+                   cudaStream_t s, const unsigned char *act) {
     if (n <= 0) return SUCCESS;
-    k_l1_first<T><<<grid_for(n), 256, 0, s>>>(n, b, d, xn, omega);
+    k_l1_first<T><<<grid_for(n), 256, 0, s>>>(n, b, d, xn, omega, act);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
@@ -729,9 +836,9 @@ int l1_first_sweep(int n, const T *b, const T *d, T *xn, const float *omega,
 template int l1_norms<float>(const DCsr<float> &, float *, cudaStream_t);
 template int l1_norms<double>(const DCsr<double> &, double *, cudaStream_t);
 template int l1_first_sweep<float>(int, const float *, const float *, float *,
-                                   const float *, cudaStream_t);
+                                   const float *, cudaStream_t, const unsigned char *);
 template int l1_first_sweep<double>(int, const double *, const double *, double *,
-                                    const float *, cudaStream_t);
+                                    const float *, cudaStream_t, const unsigned char *);
 
 // Gauss-Seidel family on independent rows.  x is read with plain loads:
 // in gs_run earlier sets of the same CTA wrote it.
@@ -979,26 +1086,28 @@ template int vcopy<int>(int, const int *, int *, cudaStream_t);
 template int vzero<double>(int, double *, cudaStream_t);
 template int vzero<float>(int, float *, cudaStream_t);
 
-__global__ void k_d2f(int n, const double *__restrict__ x, float *__restrict__ y) {
+__global__ void k_d2f(int n, const double *__restrict__ x, float *__restrict__ y,
+                      const unsigned char *__restrict__ act) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += gridDim.x * blockDim.x)
-        y[i] = (float)x[i];
+        if (!act || act[i / ACT_ROWS]) y[i] = (float)x[i];
 }
-__global__ void k_f2d(int n, const float *__restrict__ x, double *__restrict__ y) {
+__global__ void k_f2d(int n, const float *__restrict__ x, double *__restrict__ y,
+                      const unsigned char *__restrict__ act) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += gridDim.x * blockDim.x)
-        y[i] = (double)x[i];
+        if (!act || act[i / ACT_ROWS]) y[i] = (double)x[i];
 }
-int d2f(int n, const double *x, float *y, cudaStream_t s) {
+int d2f(int n, const double *x, float *y, cudaStream_t s, const unsigned char *act) {
     if (n <= 0) return SUCCESS;
-    k_d2f<<<grid_for(n), 256, 0, s>>>(n, x, y);
+    k_d2f<<<grid_for(n), 256, 0, s>>>(n, x, y, act);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
-int f2d(int n, const float *x, double *y, cudaStream_t s) {
+int f2d(int n, const float *x, double *y, cudaStream_t s, const unsigned char *act) {
     if (n <= 0) return SUCCESS;
-    k_f2d<<<grid_for(n), 256, 0, s>>>(n, x, y);
+    k_f2d<<<grid_for(n), 256, 0, s>>>(n, x, y, act);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;

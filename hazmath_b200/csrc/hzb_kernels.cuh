@@ -21,7 +21,11 @@ struct DCsr {
     // staged bundles.  A row's partial sums are combined across its lanes,
     // so this is not the sequential CSR-order sum of the FP64 kernels.
     int vec_lanes = 0;
+    // Optional activity of 256-row blocks (ACT_ROWS): kernels skip the rows
+    // of a block whose byte is 0 (batched solves skip converged systems).
+    const unsigned char *act = nullptr;
 };
+constexpr int ACT_ROWS = 256;
 
 constexpr int SPMV_ROWS = 128;          // rows per CTA in the row-bundle SpMV
 constexpr int SPMV_SMEM_MAX = 160 * 1024;
@@ -49,11 +53,11 @@ int spmv_blocks(int n);
 // b_c[c] = sum over R row c of w (R rows list fine indices ascending).
 template <typename T>
 int restrict_agg(int nc, const int *ria, const int *rja, const T *w, T *bc,
-                 cudaStream_t s);
+                 cudaStream_t s, const unsigned char *act_c = nullptr);
 // x_i (+/-)= alpha * x_c[agg_i] as dcsr_aAxpy_agg does for unit P.
 template <typename T>
 int prolong_agg(int n, const int *agg, const T *xc, T *x, T alpha,
-                cudaStream_t s);
+                cudaStream_t s, const unsigned char *act = nullptr);
 // fused: x_i += x_c[agg_i] (alpha = 1), then the first l1-Jacobi sweep
 // reads the updated x -- kept separate in parity mode.
 
@@ -70,7 +74,7 @@ template <typename T>
 int l1_norms(const DCsr<T> &A, T *d, cudaStream_t s);
 template <typename T>
 int l1_first_sweep(int n, const T *b, const T *d, T *xn, const float *omega,
-                   cudaStream_t s);
+                   cudaStream_t s, const unsigned char *act = nullptr);
 // Gauss-Seidel family on a list of independent rows (one level set / colour).
 //   kind 0: x_i = t * d_i            (GS, d_i = 1/a_ii)
 //   kind 1: x_i = w (t/d_i) + (1-w) x_i  if |d_i| > 1e-20   (SOR)
@@ -113,8 +117,8 @@ int vcopy(int n, const T *x, T *y, cudaStream_t s);
 template <typename T>
 int vzero(int n, T *y, cudaStream_t s);
 // precision conversions
-int d2f(int n, const double *x, float *y, cudaStream_t s);
-int f2d(int n, const float *x, double *y, cudaStream_t s);
+int d2f(int n, const double *x, float *y, cudaStream_t s, const unsigned char *act = nullptr);
+int f2d(int n, const float *x, double *y, cudaStream_t s, const unsigned char *act = nullptr);
 int csr_val_d2f(int nnz, const double *x, float *y, cudaStream_t s);
 // entries != 0 per row, and the FP32 copy of those entries (row pointer ia32
 // from a scan of the counts)

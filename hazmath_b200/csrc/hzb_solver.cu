@@ -143,18 +143,18 @@ int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
     const double w = cyc.relaxation;
     const DCsr<double> A = L.A64();
     switch (cyc.smoother) {
+    // Jacobi-type sweeps read x and write a new iterate: they alternate
+    // between x and t, and an odd count ends with one copy back into x.
     case SMOOTHER_JACOBI:
-        for (int k = 0; k < sweeps; ++k) {
-            HZB_TRY(jacobi_sweep(A, L.d_jac, L.b, L.x, L.t, S->s));
-            HZB_TRY(vcopy(L.n, L.t, L.x, S->s));
-        }
+        for (int k = 0; k < sweeps; ++k)
+            HZB_TRY(jacobi_sweep(A, L.d_jac, L.b, k & 1 ? L.t : L.x, k & 1 ? L.x : L.t, S->s));
+        if (sweeps & 1) HZB_TRY(vcopy(L.n, L.t, L.x, S->s));
         return SUCCESS;
     case SMOOTHER_L1DIAG: {
         const float *om = (l == 0 && S->omega_active) ? S->omega : nullptr;
-        for (int k = 0; k < sweeps; ++k) {
-            HZB_TRY(l1_sweep<double>(A, L.b, L.x, L.t, om, S->s));
-            HZB_TRY(vcopy(L.n, L.t, L.x, S->s));
-        }
+        for (int k = 0; k < sweeps; ++k)
+            HZB_TRY(l1_sweep<double>(A, L.b, k & 1 ? L.t : L.x, k & 1 ? L.x : L.t, om, S->s));
+        if (sweeps & 1) HZB_TRY(vcopy(L.n, L.t, L.x, S->s));
         return SUCCESS;
     }
     case SMOOTHER_GS:
@@ -303,7 +303,7 @@ static int smooth32(hzb_solver *S, int l, bool pre, const AMG_param &cyc, bool x
         for (int j = 0; j < sweeps; ++j) {
             float *dst = ((sweeps - 1 - j) & 1) ? L.t32 : L.x32;
             if (j == 0 && xzero)
-                HZB_TRY(l1_first_sweep<float>(L.n, L.b32, L.l1_32, dst, om, S->s));
+                HZB_TRY(l1_first_sweep<float>(L.n, L.b32, L.l1_32, dst, om, S->s, L.act));
             else
                 HZB_TRY(l1_sweep<float>(A, L.b32, prev, dst, om, S->s));
             prev = dst;
@@ -342,7 +342,8 @@ forward:
         HZB_TRY(smooth32(S, l, true, cyc, zero[l]));
         zero[l] = false;
         HZB_TRY(spmv<float>(L.A32(), SPMV_RES, L.x32, L.b32, L.w32, 1.0f, nullptr, S->s));
-        HZB_TRY(restrict_agg<float>(L.nc, L.ria, L.rja, L.w32, S->lv[l + 1].b32, S->s));
+        HZB_TRY(restrict_agg<float>(L.nc, L.ria, L.rja, L.w32, S->lv[l + 1].b32, S->s,
+                                    S->lv[l + 1].act));
         ++l;
         if (l < nl - 1) zero[l] = true;   // x_l = 0, folded into its first sweep
     }
@@ -353,7 +354,7 @@ forward:
     while (l > 0) {
         --l;
         Level &L = S->lv[l];
-        HZB_TRY(prolong_agg<float>(L.n, L.agg, S->lv[l + 1].x32, L.x32, 1.0f, S->s));
+        HZB_TRY(prolong_agg<float>(L.n, L.agg, S->lv[l + 1].x32, L.x32, 1.0f, S->s, L.act));
         HZB_TRY(smooth32(S, l, false, cyc, false));
         if (num_lvl[l] < cyc.cycle_type) break;
         else num_lvl[l] = 0;

@@ -18,6 +18,9 @@ struct Level {
     // entry adds nothing to a row sum); aliases ia/ja when there are none
     int nnz32 = 0, bundle_cap32 = 0;
     int vec32 = 0;                    // FP32 schedule: lanes per row, 0 = bundles
+    // activity of 256-row blocks while a batched solve runs (else null):
+    // the level kernels skip blocks of converged systems
+    const unsigned char *act = nullptr;
     int *ia32 = nullptr, *ja32 = nullptr;
     float *val32 = nullptr;
     bool own32 = false;
@@ -46,6 +49,7 @@ struct Level {
         DCsr<double> m;
         m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val; m.bundle_cap = bundle_cap;
         m.bundle_rows = bundle_rows;
+        m.act = act;
         return m;
     }
     DCsr<float> A32() const {
@@ -54,6 +58,7 @@ struct Level {
         m.bundle_cap = bundle_cap32;
         m.bundle_rows = bundle_rows;
         m.vec_lanes = vec32;
+        m.act = act;
         return m;
     }
     void release();
