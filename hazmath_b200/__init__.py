@@ -39,6 +39,7 @@ ERROR_SOLVER_TOLSMALL = -44
 ERROR_SOLVER_MISC = -47
 ERROR_SOLVER_MAXIT = -48
 SOLVER_CG = 1
+SOLVER_MinRes, SOLVER_VGMRES, SOLVER_VFGMRES = 2, 3, 4
 SOLVER_UMFPACK = 32
 STOP_REL_RES, STOP_REL_PRECRES, STOP_MOD_REL_RES = 1, 2, 3
 PREC_AMG = 2
@@ -189,6 +190,9 @@ def lib() -> C.CDLL:
         L.hzb_free_device.argtypes = [C.c_void_p]
         L.dcsr_pcg.argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL, INT,
                                SHORT, SHORT]
+        for name in ("dcsr_pvgmres", "dcsr_pvfgmres"):
+            getattr(L, name).argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL,
+                                         INT, SHORT, SHORT, SHORT]
         L.python_wrapper_krylov_amg.argtypes = [P(INT), P(INT), C.c_void_p, C.c_void_p,
                                                 C.c_void_p, C.c_void_p, C.c_void_p, P(REAL),
                                                 P(INT), P(INT)]
@@ -358,6 +362,14 @@ class AMGHierarchy:
         bb = np.ascontiguousarray(b, np.float64)
         return lib().dcsr_pcg(C.byref(self._A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),
                               C.byref(self.pc), tol, maxit, stop_type, prtlvl)
+
+    def gmres(self, b, x, tol=1e-8, maxit=500, restart=100, flexible=True,
+              stop_type=STOP_REL_RES, prtlvl=0):
+        """dcsr_pvfgmres (flexible) or dcsr_pvgmres with precond_amg."""
+        bb = np.ascontiguousarray(b, np.float64)
+        f = lib().dcsr_pvfgmres if flexible else lib().dcsr_pvgmres
+        return f(C.byref(self._A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),
+                 C.byref(self.pc), C.c_double(tol), maxit, restart, stop_type, prtlvl)
 
     def free(self):
         if self.mgl:

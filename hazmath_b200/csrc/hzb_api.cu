@@ -267,8 +267,13 @@ extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
     } else if (S->it.linear_itsolver_type == SOLVER_CG) {
         it = pcg(S, S->lv[0].A64(), d_b, d_x, PC_AMG, nullptr, S->it.linear_tol,
                  S->it.linear_maxit, S->it.linear_stop_type, prt, S->kw, &rel, &cond);
+    } else if (S->it.linear_itsolver_type == SOLVER_VGMRES ||
+               S->it.linear_itsolver_type == SOLVER_VFGMRES) {
+        it = gmres(S, S->lv[0].A64(), d_b, d_x, PC_AMG, nullptr, S->it.linear_tol,
+                   S->it.linear_maxit, S->it.linear_restart, S->it.linear_stop_type, prt,
+                   S->it.linear_itsolver_type == SOLVER_VFGMRES, &rel);
     } else {
-        set_error_msg("only the CG Krylov method (linear_itsolver_type = 1) is built");
+        set_error_msg("Krylov types 1 (CG), 3 (GMRES) and 4 (flexible GMRES) are built");
         return ERROR_SOLVER_TYPE;
     }
     HZB_CUDA(cudaEventRecord(S->e1, S->s));
@@ -643,8 +648,12 @@ static int upload_csr(const dCSRmat *A, TmpCsr &T, DCsr<double> &D, cudaStream_t
     return SUCCESS;
 }
 
-static INT pcg_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol,
-                    INT MaxIt, SHORT stop_type, SHORT prtlvl, double *condest) {
+// A Krylov method (type: SOLVER_CG, SOLVER_VGMRES or SOLVER_VFGMRES) on host
+// arrays with the caller's preconditioner: the setup's own AMG runs on the
+// device, any other pc->fct is called on host copies.
+static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol,
+                       INT MaxIt, SHORT stop_type, SHORT prtlvl, double *condest, int type,
+                       int restart) {
     if (!A || !b || !u || A->row != b->row || A->row != u->row) return ERROR_MAT_SIZE;
     HZB_TRY(check_csr_host(A->row, A->nnz, A->IA));
     hzb_solver *S = nullptr, *own = nullptr;
@@ -690,7 +699,11 @@ static INT pcg_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol,
         cudaMemcpyAsync(db, b->val, sizeof(double) * A->row, cudaMemcpyHostToDevice, S->s);
         cudaMemcpyAsync(du, u->val, sizeof(double) * A->row, cudaMemcpyHostToDevice, S->s);
         double rel = 0.0;
-        it = pcg(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, w, &rel, condest);
+        if (type == SOLVER_CG)
+            it = pcg(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, w, &rel, condest);
+        else
+            it = gmres(S, D, db, du, kind, &hp, tol, MaxIt, restart, stop_type, prtlvl,
+                       type == SOLVER_VFGMRES, &rel);
         if (it != ERROR_SOLVER_MISC) {
             cudaMemcpyAsync(u->val, du, sizeof(double) * A->row, cudaMemcpyDeviceToHost, S->s);
             if (cudaStreamSynchronize(S->s) != cudaSuccess) it = ERROR_SOLVER_MISC;
@@ -709,7 +722,32 @@ extern "C" INT dcsr_pcg(dCSRmat *A, dvector *b, dvector *u, precond *pc,
                         const REAL tol, const INT MaxIt, const SHORT stop_type,
                         const SHORT prtlvl) {
     // krylov.c:122-398
-    return pcg_host(A, b, u, pc, tol, MaxIt, stop_type, prtlvl, nullptr);
+    return krylov_host(A, b, u, pc, tol, MaxIt, stop_type, prtlvl, nullptr, SOLVER_CG, 0);
+}
+
+extern "C" INT dcsr_pvgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
+                            const REAL tol, const INT MaxIt, const SHORT restart,
+                            const SHORT stop_type, const SHORT prtlvl) {
+    // krylov.c:4612-4930
+    return krylov_host(A, b, x, pc, tol, MaxIt, stop_type, prtlvl, nullptr, SOLVER_VGMRES,
+                       restart);
+}
+
+extern "C" INT dcsr_pvfgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
+                             const REAL tol, const INT MaxIt, const SHORT restart,
+                             const SHORT stop_type, const SHORT prtlvl) {
+    // krylov.c:5974-6250
+    return krylov_host(A, b, x, pc, tol, MaxIt, stop_type, prtlvl, nullptr, SOLVER_VFGMRES,
+                       restart);
+}
+
+// the banner solver_dcsr_linear_itsolver prints for a Krylov type
+static void krylov_banner(SHORT prtlvl, SHORT type) {
+    if (prtlvl <= PRINT_NONE) return;
+    printf("**********************************************************\n");
+    if (type == SOLVER_CG) printf(" --> using Conjugate Gradient Method:\n");
+    else if (type == SOLVER_VGMRES) printf(" --> using GMRES Method:\n");
+    else printf(" --> using Flexible GMRES Method:\n");
 }
 
 extern "C" INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
@@ -722,18 +760,16 @@ extern "C" INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
         printf("### HAZMATH WARNING: Convergence tolerance for iterative solver is too small!\n");
     if (itparam->linear_maxit <= 0)
         printf("### HAZMATH WARNING: Max number of iterations should be a POSITIVE integer!\n");
-    if (type != SOLVER_CG) {
+    if (type != SOLVER_CG && type != SOLVER_VGMRES && type != SOLVER_VFGMRES) {
         printf("### ERROR: Unknown itertive solver type %lld!\n", (long long)type);
         return ERROR_SOLVER_TYPE;
     }
-    if (prtlvl > PRINT_NONE) {
-        printf("**********************************************************\n");
-        printf(" --> using Conjugate Gradient Method:\n");
-    }
+    krylov_banner(prtlvl, type);
     double cond = 0.0;
-    INT it = pcg_host(A, b, x, pc, itparam->linear_tol, itparam->linear_maxit,
-                      itparam->linear_stop_type, prtlvl, &cond);
-    printf("Estimated condition number = %13.6e\n", cond);
+    INT it = krylov_host(A, b, x, pc, itparam->linear_tol, itparam->linear_maxit,
+                         itparam->linear_stop_type, prtlvl, &cond, type,
+                         itparam->linear_restart);
+    if (type == SOLVER_CG) printf("Estimated condition number = %13.6e\n", cond);
     return it;
 }
 
@@ -758,18 +794,16 @@ extern "C" INT hzb_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
         if (amgparam->print_level >= PRINT_SOME) print_complexity(S);
         printf("Unsmoothed aggregation setup costs %.4f seconds.\n", S->st.setup_seconds);
     }
-    if (bp->precision != HZB_PREC_MIXED && itparam->linear_itsolver_type != SOLVER_CG) {
-        printf("### ERROR: Unknown itertive solver type %lld!\n",
-               (long long)itparam->linear_itsolver_type);
+    const SHORT type = itparam->linear_itsolver_type;
+    if (bp->precision != HZB_PREC_MIXED && type != SOLVER_CG && type != SOLVER_VGMRES &&
+        type != SOLVER_VFGMRES) {
+        printf("### ERROR: Unknown itertive solver type %lld!\n", (long long)type);
         hzb_destroy(S);
         return ERROR_SOLVER_TYPE;
     }
-    if (prtlvl > PRINT_NONE) {
-        printf("**********************************************************\n");
-        printf(" --> using Conjugate Gradient Method:\n");
-    }
+    krylov_banner(prtlvl, bp->precision == HZB_PREC_MIXED ? SOLVER_CG : type);
     INT it = hzb_solve_host(S, b->val, x->val);
-    if (bp->precision != HZB_PREC_MIXED)
+    if (bp->precision != HZB_PREC_MIXED && type == SOLVER_CG)
         printf("Estimated condition number = %13.6e\n", S->st.condest);
     if (prtlvl >= PRINT_MIN) {
         printf("AMG_Krylov method totally costs %.4f seconds.\n",

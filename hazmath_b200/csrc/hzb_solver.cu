@@ -657,6 +657,11 @@ static int apply_pc(hzb_solver *S, int kind, HostPrecond *hp, int n,
     return vcopy<double>(n, r, z, S->s);
 }
 
+int apply_precond(hzb_solver *S, int kind, HostPrecond *hp, int n, const double *r,
+                  double *z) {
+    return apply_pc(S, kind, hp, n, r, z);
+}
+
 // residual measure for the stopping type (krylov.c:157-170, 211-227)
 static int measure(hzb_solver *S, KrylovWork &w, int kind, HostPrecond *hp,
                    int stop_type, double *absres) {

@@ -136,6 +136,14 @@ int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
         int pc_kind, HostPrecond *hp, double tol, int maxit, int stop_type,
         int prtlvl, KrylovWork &w, double *relres_out, double *condest);
 enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2 };
+// z = M r for a preconditioner kind of pcg / gmres
+int apply_precond(hzb_solver *S, int kind, HostPrecond *hp, int n, const double *r,
+                  double *z);
+// variable-restart GMRES (flexible = false, dcsr_pvgmres) or flexible GMRES
+// (dcsr_pvfgmres), right-preconditioned (hzb_gmres.cu)
+int gmres(hzb_solver *S, const DCsr<double> &A, const double *b, double *x, int kind,
+          HostPrecond *hp, double tol, int MaxIt, int restart, int stop_type, int prtlvl,
+          bool flexible, double *relres_out);
 // FP32-cycle flexible CG (mixed precision)
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out);

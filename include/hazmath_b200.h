@@ -286,7 +286,9 @@ INT linear_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
  * (amg_solve, src/solver/amg_solve.c:109). */
 INT linear_solver_amg(dCSRmat *A, dvector *b, dvector *x, AMG_param *param);
 
-/* src/solver/itsolver.c:135-229: Krylov switch on a host preconditioner. */
+/* src/solver/itsolver.c:135-229: Krylov switch on a host preconditioner:
+ * type 1 CG (prints the condition estimate), 3 variable-restart GMRES, 4
+ * flexible GMRES; MINRES (2) returns ERROR_SOLVER_TYPE. */
 INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
                                 precond *pc, linear_itsolver_param *itparam);
 
@@ -308,6 +310,21 @@ void precond_amg(REAL *r, REAL *z, void *data);
 INT dcsr_pcg(dCSRmat *A, dvector *b, dvector *u, precond *pc,
              const REAL tol, const INT MaxIt, const SHORT stop_type,
              const SHORT prtlvl);
+
+/* src/solver/krylov.c:4612-4930: right-preconditioned GMRES whose restart
+ * length adapts to the convergence rate of each cycle (Baker, Jessup and
+ * Kolev).  Preconditioner handling as dcsr_pcg; MaxIt reached (iter >=
+ * MaxIt) returns ERROR_SOLVER_MAXIT. */
+INT dcsr_pvgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
+                 const REAL tol, const INT MaxIt, const SHORT restart,
+                 const SHORT stop_type, const SHORT prtlvl);
+
+/* src/solver/krylov.c:5974-6250: the flexible form (every preconditioned
+ * vector kept, stopping on ||r|| <= tol ||b||); Krylov type 4, the
+ * reference's default with restart 100. */
+INT dcsr_pvfgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
+                  const REAL tol, const INT MaxIt, const SHORT restart,
+                  const SHORT stop_type, const SHORT prtlvl);
 
 /* src/utilities/wrapper.c:36-99.  The reference reads ./input.dat; this one
  * uses the UA-AMG defaults of the HAZmath examples (V-cycle, GS 1/1, HEM,

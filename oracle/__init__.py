@@ -256,6 +256,20 @@ class Ref(_Backend):
     def timings(self):
         return self.lib.ref_setup_seconds(), self.lib.ref_solve_seconds()
 
+    def gmres(self, b, x0=None, tol=1e-8, maxit=500, restart=25, flexible=True,
+              stop_type=1, hist_cap=1024):
+        """dcsr_pvfgmres (flexible) or dcsr_pvgmres with the AMG
+        preconditioner of the last setup: (iterations, x, ||r|| at each
+        preconditioner call)."""
+        b = np.ascontiguousarray(b, np.float64).copy()
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        hist = np.zeros(hist_cap)
+        nh = ctypes.c_int()
+        it = self.lib.ref_gmres(4 if flexible else 3, _p(b), _p(x), ctypes.c_double(tol),
+                                maxit, restart, stop_type, 0, _p(hist), hist_cap,
+                                ctypes.byref(nh))
+        return it, x, hist[: min(nh.value, hist_cap)].copy()
+
     def free(self):
         self.lib.ref_free()
 

@@ -162,6 +162,31 @@ int ref_pcg(double *b, double *x, double tol, int maxit, int stop_type,
     return it;
 }
 
+/* Variable-restart GMRES (type 3: dcsr_pvgmres, krylov.c:4612) or its
+ * flexible form (type 4: dcsr_pvfgmres, krylov.c:5974) with the AMG
+ * preconditioner, as solver_dcsr_linear_itsolver (itsolver.c:135) calls
+ * them; hist as for ref_pcg.                                               */
+int ref_gmres(int type, double *b, double *x, double tol, int maxit, int restart,
+              int stop_type, int print_level, double *hist, int hist_cap, int *nhist)
+{
+    dvector bb, xx;
+    bb.row = g_A.row; bb.val = b;
+    xx.row = g_A.row; xx.val = x;
+    g_hist = hist; g_hist_cap = hist ? hist_cap : 0; g_hist_n = 0;
+    precond pc = g_pc;
+    pc.fct = hist ? hist_precond : precond_amg;
+    double t0 = now_s();
+    int it = type == 4
+        ? dcsr_pvfgmres(&g_A, &bb, &xx, &pc, tol, maxit, (SHORT)restart, (SHORT)stop_type,
+                        (SHORT)print_level)
+        : dcsr_pvgmres(&g_A, &bb, &xx, &pc, tol, maxit, (SHORT)restart, (SHORT)stop_type,
+                       (SHORT)print_level);
+    g_solve_s = now_s() - t0;
+    if (nhist) *nhist = g_hist_n;
+    g_hist = NULL; g_hist_cap = 0;
+    return it;
+}
+
 /* ---- kernel-level entry points on caller arrays -------------------------- */
 static dCSRmat wrap(int n, int m, int nnz, int *ia, int *ja, double *val)
 {

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -31,7 +31,9 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from hazmath_b200 import problems as P  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HAZ_REF", "/root/reference")
+ARGS = [a for i, a in enumerate(sys.argv[1:], 1)
+        if a != "--only" and sys.argv[i - 1] != "--only"]
+REF = ARGS[0] if ARGS else os.environ.get("HAZ_REF", "/root/reference")
 
 
 def sha(a) -> str:
@@ -94,10 +96,47 @@ printf("\"end\": 0\n");return 0;}
     return d
 
 
+def gmres_cases(R):
+    """The reference's variable-restart GMRES (type 3) and flexible GMRES
+    (type 4) with its AMG preconditioner: iterations, solution and the
+    residual norm at every preconditioner call."""
+    out = {}
+    ia, ja, val = P.read_coo(os.path.join(REF, "examples", "solvers", "A.dat"))
+    b = np.loadtxt(os.path.join(REF, "examples", "solvers", "b.dat"), skiprows=1)
+    k = P.lognormal_field(14, 1.0, 4.0, 5)
+    kia, kja, kval = P.kuhn3d_p1(14, k)
+    kb = P.rhs_uniform(len(kia) - 1, 6)
+    cases = [("fix", ia, ja, val, b, oracle.AMGParams()),
+             ("kuhn", kia, kja, kval, kb,
+              oracle.AMGParams(smoother=10, presmooth_iter=2, postsmooth_iter=2, coarse_dof=100))]
+    for name, cia, cja, cval, cb, prm in cases:
+        assert R.setup(cia, cja, cval, prm) == 0
+        out[f"{name}/A_ia"], out[f"{name}/A_ja"], out[f"{name}/A_val"] = cia, cja, cval
+        out[f"{name}/b"] = cb
+        out[f"{name}/params"] = np.array(prm.arrays()[0][:], np.int64)
+        out[f"{name}/dparams"] = np.array(prm.arrays()[1][:])
+        for flex in (0, 1):
+            for restart in (3, 7, 25, 100):
+                for stop in ((1, 2, 3) if restart == 25 else (1,)):
+                    it, x, hist = R.gmres(cb, tol=1e-8, maxit=300, restart=restart,
+                                          flexible=bool(flex), stop_type=stop)
+                    key = f"{name}/{'f' if flex else 'v'}{restart}_s{stop}"
+                    out[key + "/iters"] = np.int64(it)
+                    if restart in (3, 25) and stop == 1:
+                        out[key + "/x"] = x
+                    out[key + "/hist"] = hist
+                    print("gmres", key, it)
+        R.free()
+    np.savez_compressed(os.path.join(HERE, "gmres.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
     R = oracle.ref()
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "gmres":
+        gmres_cases(R)
+        return
     rng = np.random.default_rng(20261203)
     base = oracle.AMGParams()
 
@@ -194,6 +233,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, "rap.npz"), ia=ia, ja=ja, val=val, agg=agg,
                         nc=np.int64(nc), cia=cia, cja=cja, cval=cval)
     R.free()
+    # 7. GMRES and flexible GMRES (Krylov types 3 and 4)
+    gmres_cases(R)
     print("golden fixtures written to", HERE)
 
 

@@ -160,7 +160,7 @@ def _spmv(ia, ja, val, x):
 
 
 def test_error_codes():
-    it = hz.itsolver_param(linear_itsolver_type=3, linear_tol=1e-8)
+    it = hz.itsolver_param(linear_itsolver_type=hz.SOLVER_MinRes, linear_tol=1e-8)
     ia, ja, val = P.poisson2d_5pt(20)
     x = np.zeros(400)
     b = np.ones(400)
