@@ -39,13 +39,13 @@ ERROR_SOLVER_TOLSMALL = -44
 ERROR_SOLVER_MISC = -47
 ERROR_SOLVER_MAXIT = -48
 SOLVER_CG = 1
-SOLVER_MinRes, SOLVER_VGMRES, SOLVER_VFGMRES = 2, 3, 4
+SOLVER_MinRes, SOLVER_VGMRES, SOLVER_VFGMRES, SOLVER_GCG = 2, 3, 4, 5
 SOLVER_UMFPACK = 32
 STOP_REL_RES, STOP_REL_PRECRES, STOP_MOD_REL_RES = 1, 2, 3
 PREC_AMG = 2
 UA_AMG = 1
 VMB, HEC, HEM = 1, 4, 5
-V_CYCLE, W_CYCLE = 1, 2
+V_CYCLE, W_CYCLE, AMLI_CYCLE, NL_AMLI_CYCLE, ADD_CYCLE = 1, 2, 3, 4, 5
 SMOOTHER_JACOBI, SMOOTHER_GS, SMOOTHER_SGS = 1, 2, 3
 SMOOTHER_SOR, SMOOTHER_SSOR, SMOOTHER_GSOR, SMOOTHER_SGSOR = 5, 6, 7, 8
 SMOOTHER_L1DIAG = 10
@@ -193,6 +193,14 @@ def lib() -> C.CDLL:
         for name in ("dcsr_pvgmres", "dcsr_pvfgmres"):
             getattr(L, name).argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL,
                                          INT, SHORT, SHORT, SHORT]
+        L.dcsr_pgcg.argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL, INT,
+                                SHORT, SHORT]
+        L.amg_amli_coef.argtypes = [REAL, REAL, INT, P(REAL)]
+        L.amg_amli_coef.restype = None
+        for name in ("precond_amg", "precond_amli", "precond_nl_amli", "precond_amg_add"):
+            getattr(L, name).restype = None
+        for name in ("amli", "nl_amli", "mgcycle_add", "mgcycle"):
+            getattr(L, name).restype = None
         L.python_wrapper_krylov_amg.argtypes = [P(INT), P(INT), C.c_void_p, C.c_void_p,
                                                 C.c_void_p, C.c_void_p, C.c_void_p, P(REAL),
                                                 P(INT), P(INT)]
@@ -308,10 +316,24 @@ def python_wrapper_krylov_amg(ia, ja, val, b, u, tol=1e-8, maxit=500, print_lvl=
                                     C.byref(INT(print_lvl)))
 
 
+# the preconditioner linear_solver_dcsr_krylov_amg picks for a cycle type
+_PRECOND_OF_CYCLE = {AMLI_CYCLE: "precond_amli", NL_AMLI_CYCLE: "precond_nl_amli",
+                     ADD_CYCLE: "precond_amg_add"}
+
+
+def amli_coef(lambda_max: float, lambda_min: float, degree: int) -> np.ndarray:
+    """amg_amli_coef: the degree + 1 coefficients of the AMLI polynomial."""
+    c = np.zeros(degree + 1)
+    lib().amg_amli_coef(lambda_max, lambda_min, degree, c.ctypes.data_as(C.POINTER(REAL)))
+    return c
+
+
 class AMGHierarchy:
     """amg_data_create + amg_setup_ua on a host matrix; the pieces a caller
-    assembles itself (HAZNICS create_precond_amg style): precond_amg as a
-    preconditioner for dcsr_pcg, mgcycle, amg_data_free."""
+    assembles itself (HAZNICS create_precond_amg style): the preconditioner
+    of the cycle type (precond_amg, precond_amli, precond_nl_amli or
+    precond_amg_add) for dcsr_pcg / dcsr_pgcg / dcsr_pv(f)gmres, the cycles,
+    amg_data_free."""
 
     def __init__(self, ia, ja, val, amgparam: AMG_param):
         self._A = _HostCSR(ia, ja, val)
@@ -328,7 +350,8 @@ class AMGHierarchy:
         self.pcdata.mgl_data = self.mgl
         self.pc = precond()
         self.pc.data = C.cast(C.pointer(self.pcdata), C.c_void_p)
-        self.pc.fct = C.cast(L.precond_amg, type(self.pc.fct))
+        self.pc_name = _PRECOND_OF_CYCLE.get(amgparam.cycle_type, "precond_amg")
+        self.pc.fct = C.cast(getattr(L, self.pc_name), type(self.pc.fct))
 
     @property
     def num_levels(self) -> int:
@@ -354,9 +377,41 @@ class AMGHierarchy:
     def precond(self, r):
         r = np.ascontiguousarray(r, np.float64).copy()
         z = np.zeros_like(r)
-        lib().precond_amg(r.ctypes.data_as(C.POINTER(REAL)), z.ctypes.data_as(C.POINTER(REAL)),
-                          C.cast(C.pointer(self.pcdata), C.c_void_p))
+        getattr(lib(), self.pc_name)(r.ctypes.data_as(C.POINTER(REAL)),
+                                     z.ctypes.data_as(C.POINTER(REAL)),
+                                     C.cast(C.pointer(self.pcdata), C.c_void_p))
         return z
+
+    def cycle(self, b, x):
+        """One cycle of the setup's cycle type on mgl[0].b / mgl[0].x
+        (mgcycle, amli, nl_amli or mgcycle_add); returns the new x."""
+        n = self.mgl[0].A.row
+        bb = np.ascontiguousarray(b, np.float64).copy()
+        xx = np.ascontiguousarray(x, np.float64).copy()
+        m0 = self.mgl[0]
+        # copies: a ctypes field read is a view into mgl[0]
+        sb, sx = dvector(m0.b.row, m0.b.val), dvector(m0.x.row, m0.x.val)
+        self.mgl[0].b = _dvec(bb)
+        self.mgl[0].x = _dvec(xx)
+        ct = self.param.cycle_type
+        L = lib()
+        if ct == AMLI_CYCLE:
+            L.amli(self.mgl, C.byref(self.param), 0)
+        elif ct == NL_AMLI_CYCLE:
+            L.nl_amli(self.mgl, C.byref(self.param), 0, self.num_levels)
+        elif ct == ADD_CYCLE:
+            L.mgcycle_add(self.mgl, C.byref(self.param))
+        else:
+            L.mgcycle(self.mgl, C.byref(self.param))
+        self.mgl[0].b, self.mgl[0].x = sb, sx
+        assert n == len(xx)
+        return xx
+
+    def gcg(self, b, x, tol=1e-8, maxit=100, stop_type=STOP_REL_RES, prtlvl=0):
+        """dcsr_pgcg with the setup's preconditioner."""
+        bb = np.ascontiguousarray(b, np.float64)
+        return lib().dcsr_pgcg(C.byref(self._A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),
+                               C.byref(self.pc), tol, maxit, stop_type, prtlvl)
 
     def pcg(self, b, x, tol=1e-8, maxit=500, stop_type=STOP_REL_RES, prtlvl=0):
         bb = np.ascontiguousarray(b, np.float64)
@@ -365,7 +420,8 @@ class AMGHierarchy:
 
     def gmres(self, b, x, tol=1e-8, maxit=500, restart=100, flexible=True,
               stop_type=STOP_REL_RES, prtlvl=0):
-        """dcsr_pvfgmres (flexible) or dcsr_pvgmres with precond_amg."""
+        """dcsr_pvfgmres (flexible) or dcsr_pvgmres with the setup's
+        preconditioner."""
         bb = np.ascontiguousarray(b, np.float64)
         f = lib().dcsr_pvfgmres if flexible else lib().dcsr_pvgmres
         return f(C.byref(self._A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),

@@ -262,14 +262,20 @@ extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
     double rel = 0.0, cond = 0.0;
     int it;
     const int prt = S->it.linear_print_level;
+    // the preconditioner of linear_solver_dcsr_krylov_amg for the cycle type
+    const int kind = pc_kind_of_cycle(S->pc_cyc.cycle_type);
     if (S->bp.precision == HZB_PREC_MIXED) {
+        if (kind != PC_AMG) {
+            set_error_msg("the mixed-precision solve runs V and W cycles (cycle_type 1, 2)");
+            return ERROR_INPUT_PAR;
+        }
         it = fcg_mixed(S, d_b, d_x, S->it.linear_tol, S->it.linear_maxit, prt, &rel);
     } else if (S->it.linear_itsolver_type == SOLVER_CG) {
-        it = pcg(S, S->lv[0].A64(), d_b, d_x, PC_AMG, nullptr, S->it.linear_tol,
+        it = pcg(S, S->lv[0].A64(), d_b, d_x, kind, nullptr, S->it.linear_tol,
                  S->it.linear_maxit, S->it.linear_stop_type, prt, S->kw, &rel, &cond);
     } else if (S->it.linear_itsolver_type == SOLVER_VGMRES ||
                S->it.linear_itsolver_type == SOLVER_VFGMRES) {
-        it = gmres(S, S->lv[0].A64(), d_b, d_x, PC_AMG, nullptr, S->it.linear_tol,
+        it = gmres(S, S->lv[0].A64(), d_b, d_x, kind, nullptr, S->it.linear_tol,
                    S->it.linear_maxit, S->it.linear_restart, S->it.linear_stop_type, prt,
                    S->it.linear_itsolver_type == SOLVER_VFGMRES, &rel);
     } else {
@@ -292,6 +298,10 @@ extern "C" INT hzb_batch_setup_device(hzb_solver *S, INT nsys, const INT *off, I
                                       INT nnz, const INT *d_ia, const INT *d_ja,
                                       const REAL *d_val) {
     if (!S || n <= 0 || nnz <= 0) return ERROR_MAT_SIZE;
+    if (pc_kind_of_cycle(S->pc_cyc.cycle_type) != PC_AMG) {
+        set_error_msg("batched solves run V and W cycles (cycle_type 1, 2)");
+        return ERROR_INPUT_PAR;
+    }
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
     S->host_ia = nullptr; S->host_ja = nullptr; S->host_val = nullptr;
@@ -348,7 +358,8 @@ extern "C" INT hzb_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z) {
     if (!S || S->nl == 0) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
-    HZB_TRY(precond64(S, d_r, d_z, S->pc_cyc));
+    HZB_TRY(apply_precond(S, pc_kind_of_cycle(S->pc_cyc.cycle_type), nullptr, S->lv[0].n, d_r,
+                          d_z));
     HZB_CUDA(cudaStreamSynchronize(S->s));
     return SUCCESS;
 }
@@ -476,7 +487,10 @@ extern "C" void amg_data_free(AMG_data *mgl, AMG_param *param) {
         hzb_destroy((hzb_solver *)mgl[0].wdata);
         mgl[0].wdata = NULL;
     }
-    (void)param;
+    if (param && param->cycle_type == AMLI_CYCLE) {
+        free(param->amli_coef);
+        param->amli_coef = NULL;
+    }
 }
 
 static void print_complexity(const hzb_solver *S) {
@@ -574,12 +588,18 @@ extern "C" SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param) {
             mgl[l].num_levels = nl;
             mgl[l].b.row = mm; mgl[l].b.val = (REAL *)calloc(mm, sizeof(REAL));
             mgl[l].x.row = mm; mgl[l].x.val = (REAL *)calloc(mm, sizeof(REAL));
-            mgl[l].w.row = 2 * mm; mgl[l].w.val = (REAL *)calloc(2 * mm, sizeof(REAL));
+            const int nw = param->cycle_type == NL_AMLI_CYCLE ? 3 * mm : 2 * mm;
+            mgl[l].w.row = nw; mgl[l].w.val = (REAL *)calloc(nw, sizeof(REAL));
             mgl[l].cycle_type = param->cycle_type;
         }
     }
     mgl[0].num_levels = nl;
     mgl[0].wdata = S;
+    if (param->cycle_type == AMLI_CYCLE) {
+        // amg_setup_ua.c:1276-1281: the polynomial for lambda in [0.5, 2]
+        param->amli_coef = (REAL *)calloc(param->amli_degree + 1, sizeof(REAL));
+        hzb::amli_coefficients(2.0, 0.5, param->amli_degree, param->amli_coef);
+    }
     if (param->print_level > PRINT_NONE) {
         if (param->print_level >= PRINT_SOME) print_complexity(S);
         printf("Unsmoothed aggregation setup costs %.4f seconds.\n", S->st.setup_seconds);
@@ -605,8 +625,25 @@ extern "C" void mgcycle(AMG_data *mgl, AMG_param *param) {
     cudaStreamSynchronize(S->s);
 }
 
-extern "C" void precond_amg(REAL *r, REAL *z, void *data) {
-    // precond.c:164-184 with host arrays r, z
+// The cycle parameters a precond_* function builds from its precond_data
+// (param_amg_init, then param_prec_to_amg; maxit from the data).  AMLI
+// coefficients the data carries move into the handle.
+static AMG_param pc_param_of(hzb_solver *S, precond_data *pcd) {
+    AMG_param cyc;
+    param_amg_init(&cyc);
+    param_prec_to_amg(&cyc, pcd);
+    cyc.maxit = pcd->maxit;
+    S->amli_coef.clear();
+    if (cyc.amli_coef) {
+        S->amli_coef.assign(cyc.amli_coef, cyc.amli_coef + cyc.amli_degree + 1);
+        free(cyc.amli_coef);
+        cyc.amli_coef = NULL;
+    }
+    return cyc;
+}
+
+// z = B r on host arrays with the device preconditioner of the kind
+static void precond_host(REAL *r, REAL *z, void *data, int kind) {
     precond_data *pcdata = (precond_data *)data;
     hzb_solver *S = pcdata ? handle_of(pcdata->mgl_data) : nullptr;
     if (!S) return;
@@ -616,14 +653,86 @@ extern "C" void precond_amg(REAL *r, REAL *z, void *data) {
     if (!S->pr) {
         if (dalloc(&S->pr, n) || dalloc(&S->pz, n)) return;
     }
-    AMG_param cyc;
-    param_amg_init(&cyc);
-    param_prec_to_amg(&cyc, pcdata);
-    cyc.maxit = pcdata->maxit;
+    S->pc_cyc = pc_param_of(S, pcdata);
     cudaMemcpyAsync(S->pr, r, sizeof(double) * n, cudaMemcpyHostToDevice, S->s);
-    if (precond64(S, S->pr, S->pz, cyc) == SUCCESS)
+    if (apply_precond(S, kind, nullptr, n, S->pr, S->pz) == SUCCESS)
         cudaMemcpyAsync(z, S->pz, sizeof(double) * n, cudaMemcpyDeviceToHost, S->s);
     cudaStreamSynchronize(S->s);
+}
+
+extern "C" void precond_amg(REAL *r, REAL *z, void *data) {
+    // precond.c:164-184 with host arrays r, z
+    precond_host(r, z, data, PC_AMG);
+}
+
+extern "C" void precond_amli(REAL *r, REAL *z, void *data) {
+    // precond.c:232-250
+    precond_host(r, z, data, PC_AMLI);
+}
+
+extern "C" void precond_nl_amli(REAL *r, REAL *z, void *data) {
+    // precond.c:301-320 (the whole hierarchy of the handle)
+    precond_host(r, z, data, PC_NLAMLI);
+}
+
+extern "C" void precond_amg_add(REAL *r, REAL *z, void *data) {
+    // precond.c:336-355
+    precond_host(r, z, data, PC_ADD);
+}
+
+// One cycle of a kind on mgl[0].b / mgl[0].x (host arrays) with param as
+// given; the device hierarchy of mgl[0] is the whole of it, so only
+// level 0 (and, for nl_amli, all levels) can be asked for.
+static void cycle_host(AMG_data *mgl, AMG_param *param, int kind, INT level) {
+    hzb_solver *S = handle_of(mgl);
+    if (!S || !param) return;
+    if (level != 0) {
+        printf("### ERROR: the device hierarchy runs cycles from level 0 of mgl[0]\n");
+        return;
+    }
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    Level &L0 = S->lv[0];
+    if (cycles_prepare(S, kind, *param) != SUCCESS) return;
+    // the coarse-level Krylov solves of the nonlinear AMLI cycle precondition
+    // with precond_nl_amli on parameters rebuilt from param (mgcycle.c:620)
+    S->pc_cyc = cycle_param_of(*param);
+    cudaMemcpyAsync(L0.b, mgl[0].b.val, sizeof(double) * L0.n, cudaMemcpyHostToDevice, S->s);
+    cudaMemcpyAsync(L0.x, mgl[0].x.val, sizeof(double) * L0.n, cudaMemcpyHostToDevice, S->s);
+    int rc;
+    if (kind == PC_AMLI) rc = amli64(S, *param, S->amli_coef.data(), 0);
+    else if (kind == PC_ADD) rc = add_cycle64(S, *param);
+    else rc = nl_amli64(S, *param, 0);
+    if (rc == SUCCESS)
+        cudaMemcpyAsync(mgl[0].x.val, L0.x, sizeof(double) * L0.n, cudaMemcpyDeviceToHost, S->s);
+    cudaStreamSynchronize(S->s);
+}
+
+extern "C" void amli(AMG_data *mgl, AMG_param *param, INT level) {
+    // mgcycle.c:430-555
+    cycle_host(mgl, param, PC_AMLI, level);
+}
+
+extern "C" void nl_amli(AMG_data *mgl, AMG_param *param, INT level, INT num_levels) {
+    // mgcycle.c:561-690
+    hzb_solver *S = handle_of(mgl);
+    if (S && num_levels != S->nl) {
+        printf("### ERROR: the device hierarchy has %d levels\n", S->nl);
+        return;
+    }
+    cycle_host(mgl, param, PC_NLAMLI, level);
+}
+
+extern "C" void mgcycle_add(AMG_data *mgl, AMG_param *param) {
+    // mgcycle.c:700-820
+    cycle_host(mgl, param, PC_ADD, 0);
+}
+
+extern "C" void amg_amli_coef(const REAL lambda_max, const REAL lambda_min, const INT degree,
+                              REAL *coef) {
+    // parameters.c:714-775
+    if (hzb::amli_coefficients(lambda_max, lambda_min, degree, coef) != SUCCESS)
+        printf("### ERROR HAZMATH DANGER: Wrong AMLI degree %lld!\n", (long long)degree);
 }
 
 // ---------------------------------------------------------------------------
@@ -648,7 +757,7 @@ static int upload_csr(const dCSRmat *A, TmpCsr &T, DCsr<double> &D, cudaStream_t
     return SUCCESS;
 }
 
-// A Krylov method (type: SOLVER_CG, SOLVER_VGMRES or SOLVER_VFGMRES) on host
+// A Krylov method (type: SOLVER_CG, SOLVER_GCG, SOLVER_VGMRES or SOLVER_VFGMRES) on host
 // arrays with the caller's preconditioner: the setup's own AMG runs on the
 // device, any other pc->fct is called on host copies.
 static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol,
@@ -659,16 +768,15 @@ static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol
     hzb_solver *S = nullptr, *own = nullptr;
     int kind = PC_NONE;
     HostPrecond hp;
-    if (pc && pc->fct == precond_amg && pc->data &&
-        handle_of(((precond_data *)pc->data)->mgl_data)) {
+    const int dev_kind = !pc ? -1
+                         : pc->fct == precond_amg ? PC_AMG
+                         : pc->fct == precond_amli ? PC_AMLI
+                         : pc->fct == precond_nl_amli ? PC_NLAMLI
+                         : pc->fct == precond_amg_add ? PC_ADD : -1;
+    if (dev_kind >= 0 && pc->data && handle_of(((precond_data *)pc->data)->mgl_data)) {
         S = handle_of(((precond_data *)pc->data)->mgl_data);
-        precond_data *pcd = (precond_data *)pc->data;
-        AMG_param cyc;
-        param_amg_init(&cyc);
-        param_prec_to_amg(&cyc, pcd);
-        cyc.maxit = pcd->maxit;
-        S->pc_cyc = cyc;
-        kind = PC_AMG;
+        S->pc_cyc = pc_param_of(S, (precond_data *)pc->data);
+        kind = dev_kind;
     } else {
         HZB_TRY(hzb_create(&own, NULL, NULL, NULL));
         S = own;
@@ -687,7 +795,7 @@ static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol
     TmpCsr T;
     double *db = nullptr, *du = nullptr;
     KrylovWork w;
-    const bool same = kind == PC_AMG && S->host_ia == A->IA && S->host_ja == A->JA &&
+    const bool same = kind != PC_NONE && kind != PC_HOST && S->host_ia == A->IA && S->host_ja == A->JA &&
                       S->host_val == A->val && S->lv[0].n == A->row;
     if (same) D = S->lv[0].A64();
     else rc = upload_csr(A, T, D, S->s);
@@ -701,6 +809,8 @@ static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol
         double rel = 0.0;
         if (type == SOLVER_CG)
             it = pcg(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, w, &rel, condest);
+        else if (type == SOLVER_GCG)
+            it = gcg(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, &rel);
         else
             it = gmres(S, D, db, du, kind, &hp, tol, MaxIt, restart, stop_type, prtlvl,
                        type == SOLVER_VFGMRES, &rel);
@@ -739,6 +849,12 @@ extern "C" INT dcsr_pvfgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
     // krylov.c:5974-6250
     return krylov_host(A, b, x, pc, tol, MaxIt, stop_type, prtlvl, nullptr, SOLVER_VFGMRES,
                        restart);
+}
+
+extern "C" INT dcsr_pgcg(dCSRmat *A, dvector *b, dvector *u, precond *pc, const REAL tol,
+                         const INT MaxIt, const SHORT stop_type, const SHORT prtlvl) {
+    // krylov.c:2309-2420
+    return krylov_host(A, b, u, pc, tol, MaxIt, stop_type, prtlvl, nullptr, SOLVER_GCG, 0);
 }
 
 // the banner solver_dcsr_linear_itsolver prints for a Krylov type

@@ -89,9 +89,8 @@ __global__ void k_gm_add(int n, const double *__restrict__ x, double *y) {
         y[k] += x[k];
 }
 
-namespace {
 struct GmresWork {
-    int n = 0, restart = 0;
+    int n = 0, restart = 0, req = 0;   // allocated / requested restart
     bool flexible = false;
     std::vector<double *> p, z;       // restart + 1 each (z only when flexible)
     double *r = nullptr, *w = nullptr;
@@ -132,6 +131,12 @@ struct GmresWork {
     }
 };
 
+void gmres_release(hzb_solver *S) {
+    for (auto &g : S->gm_ws) delete g;
+    S->gm_ws.clear();
+}
+
+namespace {
 void print_row(int prt, int iter, double rel, double abs, double factor) {
     if (prt < PRINT_SOME) return;
     printf("%6lld | %13.6e   | %13.6e  | %10.4f\n", (long long)iter, rel, abs, factor);
@@ -214,26 +219,52 @@ static int combine(hzb_solver *S, GmresWork &g, double *const *d_v, int m,
 
 int gmres(hzb_solver *S, const DCsr<double> &A, const double *b, double *x, int kind,
           HostPrecond *hp, double tol, int MaxIt, int restart, int stop_type, int prtlvl,
-          bool flexible, double *relres_out) {
+          bool flexible, double *relres_out, int ws_slot) {
     const int n = A.n;
     cudaStream_t s = S->s;
     const double cr_max = 0.99, cr_min = 0.174, epsmac = SMALLREAL;
     const int d = 3, restart_min = 3, restart_max = restart;
     if (restart < 1) return ERROR_INPUT_PAR;
     int Restart = restart;
-    // the reference shrinks the restart by 5 while its work space does not fit
-    std::unique_ptr<GmresWork> gw(new GmresWork());
-    int rc = gw->alloc(n, Restart, flexible);
-    while (rc == ERROR_ALLOC_MEM && Restart > 5) {
-        Restart -= 5;
+    // A kept basis serves the coarse-level solves of the nonlinear AMLI
+    // cycle (MaxIt = degree + 1).  Its basis holds min(restart, MaxIt)
+    // vectors when MaxIt <= 4 <= restart: the restart adaptation below never
+    // takes the cycle length under 4 then, so every cycle runs to MaxIt
+    // either way and the iterates are the same.
+    const int want = (ws_slot >= 0 && MaxIt <= 4 && restart >= 4) ? std::max(MaxIt, 1) : restart;
+    std::unique_ptr<GmresWork> gw;
+    GmresWork *gp = nullptr;
+    if (ws_slot >= 0 && ws_slot < (int)S->gm_ws.size() && S->gm_ws[ws_slot] &&
+        S->gm_ws[ws_slot]->n == n && S->gm_ws[ws_slot]->req == want &&
+        S->gm_ws[ws_slot]->flexible == flexible) {
+        gp = S->gm_ws[ws_slot];
+        Restart = gp->restart;
+    } else {
+        // the reference shrinks the restart by 5 while its work space does
+        // not fit
+        Restart = want;
         gw.reset(new GmresWork());
-        rc = gw->alloc(n, Restart, flexible);
+        int rc = gw->alloc(n, Restart, flexible);
+        while (rc == ERROR_ALLOC_MEM && Restart > 5) {
+            Restart -= 5;
+            gw.reset(new GmresWork());
+            rc = gw->alloc(n, Restart, flexible);
+        }
+        if (rc) return rc;
+        gw->req = want;
+        if (prtlvl > PRINT_MIN && Restart < want)
+            printf("### WARNING: %s restart number set to %lld!\n",
+                   flexible ? "vFGMRES" : "vGMRES", (long long)Restart);
+        if (ws_slot >= 0) {
+            if ((int)S->gm_ws.size() <= ws_slot) S->gm_ws.resize(ws_slot + 1, nullptr);
+            delete S->gm_ws[ws_slot];
+            S->gm_ws[ws_slot] = gw.release();
+            gp = S->gm_ws[ws_slot];
+        } else {
+            gp = gw.get();
+        }
     }
-    if (rc) return rc;
-    if (prtlvl > PRINT_MIN && Restart < restart)
-        printf("### WARNING: %s restart number set to %lld!\n", flexible ? "vFGMRES" : "vGMRES",
-               (long long)Restart);
-    GmresWork &g = *gw;
+    GmresWork &g = *gp;
     std::vector<double> c(Restart + 1), sn(Restart + 1), rs(Restart + 2), h;
     std::vector<std::vector<double>> hh(Restart + 1, std::vector<double>(Restart + 1, 0.0));
     std::vector<double> norms(MaxIt + 2, 0.0);

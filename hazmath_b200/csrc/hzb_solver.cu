@@ -55,7 +55,7 @@ void Level::release() {
     ia32 = ja32 = nullptr;
     own32 = false;
     dfree(agg); dfree(ria); dfree(rja);
-    dfree(b); dfree(x); dfree(w); dfree(t);
+    dfree(b); dfree(x); dfree(w); dfree(t); dfree(r1);
     dfree(b32); dfree(x32); dfree(w32); dfree(t32);
     dfree(d_jac); dfree(d_gs_f); dfree(d_gs_b); dfree(d_sor_f); dfree(d_sor_b);
     dfree(d_gs32);
@@ -208,15 +208,31 @@ static bool smoother_needs_gs(int sm) {
 // ---------------------------------------------------------------------------
 // V / W cycle, mgcycle (mgcycle.c:245-415)
 // ---------------------------------------------------------------------------
-static int coarse_solve64(hzb_solver *S, const AMG_param &cyc) {
+int coarse_solve64(hzb_solver *S, const AMG_param &cyc, double ctol) {
     Level &C = S->lv[S->nl - 1];
     if (cyc.coarse_solver == SOLVER_UMFPACK && S->Ainv)
         return dense_gemv<double>(C.n, S->Ainv, C.b, C.x, S->s);
-    // coarse_itsolver (mgcycle.c:34-52): plain CG to tol*1e-2, maxit 20 n
+    // coarse_itsolver (mgcycle.c:34-52): plain CG to ctol with maxit 20 n,
+    // and GMRES(30) from CG's last iterate when CG reports a failure
+    if (S->kwc.n != C.n) HZB_TRY(S->kwc.alloc(C.n));
     double rel = 0.0;
-    int it = pcg(S, C.A64(), C.b, C.x, PC_NONE, nullptr, cyc.tol * 1e-2, 20 * C.n,
-                 STOP_REL_RES, 0, S->kwc, &rel, nullptr);
+    int it = pcg(S, C.A64(), C.b, C.x, PC_NONE, nullptr, ctol, 20 * C.n, STOP_REL_RES, 0,
+                 S->kwc, &rel, nullptr);
+    if (it < 0 && it != ERROR_SOLVER_MISC)
+        it = gmres(S, C.A64(), C.b, C.x, PC_NONE, nullptr, ctol, 20 * C.n, 30, STOP_REL_RES,
+                   0, false, &rel, S->nl - 1);
     return it == ERROR_SOLVER_MISC ? it : SUCCESS;
+}
+
+int coarse_alpha(hzb_solver *S, int c, const double *rc, double *alpha) {
+    Level &C = S->lv[c];
+    KrylovWork &w = S->kw;
+    HZB_TRY(dot(C.n, C.x, rc, w.part, w.sc + SC_X, S->s));
+    HZB_TRY(spmv<double>(C.A64(), SPMV_Y, C.x, nullptr, C.t, 1.0, nullptr, S->s));
+    HZB_TRY(dot(C.n, C.x, C.t, w.part, w.sc + SC_X + 1, S->s));
+    HZB_TRY(fetch(S, w));
+    *alpha = std::min(w.h_sc[SC_X] / w.h_sc[SC_X + 1], 2.0);
+    return SUCCESS;
 }
 
 // l0 > 0 runs the same cycle on the sub-hierarchy below level l0 (the
@@ -236,20 +252,11 @@ forward:
         ++l;
         HZB_TRY(vzero<double>(S->lv[l].n, S->lv[l].x, S->s));
     }
-    HZB_TRY(coarse_solve64(S, cyc));
+    HZB_TRY(coarse_solve64(S, cyc, cyc.tol * 1e-2));
     while (l > l0) {
         --l;
         Level &L = S->lv[l];
-        if (cyc.coarse_scaling == ON) {
-            Level &C = S->lv[l + 1];
-            KrylovWork &w = S->kw;
-            HZB_TRY(dot(C.n, C.x, C.b, w.part, w.sc + SC_X, S->s));
-            HZB_TRY(spmv<double>(C.A64(), SPMV_Y, C.x, nullptr, C.t, 1.0, nullptr, S->s));
-            HZB_TRY(dot(C.n, C.x, C.t, w.part, w.sc + SC_X + 1, S->s));
-            HZB_TRY(fetch(S, w));
-            alpha = w.h_sc[SC_X] / w.h_sc[SC_X + 1];
-            alpha = std::min(alpha, 2.0);
-        }
+        if (cyc.coarse_scaling == ON) HZB_TRY(coarse_alpha(S, l + 1, S->lv[l + 1].b, &alpha));
         HZB_TRY(prolong_agg<double>(L.n, L.agg, S->lv[l + 1].x, L.x, alpha, S->s));
         HZB_TRY(smooth64(S, l, false, cyc));
         if (num_lvl[l] < cyc.cycle_type) break;
@@ -459,6 +466,9 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
           const double *d_val, bool copy_in) {
     S->g64.release();
     S->g32.release();
+    S->gcyc.release();
+    gmres_release(S);
+    gcg_release(S);
     for (auto &L : S->lv) L.release();
     S->lv.clear();
     dfree(S->Ainv);
@@ -644,9 +654,27 @@ static void print_info(int prt, int stop_type, int iter, double rel, double abs,
     fflush(stdout);
 }
 
+int pc_kind_of_cycle(int cycle_type) {
+    switch (cycle_type) {
+    case AMLI_CYCLE: return PC_AMLI;
+    case NL_AMLI_CYCLE: return PC_NLAMLI;
+    case ADD_CYCLE: return PC_ADD;
+    default: return PC_AMG;
+    }
+}
+
+static int precond_alt(hzb_solver *S, int kind, const double *r, double *z);
+
 static int apply_pc(hzb_solver *S, int kind, HostPrecond *hp, int n,
                     const double *r, double *z) {
     if (kind == PC_AMG) return precond64(S, r, z, S->pc_cyc);
+    if (kind == PC_AMLI || kind == PC_ADD) return precond_alt(S, kind, r, z);
+    if (kind >= PC_NLAMLI) {
+        // the solve's preconditioner runs maxit cycles; the coarse-level
+        // Krylov solves of the cycle itself run one (mgcycle.c:623)
+        const int l = kind - PC_NLAMLI;
+        return precond_cycles(S, PC_NLAMLI, l, l == 0 ? S->pc_cyc.maxit : 1, r, z, S->pc_cyc);
+    }
     if (kind == PC_HOST) {
         HZB_CUDA(cudaMemcpyAsync(hp->h_r, r, sizeof(double) * n, cudaMemcpyDeviceToHost, S->s));
         HZB_CUDA(cudaStreamSynchronize(S->s));
@@ -866,9 +894,9 @@ static int apply_pc32_body(hzb_solver *S, const double *r, double *z) {
 // capture is redone whenever the key (vector pointers, tag) changes.
 template <typename F>
 static int with_graph(hzb_solver *S, GraphCache &G, const void *k0, const void *k1,
-                      long long tag, F body) {
+                      long long tag, F body, long long tag2 = 0) {
     if (!S->bp.use_graph) return body();
-    if (!G.exec || G.k0 != k0 || G.k1 != k1 || G.tag != tag) {
+    if (!G.exec || G.k0 != k0 || G.k1 != k1 || G.tag != tag || G.tag2 != tag2) {
         G.release();
         const long long before = launch_count();
         HZB_CUDA(cudaStreamBeginCapture(S->s, cudaStreamCaptureModeThreadLocal));
@@ -890,6 +918,7 @@ static int with_graph(hzb_solver *S, GraphCache &G, const void *k0, const void *
         G.k0 = k0;
         G.k1 = k1;
         G.tag = tag;
+        G.tag2 = tag2;
         G.kernels = launch_count() - before;   // counted once by the capture
     } else {
         count_launch((int)G.kernels);
@@ -920,9 +949,29 @@ int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
                       [&]() { return precond64_body(S, r, z, cyc); });
 }
 
+// precond_amli / precond_amg_add: replayed from a graph under the same
+// conditions as precond_amg; the key holds the AMLI coefficients' bits.
+static int precond_alt(hzb_solver *S, int kind, const double *r, double *z) {
+    const AMG_param &cyc = S->pc_cyc;
+    const bool capturable = cyc.coarse_solver == SOLVER_UMFPACK && S->Ainv &&
+                            cyc.coarse_scaling != ON;
+    HZB_TRY(cycles_prepare(S, kind, cyc));
+    auto body = [&]() { return precond_cycles(S, kind, 0, cyc.maxit, r, z, cyc); };
+    if (!capturable) return body();
+    unsigned long long h = 1469598103934665603ull ^ (unsigned long long)kind;
+    if (kind == PC_AMLI) {
+        for (double c : S->amli_coef) {
+            unsigned long long u;
+            memcpy(&u, &c, sizeof(u));
+            h = (h ^ u) * 1099511628211ull;
+        }
+    }
+    return with_graph(S, S->gcyc, r, z, cycle_tag(S, cyc), body, (long long)(h >> 1));
+}
+
 int solver_precond(hzb_solver *S, const double *r, double *z) {
     if (S->bp.precision == HZB_PREC_MIXED) return apply_pc32(S, r, z);
-    return precond64(S, r, z, S->pc_cyc);
+    return apply_pc(S, pc_kind_of_cycle(S->pc_cyc.cycle_type), nullptr, S->lv[0].n, r, z);
 }
 
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
@@ -989,6 +1038,9 @@ void destroy(hzb_solver *S) {
     batch_release(S);
     S->g64.release();
     S->g32.release();
+    S->gcyc.release();
+    gmres_release(S);
+    gcg_release(S);
     for (auto &L : S->lv) L.release();
     S->lv.clear();
     dfree(S->Ainv);

@@ -27,8 +27,9 @@ struct Level {
     // transfer to level + 1 (P = agg map, R = P^T with ascending rows)
     int nc = 0;
     int *agg = nullptr, *ria = nullptr, *rja = nullptr;
-    // cycle vectors
-    double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr;
+    // cycle vectors; r1 keeps the restricted residual of the AMLI cycle
+    // (allocated on levels >= 1 when that cycle first runs)
+    double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr, *r1 = nullptr;
     float *b32 = nullptr, *x32 = nullptr, *w32 = nullptr, *t32 = nullptr;
     // smoother data
     double *d_jac = nullptr, *d_gs_f = nullptr, *d_gs_b = nullptr;
@@ -79,7 +80,7 @@ struct KrylovWork {
 struct GraphCache {
     cudaGraphExec_t exec = nullptr;
     const void *k0 = nullptr, *k1 = nullptr;
-    long long tag = -1;
+    long long tag = -1, tag2 = 0;
     long long kernels = 0;
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -87,6 +88,9 @@ struct GraphCache {
         tag = -1;
     }
 };
+
+struct GmresWork;   // Krylov basis of gmres (hzb_gmres.cu)
+struct GcgWork;     // search directions of gcg (hzb_cycles.cu)
 
 struct Batch;   // packed independent systems (hzb_batch.cu)
 
@@ -113,6 +117,12 @@ struct hzb_solver {
     hzb::KrylovWork kw;               // outer Krylov loop
     hzb::KrylovWork kwc;              // coarse-level CG (coarse_solver != 32)
     hzb::GraphCache g64, g32;         // captured FP64 / FP32 preconditioners
+    hzb::GraphCache gcyc;             // captured AMLI / additive preconditioner
+    std::vector<double> amli_coef;    // polynomial of the AMLI cycle (degree + 1)
+    // Krylov work kept per level for the coarse-level solves of the
+    // nonlinear AMLI cycle and the coarse GMRES fallback
+    std::vector<hzb::GmresWork *> gm_ws;
+    std::vector<hzb::GcgWork *> gcg_ws;
     float *omega = nullptr;           // learned fine-level weights (device)
     bool omega_active = false;
     hzb_stats st{};
@@ -135,15 +145,50 @@ int cycle32(hzb_solver *S, const AMG_param &cyc, bool level0_zero);
 int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
         int pc_kind, HostPrecond *hp, double tol, int maxit, int stop_type,
         int prtlvl, KrylovWork &w, double *relres_out, double *condest);
-enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2 };
+// preconditioner kinds of pcg / gmres / gcg: none, precond_amg (V/W
+// cycles), a host callback, precond_amli, precond_amg_add, and
+// precond_nl_amli rooted at level l (PC_NLAMLI + l)
+enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2, PC_AMLI = 3, PC_ADD = 4, PC_NLAMLI = 16 };
+// the preconditioner linear_solver_dcsr_krylov_amg picks for a cycle type
+// (itsolver.c:899-917)
+int pc_kind_of_cycle(int cycle_type);
 // z = M r for a preconditioner kind of pcg / gmres
 int apply_precond(hzb_solver *S, int kind, HostPrecond *hp, int n, const double *r,
                   double *z);
 // variable-restart GMRES (flexible = false, dcsr_pvgmres) or flexible GMRES
 // (dcsr_pvfgmres), right-preconditioned (hzb_gmres.cu)
+// (hzb_gmres.cu); ws_slot >= 0 keeps the basis in S->gm_ws[ws_slot] for the
+// next call
 int gmres(hzb_solver *S, const DCsr<double> &A, const double *b, double *x, int kind,
           HostPrecond *hp, double tol, int MaxIt, int restart, int stop_type, int prtlvl,
-          bool flexible, double *relres_out);
+          bool flexible, double *relres_out, int ws_slot = -1);
+void gmres_release(hzb_solver *S);
+// generalized conjugate gradient, dcsr_pgcg (hzb_cycles.cu)
+int gcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u, int kind,
+        HostPrecond *hp, double tol, int MaxIt, int stop_type, int prtlvl, double *relres_out,
+        int ws_slot = -1);
+void gcg_release(hzb_solver *S);
+// coefficients of the AMLI polynomial, amg_amli_coef (parameters.c:714-775)
+int amli_coefficients(double lambda_max, double lambda_min, int degree, double *coef);
+// what the cycles of a kind need before they run (and before a graph
+// capture): S->amli_coef for the AMLI cycle (cyc.amli_coef when given, else
+// the setup's choice lambda in [0.5, 2], amg_setup_ua.c:1276-1281) and the
+// per-level r1 vectors
+int cycles_prepare(hzb_solver *S, int kind, const AMG_param &cyc);
+// AMLI / nonlinear AMLI / additive cycles from level l with level l's b and
+// x in place (hzb_cycles.cu)
+int amli64(hzb_solver *S, const AMG_param &cyc, const double *coef, int l);
+int nl_amli64(hzb_solver *S, const AMG_param &cyc, int l);
+int add_cycle64(hzb_solver *S, const AMG_param &cyc);
+// z = B r with maxit cycles of the kind (precond_amli / precond_nl_amli
+// rooted at level l / precond_amg_add, precond.c:232-355)
+int precond_cycles(hzb_solver *S, int kind, int l, int maxit, const double *r, double *z,
+                   const AMG_param &cyc);
+// coarsest-level solve of the cycles: the direct inverse, else
+// coarse_itsolver (mgcycle.c:34-52) to the tolerance ctol
+int coarse_solve64(hzb_solver *S, const AMG_param &cyc, double ctol);
+// alpha = min((e_c, r_c) / (e_c, A_c e_c), 2) on level c (uses the level's t)
+int coarse_alpha(hzb_solver *S, int c, const double *rc, double *alpha);
 // FP32-cycle flexible CG (mixed precision)
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out);

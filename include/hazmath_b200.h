@@ -98,6 +98,9 @@ extern "C" {
 
 #define V_CYCLE 1
 #define W_CYCLE 2
+#define AMLI_CYCLE 3
+#define NL_AMLI_CYCLE 4
+#define ADD_CYCLE 5
 
 #define SMOOTHER_JACOBI  1
 #define SMOOTHER_GS      2
@@ -304,6 +307,30 @@ void mgcycle(AMG_data *mgl, AMG_param *param);
 /* src/solver/precond.c:164-184: z = B r with host arrays r, z. */
 void precond_amg(REAL *r, REAL *z, void *data);
 
+/* src/solver/precond.c:232-250, 301-320, 336-355: z = B r with maxit AMLI,
+ * nonlinear AMLI or additive cycles of the device hierarchy.  The
+ * preconditioners linear_solver_dcsr_krylov_amg uses for cycle_type 3, 4
+ * and 5; handed to dcsr_pcg / dcsr_pgcg / dcsr_pvgmres / dcsr_pvfgmres
+ * with the setup's mgl_data, the whole Krylov loop runs on the device. */
+void precond_amli(REAL *r, REAL *z, void *data);
+void precond_nl_amli(REAL *r, REAL *z, void *data);
+void precond_amg_add(REAL *r, REAL *z, void *data);
+
+/* src/solver/mgcycle.c:430-555, 561-690, 700-820: one AMLI, nonlinear
+ * AMLI or additive cycle on mgl[0].b, mgl[0].x.  The device hierarchy in
+ * mgl[0] runs from its finest level: level must be 0 and num_levels the
+ * hierarchy's level count. */
+void amli(AMG_data *mgl, AMG_param *param, INT level);
+void nl_amli(AMG_data *mgl, AMG_param *param, INT level, INT num_levels);
+void mgcycle_add(AMG_data *mgl, AMG_param *param);
+
+/* src/utilities/parameters.c:714-775: coefficients of the polynomial of
+ * best uniform approximation of 1/x on [lambda_min, lambda_max] (degree + 1
+ * values); amg_setup_ua stores them in param->amli_coef for AMLI_CYCLE with
+ * lambda in [0.5, 2]. */
+void amg_amli_coef(const REAL lambda_max, const REAL lambda_min, const INT degree,
+                   REAL *coef);
+
 /* src/solver/krylov.c:122-398.  pc == NULL: plain CG; pc->fct ==
  * precond_amg with a B200 hierarchy: the whole loop runs on the device;
  * any other pc->fct is called on host arrays every iteration. */
@@ -325,6 +352,13 @@ INT dcsr_pvgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
 INT dcsr_pvfgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
                   const REAL tol, const INT MaxIt, const SHORT restart,
                   const SHORT stop_type, const SHORT prtlvl);
+
+/* src/solver/krylov.c:2309-2420: generalized conjugate gradient (every
+ * direction kept and A-orthogonalised, no restart), stopping on
+ * ||r|| < tol ||b||; the coarse-level solver of the nonlinear AMLI cycle
+ * when nl_amli_krylov_type is SOLVER_GCG. */
+INT dcsr_pgcg(dCSRmat *A, dvector *b, dvector *u, precond *pc, const REAL tol,
+              const INT MaxIt, const SHORT stop_type, const SHORT prtlvl);
 
 /* src/utilities/wrapper.c:36-99.  The reference reads ./input.dat; this one
  * uses the UA-AMG defaults of the HAZmath examples (V-cycle, GS 1/1, HEM,

@@ -54,16 +54,18 @@ class AMGParams:
     coarse_scaling: int = 0
     print_level: int = 0
     maxit: int = 1
+    amli_degree: int = 2
+    nl_amli_krylov_type: int = 4
     strong_coupled: float = 0.0
     relaxation: float = 1.0
     tol: float = 1e-6
 
     def arrays(self):
-        ip = (ctypes.c_int * 12)(
+        ip = (ctypes.c_int * 14)(
             self.max_levels, self.coarse_dof, self.cycle_type, self.smoother,
             self.presmooth_iter, self.postsmooth_iter, self.coarse_solver,
             self.aggregation_type, self.max_aggregation, self.coarse_scaling,
-            self.print_level, self.maxit)
+            self.print_level, self.maxit, self.amli_degree, self.nl_amli_krylov_type)
         dp = (ctypes.c_double * 3)(self.strong_coupled, self.relaxation, self.tol)
         return ip, dp
 
@@ -269,6 +271,23 @@ class Ref(_Backend):
                                 maxit, restart, stop_type, 0, _p(hist), hist_cap,
                                 ctypes.byref(nh))
         return it, x, hist[: min(nh.value, hist_cap)].copy()
+
+    def gcg(self, b, x0=None, tol=1e-8, maxit=100, hist_cap=1024):
+        """dcsr_pgcg with the preconditioner of the last setup:
+        (iterations, x, ||r|| at each preconditioner call)."""
+        b = np.ascontiguousarray(b, np.float64).copy()
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        hist = np.zeros(hist_cap)
+        nh = ctypes.c_int()
+        it = self.lib.ref_gcg(_p(b), _p(x), ctypes.c_double(tol), maxit, 0, _p(hist),
+                              hist_cap, ctypes.byref(nh))
+        return it, x, hist[: min(nh.value, hist_cap)].copy()
+
+    def amli_coef(self, lambda_max, lambda_min, degree):
+        c = np.zeros(degree + 1)
+        self.lib.ref_amli_coef(ctypes.c_double(lambda_max), ctypes.c_double(lambda_min),
+                               degree, _p(c))
+        return c
 
     def free(self):
         self.lib.ref_free()

@@ -21,6 +21,9 @@ static AMG_param g_amg;
 static dCSRmat g_A;            /* caller's matrix, wrapped (not owned) */
 static precond_data g_pcdata;
 static precond g_pc;
+/* the preconditioner linear_solver_dcsr_krylov_amg (itsolver.c:899-917)
+ * picks for the cycle type of the last setup */
+static void (*g_fct)(REAL *, REAL *, void *) = precond_amg;
 static double *g_hist = NULL;  /* ||r|| seen by each preconditioner call */
 static int g_hist_cap = 0, g_hist_n = 0;
 static double g_setup_s = 0.0, g_solve_s = 0.0;
@@ -35,6 +38,7 @@ static double now_s(void)
 /* iparam: [0] max_levels [1] coarse_dof [2] cycle_type [3] smoother
  *         [4] presmooth [5] postsmooth [6] coarse_solver [7] aggregation_type
  *         [8] max_aggregation [9] coarse_scaling [10] print_level [11] amg maxit
+ *         [12] amli_degree [13] nl_amli_krylov_type
  * dparam: [0] strong_coupled [1] relaxation [2] amg tol                      */
 static void fill_param(AMG_param *p, const int *ip, const double *dp)
 {
@@ -52,6 +56,8 @@ static void fill_param(AMG_param *p, const int *ip, const double *dp)
     p->coarse_scaling = (SHORT)ip[9];
     p->print_level = (SHORT)ip[10];
     p->maxit = ip[11];
+    p->amli_degree = (SHORT)ip[12];
+    p->nl_amli_krylov_type = (SHORT)ip[13];
     p->strong_coupled = dp[0];
     p->relaxation = dp[1];
     p->tol = dp[2];
@@ -86,7 +92,13 @@ int ref_setup(int n, int nnz, int *ia, int *ja, double *val,
     g_pcdata.max_levels = g_mgl[0].num_levels;
     g_pcdata.mgl_data = g_mgl;
     g_pc.data = &g_pcdata;
-    g_pc.fct = precond_amg;
+    switch (g_amg.cycle_type) {
+    case AMLI_CYCLE: g_fct = precond_amli; break;
+    case NL_AMLI_CYCLE: g_fct = precond_nl_amli; break;
+    case ADD_CYCLE: g_fct = precond_amg_add; break;
+    default: g_fct = precond_amg; break;
+    }
+    g_pc.fct = g_fct;
     return status;
 }
 
@@ -128,8 +140,9 @@ void ref_level_R(int l, int *ia, int *ja)
     memcpy(ja, R->JA, sizeof(int) * R->nnz);
 }
 
-/* one application of the AMG preconditioner, precond_amg (precond.c:164) */
-void ref_precond(double *r, double *z) { precond_amg(r, z, &g_pcdata); }
+/* one application of the setup's preconditioner (precond_amg, precond.c:164,
+ * or the one of its cycle type) */
+void ref_precond(double *r, double *z) { g_fct(r, z, &g_pcdata); }
 
 static void hist_precond(REAL *r, REAL *z, void *data)
 {
@@ -139,7 +152,7 @@ static void hist_precond(REAL *r, REAL *z, void *data)
         g_hist[g_hist_n] = sqrt(s);
     }
     g_hist_n++;
-    precond_amg(r, z, data);
+    g_fct(r, z, data);
 }
 
 /* PCG with the AMG preconditioner; hist receives ||r|| at every
@@ -152,7 +165,7 @@ int ref_pcg(double *b, double *x, double tol, int maxit, int stop_type,
     xx.row = g_A.row; xx.val = x;
     g_hist = hist; g_hist_cap = hist ? hist_cap : 0; g_hist_n = 0;
     precond pc = g_pc;
-    pc.fct = hist ? hist_precond : precond_amg;
+    pc.fct = hist ? hist_precond : g_fct;
     double t0 = now_s();
     int it = dcsr_pcg(&g_A, &bb, &xx, &pc, tol, maxit, (SHORT)stop_type,
                       (SHORT)print_level);
@@ -174,7 +187,7 @@ int ref_gmres(int type, double *b, double *x, double tol, int maxit, int restart
     xx.row = g_A.row; xx.val = x;
     g_hist = hist; g_hist_cap = hist ? hist_cap : 0; g_hist_n = 0;
     precond pc = g_pc;
-    pc.fct = hist ? hist_precond : precond_amg;
+    pc.fct = hist ? hist_precond : g_fct;
     double t0 = now_s();
     int it = type == 4
         ? dcsr_pvfgmres(&g_A, &bb, &xx, &pc, tol, maxit, (SHORT)restart, (SHORT)stop_type,
@@ -185,6 +198,31 @@ int ref_gmres(int type, double *b, double *x, double tol, int maxit, int restart
     if (nhist) *nhist = g_hist_n;
     g_hist = NULL; g_hist_cap = 0;
     return it;
+}
+
+/* Generalized CG (dcsr_pgcg, krylov.c:2309) with the setup's
+ * preconditioner; hist as for ref_pcg.                                     */
+int ref_gcg(double *b, double *x, double tol, int maxit, int print_level, double *hist,
+            int hist_cap, int *nhist)
+{
+    dvector bb, xx;
+    bb.row = g_A.row; bb.val = b;
+    xx.row = g_A.row; xx.val = x;
+    g_hist = hist; g_hist_cap = hist ? hist_cap : 0; g_hist_n = 0;
+    precond pc = g_pc;
+    pc.fct = hist ? hist_precond : g_fct;
+    double t0 = now_s();
+    int it = dcsr_pgcg(&g_A, &bb, &xx, &pc, tol, maxit, 1, (SHORT)print_level);
+    g_solve_s = now_s() - t0;
+    if (nhist) *nhist = g_hist_n;
+    g_hist = NULL; g_hist_cap = 0;
+    return it;
+}
+
+/* amg_amli_coef (parameters.c:714) */
+void ref_amli_coef(double lambda_max, double lambda_min, int degree, double *coef)
+{
+    amg_amli_coef(lambda_max, lambda_min, degree, coef);
 }
 
 /* ---- kernel-level entry points on caller arrays -------------------------- */

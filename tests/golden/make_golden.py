@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -130,12 +130,80 @@ def gmres_cases(R):
     np.savez_compressed(os.path.join(HERE, "gmres.npz"), **out)
 
 
+# cycle variants of cycles.npz: AMG_param overrides on top of each case's
+CYCLE_VARIANTS = {
+    "a2": dict(cycle_type=3),
+    "a1": dict(cycle_type=3, amli_degree=1),
+    "a3": dict(cycle_type=3, amli_degree=3),
+    "a2s": dict(cycle_type=3, coarse_scaling=1),
+    "a2i": dict(cycle_type=3, coarse_solver=0),
+    "a2d": dict(cycle_type=3, coarse_dof=50),
+    "n": dict(cycle_type=4),
+    "ng": dict(cycle_type=4, nl_amli_krylov_type=5),
+    "nd": dict(cycle_type=4, coarse_dof=50),
+    "ngd": dict(cycle_type=4, coarse_dof=50, nl_amli_krylov_type=5),
+    "ni": dict(cycle_type=4, coarse_solver=0),
+    "d": dict(cycle_type=5),
+    "ds": dict(cycle_type=5, coarse_scaling=1),
+    "di": dict(cycle_type=5, coarse_solver=0),
+    "v": dict(cycle_type=1),
+}
+CYCLE_X_FIX = {"a2/fgmres", "a2/pcg", "n/fgmres", "d/fgmres", "v/gcg"}
+
+
+def cycle_cases(R):
+    """The AMLI (cycle_type 3), nonlinear AMLI (4) and additive (5) cycles
+    as linear_solver_dcsr_krylov_amg hands them to the Krylov methods: PCG,
+    flexible GMRES(100) and GCG with the cycle's preconditioner, on the two
+    matrices of gmres.npz; iterations, the residual norm at every
+    preconditioner call, one preconditioner application z = B b, and
+    solutions; plus amg_amli_coef for degrees 0 to 4."""
+    out = {}
+    g = np.load(os.path.join(HERE, "gmres.npz"))
+    bases = {"fix": {}, "kuhn": dict(smoother=10, presmooth_iter=2, postsmooth_iter=2,
+                                     coarse_dof=100)}
+    for name, base in bases.items():
+        cia, cja, cval = g[f"{name}/A_ia"], g[f"{name}/A_ja"], g[f"{name}/A_val"]
+        cb = g[f"{name}/b"]
+        for var, over in CYCLE_VARIANTS.items():
+            kw = dict(base)
+            kw.update(over)
+            prm = oracle.AMGParams(**kw)
+            assert R.setup(cia, cja, cval, prm) == 0
+            key = f"{name}/{var}"
+            out[key + "/params"] = np.array(prm.arrays()[0][:], np.int64)
+            out[key + "/dparams"] = np.array(prm.arrays()[1][:])
+            out[key + "/levels"] = np.int64(R.num_levels())
+            if name == "kuhn" or var in ("a2", "n", "d"):
+                out[key + "/z"] = R.precond(cb)
+            runs = {"gcg": R.gcg(cb, tol=1e-8, maxit=100)}
+            if var != "v":
+                runs["pcg"] = R.pcg(cb, None, 1e-8, 300, 1)
+                runs["fgmres"] = R.gmres(cb, tol=1e-8, maxit=300, restart=100, flexible=True)
+            for kr, (it, x, hist) in runs.items():
+                out[f"{key}/{kr}/iters"] = np.int64(it)
+                out[f"{key}/{kr}/hist"] = hist
+                if f"{var}/{kr}" in CYCLE_X_FIX or (
+                        name == "kuhn" and (kr == "fgmres" or var in ("a2", "n", "d", "v"))):
+                    out[f"{key}/{kr}/x"] = x
+                print("cycles", key, kr, it)
+            R.free()
+    for d in range(5):
+        out[f"amli_coef/{d}"] = R.amli_coef(2.0, 0.5, d)
+    out["amli_coef/wide3"] = R.amli_coef(10.0, 0.1, 3)
+    np.savez_compressed(os.path.join(HERE, "cycles.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
     R = oracle.ref()
-    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "gmres":
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if only == "gmres":
         gmres_cases(R)
+        return
+    if only == "cycles":
+        cycle_cases(R)
         return
     rng = np.random.default_rng(20261203)
     base = oracle.AMGParams()
@@ -235,6 +303,7 @@ def main():
     R.free()
     # 7. GMRES and flexible GMRES (Krylov types 3 and 4)
     gmres_cases(R)
+    cycle_cases(R)
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,53 @@
+"""Host-side pieces of the AMLI cycle, no GPU needed: amg_amli_coef of the
+library against the reference's coefficients (tests/golden/cycles.npz), bit
+for bit, and the preconditioner each cycle type selects."""
+import numpy as np
+import pytest
+
+import hazmath_b200 as hz
+from conftest import small_case
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    from hazmath_b200 import build
+    build.build()
+
+
+@pytest.mark.parametrize("degree", range(5))
+def test_amli_coefficients_bit_exact(golden, degree):
+    ref = golden("cycles.npz")[f"amli_coef/{degree}"]
+    got = hz.amli_coef(2.0, 0.5, degree)
+    assert got.tobytes() == ref.tobytes(), (got, ref)
+
+
+def test_amli_coefficients_other_interval(golden):
+    ref = golden("cycles.npz")["amli_coef/wide3"]
+    assert hz.amli_coef(10.0, 0.1, 3).tobytes() == ref.tobytes()
+
+
+def test_amli_polynomial_approximates_inverse():
+    """x q(x) stays within the best-approximation error of 1 on [0.5, 2]."""
+    x = np.linspace(0.5, 2.0, 2001)
+    errs = []
+    for d in range(5):
+        c = hz.amli_coef(2.0, 0.5, d)
+        q = sum(c[k] * x ** k for k in range(d + 1))
+        errs.append(np.abs(1 - x * q).max())
+    assert all(errs[k + 1] < errs[k] for k in range(4)), errs
+
+
+def test_precond_of_cycle_type():
+    assert hz._PRECOND_OF_CYCLE[hz.AMLI_CYCLE] == "precond_amli"
+    assert hz._PRECOND_OF_CYCLE[hz.NL_AMLI_CYCLE] == "precond_nl_amli"
+    assert hz._PRECOND_OF_CYCLE[hz.ADD_CYCLE] == "precond_amg_add"
+    assert hz.V_CYCLE not in hz._PRECOND_OF_CYCLE
+
+
+def test_cycle_fixture_covers_every_variant(golden):
+    z = golden("cycles.npz")
+    for case in ("fix", "kuhn"):
+        for var in ("a2", "n", "d"):
+            v = small_case(z, f"{case}/{var}")
+            assert int(v["params"][2]) in (3, 4, 5)
+            assert "pcg/iters" in v and "fgmres/iters" in v and "gcg/iters" in v
