@@ -56,8 +56,13 @@ FALLBACK_HBM = 6650.0
 METRIC = "AMG-PCG time to 1e-8 FP64 residual: mixed+learned vs plain on B200; SpMV GB/s"
 
 
+_FIELD = {}   # the last per-cube coefficient field generated, by N
+
+
 def kuhn_case(N: int, sigma: float, seeds):
     k = P.lognormal_field(N, sigma, 8.0, seeds[0])
+    _FIELD.clear()
+    _FIELD[N] = k
     ia, ja, val = P.kuhn3d_p1(N, k)
     b = P.rhs_uniform(len(ia) - 1, seeds[1])
     desc = {"workload": f"3D P1 log-normal diffusion, Kuhn mesh {N}^3 cubes "
@@ -360,6 +365,10 @@ def run_single(args, rank, world, local, dist):
     sp_ms, sp_by, spmv64_gbs = kernel(S64.h, hz.HZB_K_SPMV64)
     spmv32_gbs = kernel(S.h, hz.HZB_K_SPMV32)[2]
 
+    # device assembly of the same matrix from the per-cube coefficients
+    asm = assembly_leg(hz, torch, args.workload, dja, dval, n, nnz, dev, peak) \
+        if args.workload in CASES else None
+
     # e2e: the handle API with host arrays (copies in and out inside the region)
     Se = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
     xh = np.zeros(n)
@@ -418,6 +427,7 @@ def run_single(args, rank, world, local, dist):
                                "bytes_per_launch": sp_by, "ms_per_launch": sp_ms,
                                "traffic": TRAFFIC_PER_BYTE["spmv64"] * sp_by},
             "spmv_fp32_gbs": spmv32_gbs,
+            "assembly": asm,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s",
                     "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + val.nbytes + b.nbytes
@@ -430,6 +440,43 @@ def run_single(args, rank, world, local, dist):
     for h in (S, Sp, S64, Se):
         h.close()
     gnn.close()
+
+
+def assembly_leg(hz, torch, name, dja, dval, n, nnz, dev, peak):
+    """hzb_assemble_p1_kuhn_device on the workload's per-cube field (resident
+    in HBM): device seconds per call (row counts, scan, entries) between CUDA
+    events, its bytes (row pointers, columns and values written, field read)
+    against the HBM peak, and whether it reproduced the generator's arrays."""
+    N = CASES[name][0]
+    kd = torch.from_numpy(_FIELD[N]).to(dev)
+    ia = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    ja = torch.empty(nnz, dtype=torch.int32, device=dev)
+    va = torch.empty(nnz, dtype=torch.float64, device=dev)
+    ptrs = (kd.data_ptr(), ia.data_ptr(), ja.data_ptr(), va.data_ptr())
+
+    def call():
+        rc, got = hz.assemble_p1_kuhn_device(N, *ptrs)
+        if rc < 0 or got != nnz:
+            raise RuntimeError(f"assembly failed {rc}: {hz.last_error()}")
+
+    call()
+    same = bool(torch.equal(ja, dja)) and bool(torch.equal(va.view(torch.int64),
+                                                           dval.view(torch.int64)))
+    reps = 5
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / reps
+    by = 4.0 * (n + 1) + 12.0 * nnz + 8.0 * N ** 3
+    out = {"kernel": "hzb_assemble_p1_kuhn_device (one k_kuhn_fill launch)",
+           "seconds": t, "bytes": by, "achieved": by / t / 1e9, "peak": peak, "unit": "GB/s",
+           "frac": by / t / 1e9 / peak, "matches_host_generator": same}
+    del kd, ia, ja, va
+    return out
 
 
 # DRAM bytes (read + written) per algorithmic byte of one launch, measured by

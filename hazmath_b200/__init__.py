@@ -195,6 +195,8 @@ def lib() -> C.CDLL:
                                          INT, SHORT, SHORT, SHORT]
         L.dcsr_pgcg.argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL, INT,
                                 SHORT, SHORT]
+        L.hzb_assemble_p1_kuhn_device.argtypes = [INT, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, P(INT)]
         L.amg_amli_coef.argtypes = [REAL, REAL, INT, P(REAL)]
         L.amg_amli_coef.restype = None
         for name in ("precond_amg", "precond_amli", "precond_nl_amli", "precond_amg_add"):
@@ -314,6 +316,20 @@ def python_wrapper_krylov_amg(ia, ja, val, b, u, tol=1e-8, maxit=500, print_lvl=
                                     val.ctypes.data, b.ctypes.data, u.ctypes.data,
                                     C.byref(REAL(tol)), C.byref(INT(maxit)),
                                     C.byref(INT(print_lvl)))
+
+
+def assemble_p1_kuhn_device(N: int, kcell_ptr, ia_ptr, ja_ptr=None, val_ptr=None, K=None):
+    """hzb_assemble_p1_kuhn_device on device pointers: the interior-dof P1
+    stiffness on the Kuhn mesh of N^3 cubes.  Returns (status, nnz); ja/val
+    are filled when both pointers are given."""
+    nnz = INT()
+    Kp = None
+    if K is not None:
+        Kh = np.ascontiguousarray(K, np.float64).reshape(9)
+        Kp = Kh.ctypes.data_as(C.c_void_p)
+    rc = lib().hzb_assemble_p1_kuhn_device(N, kcell_ptr, Kp, ia_ptr, ja_ptr, val_ptr,
+                                           C.byref(nnz))
+    return rc, nnz.value
 
 
 # the preconditioner linear_solver_dcsr_krylov_amg picks for a cycle type

@@ -1197,6 +1197,14 @@ done:
     return rc;
 }
 
+extern "C" INT hzb_assemble_p1_kuhn_device(INT N, const REAL *d_kcell, const REAL *K,
+                                           INT *d_ia, INT *d_ja, REAL *d_val, INT *nnz) {
+    // mesh_cube_init (mesh_cube_anydim.c:30-128) + call_assembly
+    // (examples/elliptic_p1/supporting_elliptic_p1.h:537-647) + set_essential_bc
+    if (!d_ia) return ERROR_INPUT_PAR;
+    return hzb::assemble_kuhn_p1(N, d_kcell, K, d_ia, d_ja, d_val, nnz, 0);
+}
+
 extern "C" void hzb_free_device(void *p) {
     if (p) cudaFree(p);
 }

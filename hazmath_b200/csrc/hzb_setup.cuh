@@ -73,4 +73,9 @@ int multicolor(int n, const int *ia, const int *ja, Schedule *sch,
 // is not positive.
 int dense_inverse(const DCsr<double> &A, double **Ainv, cudaStream_t s);
 
+// P1 stiffness on the Kuhn mesh of N^3 cubes, interior dofs (hzb_assemble.cu):
+// ia ((N-1)^3 + 1) always; ja, val (nnz each) when both are given.
+int assemble_kuhn_p1(int N, const double *kcell, const double *K, int *ia, int *ja,
+                     double *val, int *nnz_out, cudaStream_t s);
+
 }  // namespace hzb

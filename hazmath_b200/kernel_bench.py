@@ -3,6 +3,7 @@
     python -m hazmath_b200.kernel_bench [--case c2|c5] [--levels 0,1,2]
         [--kernels spmv64,spmv32,res64,l1_32,l1_64] [--reps 50]
         [--precision mixed|fp64] [--matching parallel|exact]
+    python -m hazmath_b200.kernel_bench --assemble [--case c2|c5] [--reps 20]
 
 Builds the UA-AMG hierarchy (l1-Jacobi V(2,2) settings) of the 3D P1
 log-normal diffusion problem on the Kuhn mesh of 128^3 (c2, sigma 1) or
@@ -12,6 +13,10 @@ handle's stream between CUDA events, after one warm-up launch.  Prints
 achieved GB/s from the kernel's algorithmic bytes and the fraction of the
 measured HBM copy bandwidth.  The timed launches are bracketed by
 cudaProfilerStart/Stop, so `ncu --profile-from-start off` sees only them.
+
+--assemble times the device assembly of the case's matrix from its per-cube
+field instead (hzb_assemble_p1_kuhn_device, `reps` calls between CUDA events):
+algorithmic bytes = row pointers, columns and values written + the field read.
 """
 from __future__ import annotations
 
@@ -42,8 +47,11 @@ def main():
     ap.add_argument("--reps", type=int, default=50)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--matching", default="parallel", choices=["parallel", "exact"])
+    ap.add_argument("--assemble", action="store_true")
     a = ap.parse_args()
     import torch
+    if a.assemble:
+        return assemble(a, torch)
     N, sigma, seed = CASES[a.case]
     ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, sigma, 8.0, seed))
     n = len(ia) - 1
@@ -55,10 +63,7 @@ def main():
     rc = S.setup_device(n, len(ja), dia.data_ptr(), dja.data_ptr(), dval.data_ptr())
     if rc:
         raise SystemExit(f"setup failed {rc}: {last_error()}")
-    try:
-        peak = float(json.load(open(PEAKS))["hbm_gbs"])
-    except (OSError, KeyError, ValueError):
-        peak = 6650.0
+    peak = hbm_peak()
     st = S.stats()
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
@@ -80,6 +85,43 @@ def main():
                               "frac_of_measured_peak": gbs / peak}), flush=True)
     torch.cuda.profiler.stop()
     S.close()
+
+
+def hbm_peak() -> float:
+    try:
+        return float(json.load(open(PEAKS))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+def assemble(a, torch):
+    from . import assemble_p1_kuhn_device
+    N, sigma, seed = CASES[a.case]
+    k = torch.from_numpy(P.lognormal_field(N, sigma, 8.0, seed)).cuda()
+    m = N - 1
+    ia = torch.empty(m ** 3 + 1, dtype=torch.int32, device="cuda")
+    rc, nnz = assemble_p1_kuhn_device(N, k.data_ptr(), ia.data_ptr())
+    ja = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    va = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    args = (N, k.data_ptr(), ia.data_ptr(), ja.data_ptr(), va.data_ptr())
+    rc = assemble_p1_kuhn_device(*args)[0]   # warm-up
+    if rc:
+        raise SystemExit(f"assembly failed {rc}: {last_error()}")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()
+    e0.record()
+    for _ in range(a.reps):
+        assemble_p1_kuhn_device(*args)
+    e1.record()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    t = e0.elapsed_time(e1) * 1e-3 / a.reps
+    by = 4.0 * (m ** 3 + 1) + 12.0 * nnz + 8.0 * N ** 3
+    gbs = by / t / 1e9
+    print(json.dumps({"case": a.case, "kernel": "assemble_p1_kuhn", "rows": m ** 3, "nnz": nnz,
+                      "us_per_call": t * 1e6, "bytes_per_call": by, "gbs": gbs,
+                      "frac_of_measured_peak": gbs / hbm_peak()}), flush=True)
 
 
 if __name__ == "__main__":

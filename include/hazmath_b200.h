@@ -563,6 +563,25 @@ INT hzb_rap_agg_device(INT n, INT nnz, const INT *ia, const INT *ja,
                        INT *rap_nnz, INT **rap_ia, INT **rap_ja,
                        REAL **rap_val);
 void hzb_free_device(void *p);
+
+/* P1 stiffness matrix of -div(k K grad u) on the Kuhn (Freudenthal) mesh of
+ * N^3 cubes of the unit cube (each cube split into the 6 simplices
+ * 0 -> e_a -> e_a + e_b -> (1,1,1)), with the Dirichlet vertices eliminated,
+ * assembled on the device.  Replaces the cube mesh of mesh_cube_init
+ * (src/amr/mesh_cube_anydim.c:30-128), the element loop of call_assembly
+ * (examples/elliptic_p1/supporting_elliptic_p1.h:537-647) and
+ * set_essential_bc for this mesh.
+ *  - rows: the (N-1)^3 interior vertices, x fastest; columns ascending; the
+ *    15-point pattern (0, +-e_a, +-(e_a + e_b), +-(1,1,1)) cut at the
+ *    boundary, couplings that are exactly zero stay stored.
+ *  - d_kcell: per-cube coefficient [z][y][x] (N^3, device), NULL = 1;
+ *    K: constant 3x3 tensor, row-major (host), NULL = identity.
+ *  - d_ia ((N-1)^3 + 1 ints, device) is always filled and *nnz (host)
+ *    receives the entry count; d_ja / d_val (device, nnz each) are filled
+ *    when both are given (call once without them to size them).
+ *  - ERROR_MAT_SIZE when N < 2 or 15 (N-1)^3 does not fit an INT. */
+INT hzb_assemble_p1_kuhn_device(INT N, const REAL *d_kcell, const REAL *K, INT *d_ia,
+                                INT *d_ja, REAL *d_val, INT *nnz);
 /* copy bytes from device memory returned above into host memory */
 INT hzb_copy_to_host(void *dst, const void *src_device, size_t bytes);
 

@@ -283,6 +283,22 @@ class Ref(_Backend):
                               hist_cap, ctypes.byref(nh))
         return it, x, hist[: min(nh.value, hist_cap)].copy()
 
+    def cube_p1(self, ndiv):
+        """The reference's own P1 stiffness on its cube mesh with ndiv
+        divisions per edge (mesh_cube_init + call_assembly, Dirichlet rows
+        set to identity): (ia, ja, val, vertex coordinates (nv, 3),
+        Dirichlet flags)."""
+        out = (ctypes.c_int * 3)()
+        self.lib.ref_cube_p1(ndiv, out)
+        nv, nnz = out[0], out[1]
+        ia = np.empty(nv + 1, np.int32)
+        ja = np.empty(nnz, np.int32)
+        val = np.empty(nnz)
+        xv = np.empty(3 * nv)
+        d = np.empty(nv, np.int32)
+        self.lib.ref_cube_p1_get(_p(ia), _p(ja), _p(val), _p(xv), _p(d))
+        return ia, ja, val, xv.reshape(nv, 3), d
+
     def amli_coef(self, lambda_max, lambda_min, degree):
         c = np.zeros(degree + 1)
         self.lib.ref_amli_coef(ctypes.c_double(lambda_max), ctypes.c_double(lambda_min),

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -194,6 +194,38 @@ def cycle_cases(R):
     np.savez_compressed(os.path.join(HERE, "cycles.npz"), **out)
 
 
+def cube_cases(R):
+    """The reference's own P1 stiffness matrix on its own cube mesh
+    (mesh_cube_init with uniform refinement + the elliptic_p1 example's
+    call_assembly, unit coefficient), restricted to the interior vertices and
+    renumbered lexicographically (x fastest) through the vertex coordinates:
+    the matrix the Kuhn-mesh generator and the device assembly reproduce."""
+    out = {}
+    for ndiv in (4, 8, 12):
+        ia, ja, val, xv, d = R.cube_p1(ndiv)
+        g = np.rint(xv * ndiv).astype(np.int64)
+        assert np.abs(g - xv * ndiv).max() < 1e-9
+        m = ndiv - 1
+        lex = (g[:, 0] - 1) + m * ((g[:, 1] - 1) + m * (g[:, 2] - 1))
+        rows, cols, vals = [], [], []
+        for i in np.where(d == 0)[0]:
+            for k in range(ia[i], ia[i + 1]):
+                assert d[ja[k]] == 0
+                rows.append(lex[i])
+                cols.append(lex[ja[k]])
+                vals.append(val[k])
+        rows, cols, vals = np.array(rows), np.array(cols), np.array(vals)
+        order = np.lexsort((cols, rows))
+        rows, cols, vals = rows[order], cols[order], vals[order]
+        cia = np.zeros(m ** 3 + 1, np.int32)
+        np.add.at(cia, rows + 1, 1)
+        out[f"n{ndiv}/ia"] = np.cumsum(cia).astype(np.int32)
+        out[f"n{ndiv}/ja"] = cols.astype(np.int32)
+        out[f"n{ndiv}/val"] = vals
+        print("cube", ndiv, len(vals))
+    np.savez_compressed(os.path.join(HERE, "cube_p1.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
@@ -204,6 +236,9 @@ def main():
         return
     if only == "cycles":
         cycle_cases(R)
+        return
+    if only == "cube":
+        cube_cases(R)
         return
     rng = np.random.default_rng(20261203)
     base = oracle.AMGParams()
@@ -304,6 +339,7 @@ def main():
     # 7. GMRES and flexible GMRES (Krylov types 3 and 4)
     gmres_cases(R)
     cycle_cases(R)
+    cube_cases(R)
     print("golden fixtures written to", HERE)
 
 
