@@ -193,8 +193,9 @@ def lib() -> C.CDLL:
         for name in ("dcsr_pvgmres", "dcsr_pvfgmres"):
             getattr(L, name).argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL,
                                          INT, SHORT, SHORT, SHORT]
-        L.dcsr_pgcg.argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL, INT,
-                                SHORT, SHORT]
+        for name in ("dcsr_pgcg", "dcsr_pminres"):
+            getattr(L, name).argtypes = [P(dCSRmat), P(dvector), P(dvector), P(precond), REAL,
+                                         INT, SHORT, SHORT]
         L.hzb_assemble_p1_kuhn_device.argtypes = [INT, C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p, C.c_void_p, P(INT)]
         L.amg_amli_coef.argtypes = [REAL, REAL, INT, P(REAL)]
@@ -422,6 +423,12 @@ class AMGHierarchy:
         self.mgl[0].b, self.mgl[0].x = sb, sx
         assert n == len(xx)
         return xx
+
+    def minres(self, b, x, tol=1e-8, maxit=500, stop_type=STOP_REL_RES, prtlvl=0):
+        """dcsr_pminres with the setup's preconditioner."""
+        bb = np.ascontiguousarray(b, np.float64)
+        return lib().dcsr_pminres(C.byref(self._A.mat), C.byref(_dvec(bb)), C.byref(_dvec(x)),
+                                  C.byref(self.pc), tol, maxit, stop_type, prtlvl)
 
     def gcg(self, b, x, tol=1e-8, maxit=100, stop_type=STOP_REL_RES, prtlvl=0):
         """dcsr_pgcg with the setup's preconditioner."""

@@ -30,6 +30,7 @@ SOURCES = [
     ("hzb_batch.cu", False),
     ("hzb_gmres.cu", False),
     ("hzb_cycles.cu", False),
+    ("hzb_minres.cu", False),
     ("hzb_assemble.cu", False),
     ("hzb_learn.cu", False),
     ("hzb_gnn.cu", True),

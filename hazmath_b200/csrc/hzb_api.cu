@@ -278,8 +278,12 @@ extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
         it = gmres(S, S->lv[0].A64(), d_b, d_x, kind, nullptr, S->it.linear_tol,
                    S->it.linear_maxit, S->it.linear_restart, S->it.linear_stop_type, prt,
                    S->it.linear_itsolver_type == SOLVER_VFGMRES, &rel);
+    } else if (S->it.linear_itsolver_type == SOLVER_MinRes) {
+        it = minres(S, S->lv[0].A64(), d_b, d_x, kind, nullptr, S->it.linear_tol,
+                    S->it.linear_maxit, S->it.linear_stop_type, prt, &rel);
     } else {
-        set_error_msg("Krylov types 1 (CG), 3 (GMRES) and 4 (flexible GMRES) are built");
+        set_error_msg("Krylov types 1 (CG), 2 (MINRES), 3 (GMRES) and 4 (flexible GMRES) "
+                      "are the ones solver_dcsr_linear_itsolver dispatches");
         return ERROR_SOLVER_TYPE;
     }
     HZB_CUDA(cudaEventRecord(S->e1, S->s));
@@ -742,7 +746,8 @@ extern "C" void amg_amli_coef(const REAL lambda_max, const REAL lambda_min, cons
 struct TmpCsr {
     int *ia = nullptr, *ja = nullptr;
     double *val = nullptr;
-    ~TmpCsr() { dfree(ia); dfree(ja); dfree(val); }
+    void release() { dfree(ia); dfree(ja); dfree(val); }
+    ~TmpCsr() { release(); }
 };
 
 static int upload_csr(const dCSRmat *A, TmpCsr &T, DCsr<double> &D, cudaStream_t s) {
@@ -757,7 +762,7 @@ static int upload_csr(const dCSRmat *A, TmpCsr &T, DCsr<double> &D, cudaStream_t
     return SUCCESS;
 }
 
-// A Krylov method (type: SOLVER_CG, SOLVER_GCG, SOLVER_VGMRES or SOLVER_VFGMRES) on host
+// A Krylov method (SOLVER_CG, SOLVER_MinRes, SOLVER_GCG, SOLVER_VGMRES, SOLVER_VFGMRES) on host
 // arrays with the caller's preconditioner: the setup's own AMG runs on the
 // device, any other pc->fct is called on host copies.
 static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol,
@@ -811,6 +816,8 @@ static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol
             it = pcg(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, w, &rel, condest);
         else if (type == SOLVER_GCG)
             it = gcg(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, &rel);
+        else if (type == SOLVER_MinRes)
+            it = minres(S, D, db, du, kind, &hp, tol, MaxIt, stop_type, prtlvl, &rel);
         else
             it = gmres(S, D, db, du, kind, &hp, tol, MaxIt, restart, stop_type, prtlvl,
                        type == SOLVER_VFGMRES, &rel);
@@ -819,7 +826,9 @@ static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol
             if (cudaStreamSynchronize(S->s) != cudaSuccess) it = ERROR_SOLVER_MISC;
         }
     }
+    // everything allocated on the handle's stream goes before the stream
     w.release();
+    T.release();
     dfree(db);
     dfree(du);
     free(hp.h_r);
@@ -851,6 +860,12 @@ extern "C" INT dcsr_pvfgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
                        restart);
 }
 
+extern "C" INT dcsr_pminres(dCSRmat *A, dvector *b, dvector *u, precond *pc, const REAL tol,
+                            const INT MaxIt, const SHORT stop_type, const SHORT prtlvl) {
+    // krylov.c:2449-2840
+    return krylov_host(A, b, u, pc, tol, MaxIt, stop_type, prtlvl, nullptr, SOLVER_MinRes, 0);
+}
+
 extern "C" INT dcsr_pgcg(dCSRmat *A, dvector *b, dvector *u, precond *pc, const REAL tol,
                          const INT MaxIt, const SHORT stop_type, const SHORT prtlvl) {
     // krylov.c:2309-2420
@@ -862,6 +877,7 @@ static void krylov_banner(SHORT prtlvl, SHORT type) {
     if (prtlvl <= PRINT_NONE) return;
     printf("**********************************************************\n");
     if (type == SOLVER_CG) printf(" --> using Conjugate Gradient Method:\n");
+    else if (type == SOLVER_MinRes) printf(" --> using MINRES Method:\n");
     else if (type == SOLVER_VGMRES) printf(" --> using GMRES Method:\n");
     else printf(" --> using Flexible GMRES Method:\n");
 }
@@ -876,7 +892,8 @@ extern "C" INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
         printf("### HAZMATH WARNING: Convergence tolerance for iterative solver is too small!\n");
     if (itparam->linear_maxit <= 0)
         printf("### HAZMATH WARNING: Max number of iterations should be a POSITIVE integer!\n");
-    if (type != SOLVER_CG && type != SOLVER_VGMRES && type != SOLVER_VFGMRES) {
+    if (type != SOLVER_CG && type != SOLVER_MinRes && type != SOLVER_VGMRES &&
+        type != SOLVER_VFGMRES) {
         printf("### ERROR: Unknown itertive solver type %lld!\n", (long long)type);
         return ERROR_SOLVER_TYPE;
     }
@@ -886,6 +903,7 @@ extern "C" INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
                          itparam->linear_stop_type, prtlvl, &cond, type,
                          itparam->linear_restart);
     if (type == SOLVER_CG) printf("Estimated condition number = %13.6e\n", cond);
+    if (type == SOLVER_MinRes) printf(" NOTHING IMPLEMENTED FOR MINRES\n");   // itsolver.c:176
     return it;
 }
 
@@ -911,8 +929,8 @@ extern "C" INT hzb_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
         printf("Unsmoothed aggregation setup costs %.4f seconds.\n", S->st.setup_seconds);
     }
     const SHORT type = itparam->linear_itsolver_type;
-    if (bp->precision != HZB_PREC_MIXED && type != SOLVER_CG && type != SOLVER_VGMRES &&
-        type != SOLVER_VFGMRES) {
+    if (bp->precision != HZB_PREC_MIXED && type != SOLVER_CG && type != SOLVER_MinRes &&
+        type != SOLVER_VGMRES && type != SOLVER_VFGMRES) {
         printf("### ERROR: Unknown itertive solver type %lld!\n", (long long)type);
         hzb_destroy(S);
         return ERROR_SOLVER_TYPE;
@@ -921,6 +939,8 @@ extern "C" INT hzb_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
     INT it = hzb_solve_host(S, b->val, x->val);
     if (bp->precision != HZB_PREC_MIXED && type == SOLVER_CG)
         printf("Estimated condition number = %13.6e\n", S->st.condest);
+    if (bp->precision != HZB_PREC_MIXED && type == SOLVER_MinRes)
+        printf(" NOTHING IMPLEMENTED FOR MINRES\n");
     if (prtlvl >= PRINT_MIN) {
         printf("AMG_Krylov method totally costs %.4f seconds.\n",
                S->st.setup_seconds + S->st.solve_seconds);

@@ -163,6 +163,10 @@ int gmres(hzb_solver *S, const DCsr<double> &A, const double *b, double *x, int 
           HostPrecond *hp, double tol, int MaxIt, int restart, int stop_type, int prtlvl,
           bool flexible, double *relres_out, int ws_slot = -1);
 void gmres_release(hzb_solver *S);
+// preconditioned MINRES, dcsr_pminres (hzb_minres.cu)
+int minres(hzb_solver *S, const DCsr<double> &A, const double *b, double *u, int kind,
+           HostPrecond *hp, double tol, int MaxIt, int stop_type, int prtlvl,
+           double *relres_out);
 // generalized conjugate gradient, dcsr_pgcg (hzb_cycles.cu)
 int gcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u, int kind,
         HostPrecond *hp, double tol, int MaxIt, int stop_type, int prtlvl, double *relres_out,

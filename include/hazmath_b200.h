@@ -290,8 +290,9 @@ INT linear_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
 INT linear_solver_amg(dCSRmat *A, dvector *b, dvector *x, AMG_param *param);
 
 /* src/solver/itsolver.c:135-229: Krylov switch on a host preconditioner:
- * type 1 CG (prints the condition estimate), 3 variable-restart GMRES, 4
- * flexible GMRES; MINRES (2) returns ERROR_SOLVER_TYPE. */
+ * type 1 CG (prints the condition estimate), 2 MINRES (prints the
+ * reference's " NOTHING IMPLEMENTED FOR MINRES" line), 3 variable-restart
+ * GMRES, 4 flexible GMRES; any other type returns ERROR_SOLVER_TYPE. */
 INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
                                 precond *pc, linear_itsolver_param *itparam);
 
@@ -352,6 +353,12 @@ INT dcsr_pvgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
 INT dcsr_pvfgmres(dCSRmat *A, dvector *b, dvector *x, precond *pc,
                   const REAL tol, const INT MaxIt, const SHORT restart,
                   const SHORT stop_type, const SHORT prtlvl);
+
+/* src/solver/krylov.c:2449-2840: preconditioned MINRES (three-term
+ * recurrence, B-normalised directions, the CG's three safety checks);
+ * Krylov type 2. */
+INT dcsr_pminres(dCSRmat *A, dvector *b, dvector *u, precond *pc, const REAL tol,
+                 const INT MaxIt, const SHORT stop_type, const SHORT prtlvl);
 
 /* src/solver/krylov.c:2309-2420: generalized conjugate gradient (every
  * direction kept and A-orthogonalised, no restart), stopping on

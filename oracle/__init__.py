@@ -272,6 +272,17 @@ class Ref(_Backend):
                                 ctypes.byref(nh))
         return it, x, hist[: min(nh.value, hist_cap)].copy()
 
+    def minres(self, b, x0=None, tol=1e-8, maxit=500, stop_type=1, use_pc=True, hist_cap=1024):
+        """dcsr_pminres with the preconditioner of the last setup (or none):
+        (iterations, x, ||r|| at each preconditioner call)."""
+        b = np.ascontiguousarray(b, np.float64).copy()
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        hist = np.zeros(hist_cap)
+        nh = ctypes.c_int()
+        it = self.lib.ref_minres(_p(b), _p(x), ctypes.c_double(tol), maxit, stop_type,
+                                 int(use_pc), _p(hist), hist_cap, ctypes.byref(nh))
+        return it, x, hist[: min(nh.value, hist_cap)].copy()
+
     def gcg(self, b, x0=None, tol=1e-8, maxit=100, hist_cap=1024):
         """dcsr_pgcg with the preconditioner of the last setup:
         (iterations, x, ||r|| at each preconditioner call)."""

@@ -200,6 +200,25 @@ int ref_gmres(int type, double *b, double *x, double tol, int maxit, int restart
     return it;
 }
 
+/* Preconditioned MINRES (dcsr_pminres, krylov.c:2449) with the setup's
+ * preconditioner (use_pc != 0) or none; hist as for ref_pcg.              */
+int ref_minres(double *b, double *x, double tol, int maxit, int stop_type, int use_pc,
+               double *hist, int hist_cap, int *nhist)
+{
+    dvector bb, xx;
+    bb.row = g_A.row; bb.val = b;
+    xx.row = g_A.row; xx.val = x;
+    g_hist = hist; g_hist_cap = hist ? hist_cap : 0; g_hist_n = 0;
+    precond pc = g_pc;
+    pc.fct = hist ? hist_precond : g_fct;
+    double t0 = now_s();
+    int it = dcsr_pminres(&g_A, &bb, &xx, use_pc ? &pc : NULL, tol, maxit, (SHORT)stop_type, 0);
+    g_solve_s = now_s() - t0;
+    if (nhist) *nhist = g_hist_n;
+    g_hist = NULL; g_hist_cap = 0;
+    return it;
+}
+
 /* Generalized CG (dcsr_pgcg, krylov.c:2309) with the setup's
  * preconditioner; hist as for ref_pcg.                                     */
 int ref_gcg(double *b, double *x, double tol, int maxit, int print_level, double *hist,

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -226,6 +226,35 @@ def cube_cases(R):
     np.savez_compressed(os.path.join(HERE, "cube_p1.npz"), **out)
 
 
+def minres_cases(R):
+    """The reference's preconditioned MINRES (dcsr_pminres) on the matrices
+    of gmres.npz with the V-cycle preconditioner, for the three stopping
+    types, and without a preconditioner: iterations, the residual norm at
+    every preconditioner call, solutions."""
+    out = {}
+    g = np.load(os.path.join(HERE, "gmres.npz"))
+    bases = {"fix": {}, "kuhn": dict(smoother=10, presmooth_iter=2, postsmooth_iter=2,
+                                     coarse_dof=100)}
+    for name, base in bases.items():
+        cia, cja, cval = g[f"{name}/A_ia"], g[f"{name}/A_ja"], g[f"{name}/A_val"]
+        cb = g[f"{name}/b"]
+        prm = oracle.AMGParams(**base)
+        assert R.setup(cia, cja, cval, prm) == 0
+        for stop in (1, 2, 3):
+            it, x, hist = R.minres(cb, tol=1e-8, maxit=500, stop_type=stop)
+            out[f"{name}/s{stop}/iters"] = np.int64(it)
+            out[f"{name}/s{stop}/x"] = x
+            out[f"{name}/s{stop}/hist"] = hist
+            print("minres", name, stop, it)
+        if name == "kuhn":
+            it, x, _ = R.minres(cb, tol=1e-6, maxit=2000, stop_type=1, use_pc=False)
+            out[f"{name}/nopc/iters"] = np.int64(it)
+            out[f"{name}/nopc/x"] = x
+            print("minres", name, "no pc", it)
+        R.free()
+    np.savez_compressed(os.path.join(HERE, "minres.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
@@ -239,6 +268,9 @@ def main():
         return
     if only == "cube":
         cube_cases(R)
+        return
+    if only == "minres":
+        minres_cases(R)
         return
     rng = np.random.default_rng(20261203)
     base = oracle.AMGParams()
@@ -340,6 +372,7 @@ def main():
     gmres_cases(R)
     cycle_cases(R)
     cube_cases(R)
+    minres_cases(R)
     print("golden fixtures written to", HERE)
 
 

@@ -76,7 +76,7 @@ def test_gmres_maxit_and_unknown_type(golden):
     assert S.solve_host(c["b"], x) == hz.ERROR_SOLVER_MAXIT   # iter >= MaxIt, as the reference
     S.close()
     S = hz.Solver(amg_from_case(c), hz.itsolver_param(
-        linear_itsolver_type=hz.SOLVER_MinRes, linear_precond_type=hz.PREC_AMG,
+        linear_itsolver_type=6, linear_precond_type=hz.PREC_AMG,
         linear_tol=1e-8, linear_maxit=50))
     assert S.setup_host(c["A_ia"], c["A_ja"], c["A_val"]) == 0
     assert S.solve_host(c["b"], np.zeros(len(c["b"]))) == hz.ERROR_SOLVER_TYPE

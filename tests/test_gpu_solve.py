@@ -160,7 +160,8 @@ def _spmv(ia, ja, val, x):
 
 
 def test_error_codes():
-    it = hz.itsolver_param(linear_itsolver_type=hz.SOLVER_MinRes, linear_tol=1e-8)
+    # GCR (6) is not one of solver_dcsr_linear_itsolver's types
+    it = hz.itsolver_param(linear_itsolver_type=6, linear_tol=1e-8)
     ia, ja, val = P.poisson2d_5pt(20)
     x = np.zeros(400)
     b = np.ones(400)
