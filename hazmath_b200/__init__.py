@@ -43,7 +43,7 @@ SOLVER_MinRes, SOLVER_VGMRES, SOLVER_VFGMRES, SOLVER_GCG = 2, 3, 4, 5
 SOLVER_UMFPACK = 32
 STOP_REL_RES, STOP_REL_PRECRES, STOP_MOD_REL_RES = 1, 2, 3
 PREC_AMG = 2
-UA_AMG = 1
+UA_AMG, SA_AMG = 1, 2
 VMB, HEC, HEM = 1, 4, 5
 V_CYCLE, W_CYCLE, AMLI_CYCLE, NL_AMLI_CYCLE, ADD_CYCLE = 1, 2, 3, 4, 5
 SMOOTHER_JACOBI, SMOOTHER_GS, SMOOTHER_SGS = 1, 2, 3
@@ -153,6 +153,7 @@ def lib() -> C.CDLL:
         L.hzb_last_error.restype = C.c_char_p
         L.amg_data_create.restype = P(AMG_data)
         L.amg_setup_ua.restype = SHORT
+        L.amg_setup_sa.restype = SHORT
         L.hzb_create.argtypes = [P(C.c_void_p), P(AMG_param), P(linear_itsolver_param),
                                  P(hzb_param)]
         for name in ("hzb_setup_device", "hzb_solve_device", "hzb_precond_device",
@@ -352,14 +353,16 @@ class AMGHierarchy:
     precond_amg_add) for dcsr_pcg / dcsr_pgcg / dcsr_pv(f)gmres, the cycles,
     amg_data_free."""
 
-    def __init__(self, ia, ja, val, amgparam: AMG_param):
+    def __init__(self, ia, ja, val, amgparam: AMG_param, smoothed: bool = False):
+        """smoothed: amg_setup_sa instead of amg_setup_ua."""
         self._A = _HostCSR(ia, ja, val)
         self.param = amgparam
         L = lib()
         self.mgl = L.amg_data_create(amgparam.max_levels)
         self.mgl[0].A = self._A.mat   # the caller's arrays, as dcsr_cp'd in the reference
         self._owned_A0 = True
-        self.status = L.amg_setup_ua(self.mgl, C.byref(amgparam))
+        setup = L.amg_setup_sa if smoothed else L.amg_setup_ua
+        self.status = setup(self.mgl, C.byref(amgparam))
         self.pcdata = precond_data()
         L.precond_data_null(C.byref(self.pcdata))
         L.param_amg_to_prec(C.byref(self.pcdata), C.byref(amgparam))
@@ -535,6 +538,23 @@ class Solver:
         if rc:
             raise RuntimeError(f"hzb_level_copy: {rc} {last_error()}")
         return ia, ja, val, agg
+
+    def prolongation(self, l: int):
+        """The smoothed prolongation of level l as (ia, ja, val), or None for
+        an unsmoothed level."""
+        n = self.stats().rows[l]
+        nnz = INT()
+        rc = lib().hzb_level_prolongation(self.h, l, None, None, None, C.byref(nnz))
+        if rc:
+            raise RuntimeError(f"hzb_level_prolongation: {rc} {last_error()}")
+        if nnz.value == 0:
+            return None
+        ia = np.empty(n + 1, np.int32)
+        ja = np.empty(nnz.value, np.int32)
+        val = np.empty(nnz.value)
+        lib().hzb_level_prolongation(self.h, l, ia.ctypes.data, ja.ctypes.data, val.ctypes.data,
+                                     C.byref(nnz))
+        return ia, ja, val
 
     def close(self):
         if self.h:

@@ -31,6 +31,7 @@ SOURCES = [
     ("hzb_gmres.cu", False),
     ("hzb_cycles.cu", False),
     ("hzb_minres.cu", False),
+    ("hzb_sa.cu", False),
     ("hzb_assemble.cu", False),
     ("hzb_learn.cu", False),
     ("hzb_gnn.cu", True),

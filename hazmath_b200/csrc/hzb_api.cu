@@ -306,6 +306,10 @@ extern "C" INT hzb_batch_setup_device(hzb_solver *S, INT nsys, const INT *off, I
         set_error_msg("batched solves run V and W cycles (cycle_type 1, 2)");
         return ERROR_INPUT_PAR;
     }
+    if (S->amg.AMG_type == SA_AMG) {
+        set_error_msg("batched solves run unsmoothed aggregation");
+        return ERROR_INPUT_PAR;
+    }
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
     S->host_ia = nullptr; S->host_ja = nullptr; S->host_val = nullptr;
@@ -526,7 +530,25 @@ static int export_level(hzb_solver *S, AMG_data *mgl, int l) {
         mgl[l].A.val = (REAL *)malloc(sizeof(REAL) * (L.nnz > 0 ? L.nnz : 1));
         HZB_TRY(hzb_level_copy(S, l, mgl[l].A.IA, mgl[l].A.JA, mgl[l].A.val, NULL));
     }
-    if (l < S->nl - 1) {
+    if (l < S->nl - 1 && L.sa) {
+        // smoothed aggregation: P and R = P^T as stored, with their values
+        dCSRmat &P = mgl[l].P, &R = mgl[l].R;
+        const int nr = L.pnnz;
+        P.row = L.n; P.col = L.nc; P.nnz = nr;
+        R.row = L.nc; R.col = L.n; R.nnz = nr;
+        P.IA = (INT *)malloc(sizeof(INT) * (L.n + 1));
+        P.JA = (INT *)malloc(sizeof(INT) * (nr > 0 ? nr : 1));
+        P.val = (REAL *)malloc(sizeof(REAL) * (nr > 0 ? nr : 1));
+        R.IA = (INT *)malloc(sizeof(INT) * (L.nc + 1));
+        R.JA = (INT *)malloc(sizeof(INT) * (nr > 0 ? nr : 1));
+        R.val = (REAL *)malloc(sizeof(REAL) * (nr > 0 ? nr : 1));
+        HZB_CUDA(cudaMemcpy(P.IA, L.pia, sizeof(int) * (L.n + 1), cudaMemcpyDeviceToHost));
+        HZB_CUDA(cudaMemcpy(P.JA, L.pja, sizeof(int) * nr, cudaMemcpyDeviceToHost));
+        HZB_CUDA(cudaMemcpy(P.val, L.pval, sizeof(double) * nr, cudaMemcpyDeviceToHost));
+        HZB_CUDA(cudaMemcpy(R.IA, L.ria, sizeof(int) * (L.nc + 1), cudaMemcpyDeviceToHost));
+        HZB_CUDA(cudaMemcpy(R.JA, L.rja, sizeof(int) * nr, cudaMemcpyDeviceToHost));
+        HZB_CUDA(cudaMemcpy(R.val, L.rval, sizeof(double) * nr, cudaMemcpyDeviceToHost));
+    } else if (l < S->nl - 1) {
         // P (n x nc, one unit entry per aggregated row) and R = P^T
         std::vector<int> agg(L.n), ria(L.nc + 1), rja(L.n);
         HZB_CUDA(cudaMemcpy(agg.data(), L.agg, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
@@ -555,8 +577,8 @@ static int export_level(hzb_solver *S, AMG_data *mgl, int l) {
     return SUCCESS;
 }
 
-extern "C" SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param) {
-    // amg_setup_ua.c:53 -> amg_setup_unsmoothP_unsmoothR (:1228-1452)
+// amg_setup_ua / amg_setup_sa: the device hierarchy hangs off mgl[0].wdata
+static SHORT amg_setup_common(AMG_data *mgl, AMG_param *param, SHORT type) {
     if (!mgl || !param) return ERROR_INPUT_PAR;
     hzb_param bp;
     hzb_param_init(&bp);
@@ -567,6 +589,7 @@ extern "C" SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param) {
     hzb_solver *S = nullptr;
     INT rc = hzb_create(&S, param, NULL, &bp);
     if (rc) return (SHORT)rc;
+    S->amg.AMG_type = type;   // the entry point decides, as in the reference
     S->caller_amg = param;
     rc = hzb_setup_host(S, &mgl[0].A);
     if (rc) { hzb_destroy(S); return (SHORT)rc; }
@@ -606,8 +629,33 @@ extern "C" SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param) {
     }
     if (param->print_level > PRINT_NONE) {
         if (param->print_level >= PRINT_SOME) print_complexity(S);
-        printf("Unsmoothed aggregation setup costs %.4f seconds.\n", S->st.setup_seconds);
+        printf("%s aggregation setup costs %.4f seconds.\n",
+               type == SA_AMG ? "Smoothed" : "Unsmoothed", S->st.setup_seconds);
     }
+    return SUCCESS;
+}
+
+extern "C" SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param) {
+    // amg_setup_ua.c:53 -> amg_setup_unsmoothP_unsmoothR (:1228-1452)
+    return amg_setup_common(mgl, param, UA_AMG);
+}
+
+extern "C" SHORT amg_setup_sa(AMG_data *mgl, AMG_param *param) {
+    // amg_setup_ua.c:76 -> amg_setup_smoothP_smoothR (:1461-1700)
+    return amg_setup_common(mgl, param, SA_AMG);
+}
+
+extern "C" INT hzb_level_prolongation(const hzb_solver *S, INT l, INT *ia, INT *ja,
+                                      REAL *val, INT *nnz) {
+    if (!S || l < 0 || l >= S->nl - 1) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    const Level &L = S->lv[l];
+    if (nnz) *nnz = L.sa ? L.pnnz : 0;
+    if (!L.sa) return SUCCESS;
+    if (ia) HZB_CUDA(cudaMemcpy(ia, L.pia, sizeof(int) * (L.n + 1), cudaMemcpyDeviceToHost));
+    if (ja) HZB_CUDA(cudaMemcpy(ja, L.pja, sizeof(int) * L.pnnz, cudaMemcpyDeviceToHost));
+    if (val) HZB_CUDA(cudaMemcpy(val, L.pval, sizeof(double) * L.pnnz, cudaMemcpyDeviceToHost));
     return SUCCESS;
 }
 
@@ -917,7 +965,8 @@ extern "C" INT hzb_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
     hzb_param dflt;
     hzb_param_init(&dflt);
     if (!bp) bp = &dflt;
-    if (prtlvl > PRINT_NONE) printf("\n Calling UA AMG ...\n");
+    if (prtlvl > PRINT_NONE)
+        printf("\n Calling %s AMG ...\n", amgparam->AMG_type == SA_AMG ? "SA" : "UA");
     hzb_solver *S = nullptr;
     INT rc = hzb_create(&S, amgparam, itparam, bp);
     if (rc) return rc;
@@ -926,7 +975,8 @@ extern "C" INT hzb_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
     if (rc) { hzb_destroy(S); return rc; }
     if (amgparam->print_level > PRINT_NONE) {
         if (amgparam->print_level >= PRINT_SOME) print_complexity(S);
-        printf("Unsmoothed aggregation setup costs %.4f seconds.\n", S->st.setup_seconds);
+        printf("%s aggregation setup costs %.4f seconds.\n",
+               amgparam->AMG_type == SA_AMG ? "Smoothed" : "Unsmoothed", S->st.setup_seconds);
     }
     const SHORT type = itparam->linear_itsolver_type;
     if (bp->precision != HZB_PREC_MIXED && type != SOLVER_CG && type != SOLVER_MinRes &&
@@ -968,7 +1018,8 @@ extern "C" INT linear_solver_amg(dCSRmat *A, dvector *b, dvector *x, AMG_param *
         return ERROR_MAT_SIZE;
     }
     const SHORT prtlvl = param->print_level;
-    if (prtlvl > PRINT_NONE) printf("\n Calling UA AMG ...\n");
+    if (prtlvl > PRINT_NONE)
+        printf("\n Calling %s AMG ...\n", param->AMG_type == SA_AMG ? "SA" : "UA");
     hzb_solver *S = nullptr;
     INT rc = hzb_create(&S, param, NULL, NULL);
     if (rc) return rc;

@@ -124,7 +124,7 @@ int amli64(hzb_solver *S, const AMG_param &cyc, const double *coef, int l) {
     const int degree = cyc.amli_degree;
     HZB_TRY(smooth64(S, l, true, cyc));
     HZB_TRY(spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, s));
-    HZB_TRY(restrict_agg<double>(L.nc, L.ria, L.rja, L.w, C.b, s));
+    HZB_TRY(restrict_level(S, l, L.w, C.b));
     HZB_TRY(vcopy<double>(C.n, C.b, C.r1, s));
     // b_c = A_c e_c + (q_{degree-i} / q_degree) r_c after each inner cycle
     for (int i = 1; i <= degree; ++i) {
@@ -138,7 +138,7 @@ int amli64(hzb_solver *S, const AMG_param &cyc, const double *coef, int l) {
     HZB_TRY(scale(C.n, coef[degree], C.x, s));
     double alpha = 1.0;
     if (cyc.coarse_scaling == ON) HZB_TRY(coarse_alpha(S, l + 1, C.r1, &alpha));
-    HZB_TRY(prolong_agg<double>(L.n, L.agg, C.x, L.x, alpha, s));
+    HZB_TRY(prolong_level(S, l, C.x, L.x, alpha));
     return smooth64(S, l, false, cyc);
 }
 
@@ -149,7 +149,7 @@ int nl_amli64(hzb_solver *S, const AMG_param &cyc, int l) {
     Level &L = S->lv[l], &C = S->lv[l + 1];
     HZB_TRY(smooth64(S, l, true, cyc));
     HZB_TRY(spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, s));
-    HZB_TRY(restrict_agg<double>(L.nc, L.ria, L.rja, L.w, C.b, s));
+    HZB_TRY(restrict_level(S, l, L.w, C.b));
     HZB_TRY(vzero<double>(C.n, C.x, s));
     if (l == S->nl - 2) {
         HZB_TRY(nl_amli64(S, cyc, l + 1));
@@ -170,7 +170,7 @@ int nl_amli64(hzb_solver *S, const AMG_param &cyc, int l) {
                        STOP_REL_RES, PRINT_NONE, true, &rel, l + 1);
         if (it < 0 && it != ERROR_SOLVER_MAXIT) return it;
     }
-    HZB_TRY(prolong_agg<double>(L.n, L.agg, C.x, L.x, 1.0, s));
+    HZB_TRY(prolong_level(S, l, C.x, L.x, 1.0));
     return smooth64(S, l, false, cyc);
 }
 
@@ -185,7 +185,7 @@ int add_cycle64(hzb_solver *S, const AMG_param &cyc) {
     while (l < nl - 1) {
         Level &L = S->lv[l];
         HZB_TRY(smooth64(S, l, true, cyc));
-        HZB_TRY(restrict_agg<double>(L.nc, L.ria, L.rja, l == 0 ? L.w : L.b, S->lv[l + 1].b, s));
+        HZB_TRY(restrict_level(S, l, l == 0 ? L.w : L.b, S->lv[l + 1].b));
         ++l;
         HZB_TRY(vzero<double>(S->lv[l].n, S->lv[l].x, s));
     }
@@ -195,7 +195,7 @@ int add_cycle64(hzb_solver *S, const AMG_param &cyc) {
         --l;
         Level &L = S->lv[l];
         if (cyc.coarse_scaling == ON) HZB_TRY(coarse_alpha(S, l + 1, S->lv[l + 1].b, &alpha));
-        HZB_TRY(prolong_agg<double>(L.n, L.agg, S->lv[l + 1].x, L.x, alpha, s));
+        HZB_TRY(prolong_level(S, l, S->lv[l + 1].x, L.x, alpha));
     }
     return SUCCESS;
 }

@@ -125,18 +125,18 @@ static int coarse_apply(hzb_solver *S) {
 static int coarse_correct(hzb_solver *S, LearnWork &w, double *e) {
     Level &L0 = S->lv[0], &L1 = S->lv[1];
     HZB_TRY(spmv<double>(L0.A64(), SPMV_Y, e, nullptr, w.r, 1.0, nullptr, S->s));
-    HZB_TRY(restrict_agg<double>(L0.nc, L0.ria, L0.rja, w.r, L1.b, S->s));
+    HZB_TRY(restrict_level(S, 0, w.r, L1.b));
     HZB_TRY(coarse_apply(S));
-    return prolong_agg<double>(L0.n, L0.agg, L1.x, e, -1.0, S->s);
+    return prolong_level(S, 0, L1.x, e, -1.0);
 }
 
 // g <- g - A P B_c R g          (adjoint coarse correction)
 static int coarse_correct_adj(hzb_solver *S, LearnWork &w, double *g) {
     Level &L0 = S->lv[0], &L1 = S->lv[1];
-    HZB_TRY(restrict_agg<double>(L0.nc, L0.ria, L0.rja, g, L1.b, S->s));
+    HZB_TRY(restrict_level(S, 0, g, L1.b));
     HZB_TRY(coarse_apply(S));
     HZB_TRY(vzero<double>(L0.n, w.t, S->s));
-    HZB_TRY(prolong_agg<double>(L0.n, L0.agg, L1.x, w.t, 1.0, S->s));
+    HZB_TRY(prolong_level(S, 0, L1.x, w.t, 1.0));
     return spmv<double>(L0.A64(), SPMV_AXPY, w.t, nullptr, g, -1.0, nullptr, S->s);
 }
 

@@ -73,6 +73,20 @@ int multicolor(int n, const int *ia, const int *ja, Schedule *sch,
 // is not positive.
 int dense_inverse(const DCsr<double> &A, double **Ainv, cudaStream_t s);
 
+// Smoothed aggregation (hzb_sa.cu).  sa_prolongation turns N (nval, in
+// place: the strength graph, filtered, or a copy of A without the filter)
+// into S = I - omega D^{-1} N and forms P = S P_tent for the aggregate map;
+// transpose_rect is dcsr_trans of an n x ncols CSR; rap_general is dcsr_rap
+// in the reference's traversal order.
+int sa_prolongation(const DCsr<double> &A, const int *nia, const int *nja, double *nval,
+                    int nc, const int *agg, double omega, bool filter, int **pia, int **pja,
+                    double **pval, int *pnnz, cudaStream_t s);
+int transpose_rect(int n, int ncols, int nnz, const int *ia, const int *ja, const double *val,
+                   int **tia, int **tja, double **tval, cudaStream_t s);
+int rap_general(int nc, const int *ria, const int *rja, const double *rval,
+                const DCsr<double> &A, const int *pia, const int *pja, const double *pval,
+                int **cia, int **cja, double **cval, int *cnnz, cudaStream_t s);
+
 // P1 stiffness on the Kuhn mesh of N^3 cubes, interior dofs (hzb_assemble.cu):
 // ia ((N-1)^3 + 1) always; ja, val (nnz each) when both are given.
 int assemble_kuhn_p1(int N, const double *kcell, const double *K, int *ia, int *ja,

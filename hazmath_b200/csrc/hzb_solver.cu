@@ -55,6 +55,8 @@ void Level::release() {
     ia32 = ja32 = nullptr;
     own32 = false;
     dfree(agg); dfree(ria); dfree(rja);
+    dfree(pia); dfree(pja); dfree(pval); dfree(rval);
+    sa = false;
     dfree(b); dfree(x); dfree(w); dfree(t); dfree(r1);
     dfree(b32); dfree(x32); dfree(w32); dfree(t32);
     dfree(d_jac); dfree(d_gs_f); dfree(d_gs_b); dfree(d_sor_f); dfree(d_sor_b);
@@ -208,6 +210,17 @@ static bool smoother_needs_gs(int sm) {
 // ---------------------------------------------------------------------------
 // V / W cycle, mgcycle (mgcycle.c:245-415)
 // ---------------------------------------------------------------------------
+int restrict_level(hzb_solver *S, int l, const double *w, double *bc) {
+    const Level &L = S->lv[l];
+    if (L.sa) return spmv<double>(L.R64(), SPMV_Y, w, nullptr, bc, 1.0, nullptr, S->s);
+    return restrict_agg<double>(L.nc, L.ria, L.rja, w, bc, S->s);
+}
+
+int prolong_level(hzb_solver *S, int l, const double *xc, double *x, double alpha) {
+    const Level &L = S->lv[l];
+    if (L.sa) return spmv<double>(L.P64(), SPMV_AXPY, xc, nullptr, x, alpha, nullptr, S->s);
+    return prolong_agg<double>(L.n, L.agg, xc, x, alpha, S->s);
+}
 int coarse_solve64(hzb_solver *S, const AMG_param &cyc, double ctol) {
     Level &C = S->lv[S->nl - 1];
     if (cyc.coarse_solver == SOLVER_UMFPACK && S->Ainv)
@@ -248,7 +261,7 @@ forward:
         num_lvl[l]++;
         HZB_TRY(smooth64(S, l, true, cyc));
         HZB_TRY(spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, S->s));
-        HZB_TRY(restrict_agg<double>(L.nc, L.ria, L.rja, L.w, S->lv[l + 1].b, S->s));
+        HZB_TRY(restrict_level(S, l, L.w, S->lv[l + 1].b));
         ++l;
         HZB_TRY(vzero<double>(S->lv[l].n, S->lv[l].x, S->s));
     }
@@ -257,7 +270,7 @@ forward:
         --l;
         Level &L = S->lv[l];
         if (cyc.coarse_scaling == ON) HZB_TRY(coarse_alpha(S, l + 1, S->lv[l + 1].b, &alpha));
-        HZB_TRY(prolong_agg<double>(L.n, L.agg, S->lv[l + 1].x, L.x, alpha, S->s));
+        HZB_TRY(prolong_level(S, l, S->lv[l + 1].x, L.x, alpha));
         HZB_TRY(smooth64(S, l, false, cyc));
         if (num_lvl[l] < cyc.cycle_type) break;
         else num_lvl[l] = 0;
@@ -498,6 +511,12 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
     }
     const short min_cdof = (short)std::max(S->amg.coarse_dof, 1);
     const int max_levels = std::min<int>(S->amg.max_levels, MAX_AMG_LVL);
+    // smoothed aggregation (amg_setup_sa) for SA_AMG, else unsmoothed
+    const bool sa = S->amg.AMG_type == SA_AMG;
+    if (sa && S->bp.precision == HZB_PREC_MIXED) {
+        set_error_msg("the mixed-precision cycle runs unsmoothed aggregation");
+        return ERROR_INPUT_PAR;
+    }
     int lvl = 0;
     int *tmp = nullptr;
     HZB_TRY(dalloc(&tmp, scan_tmp_size(n + 2)));
@@ -521,21 +540,54 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
             if (par) rc = hem_parallel(m, nia, nja, nval, agg, &nagg, work, s);
             else rc = hem_exact(m, nia, nja, nval, agg, &nagg, work, s);
         }
-        dfree(nia); dfree(nja); dfree(nval); dfree(work);
-        if (rc) { dfree(agg); break; }
+        dfree(work);
+        // smoothed aggregation still needs the strength graph (or A's copy)
+        if (!rc && sa && S->amg.smooth_filter != ON) {
+            dfree(nia); dfree(nja); dfree(nval);
+            if (!(rc = dalloc(&nval, L.nnz)))
+                rc = cudaMemcpyAsync(nval, L.val, sizeof(double) * L.nnz,
+                                     cudaMemcpyDeviceToDevice, s) == cudaSuccess
+                         ? SUCCESS : ERROR_SOLVER_MISC;
+        }
+        if (!sa || rc) { dfree(nia); dfree(nja); dfree(nval); }
+        if (rc) { dfree(agg); dfree(nval); break; }
         // adaptive threshold (amg_setup_ua.c:1325-1328), caller's param too
         if (nagg * 4 > m) S->amg.strong_coupled /= 2;
         else if (nagg * 1.25 < m) S->amg.strong_coupled *= 2;
         if (S->caller_amg) S->caller_amg->strong_coupled = S->amg.strong_coupled;
-        if (nagg < MIN_CDOF) { dfree(agg); break; }
+        if (nagg < MIN_CDOF) {
+            dfree(agg);
+            if (sa) { dfree(nia); dfree(nja); dfree(nval); }
+            break;
+        }
         L.nc = nagg;
         L.agg = agg;
-        if ((rc = dalloc(&L.ria, nagg + 1)) || (rc = dalloc(&L.rja, m))) break;
-        if ((rc = restriction_pattern(m, nagg, agg, L.ria, L.rja, tmp, s))) break;
         int *cia = nullptr, *cja = nullptr, cnnz = 0;
         double *cval = nullptr;
-        if ((rc = rap_agg(L.A64(), nagg, agg, L.ria, L.rja, &cia, &cja, &cval, &cnnz, s)))
-            break;
+        if (sa) {
+            // smooth_aggregation_p, dcsr_trans, dcsr_rap (amg_setup_ua.c:1600-1624)
+            const bool filter = S->amg.smooth_filter == ON;
+            rc = sa_prolongation(L.A64(), filter ? nia : L.ia, filter ? nja : L.ja, nval, nagg,
+                                 agg, S->amg.tentative_smooth, filter, &L.pia, &L.pja, &L.pval,
+                                 &L.pnnz, s);
+            dfree(nia); dfree(nja); dfree(nval);
+            L.sa = true;
+            if (rc) break;
+            if ((rc = transpose_rect(m, nagg, L.pnnz, L.pia, L.pja, L.pval, &L.ria, &L.rja,
+                                     &L.rval, s)))
+                break;
+            if ((rc = bundle_capacity(m, L.pia, s, &L.pcap)) ||
+                (rc = bundle_capacity(nagg, L.ria, s, &L.rcap)))
+                break;
+            if ((rc = rap_general(nagg, L.ria, L.rja, L.rval, L.A64(), L.pia, L.pja, L.pval,
+                                  &cia, &cja, &cval, &cnnz, s)))
+                break;
+        } else {
+            if ((rc = dalloc(&L.ria, nagg + 1)) || (rc = dalloc(&L.rja, m))) break;
+            if ((rc = restriction_pattern(m, nagg, agg, L.ria, L.rja, tmp, s))) break;
+            if ((rc = rap_agg(L.A64(), nagg, agg, L.ria, L.rja, &cia, &cja, &cval, &cnnz, s)))
+                break;
+        }
         S->lv.emplace_back();
         Level &C = S->lv.back();
         C.n = nagg; C.nnz = cnnz; C.ia = cia; C.ja = cja; C.val = cval; C.own_A = true;

@@ -24,9 +24,23 @@ struct Level {
     int *ia32 = nullptr, *ja32 = nullptr;
     float *val32 = nullptr;
     bool own32 = false;
-    // transfer to level + 1 (P = agg map, R = P^T with ascending rows)
+    // transfer to level + 1 (P = agg map, R = P^T with ascending rows);
+    // smoothed aggregation keeps P as a CSR with values and R's values too
     int nc = 0;
     int *agg = nullptr, *ria = nullptr, *rja = nullptr;
+    bool sa = false;
+    int *pia = nullptr, *pja = nullptr, pnnz = 0, pcap = 0, rcap = 0;
+    double *pval = nullptr, *rval = nullptr;
+    DCsr<double> P64() const {
+        DCsr<double> m;
+        m.n = n; m.nnz = pnnz; m.ia = pia; m.ja = pja; m.val = pval; m.bundle_cap = pcap;
+        return m;
+    }
+    DCsr<double> R64() const {
+        DCsr<double> m;
+        m.n = nc; m.nnz = pnnz; m.ia = ria; m.ja = rja; m.val = rval; m.bundle_cap = rcap;
+        return m;
+    }
     // cycle vectors; r1 keeps the restricted residual of the AMLI cycle
     // (allocated on levels >= 1 when that cycle first runs)
     double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr, *r1 = nullptr;
@@ -209,6 +223,11 @@ int learn_errors(hzb_solver *S, int ns, unsigned long long seed, double *E,
                  const float *omega, int ncyc);
 int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, int ncyc,
                     double *loss, float *domega);
+// transfers of mgcycle: b_{l+1} = R w (dcsr_mxv_agg, or dcsr_mxv for
+// smoothed aggregation) and x_l += alpha P x_{l+1} (dcsr_aAxpy_agg /
+// dcsr_aAxpy)
+int restrict_level(hzb_solver *S, int l, const double *w, double *bc);
+int prolong_level(hzb_solver *S, int l, const double *xc, double *x, double alpha);
 // smoothing of level l as mgcycle's pre (pre = true) / post smoothing calls
 int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc);
 // diagonals and sweep schedules the configured smoother needs on level L

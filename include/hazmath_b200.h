@@ -302,6 +302,14 @@ INT solver_dcsr_linear_itsolver(dCSRmat *A, dvector *b, dvector *x,
  * the device hierarchy in mgl[0].wdata (released by amg_data_free). */
 SHORT amg_setup_ua(AMG_data *mgl, AMG_param *param);
 
+/* src/solver/amg_setup_ua.c:76 (-> amg_setup_smoothP_smoothR, :1461-1700):
+ * smoothed aggregation: the aggregates of amg_setup_ua, P = S P_tent with the
+ * damped-Jacobi smoother S of the filtered strength graph (tentative_smooth,
+ * smooth_filter), R = P^T, A_c = R A P by the general Galerkin product; the
+ * device hierarchy as for amg_setup_ua.  linear_solver_dcsr_krylov_amg and
+ * linear_solver_amg take this path for AMG_type SA_AMG. */
+SHORT amg_setup_sa(AMG_data *mgl, AMG_param *param);
+
 /* src/solver/mgcycle.c:245-415: one V/W cycle on mgl[0].b, mgl[0].x. */
 void mgcycle(AMG_data *mgl, AMG_param *param);
 
@@ -480,6 +488,11 @@ INT  hzb_set_omega_device(hzb_solver *s, const float *d_omega);
 INT  hzb_get_stats(const hzb_solver *s, hzb_stats *st);
 /* level l of the device hierarchy copied to host arrays sized from stats;
  * agg (rows of level l) is the aggregate map, -1 for an empty row of P.   */
+/* the smoothed prolongation P of level l (n_l x n_{l+1}, CSR with values)
+ * into host arrays; *nnz receives its entry count (0 for an unsmoothed level,
+ * whose P is the aggregate map of hzb_level_copy) */
+INT  hzb_level_prolongation(const hzb_solver *s, INT l, INT *ia, INT *ja, REAL *val,
+                            INT *nnz);
 INT  hzb_level_copy(const hzb_solver *s, INT l, INT *ia, INT *ja, REAL *val,
                     INT *agg);
 void hzb_destroy(hzb_solver *s);

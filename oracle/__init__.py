@@ -56,17 +56,22 @@ class AMGParams:
     maxit: int = 1
     amli_degree: int = 2
     nl_amli_krylov_type: int = 4
+    AMG_type: int = 1
+    smooth_filter: int = 1
     strong_coupled: float = 0.0
     relaxation: float = 1.0
     tol: float = 1e-6
+    tentative_smooth: float = 0.67
 
     def arrays(self):
-        ip = (ctypes.c_int * 14)(
+        ip = (ctypes.c_int * 16)(
             self.max_levels, self.coarse_dof, self.cycle_type, self.smoother,
             self.presmooth_iter, self.postsmooth_iter, self.coarse_solver,
             self.aggregation_type, self.max_aggregation, self.coarse_scaling,
-            self.print_level, self.maxit, self.amli_degree, self.nl_amli_krylov_type)
-        dp = (ctypes.c_double * 3)(self.strong_coupled, self.relaxation, self.tol)
+            self.print_level, self.maxit, self.amli_degree, self.nl_amli_krylov_type,
+            self.AMG_type, self.smooth_filter)
+        dp = (ctypes.c_double * 4)(self.strong_coupled, self.relaxation, self.tol,
+                                   self.tentative_smooth)
         return ip, dp
 
 
@@ -293,6 +298,15 @@ class Ref(_Backend):
         it = self.lib.ref_gcg(_p(b), _p(x), ctypes.c_double(tol), maxit, 0, _p(hist),
                               hist_cap, ctypes.byref(nh))
         return it, x, hist[: min(nh.value, hist_cap)].copy()
+
+    def level_P(self, l: int):
+        """P of level l with its values."""
+        n, _, nc, pnnz = self.level_info(l)[:4]
+        ia = np.empty(n + 1, np.int32)
+        ja = np.empty(pnnz, np.int32)
+        val = np.empty(pnnz)
+        self.lib.ref_level_P(l, _p(ia), _p(ja), _p(val))
+        return ia, ja, val
 
     def cube_p1(self, ndiv):
         """The reference's own P1 stiffness on its cube mesh with ndiv

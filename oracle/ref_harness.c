@@ -38,12 +38,12 @@ static double now_s(void)
 /* iparam: [0] max_levels [1] coarse_dof [2] cycle_type [3] smoother
  *         [4] presmooth [5] postsmooth [6] coarse_solver [7] aggregation_type
  *         [8] max_aggregation [9] coarse_scaling [10] print_level [11] amg maxit
- *         [12] amli_degree [13] nl_amli_krylov_type
- * dparam: [0] strong_coupled [1] relaxation [2] amg tol                      */
+ *         [12] amli_degree [13] nl_amli_krylov_type [14] AMG_type
+ *         [15] smooth_filter
+ * dparam: [0] strong_coupled [1] relaxation [2] amg tol [3] tentative_smooth */
 static void fill_param(AMG_param *p, const int *ip, const double *dp)
 {
     param_amg_init(p);
-    p->AMG_type = UA_AMG;
     p->max_levels = (SHORT)ip[0];
     p->coarse_dof = ip[1];
     p->cycle_type = (SHORT)ip[2];
@@ -58,6 +58,9 @@ static void fill_param(AMG_param *p, const int *ip, const double *dp)
     p->maxit = ip[11];
     p->amli_degree = (SHORT)ip[12];
     p->nl_amli_krylov_type = (SHORT)ip[13];
+    p->AMG_type = (SHORT)ip[14];
+    p->smooth_filter = (SHORT)ip[15];
+    p->tentative_smooth = dp[3];
     p->strong_coupled = dp[0];
     p->relaxation = dp[1];
     p->tol = dp[2];
@@ -85,7 +88,9 @@ int ref_setup(int n, int nnz, int *ia, int *ja, double *val,
     g_mgl[0].b = dvec_create(n);
     g_mgl[0].x = dvec_create(n);
     double t0 = now_s();
-    SHORT status = amg_setup_ua(g_mgl, &g_amg);
+    /* linear_solver_dcsr_krylov_amg's choice (itsolver.c:870-885) */
+    SHORT status = g_amg.AMG_type == SA_AMG ? amg_setup_sa(g_mgl, &g_amg)
+                                            : amg_setup_ua(g_mgl, &g_amg);
     g_setup_s = now_s() - t0;
     precond_data_null(&g_pcdata);
     param_amg_to_prec(&g_pcdata, &g_amg);
@@ -131,6 +136,15 @@ void ref_level_agg(int l, int *agg)
     dCSRmat *P = &g_mgl[l].P;
     for (int i = 0; i < P->row; ++i)
         agg[i] = (P->IA[i + 1] > P->IA[i]) ? P->JA[P->IA[i]] : -1;
+}
+
+/* P of level l with its values (smoothed aggregation) */
+void ref_level_P(int l, int *ia, int *ja, double *val)
+{
+    dCSRmat *P = &g_mgl[l].P;
+    memcpy(ia, P->IA, sizeof(int) * (P->row + 1));
+    memcpy(ja, P->JA, sizeof(int) * P->nnz);
+    memcpy(val, P->val, sizeof(double) * P->nnz);
 }
 
 void ref_level_R(int l, int *ia, int *ja)

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -255,6 +255,55 @@ def minres_cases(R):
     np.savez_compressed(os.path.join(HERE, "minres.npz"), **out)
 
 
+SA_VARIANTS = {
+    "fix/sa": ("fix", {}),
+    "fix/sa_nf": ("fix", dict(smooth_filter=0)),
+    "kuhn/sa": ("kuhn", {}),
+    "kuhn/sa_nf": ("kuhn", dict(smooth_filter=0)),
+    "kuhn/sa_t": ("kuhn", dict(strong_coupled=0.08)),
+    "kuhn/sa_w": ("kuhn", dict(cycle_type=2, coarse_solver=0)),
+}
+
+
+def sa_cases(R):
+    """Smoothed aggregation (amg_setup_sa) on the matrices of gmres.npz: the
+    level sizes, SHA-256 digests of every coarse operator and of every
+    smoothed prolongation (their arrays are large: the coarse levels of
+    smoothed aggregation fill in), the adapted threshold, and PCG /
+    flexible GMRES(100) iterations and solutions with the V-cycle (W-cycle
+    with the iterative coarse solver for one variant)."""
+    out = {}
+    g = np.load(os.path.join(HERE, "gmres.npz"))
+    bases = {"fix": {}, "kuhn": dict(smoother=10, presmooth_iter=2, postsmooth_iter=2,
+                                     coarse_dof=100)}
+    for key, (name, over) in SA_VARIANTS.items():
+        cia, cja, cval = g[f"{name}/A_ia"], g[f"{name}/A_ja"], g[f"{name}/A_val"]
+        cb = g[f"{name}/b"]
+        kw = dict(bases[name])
+        kw.update(over)
+        kw["AMG_type"] = 2
+        prm = oracle.AMGParams(**kw)
+        assert R.setup(cia, cja, cval, prm) == 0
+        nl = R.num_levels()
+        out[key + "/params"] = np.array(prm.arrays()[0][:], np.int64)
+        out[key + "/dparams"] = np.array(prm.arrays()[1][:])
+        out[key + "/info"] = np.array([R.level_info(l)[:4] for l in range(nl)], np.int64)
+        out[key + "/theta_after"] = np.float64(R.strong_coupled())
+        for l in range(nl):
+            out[f"{key}/A{l}_sha"] = np.array([sha(a) for a in R.level_A(l)])
+            if l < nl - 1:
+                out[f"{key}/P{l}_sha"] = np.array([sha(a) for a in R.level_P(l)])
+        it, x, hist = R.pcg(cb, None, 1e-8, 300, 1)
+        out[key + "/pcg/iters"] = np.int64(it)
+        out[key + "/pcg/x"] = x
+        out[key + "/pcg/hist"] = hist
+        it, x, _ = R.gmres(cb, tol=1e-8, maxit=300, restart=100, flexible=True)
+        out[key + "/fgmres/iters"] = np.int64(it)
+        print("sa", key, nl, out[key + "/pcg/iters"], it)
+        R.free()
+    np.savez_compressed(os.path.join(HERE, "sa.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
@@ -271,6 +320,9 @@ def main():
         return
     if only == "minres":
         minres_cases(R)
+        return
+    if only == "sa":
+        sa_cases(R)
         return
     rng = np.random.default_rng(20261203)
     base = oracle.AMGParams()
@@ -373,6 +425,7 @@ def main():
     cycle_cases(R)
     cube_cases(R)
     minres_cases(R)
+    sa_cases(R)
     print("golden fixtures written to", HERE)
 
 
