@@ -169,6 +169,8 @@ def lib() -> C.CDLL:
         L.hzb_level_copy.argtypes = [C.c_void_p, INT, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
         L.hzb_get_stats.argtypes = [C.c_void_p, P(hzb_stats)]
+        L.hzb_level_prolongation.argtypes = [C.c_void_p, INT, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, P(INT)]
         L.hzb_destroy.argtypes = [C.c_void_p]
         L.hzb_time_kernel.argtypes = [C.c_void_p, INT, INT, INT, P(REAL), P(REAL)]
         L.hzb_batch_setup_device.argtypes = [C.c_void_p, INT, P(INT), INT, INT, C.c_void_p,
