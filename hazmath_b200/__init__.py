@@ -62,6 +62,12 @@ class dCSRmat(C.Structure):
                 ("JA", C.POINTER(INT)), ("val", C.POINTER(REAL))]
 
 
+class dBSRmat(C.Structure):
+    _fields_ = [("ROW", INT), ("COL", INT), ("NNZ", INT), ("nb", INT),
+                ("storage_manner", INT), ("val", C.POINTER(REAL)), ("IA", C.POINTER(INT)),
+                ("JA", C.POINTER(INT))]
+
+
 class dvector(C.Structure):
     _fields_ = [("row", INT), ("val", C.POINTER(REAL))]
 
@@ -172,6 +178,13 @@ def lib() -> C.CDLL:
         L.hzb_level_prolongation.argtypes = [C.c_void_p, INT, C.c_void_p, C.c_void_p,
                                              C.c_void_p, P(INT)]
         L.hzb_destroy.argtypes = [C.c_void_p]
+        L.hzb_bsr_setup_host.argtypes = [C.c_void_p, P(dBSRmat)]
+        L.hzb_bsr_level.argtypes = [C.c_void_p, INT, P(dBSRmat), C.c_void_p]
+        for name in ("hzb_bsr_precond_device", "hzb_bsr_precond_host", "hzb_bsr_solve_device",
+                     "hzb_bsr_solve_host"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.linear_solver_dbsr_krylov_amg.argtypes = [P(dBSRmat), P(dvector), P(dvector),
+                                                    P(linear_itsolver_param), P(AMG_param)]
         L.hzb_time_kernel.argtypes = [C.c_void_p, INT, INT, INT, P(REAL), P(REAL)]
         L.hzb_batch_setup_device.argtypes = [C.c_void_p, INT, P(INT), INT, INT, C.c_void_p,
                                              C.c_void_p, C.c_void_p]
@@ -301,6 +314,32 @@ def linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, itparam, amgparam, b200=Non
     return lib().hzb_solver_dcsr_krylov_amg(C.byref(A.mat), C.byref(_dvec(bb)),
                                             C.byref(_dvec(x)), C.byref(itparam),
                                             C.byref(amgparam), C.byref(b200))
+
+
+class _HostBSR:
+    """Keeps numpy arrays alive behind a dBSRmat (blocks row-major)."""
+
+    def __init__(self, nb, ia, ja, val):
+        self.ia = np.ascontiguousarray(ia, np.int32)
+        self.ja = np.ascontiguousarray(ja, np.int32)
+        self.val = np.ascontiguousarray(val, np.float64)
+        n = len(self.ia) - 1
+        self.mat = dBSRmat(n, n, int(self.ia[-1]), int(nb), 0,
+                           self.val.ctypes.data_as(C.POINTER(REAL)),
+                           self.ia.ctypes.data_as(C.POINTER(INT)),
+                           self.ja.ctypes.data_as(C.POINTER(INT)))
+
+
+def linear_solver_dbsr_krylov_amg(nb, ia, ja, val, b, x, itparam, amgparam):
+    """itsolver.c:2104 semantics on a block matrix of nb x nb blocks; x
+    (float64 array, ROW * nb) is updated in place.  Returns the iteration
+    count or a negative ERROR_* code."""
+    A = _HostBSR(nb, ia, ja, val)
+    assert x.dtype == np.float64 and x.flags.c_contiguous
+    bb = np.ascontiguousarray(b, np.float64)
+    return lib().linear_solver_dbsr_krylov_amg(C.byref(A.mat), C.byref(_dvec(bb)),
+                                               C.byref(_dvec(x)), C.byref(itparam),
+                                               C.byref(amgparam))
 
 
 def linear_solver_amg(ia, ja, val, b, x, amgparam):
@@ -557,6 +596,51 @@ class Solver:
         lib().hzb_level_prolongation(self.h, l, ia.ctypes.data, ja.ctypes.data, val.ctypes.data,
                                      C.byref(nnz))
         return ia, ja, val
+
+    # -- block (BSR) matrices -------------------------------------------
+    def setup_bsr_host(self, nb, ia, ja, val) -> int:
+        """amg_setup_ua_bsr on the device for a host block matrix."""
+        self._keep_bsr = _HostBSR(nb, ia, ja, val)
+        return lib().hzb_bsr_setup_host(self.h, C.byref(self._keep_bsr.mat))
+
+    def bsr_level(self, l: int):
+        """Block matrix of level l as (ia, ja, val) and its block
+        aggregates (None on the coarsest level)."""
+        m = dBSRmat()
+        rc = lib().hzb_bsr_level(self.h, l, C.byref(m), None)
+        if rc:
+            raise RuntimeError(f"hzb_bsr_level: {rc} {last_error()}")
+        n, nnzb, nb = m.ROW, m.NNZ, m.nb
+        ia = np.empty(n + 1, np.int32)
+        ja = np.empty(nnzb, np.int32)
+        val = np.empty(nnzb * nb * nb)
+        agg = np.empty(n, np.int32)
+        m.IA = ia.ctypes.data_as(C.POINTER(INT))
+        m.JA = ja.ctypes.data_as(C.POINTER(INT))
+        m.val = val.ctypes.data_as(C.POINTER(REAL))
+        last = l == self.stats().num_levels - 1
+        rc = lib().hzb_bsr_level(self.h, l, C.byref(m), None if last else agg.ctypes.data)
+        if rc:
+            raise RuntimeError(f"hzb_bsr_level: {rc} {last_error()}")
+        return ia, ja, val, (None if last else agg)
+
+    def bsr_precond_host(self, r):
+        rr = np.ascontiguousarray(r, np.float64)
+        z = np.zeros_like(rr)
+        rc = lib().hzb_bsr_precond_host(self.h, rr.ctypes.data, z.ctypes.data)
+        if rc:
+            raise RuntimeError(f"hzb_bsr_precond_host: {rc} {last_error()}")
+        return z
+
+    def bsr_precond_device(self, r_ptr, z_ptr) -> int:
+        return lib().hzb_bsr_precond_device(self.h, r_ptr, z_ptr)
+
+    def bsr_solve_device(self, b_ptr, x_ptr) -> int:
+        return lib().hzb_bsr_solve_device(self.h, b_ptr, x_ptr)
+
+    def bsr_solve_host(self, b, x) -> int:
+        bb = np.ascontiguousarray(b, np.float64)
+        return lib().hzb_bsr_solve_host(self.h, bb.ctypes.data, x.ctypes.data)
 
     def close(self):
         if self.h:

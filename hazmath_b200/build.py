@@ -32,6 +32,7 @@ SOURCES = [
     ("hzb_cycles.cu", False),
     ("hzb_minres.cu", False),
     ("hzb_sa.cu", False),
+    ("hzb_bsr.cu", False),
     ("hzb_assemble.cu", False),
     ("hzb_learn.cu", False),
     ("hzb_gnn.cu", True),

@@ -1006,6 +1006,172 @@ extern "C" INT linear_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
     return hzb_solver_dcsr_krylov_amg(A, b, x, itparam, amgparam, NULL);
 }
 
+// ---------------------------------------------------------------------------
+// block (BSR) matrices: amg_setup_ua_bsr, precond_dbsr_amg and
+// solver_dbsr_linear_itsolver behind linear_solver_dbsr_krylov_amg
+// (amg_setup_ua.c:145, precond.c:1311-1339, itsolver.c:232-305, 2104-2200)
+// ---------------------------------------------------------------------------
+static int check_bsr_host(const dBSRmat *A) {
+    if (!A || !A->IA || !A->JA || !A->val) return ERROR_INPUT_PAR;
+    if (A->ROW != A->COL || A->ROW <= 0 || A->NNZ <= 0) return ERROR_MAT_SIZE;
+    if (A->IA[0] != 0 || A->IA[A->ROW] != A->NNZ) return ERROR_DATA_STRUCTURE;
+    if (A->storage_manner != 0) {
+        set_error_msg("blocks are stored row by row (storage_manner 0)");
+        return ERROR_INPUT_PAR;
+    }
+    return SUCCESS;
+}
+
+// precond_dbsr_amg rebuilds its cycle parameters from param_amg_init with
+// these fields of the caller's AMG_param (precond.c:1322-1330): the coarse
+// solver and tolerance stay at their defaults
+static AMG_param bsr_cycle_param_of(const AMG_param &amg) {
+    AMG_param c;
+    param_amg_init(&c);
+    c.cycle_type = amg.cycle_type;
+    c.smoother = amg.smoother;
+    c.presmooth_iter = amg.presmooth_iter;
+    c.postsmooth_iter = amg.postsmooth_iter;
+    c.relaxation = amg.relaxation;
+    c.coarse_scaling = amg.coarse_scaling;
+    c.tentative_smooth = amg.tentative_smooth;
+    c.maxit = amg.maxit;   // precdata.maxit: the cycles per application
+    return c;
+}
+
+extern "C" INT hzb_bsr_setup_host(hzb_solver *S, const dBSRmat *A) {
+    if (!S) return ERROR_INPUT_PAR;
+    HZB_TRY(check_bsr_host(A));
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    S->bsr_cyc = bsr_cycle_param_of(S->amg);
+    return hzb::bsr_setup(S, A->ROW, A->NNZ, A->nb, A->IA, A->JA, A->val);
+}
+
+extern "C" INT hzb_bsr_level(const hzb_solver *S, INT l, dBSRmat *out, INT *agg) {
+    if (!S || !S->bsr || !out) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    int nrow = 0, nnzb = 0;
+    HZB_TRY(hzb::bsr_level_copy(S, l, &nrow, &nnzb, out->IA, out->JA, out->val, agg));
+    out->ROW = out->COL = nrow;
+    out->NNZ = nnzb;
+    out->nb = hzb::bsr_block_size(S);
+    out->storage_manner = 0;
+    return SUCCESS;
+}
+
+extern "C" INT hzb_bsr_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z) {
+    if (!S || !S->bsr) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    HZB_TRY(hzb::bsr_precond(S, d_r, d_z));
+    HZB_CUDA(cudaStreamSynchronize(S->s));
+    return SUCCESS;
+}
+
+extern "C" INT hzb_bsr_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
+    if (!S || !S->bsr) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    const long long l0 = hzb::launch_count();
+    HZB_CUDA(cudaEventRecord(S->e0, S->s));
+    double rel = 0.0, cond = 0.0;
+    int it;
+    const int prt = S->it.linear_print_level;
+    const DCsr<double> A = bsr_scalar_A(S);
+    switch (S->it.linear_itsolver_type) {
+    case SOLVER_CG:   // dbsr_pcg_w_cond_est
+        it = pcg(S, A, d_b, d_x, PC_BSR, nullptr, S->it.linear_tol, S->it.linear_maxit,
+                 S->it.linear_stop_type, prt, S->kw, &rel, &cond);
+        break;
+    case SOLVER_VGMRES:
+    case SOLVER_VFGMRES:   // dbsr_pvgmres / dbsr_pvfgmres
+        it = gmres(S, A, d_b, d_x, PC_BSR, nullptr, S->it.linear_tol, S->it.linear_maxit,
+                   S->it.linear_restart, S->it.linear_stop_type, prt,
+                   S->it.linear_itsolver_type == SOLVER_VFGMRES, &rel);
+        break;
+    default:
+        set_error_msg("Krylov types 1 (CG), 3 (GMRES) and 4 (flexible GMRES) are the ones "
+                      "solver_dbsr_linear_itsolver dispatches");
+        return ERROR_SOLVER_TYPE;
+    }
+    HZB_CUDA(cudaEventRecord(S->e1, S->s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S->e0, S->e1);
+    S->st.solve_seconds = ms * 1e-3;
+    S->st.iterations = it;
+    S->st.final_relres = rel;
+    S->st.condest = cond;
+    S->st.launches = (INT)(hzb::launch_count() - l0);
+    return it;
+}
+
+// host vectors through device copies; op 0 solves, 1 applies the
+// preconditioner
+static INT bsr_host_call(hzb_solver *S, const REAL *in, REAL *out, int op) {
+    if (!S || !S->bsr) return ERROR_INPUT_PAR;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    const int n = bsr_scalar_A(S).n;
+    double *di = nullptr, *dout = nullptr;
+    HZB_TRY(dalloc(&di, n));
+    int rc = dalloc(&dout, n);
+    if (rc) { dfree(di); return rc; }
+    cudaMemcpyAsync(di, in, sizeof(double) * n, cudaMemcpyHostToDevice, S->s);
+    if (op == 0) cudaMemcpyAsync(dout, out, sizeof(double) * n, cudaMemcpyHostToDevice, S->s);
+    const int it = op == 0 ? hzb_bsr_solve_device(S, di, dout)
+                           : hzb_bsr_precond_device(S, di, dout);
+    cudaError_t e = cudaMemcpyAsync(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, S->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->s);
+    dfree(di);
+    dfree(dout);
+    if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+    return it;
+}
+
+extern "C" INT hzb_bsr_solve_host(hzb_solver *S, const REAL *b, REAL *x) {
+    return bsr_host_call(S, b, x, 0);
+}
+
+extern "C" INT hzb_bsr_precond_host(hzb_solver *S, const REAL *r, REAL *z) {
+    return bsr_host_call(S, r, z, 1);
+}
+
+extern "C" INT linear_solver_dbsr_krylov_amg(dBSRmat *A, dvector *b, dvector *x,
+                                             linear_itsolver_param *itparam,
+                                             AMG_param *amgparam) {
+    if (!A || !b || !x || !itparam || !amgparam) return ERROR_INPUT_PAR;
+    HZB_TRY(check_bsr_host(A));
+    if (b->row != A->ROW * A->nb || x->row != A->ROW * A->nb) return ERROR_MAT_SIZE;
+    const SHORT prtlvl = itparam->linear_print_level;
+    hzb_solver *S = nullptr;
+    INT rc = hzb_create(&S, amgparam, itparam, NULL);
+    if (rc) return rc;
+    rc = hzb_bsr_setup_host(S, A);
+    if (rc) { hzb_destroy(S); return rc; }
+    if (prtlvl >= PRINT_MIN) printf("BSR AMG setup costs %.4f seconds.\n", S->st.setup_seconds);
+    // solver_dbsr_linear_itsolver (itsolver.c:232-305)
+    if (itparam->linear_tol < SMALLREAL)
+        printf("### HAZMATH WARNING: Convergence tolerance for iterative solver is too small!\n");
+    if (itparam->linear_maxit <= 0)
+        printf("### HAZMATH WARNING: Max number of iterations should be a POSITIVE integer!\n");
+    const SHORT type = itparam->linear_itsolver_type;
+    if (type != SOLVER_CG && type != SOLVER_VGMRES && type != SOLVER_VFGMRES) {
+        printf("### ERROR: Unknown itertive solver type %lld!\n", (long long)type);
+        hzb_destroy(S);
+        return ERROR_SOLVER_TYPE;
+    }
+    krylov_banner(prtlvl, type);
+    const INT it = hzb_bsr_solve_host(S, b->val, x->val);
+    if (type == SOLVER_CG) printf("Estimated condition number = %13.6e\n", S->st.condest);
+    if (prtlvl >= PRINT_MIN)
+        printf("BSR Krylov method costs %.4f seconds.\n",
+               S->st.setup_seconds + S->st.solve_seconds);
+    hzb_destroy(S);
+    return it;
+}
+
 extern "C" INT linear_solver_amg(dCSRmat *A, dvector *b, dvector *x, AMG_param *param) {
     // itsolver.c:524-630 + amg_solve (amg_solve.c:109-160)
     if (!A || !b || !x || !param) return ERROR_INPUT_PAR;

@@ -1,0 +1,652 @@
+// hzb_bsr.cu -- UA-AMG for block (BSR) matrices: amg_setup_ua_bsr
+// (amg_setup_ua.c:145 -> amg_setup_unsmoothP_unsmoothR_bsr, :2183-2425),
+// mgcycle_bsr (mgcycle.c:952-1160) and precond_dbsr_amg (precond.c:1311-1335),
+// behind linear_solver_dbsr_krylov_amg (itsolver.c:2104-2190).
+//
+// Setup, per level while the level has more than max(coarse_dof, 50) block
+// rows: the inverses of the diagonal blocks (dbsr_getdiaginv, sparse.c:6122,
+// Gauss-Jordan as ddense_inv_inplace, dense.c:1266); the condensed scalar
+// matrix (condenseBSRLinf, sparse.c:6223: each block's max row sum of |a|,
+// negated off the diagonal, entries <= 1e-8 dropped) aggregated by heavy
+// edge matching; the boolean P (identity blocks, form_boolean_p_bsr); and
+// A_c = R A P by dbsr_rap (sparse.c:5840-5980): with identity blocks every
+// coarse block is the sum of A's blocks in the traversal order (R row, A
+// row), the diagonal block first (from zero), new blocks copied.  The
+// threshold does not adapt on this path.
+//
+// Cycle: block Jacobi, or block Gauss-Seidel ascending before and descending
+// after the coarse correction (SGS: both), each block row
+// x_I = D_I^{-1} (b_I - sum_{J != I} A_IJ x_J) in the reference's element
+// order, Gauss-Seidel on level schedules of the block pattern; both
+// smoothings take presmooth_iter sweeps (mgcycle_bsr uses that count after
+// the coarse correction too).  Residuals, transfers and the Krylov method
+// run on the level's scalar expansion (row I nb + r lists block columns in
+// block order, components in order); the boolean transfers are the scalar
+// aggregate maps agg_s[I nb + r] = agg[I] nb + r.  precond_dbsr_amg rebuilds
+// its cycle parameters from param_amg_init without the coarse solver, so
+// the coarsest level is always solved by GMRES(25) to 1e-6 (at most
+// min(n^2, 200) steps) from zero, as here.
+#include "hzb_solver.cuh"
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+namespace hzb {
+
+namespace {
+constexpr int BSR_MAXNB = 8;   // largest block size the kernels hold in registers
+
+// inverse of the diagonal block of every block row (the last diagonal block
+// of the row, as dbsr_getdiaginv copies them); *bad > 0 on a near-zero pivot
+__global__ void k_bsr_diaginv(int nrow, int nb, const int *__restrict__ ia,
+                              const int *__restrict__ ja, const double *__restrict__ val,
+                              double *__restrict__ dinv, int *bad) {
+    const int nb2 = nb * nb;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+        double *a = dinv + (size_t)i * nb2;
+        for (int q = 0; q < nb2; ++q) a[q] = 0.0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+            if (ja[k] == i)
+                for (int q = 0; q < nb2; ++q) a[q] = val[(size_t)k * nb2 + q];
+        if (nb == 1) {
+            a[0] = 1.0 / a[0];
+            continue;
+        }
+        for (int k = 0; k < nb; ++k) {
+            const int kn = k * nb, l = kn + k;
+            if (fabs(a[l]) < SMALLREAL) { atomicAdd(bad, 1); break; }
+            const double alinv = 1.0 / a[l];
+            a[l] = alinv;
+            for (int j = 0; j < k; ++j) a[kn + j] *= alinv;
+            for (int j = k + 1; j < nb; ++j) a[kn + j] *= alinv;
+            for (int r = 0; r < k; ++r) {
+                const int rn = r * nb;
+                for (int j = 0; j < nb; ++j)
+                    if (j != k) a[rn + j] -= a[rn + k] * a[kn + j];
+            }
+            for (int r = k + 1; r < nb; ++r) {
+                const int rn = r * nb;
+                for (int j = 0; j < nb; ++j)
+                    if (j != k) a[rn + j] -= a[rn + k] * a[kn + j];
+            }
+            for (int r = 0; r < k; ++r) a[r * nb + k] *= -alinv;
+            for (int r = k + 1; r < nb; ++r) a[r * nb + k] *= -alinv;
+        }
+    }
+}
+
+// condensed value of block k: max over rows of sum |a|, negated off the
+// diagonal
+__device__ __forceinline__ double bsr_linf(const double *b, int nb) {
+    double norm = 0.0;
+    for (int r = 0; r < nb; ++r) {
+        double v = 0.0;
+        for (int c = 0; c < nb; ++c) v = v + fabs(b[r * nb + c]);
+        norm = fmax(norm, v);
+    }
+    return norm;
+}
+
+__global__ void k_bsr_condense_count(int nrow, int nb, const int *__restrict__ ia,
+                                     const int *__restrict__ ja, const double *__restrict__ val,
+                                     int *cnt) {
+    const int nb2 = nb * nb;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+        int c = 0;
+        for (int k = ia[i]; k < ia[i + 1]; ++k) c += bsr_linf(val + (size_t)k * nb2, nb) > 1e-8;
+        cnt[i] = c;
+    }
+}
+
+__global__ void k_bsr_condense_fill(int nrow, int nb, const int *__restrict__ ia,
+                                    const int *__restrict__ ja, const double *__restrict__ val,
+                                    const int *__restrict__ cia, int *cja, double *cval) {
+    const int nb2 = nb * nb;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow; i += gridDim.x * blockDim.x) {
+        int p = cia[i];
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            double v = bsr_linf(val + (size_t)k * nb2, nb);
+            if (ja[k] != i) v = -v;
+            if (fabs(v) > 1e-8) {
+                cja[p] = ja[k];
+                cval[p] = v;
+                ++p;
+            }
+        }
+    }
+}
+
+// scalar expansion: row I nb + r lists the blocks of row I in order, the
+// block's columns in order
+__global__ void k_bsr_expand(int nrow, int nb, const int *__restrict__ ia,
+                             const int *__restrict__ ja, const double *__restrict__ val,
+                             int *sia, int *sja, double *sval) {
+    const int nb2 = nb * nb;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow * nb;
+         i += gridDim.x * blockDim.x) {
+        const int I = i / nb, r = i - I * nb;
+        const int len = (ia[I + 1] - ia[I]) * nb;
+        int p = ia[I] * nb2 + r * len;
+        sia[i] = p;
+        if (i == nrow * nb - 1) sia[i + 1] = ia[nrow] * nb2;
+        for (int k = ia[I]; k < ia[I + 1]; ++k)
+            for (int c = 0; c < nb; ++c, ++p) {
+                sja[p] = ja[k] * nb + c;
+                sval[p] = val[(size_t)k * nb2 + r * nb + c];
+            }
+    }
+}
+
+__global__ void k_bsr_scalar_agg(int nrow, int nb, const int *__restrict__ agg, int *sagg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrow * nb;
+         i += gridDim.x * blockDim.x) {
+        const int I = i / nb, a = agg[I];
+        sagg[i] = a < 0 ? -1 : a * nb + (i - I * nb);
+    }
+}
+
+// block Galerkin product with boolean P: blocks of coarse row C, the
+// diagonal first, others in first-encounter order over (R row, A row)
+__global__ void k_bsr_rap_count(int nc, const int *__restrict__ ria, const int *__restrict__ rja,
+                                const int *__restrict__ ia, const int *__restrict__ ja,
+                                const int *__restrict__ agg, int *cnt, int *list, int cap,
+                                int *err) {
+    for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < nc; C += gridDim.x * blockDim.x) {
+        int *seen = list + (size_t)C * cap;   // caller-sized scratch per coarse row
+        int c = 1;
+        seen[0] = C;
+        for (int j1 = ria[C]; j1 < ria[C + 1]; ++j1) {
+            const int I = rja[j1];
+            for (int k = ia[I]; k < ia[I + 1]; ++k) {
+                const int D = agg[ja[k]];
+                if (D < 0) continue;
+                bool found = false;
+                for (int q = 0; q < c && !found; ++q) found = seen[q] == D;
+                if (!found) {
+                    if (c >= cap) { *err = 1; break; }
+                    seen[c++] = D;
+                }
+            }
+        }
+        cnt[C] = c;
+    }
+}
+
+__global__ void k_bsr_rap_fill(int nc, int nb, const int *__restrict__ ria,
+                               const int *__restrict__ rja, const int *__restrict__ ia,
+                               const int *__restrict__ ja, const double *__restrict__ val,
+                               const int *__restrict__ agg, const int *__restrict__ cia,
+                               int *cja, double *cval) {
+    const int nb2 = nb * nb;
+    for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < nc; C += gridDim.x * blockDim.x) {
+        const int base = cia[C];
+        int c = 1;
+        cja[base] = C;
+        for (int q = 0; q < nb2; ++q) cval[(size_t)base * nb2 + q] = 0.0;
+        for (int j1 = ria[C]; j1 < ria[C + 1]; ++j1) {
+            const int I = rja[j1];
+            for (int k = ia[I]; k < ia[I + 1]; ++k) {
+                const int D = agg[ja[k]];
+                if (D < 0) continue;
+                int slot = -1;
+                for (int q = 0; q < c; ++q)
+                    if (cja[base + q] == D) { slot = q; break; }
+                // R_CI A_IJ P_JD by ddense_mul with identity blocks: sums
+                // from 0.0, so each entry is A's value with -0.0 made +0.0
+                const double *src = val + (size_t)k * nb2;
+                double *dst = cval + (size_t)(base + (slot < 0 ? c : slot)) * nb2;
+                if (slot < 0) {
+                    cja[base + c] = D;
+                    ++c;
+                    for (int q = 0; q < nb2; ++q) dst[q] = src[q] + 0.0;
+                } else {
+                    for (int q = 0; q < nb2; ++q) dst[q] += src[q] + 0.0;
+                }
+            }
+        }
+    }
+}
+
+// w = b - A x on the scalar expansion with the subtractions in row order:
+// dbsr_aAxpy(-1, A, x, w) on w = b negates w, adds the products and negates
+// back, which rounds as the sequential subtraction
+__global__ void k_bsr_residual(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                               const double *__restrict__ val, const double *__restrict__ b,
+                               const double *__restrict__ x, double *__restrict__ w) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double v = b[i];
+        for (int p = ia[i]; p < ia[i + 1]; ++p) v -= val[p] * x[ja[p]];
+        w[i] = v;
+    }
+}
+
+// one block row of Jacobi / Gauss-Seidel: x_I = D_I^{-1} (b_I - sum_{J != I}
+// A_IJ x_J), reading x from xin and writing xout (the same array for GS)
+__device__ __forceinline__ void bsr_relax_row(int I, int nb, const int *__restrict__ ia,
+                                              const int *__restrict__ ja,
+                                              const double *__restrict__ val,
+                                              const double *__restrict__ dinv,
+                                              const double *__restrict__ b, const double *xin,
+                                              double *xout) {
+    const int nb2 = nb * nb;
+    double t[BSR_MAXNB];
+    for (int r = 0; r < nb; ++r) t[r] = b[I * nb + r];
+    for (int k = ia[I]; k < ia[I + 1]; ++k) {
+        const int J = ja[k];
+        if (J == I) continue;
+        const double *a = val + (size_t)k * nb2;
+        for (int r = 0; r < nb; ++r)
+            for (int c = 0; c < nb; ++c) t[r] -= a[r * nb + c] * xin[J * nb + c];
+    }
+    const double *d = dinv + (size_t)I * nb2;
+    for (int r = 0; r < nb; ++r) {
+        double v = 0.0;
+        for (int c = 0; c < nb; ++c) v += d[r * nb + c] * t[c];
+        xout[I * nb + r] = v;
+    }
+}
+
+__global__ void k_bsr_jacobi(int nrow, int nb, const int *__restrict__ ia,
+                             const int *__restrict__ ja, const double *__restrict__ val,
+                             const double *__restrict__ dinv, const double *__restrict__ b,
+                             const double *__restrict__ x, double *__restrict__ xn) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nrow; I += gridDim.x * blockDim.x)
+        bsr_relax_row(I, nb, ia, ja, val, dinv, b, x, xn);
+}
+
+// the rows of one level set, in parallel
+__global__ void k_bsr_gs_set(const int *__restrict__ rows, int cnt, int nb,
+                             const int *__restrict__ ia, const int *__restrict__ ja,
+                             const double *__restrict__ val, const double *__restrict__ dinv,
+                             const double *__restrict__ b, double *x) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x)
+        bsr_relax_row(rows[q], nb, ia, ja, val, dinv, b, x, x);
+}
+
+// a run of small level sets [first, last) by one CTA, sets in order
+__global__ void k_bsr_gs_run(const int *__restrict__ rows, const int *__restrict__ set_ptr,
+                             int first, int last, int nb, const int *__restrict__ ia,
+                             const int *__restrict__ ja, const double *__restrict__ val,
+                             const double *__restrict__ dinv, const double *__restrict__ b,
+                             double *x) {
+    for (int k = first; k < last; ++k) {
+        for (int q = set_ptr[k] + threadIdx.x; q < set_ptr[k + 1]; q += blockDim.x)
+            bsr_relax_row(rows[q], nb, ia, ja, val, dinv, b, x, x);
+        __syncthreads();
+    }
+}
+}  // namespace
+
+struct BsrLevel {
+    int nrow = 0, nnzb = 0, nb = 1, nc = 0;
+    int *ia = nullptr, *ja = nullptr;
+    double *val = nullptr, *dinv = nullptr;
+    int *agg = nullptr;
+    // scalar expansion and scalar aggregate transfer
+    Level s;
+    Schedule asc, desc;
+    void release() {
+        dfree(ia); dfree(ja); dfree(val); dfree(dinv); dfree(agg);
+        s.release();
+        asc.release();
+        desc.release();
+    }
+};
+
+struct BsrHier {
+    std::vector<BsrLevel> lv;
+    int nl = 0, nb = 1;
+    KrylovWork kwc;   // coarse GMRES runs on its own scratch
+    void release() {
+        for (auto &L : lv) L.release();
+        lv.clear();
+        kwc.release();
+        nl = 0;
+    }
+};
+
+void bsr_release(hzb_solver *S) {
+    if (!S->bsr) return;
+    S->bsr->release();
+    delete S->bsr;
+    S->bsr = nullptr;
+}
+
+static int expand(BsrLevel &L, cudaStream_t s) {
+    const int n = L.nrow * L.nb, nnz = L.nnzb * L.nb * L.nb;
+    Level &E = L.s;
+    E.n = n;
+    E.nnz = nnz;
+    E.own_A = true;
+    HZB_TRY(dalloc(&E.ia, n + 1));
+    HZB_TRY(dalloc(&E.ja, nnz));
+    HZB_TRY(dalloc(&E.val, nnz));
+    k_bsr_expand<<<grid_for(n), 256, 0, s>>>(L.nrow, L.nb, L.ia, L.ja, L.val, E.ia, E.ja, E.val);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    HZB_TRY(bundle_capacity(n, E.ia, s, &E.bundle_cap));
+    HZB_TRY(dalloc(&E.b, n));
+    HZB_TRY(dalloc(&E.x, n));
+    HZB_TRY(dalloc(&E.w, n));
+    HZB_TRY(dalloc(&E.t, n));
+    HZB_TRY(dalloc(&E.r1, n));   // A P e of the coarse scaling
+    return SUCCESS;
+}
+
+static int bsr_build(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia,
+                     const int *d_ja, const double *d_val) {
+    if (nb < 1 || nb > BSR_MAXNB) {
+        set_error_msg("block size must be 1 .. 8");
+        return ERROR_INPUT_PAR;
+    }
+    if (nrow < 1 || nnzb < 1) return ERROR_MAT_SIZE;
+    bsr_release(S);
+    cudaStream_t s = S->s;
+    HZB_CUDA(cudaEventRecord(S->e0, s));
+    S->bsr = new BsrHier();
+    BsrHier &H = *S->bsr;
+    H.nb = nb;
+    const int nb2 = nb * nb;
+    H.lv.emplace_back();
+    {
+        BsrLevel &L0 = H.lv[0];
+        L0.nrow = nrow; L0.nnzb = nnzb; L0.nb = nb;
+        HZB_TRY(dalloc(&L0.ia, nrow + 1));
+        HZB_TRY(dalloc(&L0.ja, nnzb));
+        HZB_TRY(dalloc(&L0.val, (size_t)nnzb * nb2));
+        HZB_CUDA(cudaMemcpyAsync(L0.ia, d_ia, sizeof(int) * (nrow + 1), cudaMemcpyDefault, s));
+        HZB_CUDA(cudaMemcpyAsync(L0.ja, d_ja, sizeof(int) * nnzb, cudaMemcpyDefault, s));
+        HZB_CUDA(cudaMemcpyAsync(L0.val, d_val, sizeof(double) * nnzb * nb2, cudaMemcpyDefault,
+                                 s));
+    }
+    const int min_cdof = std::max<int>(S->amg.coarse_dof, 50);
+    const int max_levels = std::min<int>(S->amg.max_levels, MAX_AMG_LVL);
+    const bool par = S->bp.matching == HZB_MATCH_PARALLEL || S->amg.aggregation_type == HEC;
+    int *bad = nullptr, *tmp = nullptr;
+    HZB_TRY(dalloc(&bad, 1));
+    int lvl = 0, rc = SUCCESS;
+    for (;;) {
+        BsrLevel &L = H.lv[lvl];
+        if ((rc = expand(L, s))) break;
+        if (!(L.nrow > min_cdof && lvl < max_levels - 1)) break;
+        // the diagonal inverses of the levels that get a coarser one (the
+        // smoothed levels); a near-zero pivot ends the process in the
+        // reference, an error here
+        if ((rc = dalloc(&L.dinv, (size_t)L.nrow * nb2))) break;
+        HZB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+        k_bsr_diaginv<<<grid_for(L.nrow), 128, 0, s>>>(L.nrow, nb, L.ia, L.ja, L.val, L.dinv,
+                                                        bad);
+        count_launch();
+        int hbad = 0;
+        HZB_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HZB_CUDA(cudaStreamSynchronize(s));
+        if (hbad) {
+            set_error_msg("a diagonal block has a pivot close to zero");
+            rc = ERROR_DATA_ZERODIAG;
+            break;
+        }
+        // condensed scalar matrix, then heavy edge matching on it
+        const int m = L.nrow;
+        int *cnt = nullptr, *pia = nullptr, *pja = nullptr, *nia = nullptr, *nja = nullptr,
+            *work = nullptr, pnnz = 0, nnnz = 0, nagg = 0;
+        double *pval = nullptr, *nval = nullptr;
+        dfree(tmp);
+        if ((rc = dalloc(&tmp, scan_tmp_size(m + 2))) || (rc = dalloc(&cnt, m)) ||
+            (rc = dalloc(&pia, m + 1)))
+            break;
+        k_bsr_condense_count<<<grid_for(m), 256, 0, s>>>(m, nb, L.ia, L.ja, L.val, cnt);
+        count_launch();
+        if ((rc = scan_exclusive(cnt, pia, m, tmp, s))) break;
+        HZB_CUDA(cudaMemcpyAsync(&pnnz, pia + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HZB_CUDA(cudaStreamSynchronize(s));
+        dfree(cnt);
+        if ((rc = dalloc(&pja, pnnz > 0 ? pnnz : 1)) || (rc = dalloc(&pval, pnnz > 0 ? pnnz : 1)))
+            break;
+        k_bsr_condense_fill<<<grid_for(m), 256, 0, s>>>(m, nb, L.ia, L.ja, L.val, pia, pja, pval);
+        count_launch();
+        DCsr<double> PP;
+        PP.n = m; PP.nnz = pnnz; PP.ia = pia; PP.ja = pja; PP.val = pval;
+        if ((rc = bundle_capacity(m, pia, s, &PP.bundle_cap))) break;
+        if ((rc = dalloc(&nia, m + 1)) || (rc = dalloc(&nja, pnnz > 0 ? pnnz : 1)) ||
+            (rc = dalloc(&nval, pnnz > 0 ? pnnz : 1)) || (rc = dalloc(&L.agg, m)) ||
+            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8 : (size_t)m)))
+            break;
+        rc = strength_graph(PP, S->amg.strong_coupled, nia, nja, nval, &nnnz, tmp, s);
+        if (!rc) {
+            if (par) rc = hem_parallel(m, nia, nja, nval, L.agg, &nagg, work, s);
+            else rc = hem_exact(m, nia, nja, nval, L.agg, &nagg, work, s);
+        }
+        dfree(pia); dfree(pja); dfree(pval); dfree(nia); dfree(nja); dfree(nval); dfree(work);
+        if (rc) break;
+        if (nagg < 1) break;
+        L.nc = nagg;
+        // R (block pattern, fine rows ascending) and the scalar aggregate maps
+        int *ria = nullptr, *rja = nullptr;
+        if ((rc = dalloc(&ria, nagg + 1)) || (rc = dalloc(&rja, m))) break;
+        if ((rc = restriction_pattern(m, nagg, L.agg, ria, rja, tmp, s))) break;
+        Level &E = L.s;
+        E.nc = nagg * nb;
+        if ((rc = dalloc(&E.agg, E.n))) break;
+        k_bsr_scalar_agg<<<grid_for(E.n), 256, 0, s>>>(m, nb, L.agg, E.agg);
+        count_launch();
+        int *stmp = nullptr;
+        if ((rc = dalloc(&E.ria, E.nc + 1)) || (rc = dalloc(&E.rja, E.n)) ||
+            (rc = dalloc(&stmp, scan_tmp_size(E.n + 1))))
+            break;
+        rc = restriction_pattern(E.n, E.nc, E.agg, E.ria, E.rja, stmp, s);
+        dfree(stmp);
+        if (rc) break;
+        // coarse blocks: count (row lengths bounded by a table per row), fill
+        int *ccnt = nullptr, *cia = nullptr, *list = nullptr, *err = nullptr, cnnz = 0, herr = 0;
+        int cap = 64;
+        for (;;) {
+            dfree(list);
+            if ((rc = dalloc(&ccnt, nagg)) || (rc = dalloc(&list, (size_t)nagg * cap)) ||
+                (rc = dalloc(&err, 1)))
+                break;
+            HZB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+            k_bsr_rap_count<<<grid_for(nagg), 128, 0, s>>>(nagg, ria, rja, L.ia, L.ja, L.agg,
+                                                            ccnt, list, cap, err);
+            count_launch();
+            HZB_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+            HZB_CUDA(cudaStreamSynchronize(s));
+            dfree(err);
+            if (!herr || cap >= nagg) break;
+            dfree(ccnt);
+            cap = std::min(cap * 4, nagg);
+        }
+        dfree(list);
+        if (rc) break;
+        if ((rc = dalloc(&cia, nagg + 1)) || (rc = scan_exclusive(ccnt, cia, nagg, tmp, s)))
+            break;
+        dfree(ccnt);
+        HZB_CUDA(cudaMemcpyAsync(&cnnz, cia + nagg, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HZB_CUDA(cudaStreamSynchronize(s));
+        H.lv.emplace_back();
+        BsrLevel &C = H.lv.back();
+        BsrLevel &Lf = H.lv[lvl];   // re-bind: emplace_back may move the levels
+        C.nrow = nagg; C.nnzb = cnnz; C.nb = nb; C.ia = cia;
+        if ((rc = dalloc(&C.ja, cnnz)) || (rc = dalloc(&C.val, (size_t)cnnz * nb2))) break;
+        k_bsr_rap_fill<<<grid_for(nagg), 128, 0, s>>>(nagg, nb, ria, rja, Lf.ia, Lf.ja, Lf.val,
+                                                       Lf.agg, cia, C.ja, C.val);
+        count_launch();
+        HZB_LAUNCH_CHECK();
+        dfree(ria);
+        dfree(rja);
+        ++lvl;
+    }
+    dfree(bad);
+    dfree(tmp);
+    if (rc) return rc;
+    H.nl = lvl + 1;
+    // Gauss-Seidel level sets of the block pattern on the smoothed levels
+    if (S->amg.smoother == SMOOTHER_GS || S->amg.smoother == SMOOTHER_SGS)
+        for (int l = 0; l < H.nl - 1; ++l) {
+            BsrLevel &L = H.lv[l];
+            HZB_TRY(gs_schedule(L.nrow, L.ia, L.ja, L.nnzb, 0, &L.asc, s));
+            HZB_TRY(gs_schedule(L.nrow, L.ia, L.ja, L.nnzb, 1, &L.desc, s));
+        }
+    HZB_TRY(H.kwc.alloc(H.lv[0].s.n));
+    HZB_TRY(S->kw.alloc(H.lv[0].s.n));
+    HZB_CUDA(cudaEventRecord(S->e1, s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S->e0, S->e1);
+    S->st.setup_seconds = ms * 1e-3;
+    S->st.num_levels = H.nl;
+    for (int l = 0; l < H.nl && l < MAX_AMG_LVL; ++l) {
+        S->st.rows[l] = H.lv[l].nrow;
+        S->st.nnz[l] = H.lv[l].nnzb;
+    }
+    return SUCCESS;
+}
+
+int bsr_setup(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia, const int *d_ja,
+              const double *d_val) {
+    const int rc = bsr_build(S, nrow, nnzb, nb, d_ia, d_ja, d_val);
+    if (rc != SUCCESS) bsr_release(S);
+    return rc;
+}
+
+DCsr<double> bsr_scalar_A(hzb_solver *S) { return S->bsr->lv[0].s.A64(); }
+
+int bsr_block_size(const hzb_solver *S) { return S->bsr ? S->bsr->nb : 0; }
+
+int bsr_level_copy(const hzb_solver *S, int l, int *nrow, int *nnzb, int *ia, int *ja,
+                   double *val, int *agg) {
+    if (!S->bsr || l < 0 || l >= S->bsr->nl) return ERROR_INPUT_PAR;
+    const BsrLevel &L = S->bsr->lv[l];
+    if (nrow) *nrow = L.nrow;
+    if (nnzb) *nnzb = L.nnzb;
+    const int nb2 = L.nb * L.nb;
+    if (ia) HZB_CUDA(cudaMemcpy(ia, L.ia, sizeof(int) * (L.nrow + 1), cudaMemcpyDeviceToHost));
+    if (ja) HZB_CUDA(cudaMemcpy(ja, L.ja, sizeof(int) * L.nnzb, cudaMemcpyDeviceToHost));
+    if (val)
+        HZB_CUDA(cudaMemcpy(val, L.val, sizeof(double) * (size_t)L.nnzb * nb2,
+                            cudaMemcpyDeviceToHost));
+    if (agg && l < S->bsr->nl - 1)
+        HZB_CUDA(cudaMemcpy(agg, L.agg, sizeof(int) * L.nrow, cudaMemcpyDeviceToHost));
+    return SUCCESS;
+}
+
+static int bsr_smooth(hzb_solver *S, BsrLevel &L, int kind, int sweeps) {
+    cudaStream_t s = S->s;
+    Level &E = L.s;
+    for (int it = 0; it < sweeps; ++it) {
+        if (kind == 0) {   // Jacobi: a new iterate from the old one
+            k_bsr_jacobi<<<grid_for(L.nrow), 128, 0, s>>>(L.nrow, L.nb, L.ia, L.ja, L.val, L.dinv,
+                                                          E.b, E.x, E.t);
+            count_launch();
+            HZB_TRY(vcopy<double>(E.n, E.t, E.x, s));
+            continue;
+        }
+        const Schedule &sc = kind == 1 ? L.asc : L.desc;
+        for (size_t q = 0; q < sc.run_first.size(); ++q) {
+            const int f = sc.run_first[q], l = sc.run_last[q];
+            if (l < 0) {
+                const int cnt = sc.h_ptr[f + 1] - sc.h_ptr[f];
+                k_bsr_gs_set<<<grid_for(cnt), 128, 0, s>>>(sc.rows + sc.h_ptr[f], cnt, L.nb, L.ia,
+                                                           L.ja, L.val, L.dinv, E.b, E.x);
+            } else {
+                k_bsr_gs_run<<<1, 256, 0, s>>>(sc.rows, sc.set_ptr, f, l, L.nb, L.ia, L.ja, L.val,
+                                               L.dinv, E.b, E.x);
+            }
+            count_launch();
+        }
+    }
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+// the smoothing of mgcycle_bsr: Jacobi, GS (ascending before, descending
+// after), SGS (both)
+static int bsr_smoothing(hzb_solver *S, BsrLevel &L, const AMG_param &cyc, bool pre) {
+    const int steps = cyc.presmooth_iter;
+    if (steps <= 0) return SUCCESS;
+    switch (cyc.smoother) {
+    case SMOOTHER_JACOBI: return bsr_smooth(S, L, 0, steps);
+    case SMOOTHER_GS: return bsr_smooth(S, L, pre ? 1 : 2, steps);
+    case SMOOTHER_SGS:
+        for (int i = 0; i < steps; ++i) {
+            HZB_TRY(bsr_smooth(S, L, 1, 1));
+            HZB_TRY(bsr_smooth(S, L, 2, 1));
+        }
+        return SUCCESS;
+    }
+    set_error_msg("block smoothers: Jacobi, GS, SGS");
+    return ERROR_AMG_SMOOTH_TYPE;
+}
+
+int bsr_cycle(hzb_solver *S, const AMG_param &cyc) {
+    BsrHier &H = *S->bsr;
+    cudaStream_t s = S->s;
+    const int nl = H.nl;
+    int nu[MAX_AMG_LVL] = {0};
+    int l = 0;
+forward:
+    while (l < nl - 1) {
+        BsrLevel &L = H.lv[l];
+        Level &E = L.s;
+        nu[l]++;
+        HZB_TRY(bsr_smoothing(S, L, cyc, true));
+        k_bsr_residual<<<grid_for(E.n), 256, 0, s>>>(E.n, E.ia, E.ja, E.val, E.b, E.x, E.w);
+        count_launch();
+        Level &Cn = H.lv[l + 1].s;
+        HZB_TRY(restrict_agg<double>(E.nc, E.ria, E.rja, E.w, Cn.b, s));
+        ++l;
+        HZB_TRY(vzero<double>(Cn.n, Cn.x, s));
+    }
+    {
+        // GMRES(25) to the tolerance of param_amg_init, at most min(n^2, 200)
+        Level &Cn = H.lv[nl - 1].s;
+        const int csize = Cn.n;
+        const int cmaxit = (int)std::min<long long>((long long)csize * csize, 200);
+        double rel = 0.0;
+        const int it = gmres(S, Cn.A64(), Cn.b, Cn.x, PC_NONE, nullptr, cyc.tol, cmaxit, 25,
+                             STOP_REL_RES, 0, false, &rel, MAX_AMG_LVL + 1);
+        if (it == ERROR_SOLVER_MISC || it == ERROR_ALLOC_MEM) return it;
+    }
+    while (l > 0) {
+        --l;
+        BsrLevel &L = H.lv[l];
+        Level &E = L.s, &Cn = H.lv[l + 1].s;
+        if (cyc.coarse_scaling == ON) {
+            // PeH = P e, Aeh = A PeH, alpha = min((Aeh, w) / (Aeh, Aeh), 1),
+            // x += alpha PeH (mgcycle.c:1075-1090)
+            KrylovWork &w = H.kwc;
+            HZB_TRY(vzero<double>(E.n, E.t, s));
+            HZB_TRY(prolong_agg<double>(E.n, E.agg, Cn.x, E.t, 1.0, s));
+            HZB_TRY(spmv<double>(E.A64(), SPMV_Y, E.t, nullptr, E.r1, 1.0, nullptr, s));
+            HZB_TRY(dot(E.n, E.r1, E.w, w.part, w.sc + 8, s));
+            HZB_TRY(dot(E.n, E.r1, E.r1, w.part, w.sc + 9, s));
+            HZB_CUDA(cudaMemcpyAsync(w.h_sc + 8, w.sc + 8, 2 * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s));
+            HZB_CUDA(cudaStreamSynchronize(s));
+            const double alpha = std::min(w.h_sc[8] / w.h_sc[9], 1.0);
+            HZB_TRY(prolong_agg<double>(E.n, E.agg, Cn.x, E.x, alpha, s));
+        } else {
+            HZB_TRY(prolong_agg<double>(E.n, E.agg, Cn.x, E.x, 1.0, s));
+        }
+        HZB_TRY(bsr_smoothing(S, L, cyc, false));
+        if (nu[l] < cyc.cycle_type) break;
+        nu[l] = 0;
+    }
+    if (l > 0) goto forward;
+    return SUCCESS;
+}
+
+// precond_dbsr_amg (precond.c:1311-1335): maxit cycles from zero
+int bsr_precond(hzb_solver *S, const double *r, double *z) {
+    BsrHier &H = *S->bsr;
+    Level &E = H.lv[0].s;
+    double *sx = E.x;
+    HZB_TRY(vcopy<double>(E.n, r, E.b, S->s));   // the residual is an input
+    E.x = z;
+    int rc = vzero<double>(E.n, z, S->s);
+    for (int i = 0; rc == SUCCESS && i < S->bsr_cyc.maxit; ++i) rc = bsr_cycle(S, S->bsr_cyc);
+    E.x = sx;
+    return rc;
+}
+
+}  // namespace hzb

@@ -721,6 +721,7 @@ static int apply_pc(hzb_solver *S, int kind, HostPrecond *hp, int n,
                     const double *r, double *z) {
     if (kind == PC_AMG) return precond64(S, r, z, S->pc_cyc);
     if (kind == PC_AMLI || kind == PC_ADD) return precond_alt(S, kind, r, z);
+    if (kind == PC_BSR) return bsr_precond(S, r, z);
     if (kind >= PC_NLAMLI) {
         // the solve's preconditioner runs maxit cycles; the coarse-level
         // Krylov solves of the cycle itself run one (mgcycle.c:623)
@@ -1088,6 +1089,7 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
 
 void destroy(hzb_solver *S) {
     batch_release(S);
+    bsr_release(S);
     S->g64.release();
     S->g32.release();
     S->gcyc.release();

@@ -107,6 +107,7 @@ struct GmresWork;   // Krylov basis of gmres (hzb_gmres.cu)
 struct GcgWork;     // search directions of gcg (hzb_cycles.cu)
 
 struct Batch;   // packed independent systems (hzb_batch.cu)
+struct BsrHier; // hierarchy of a block (BSR) matrix (hzb_bsr.cu)
 
 // Host-side preconditioner callback used when a foreign pc->fct is given.
 struct HostPrecond {
@@ -145,6 +146,8 @@ struct hzb_solver {
     const double *host_val = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     hzb::Batch *batch = nullptr;      // set by batch_setup
+    hzb::BsrHier *bsr = nullptr;      // set by bsr_setup
+    AMG_param bsr_cyc;                // cycle parameters of precond_dbsr_amg
 };
 
 namespace hzb {
@@ -162,7 +165,8 @@ int pcg(hzb_solver *S, const DCsr<double> &A, const double *b, double *u,
 // preconditioner kinds of pcg / gmres / gcg: none, precond_amg (V/W
 // cycles), a host callback, precond_amli, precond_amg_add, and
 // precond_nl_amli rooted at level l (PC_NLAMLI + l)
-enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2, PC_AMLI = 3, PC_ADD = 4, PC_NLAMLI = 16 };
+enum { PC_NONE = 0, PC_AMG = 1, PC_HOST = 2, PC_AMLI = 3, PC_ADD = 4, PC_BSR = 5,
+       PC_NLAMLI = 16 };
 // the preconditioner linear_solver_dcsr_krylov_amg picks for a cycle type
 // (itsolver.c:899-917)
 int pc_kind_of_cycle(int cycle_type);
@@ -239,4 +243,18 @@ int batch_setup(hzb_solver *S, int nsys, const int *off, int n, int nnz, const i
 int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit,
                 int *h_iters, double *h_relres, double *h_seconds);
 void batch_release(hzb_solver *S);
+// UA-AMG of a block matrix (hzb_bsr.cu): amg_setup_ua_bsr on nrow block rows
+// of nb x nb blocks (row-major); z = B r of precond_dbsr_amg with the cycle
+// parameters S->bsr_cyc; the scalar expansion of the level-0 matrix (the
+// operator of the Krylov loop); a level's block matrix (sizes always, the
+// arrays where given) and its block aggregates
+int bsr_setup(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia, const int *d_ja,
+              const double *d_val);
+int bsr_precond(hzb_solver *S, const double *r, double *z);
+int bsr_cycle(hzb_solver *S, const AMG_param &cyc);
+DCsr<double> bsr_scalar_A(hzb_solver *S);
+int bsr_block_size(const hzb_solver *S);
+int bsr_level_copy(const hzb_solver *S, int l, int *nrow, int *nnzb, int *ia, int *ja,
+                   double *val, int *agg);
+void bsr_release(hzb_solver *S);
 }  // namespace hzb

@@ -255,3 +255,50 @@ def batch_anisotropic(nsys: int = 512, seed: int = 11, dof_lo: int = 1000,
         ub[r0:r1] = b
     uia[n] = nnz
     return systems, (off.astype(np.int32), uia.astype(np.int32), uja, uval, ub)
+
+
+BLOCK_COUPLING = {
+    2: np.array([[2.0, 0.5], [0.5, 1.0]]),
+    3: np.array([[3.0, 0.5, 0.2], [0.5, 2.0, 0.3], [0.2, 0.3, 1.0]]),
+}
+
+
+def block_system(ia, ja, val, nb: int, seed: int, shift: float = 0.1):
+    """Block (BSR) SPD system with the pattern of a scalar SPD CSR matrix K:
+    block (I, J) = K_IJ B for the fixed SPD coupling B = BLOCK_COUPLING[nb],
+    plus on every diagonal block a seeded SPD term shift G G^T / nb (G with
+    standard normal entries), so that the diagonal blocks differ row by row.
+    Returns (ia, ja, val) with val holding the nnz blocks row-major
+    (nnz * nb^2 values)."""
+    B = BLOCK_COUPLING[nb]
+    ia = np.asarray(ia, np.int32)
+    ja = np.asarray(ja, np.int32)
+    n = len(ia) - 1
+    blocks = np.asarray(val, np.float64)[:, None, None] * B[None, :, :]
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, nb, nb))
+    M = shift * np.einsum("nij,nkj->nik", G, G) / nb
+    rows = np.repeat(np.arange(n), np.diff(ia))
+    diag = np.nonzero(ja == rows)[0]
+    blocks[diag] += M[rows[diag]]
+    return ia.copy(), ja.copy(), np.ascontiguousarray(blocks.reshape(-1))
+
+
+def bsr_to_csr(ia, ja, val, nb: int):
+    """Scalar CSR of a block matrix: row I nb + r lists the blocks of row I
+    in order, each block's columns in order."""
+    ia = np.asarray(ia, np.int64)
+    ja = np.asarray(ja, np.int64)
+    n = len(ia) - 1
+    blocks = np.asarray(val).reshape(-1, nb, nb)
+    sia = [0]
+    sja, sval = [], []
+    for I in range(n):
+        k0, k1 = ia[I], ia[I + 1]
+        for r in range(nb):
+            cols = (ja[k0:k1, None] * nb + np.arange(nb)[None, :]).reshape(-1)
+            sja.append(cols)
+            sval.append(blocks[k0:k1, r, :].reshape(-1))
+            sia.append(sia[-1] + len(cols))
+    return (np.asarray(sia, np.int32), np.concatenate(sja).astype(np.int32),
+            np.concatenate(sval))

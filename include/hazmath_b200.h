@@ -131,6 +131,20 @@ typedef struct dCSRmat {
     REAL *val;  /* values, nnz */
 } dCSRmat;
 
+/* include/sparse.h:185-213: block sparse row matrix; ROW x COL blocks of
+ * nb x nb values, block k at val[k nb^2 ..], row-major inside the block
+ * (storage_manner 0, the only manner this library takes) */
+typedef struct dBSRmat {
+    INT ROW;            /* block rows */
+    INT COL;            /* block columns */
+    INT NNZ;            /* stored blocks */
+    INT nb;             /* block size */
+    INT storage_manner; /* 0: row-wise inside each block */
+    REAL *val;          /* NNZ nb^2 values */
+    INT *IA;            /* block row pointers, ROW+1 */
+    INT *JA;            /* block column indices, NNZ */
+} dBSRmat;
+
 /* include/vec.h:20-28 */
 typedef struct dvector {
     INT row;
@@ -288,6 +302,21 @@ INT linear_solver_dcsr_krylov_amg(dCSRmat *A, dvector *b, dvector *x,
 /* src/solver/itsolver.c:524-630: AMG as a stand-alone iterative solver
  * (amg_solve, src/solver/amg_solve.c:109). */
 INT linear_solver_amg(dCSRmat *A, dvector *b, dvector *x, AMG_param *param);
+
+/* src/solver/itsolver.c:2104-2200: UA-AMG preconditioned Krylov method for
+ * a block (BSR) matrix.  Setup as amg_setup_ua_bsr (amg_setup_ua.c:145):
+ * diagonal-block inverses, the L-infinity condensed matrix aggregated by
+ * heavy edge matching (threshold fixed), boolean block P, A_c = R A P by
+ * dbsr_rap; levels while more than max(coarse_dof, 50) block rows.
+ * Preconditioner precond_dbsr_amg (precond.c:1311): maxit cycles of
+ * mgcycle_bsr (block Jacobi / Gauss-Seidel / symmetric Gauss-Seidel,
+ * presmooth_iter sweeps on both sides, coarsest level by GMRES(25) to
+ * 1e-6).  Krylov types 1 (CG, prints the condition estimate), 3 (GMRES) and
+ * 4 (flexible GMRES); any other type returns ERROR_SOLVER_TYPE.  Block
+ * sizes 1 to 8.  x: initial guess in, solution out. */
+INT linear_solver_dbsr_krylov_amg(dBSRmat *A, dvector *b, dvector *x,
+                                  linear_itsolver_param *itparam,
+                                  AMG_param *amgparam);
 
 /* src/solver/itsolver.c:135-229: Krylov switch on a host preconditioner:
  * type 1 CG (prints the condition estimate), 2 MINRES (prints the
@@ -495,6 +524,19 @@ INT  hzb_level_prolongation(const hzb_solver *s, INT l, INT *ia, INT *ja, REAL *
                             INT *nnz);
 INT  hzb_level_copy(const hzb_solver *s, INT l, INT *ia, INT *ja, REAL *val,
                     INT *agg);
+/* Block (BSR) hierarchy on the handle (the pieces of
+ * linear_solver_dbsr_krylov_amg): amg_setup_ua_bsr of a host matrix with the
+ * handle's AMG_param; level l's block matrix (ROW, NNZ and nb always; the
+ * arrays copied where out->IA / JA / val are given) and its block aggregates
+ * (agg, ROW entries, levels below the coarsest); precond_dbsr_amg on device
+ * or host vectors; the handle's Krylov type (1, 3, 4) preconditioned by it,
+ * x holding the initial guess. */
+INT  hzb_bsr_setup_host(hzb_solver *s, const dBSRmat *A);
+INT  hzb_bsr_level(const hzb_solver *s, INT l, dBSRmat *out, INT *agg);
+INT  hzb_bsr_precond_device(hzb_solver *s, const REAL *d_r, REAL *d_z);
+INT  hzb_bsr_precond_host(hzb_solver *s, const REAL *r, REAL *z);
+INT  hzb_bsr_solve_device(hzb_solver *s, const REAL *d_b, REAL *d_x);
+INT  hzb_bsr_solve_host(hzb_solver *s, const REAL *b, REAL *x);
 void hzb_destroy(hzb_solver *s);
 /* last CUDA error message of this thread ("" if none) */
 const char *hzb_last_error(void);

@@ -333,6 +333,61 @@ class Ref(_Backend):
     def free(self):
         self.lib.ref_free()
 
+    # -- block (BSR) matrices: amg_setup_ua_bsr, precond_dbsr_amg ----------
+    def bsr_setup(self, nb, ia, ja, val, params: AMGParams | None = None) -> int:
+        params = params or AMGParams()
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        self._keep_bsr = (ia, ja, val)
+        ip, dp = params.arrays()
+        return self.lib.ref_bsr_setup(len(ia) - 1, int(ia[-1]), nb, _p(ia), _p(ja), _p(val),
+                                      ip, dp)
+
+    def bsr_num_levels(self) -> int:
+        return self.lib.ref_bsr_num_levels()
+
+    def bsr_level_A(self, l: int, nb: int):
+        out = (ctypes.c_int * 2)()
+        self.lib.ref_bsr_level_info(l, out)
+        n, nnzb = out[0], out[1]
+        ia = np.empty(n + 1, np.int32)
+        ja = np.empty(nnzb, np.int32)
+        val = np.empty(nnzb * nb * nb)
+        self.lib.ref_bsr_level_A(l, _p(ia), _p(ja), _p(val))
+        return ia, ja, val
+
+    def bsr_level_agg(self, l: int):
+        out = (ctypes.c_int * 2)()
+        self.lib.ref_bsr_level_info(l, out)
+        agg = np.empty(out[0], np.int32)
+        self.lib.ref_bsr_level_agg(l, _p(agg))
+        return agg
+
+    def bsr_precond(self, r):
+        r = np.ascontiguousarray(r, np.float64).copy()
+        z = np.zeros_like(r)
+        self.lib.ref_bsr_precond(_p(r), _p(z))
+        return z
+
+    def bsr_free(self):
+        self.lib.ref_bsr_free()
+
+    def bsr_krylov_amg(self, nb, ia, ja, val, b, type_, tol=1e-8, maxit=500, stop_type=1,
+                       restart=25, params: AMGParams | None = None):
+        """linear_solver_dbsr_krylov_amg from x = 0: (iterations, x)."""
+        params = params or AMGParams()
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        b = np.ascontiguousarray(b, np.float64).copy()
+        x = np.zeros_like(b)
+        ip, dp = params.arrays()
+        it = self.lib.ref_bsr_krylov_amg(len(ia) - 1, int(ia[-1]), nb, _p(ia), _p(ja), _p(val),
+                                         _p(b), _p(x), type_, ctypes.c_double(tol), maxit,
+                                         stop_type, restart, ip, dp)
+        return it, x
+
     def mxv(self, ia, ja, val, x):
         n = len(ia) - 1
         y = np.empty(n)

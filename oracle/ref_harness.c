@@ -359,3 +359,123 @@ int ref_rap_agg(int n, int nnz, int *ia, int *ja, double *val, int nc,
     memcpy(rap_val, g_rap.val, sizeof(double) * g_rap.nnz);
     return g_rap.nnz;
 }
+
+/* ---- UA-AMG for BSR matrices: amg_setup_ua_bsr (amg_setup_ua.c:145),
+ * precond_dbsr_amg (precond.c:1311) and linear_solver_dbsr_krylov_amg
+ * (itsolver.c:2104), on one global hierarchy.  ip/dp as fill_param.       */
+static AMG_data_bsr *g_bmgl = NULL;
+static AMG_param g_bamg;
+static dBSRmat g_bA;
+static precond_data_bsr g_bpd;
+
+static dBSRmat wrap_bsr(int nrow, int nnzb, int nb, int *ia, int *ja, double *val)
+{
+    dBSRmat A;
+    A.ROW = nrow; A.COL = nrow; A.NNZ = nnzb; A.nb = nb; A.storage_manner = 0;
+    A.IA = ia; A.JA = ja; A.val = val;
+    return A;
+}
+
+void ref_bsr_free(void)
+{
+    if (g_bmgl) {
+        amg_data_bsr_free(g_bmgl);
+        g_bmgl = NULL;
+    }
+}
+
+int ref_bsr_setup(int nrow, int nnzb, int nb, int *ia, int *ja, double *val,
+                  const int *iparam, const double *dparam)
+{
+    ref_bsr_free();
+    fill_param(&g_bamg, iparam, dparam);
+    g_bA = wrap_bsr(nrow, nnzb, nb, ia, ja, val);
+    g_bmgl = amg_data_bsr_create(g_bamg.max_levels);
+    g_bmgl[0].A = dbsr_create(nrow, nrow, nnzb, nb, 0);
+    g_bmgl[0].b = dvec_create(nrow * nb);
+    g_bmgl[0].x = dvec_create(nrow * nb);
+    dbsr_cp(&g_bA, &g_bmgl[0].A);
+    double t0 = now_s();
+    SHORT status = amg_setup_ua_bsr(g_bmgl, &g_bamg);
+    g_setup_s = now_s() - t0;
+    /* the preconditioner data of linear_solver_dbsr_krylov_amg */
+    memset(&g_bpd, 0, sizeof(g_bpd));
+    g_bpd.print_level = g_bamg.print_level;
+    g_bpd.maxit = g_bamg.maxit;
+    g_bpd.tol = g_bamg.tol;
+    g_bpd.cycle_type = g_bamg.cycle_type;
+    g_bpd.smoother = g_bamg.smoother;
+    g_bpd.presmooth_iter = g_bamg.presmooth_iter;
+    g_bpd.postsmooth_iter = g_bamg.postsmooth_iter;
+    g_bpd.relaxation = g_bamg.relaxation;
+    g_bpd.coarse_solver = g_bamg.coarse_solver;
+    g_bpd.coarse_scaling = g_bamg.coarse_scaling;
+    g_bpd.amli_degree = g_bamg.amli_degree;
+    g_bpd.amli_coef = g_bamg.amli_coef;
+    g_bpd.tentative_smooth = g_bamg.tentative_smooth;
+    g_bpd.max_levels = g_bmgl[0].num_levels;
+    g_bpd.mgl_data = g_bmgl;
+    g_bpd.A = &g_bA;
+    return status;
+}
+
+int ref_bsr_num_levels(void) { return g_bmgl ? g_bmgl[0].num_levels : 0; }
+
+/* out: ROW, NNZ of level l */
+void ref_bsr_level_info(int l, int *out)
+{
+    out[0] = g_bmgl[l].A.ROW;
+    out[1] = g_bmgl[l].A.NNZ;
+}
+
+void ref_bsr_level_A(int l, int *ia, int *ja, double *val)
+{
+    const dBSRmat *A = &g_bmgl[l].A;
+    memcpy(ia, A->IA, sizeof(int) * (A->ROW + 1));
+    memcpy(ja, A->JA, sizeof(int) * A->NNZ);
+    memcpy(val, A->val, sizeof(double) * A->NNZ * A->nb * A->nb);
+}
+
+/* block aggregate of every row of level l (the column of its P block, -1
+ * for an empty row) */
+void ref_bsr_level_agg(int l, int *agg)
+{
+    const dBSRmat *P = &g_bmgl[l].P;
+    for (int i = 0; i < P->ROW; ++i)
+        agg[i] = P->IA[i + 1] > P->IA[i] ? P->JA[P->IA[i]] : -1;
+}
+
+void ref_bsr_precond(double *r, double *z) { precond_dbsr_amg(r, z, &g_bpd); }
+
+/* linear_solver_dbsr_krylov_amg (itsolver.c:2104) on its own hierarchy:
+ * amg_setup_ua_bsr, precond_dbsr_amg, then the Krylov method of
+ * solver_dbsr_linear_itsolver (type 1, 3 or 4).  Type 1 calls dbsr_pcg:
+ * dbsr_pcg_w_cond_est takes the same iterates and adds a LAPACK condition
+ * estimate, and this build has no LAPACK.                                   */
+int ref_bsr_krylov_amg(int nrow, int nnzb, int nb, int *ia, int *ja, double *val,
+                       double *b, double *x, int type, double tol, int maxit,
+                       int stop_type, int restart, const int *iparam,
+                       const double *dparam)
+{
+    int st = ref_bsr_setup(nrow, nnzb, nb, ia, ja, val, iparam, dparam);
+    if (st < 0) return st;
+    precond pc;
+    pc.data = &g_bpd;
+    pc.fct = precond_dbsr_amg;
+    dvector bv, xv;
+    bv.row = nrow * nb; bv.val = b;
+    xv.row = nrow * nb; xv.val = x;
+    double t0 = now_s();
+    int it_n;
+    switch (type) {
+    case 1: it_n = dbsr_pcg(&g_bA, &bv, &xv, &pc, tol, maxit, (SHORT)stop_type, 0); break;
+    case 3: it_n = dbsr_pvgmres(&g_bA, &bv, &xv, &pc, tol, maxit, (SHORT)restart,
+                                (SHORT)stop_type, 0); break;
+    case 4: it_n = dbsr_pvfgmres(&g_bA, &bv, &xv, &pc, tol, maxit, (SHORT)restart,
+                                 (SHORT)stop_type, 0); break;
+    default: it_n = ERROR_SOLVER_TYPE; break;
+    }
+    g_solve_s = now_s() - t0;
+    ref_bsr_free();
+    return it_n;
+}

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|layout]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -82,6 +82,7 @@ O(AMG_data,b)O(AMG_data,x)O(AMG_data,Numeric)O(AMG_data,near_kernel_dim)
 O(AMG_data,Schwarz)O(AMG_data,w)O(AMG_data,cycle_type)O(AMG_data,wdata)
 O(precond_data,tol)O(precond_data,amli_coef)O(precond_data,mgl_data)
 O(precond_data,fpwr)O(precond_data,A)O(precond_data,w)
+S(dBSRmat)O(dBSRmat,nb)O(dBSRmat,val)O(dBSRmat,IA)O(dBSRmat,JA)
 printf("\"end\": 0\n");return 0;}
 """
     with tempfile.TemporaryDirectory() as d:
@@ -304,6 +305,66 @@ def sa_cases(R):
     np.savez_compressed(os.path.join(HERE, "sa.npz"), **out)
 
 
+BSR_VARIANTS = {
+    "kuhn/gs": ("kuhn", {}),
+    "kuhn/jac": ("kuhn", dict(smoother=1, presmooth_iter=2, postsmooth_iter=2)),
+    "kuhn/sgs": ("kuhn", dict(smoother=3)),
+    "kuhn/w": ("kuhn", dict(cycle_type=2)),
+    "kuhn/cs": ("kuhn", dict(coarse_scaling=1)),
+    "kuhn/m2": ("kuhn", dict(maxit=2)),
+    "kuhn/t": ("kuhn", dict(strong_coupled=0.08)),
+    "fix/gs": ("fix", {}),
+}
+BSR_NB = {"kuhn": 3, "fix": 2}
+BSR_SEED = {"kuhn": 31, "fix": 32}
+
+
+def bsr_cases(R):
+    """UA-AMG for block matrices (amg_setup_ua_bsr, precond_dbsr_amg,
+    linear_solver_dbsr_krylov_amg) on problems.block_system of the matrices
+    of gmres.npz (nb = 3 on the Kuhn case, 2 on the 5-point case): the
+    level sizes, block aggregates, SHA-256 digests of every level's block
+    matrix, one preconditioner application on b, and CG / GMRES(25) /
+    flexible GMRES(25) iterations (and solutions on the Kuhn case)."""
+    out = {}
+    g = np.load(os.path.join(HERE, "gmres.npz"))
+    bases = {"kuhn": dict(coarse_dof=100, coarse_solver=0),
+             "fix": dict(coarse_solver=0)}
+    for key, (name, over) in BSR_VARIANTS.items():
+        nb = BSR_NB[name]
+        ia, ja, val = P.block_system(g[f"{name}/A_ia"], g[f"{name}/A_ja"], g[f"{name}/A_val"],
+                                     nb, BSR_SEED[name])
+        if f"{name}/A_sha" not in out:
+            out[f"{name}/A_sha"] = np.array([sha(ia), sha(ja), sha(val)])
+            out[f"{name}/b"] = P.rhs_uniform((len(ia) - 1) * nb, BSR_SEED[name] + 1)
+        b = out[f"{name}/b"]
+        kw = dict(bases[name])
+        kw.update(over)
+        prm = oracle.AMGParams(**kw)
+        assert R.bsr_setup(nb, ia, ja, val, prm) == 0
+        nl = R.bsr_num_levels()
+        out[key + "/params"] = np.array(prm.arrays()[0][:], np.int64)
+        out[key + "/dparams"] = np.array(prm.arrays()[1][:])
+        info = []
+        for l in range(nl):
+            A = R.bsr_level_A(l, nb)
+            info.append((len(A[0]) - 1, len(A[1])))
+            out[f"{key}/A{l}_sha"] = np.array([sha(a) for a in A])
+            if l < nl - 1:
+                out[f"{key}/agg{l}"] = R.bsr_level_agg(l)
+        out[key + "/info"] = np.array(info, np.int64)
+        out[key + "/z"] = R.bsr_precond(b)
+        R.bsr_free()
+        for typ, tag in ((1, "pcg"), (3, "gmres"), (4, "fgmres")):
+            it, x = R.bsr_krylov_amg(nb, ia, ja, val, b, typ, tol=1e-8, maxit=300,
+                                     restart=25, params=prm)
+            out[f"{key}/{tag}/iters"] = np.int64(it)
+            if name == "kuhn":
+                out[f"{key}/{tag}/x"] = x
+        print("bsr", key, info, [int(out[f"{key}/{t}/iters"]) for t in ("pcg", "gmres", "fgmres")])
+    np.savez_compressed(os.path.join(HERE, "bsr.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
@@ -323,6 +384,13 @@ def main():
         return
     if only == "sa":
         sa_cases(R)
+        return
+    if only == "bsr":
+        bsr_cases(R)
+        return
+    if only == "layout":
+        with open(os.path.join(HERE, "layout.json"), "w") as f:
+            json.dump(layout(), f, indent=1, sort_keys=True)
         return
     rng = np.random.default_rng(20261203)
     base = oracle.AMGParams()
