@@ -33,6 +33,7 @@ SOURCES = [
     ("hzb_minres.cu", False),
     ("hzb_sa.cu", False),
     ("hzb_bsr.cu", False),
+    ("hzb_vmb.cu", False),
     ("hzb_assemble.cu", False),
     ("hzb_learn.cu", False),
     ("hzb_gnn.cu", True),

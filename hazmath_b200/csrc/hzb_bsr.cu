@@ -8,7 +8,7 @@
 // Gauss-Jordan as ddense_inv_inplace, dense.c:1266); the condensed scalar
 // matrix (condenseBSRLinf, sparse.c:6223: each block's max row sum of |a|,
 // negated off the diagonal, entries <= 1e-8 dropped) aggregated by heavy
-// edge matching; the boolean P (identity blocks, form_boolean_p_bsr); and
+// edge matching or VMB as aggregation_type says; the boolean P (identity blocks, form_boolean_p_bsr); and
 // A_c = R A P by dbsr_rap (sparse.c:5840-5980): with identity blocks every
 // coarse block is the sum of A's blocks in the traversal order (R row, A
 // row), the diagonal block first (from zero), new blocks copied.  The
@@ -362,7 +362,9 @@ static int bsr_build(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia,
     }
     const int min_cdof = std::max<int>(S->amg.coarse_dof, 50);
     const int max_levels = std::min<int>(S->amg.max_levels, MAX_AMG_LVL);
-    const bool par = S->bp.matching == HZB_MATCH_PARALLEL || S->amg.aggregation_type == HEC;
+    const bool vmb = S->amg.aggregation_type == VMB;
+    const bool par = !vmb && (S->bp.matching == HZB_MATCH_PARALLEL ||
+                              S->amg.aggregation_type == HEC);
     int *bad = nullptr, *tmp = nullptr;
     HZB_TRY(dalloc(&bad, 1));
     int lvl = 0, rc = SUCCESS;
@@ -410,11 +412,14 @@ static int bsr_build(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia,
         if ((rc = bundle_capacity(m, pia, s, &PP.bundle_cap))) break;
         if ((rc = dalloc(&nia, m + 1)) || (rc = dalloc(&nja, pnnz > 0 ? pnnz : 1)) ||
             (rc = dalloc(&nval, pnnz > 0 ? pnnz : 1)) || (rc = dalloc(&L.agg, m)) ||
-            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8 : (size_t)m)))
+            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8
+                                    : (size_t)(vmb ? 2 : 1) * m)))
             break;
         rc = strength_graph(PP, S->amg.strong_coupled, nia, nja, nval, &nnnz, tmp, s);
         if (!rc) {
-            if (par) rc = hem_parallel(m, nia, nja, nval, L.agg, &nagg, work, s);
+            if (vmb)
+                rc = vmb_aggregate(m, nia, nja, S->amg.max_aggregation, L.agg, &nagg, work, s);
+            else if (par) rc = hem_parallel(m, nia, nja, nval, L.agg, &nagg, work, s);
             else rc = hem_exact(m, nia, nja, nval, L.agg, &nagg, work, s);
         }
         dfree(pia); dfree(pja); dfree(pval); dfree(nia); dfree(nja); dfree(nval); dfree(work);

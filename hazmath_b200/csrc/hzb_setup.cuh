@@ -27,6 +27,13 @@ int hem_exact(int n, const int *nia, const int *nja, const double *nval,
 int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
                  int *agg, int *nagg, int *work, cudaStream_t s);
 
+// VMB aggregation (aggregation_vmb, amg_setup_ua.c:596-736) on the strength
+// graph in the reference's three sequential steps and visiting orders;
+// *nagg = 0 where the reference fails (no aggregate after step 1).
+// work: 2n ints.
+int vmb_aggregate(int n, const int *nia, const int *nja, int max_agg, int *agg, int *nagg,
+                  int *work, cudaStream_t s);
+
 // R = P^T: rows of R list fine indices ascending (dcsr_trans, sparse.c:770).
 int restriction_pattern(int n, int nc, const int *agg, int *ria, int *rja,
                         int *tmp, cudaStream_t s);

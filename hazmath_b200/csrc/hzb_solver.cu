@@ -527,17 +527,23 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
         int *nia = nullptr, *nja = nullptr, *agg = nullptr, *work = nullptr;
         double *nval = nullptr;
         int nnnz = 0, nagg = 0;
-        const bool par = S->bp.matching == HZB_MATCH_PARALLEL ||
-                         S->amg.aggregation_type == HEC;
+        // aggregation_type: VMB in the reference's order; HEM exact, or the
+        // deterministic parallel matching (hzb_param.matching, and for HEC,
+        // whose reference order comes from an unseeded rand())
+        const bool vmb = S->amg.aggregation_type == VMB;
+        const bool par = !vmb && (S->bp.matching == HZB_MATCH_PARALLEL ||
+                                  S->amg.aggregation_type == HEC);
         if ((rc = dalloc(&nia, m + 1)) || (rc = dalloc(&nja, L.nnz)) ||
             (rc = dalloc(&nval, L.nnz)) || (rc = dalloc(&agg, m)) ||
-            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8 : (size_t)m))) {
+            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8
+                                    : (size_t)(vmb ? 2 : 1) * m))) {
             dfree(nia); dfree(nja); dfree(nval); dfree(agg); dfree(work);
             break;
         }
         rc = strength_graph(L.A64(), S->amg.strong_coupled, nia, nja, nval, &nnnz, tmp, s);
         if (!rc) {
-            if (par) rc = hem_parallel(m, nia, nja, nval, agg, &nagg, work, s);
+            if (vmb) rc = vmb_aggregate(m, nia, nja, S->amg.max_aggregation, agg, &nagg, work, s);
+            else if (par) rc = hem_parallel(m, nia, nja, nval, agg, &nagg, work, s);
             else rc = hem_exact(m, nia, nja, nval, agg, &nagg, work, s);
         }
         dfree(work);

@@ -234,6 +234,14 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def vmb(self, ia, ja, val, theta=0.0, max_aggregation=20):
+        """aggregation_vmb on the strength graph of (ia, ja, val)."""
+        n = len(ia) - 1
+        agg = np.empty(n, np.int32)
+        nc = self.lib.or_vmb_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta),
+                                 max_aggregation, _p(agg))
+        return nc, agg
+
     def rap(self, ia, ja, val, nc, agg):
         n = len(ia) - 1
         agg = np.ascontiguousarray(agg, np.int32)

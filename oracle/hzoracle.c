@@ -815,6 +815,69 @@ int or_hem_agg(int n, const int *ia, const int *ja, const double *a,
     return nc;
 }
 
+/* aggregation_vmb amg_setup_ua.c:596-736 on the strength graph (the three
+ * greedy steps in the reference's orders, with its count of unvisited rows).
+ * Returns the number of aggregates, 0 where the reference returns
+ * ERROR_AMG_COARSEING (none after step 1); rows without an aggregate -> -1. */
+static int or_vmb(int n, const int *ia, const int *ja, int max_agg, int *v)
+{
+    int na = 0, left = n;
+    for (int i = 0; i < n; ++i) v[i] = -2;
+    for (int i = n - 1; i >= 0; --i) {                       /* step 1 */
+        if (ia[i + 1] - ia[i] == 1) { v[i] = -1; --left; continue; }
+        int subset = 1;
+        for (int p = ia[i]; p < ia[i + 1]; ++p)
+            if (v[ja[p]] >= -1) { subset = 0; break; }
+        if (!subset) continue;
+        int count = 1;
+        v[i] = na; --left;
+        for (int p = ia[i]; p < ia[i + 1]; ++p)
+            if (ja[p] != i && count < max_agg) { v[ja[p]] = na; --left; ++count; }
+        ++na;
+    }
+    if (na < 1) return 0;
+    int *t = (int *)malloc(sizeof(int) * n);
+    int *cnt = (int *)calloc(na, sizeof(int));
+    for (int i = 0; i < n; ++i) { t[i] = v[i]; if (v[i] >= 0) cnt[v[i]]++; }
+    for (int i = n - 1; i >= 0; --i) {                       /* step 2 */
+        if (v[i] >= -1) continue;
+        for (int p = ia[i]; p < ia[i + 1]; ++p) {
+            int a = t[ja[p]];
+            if (a > -1 && cnt[a] < max_agg) { v[i] = a; --left; cnt[a]++; break; }
+        }
+    }
+    while (left > 0) {                                        /* step 3 */
+        int before = left;
+        for (int i = 0; i < n; ++i) {
+            if (v[i] >= -1) continue;
+            int count = 1;
+            v[i] = na; --left;
+            for (int p = ia[i]; p < ia[i + 1]; ++p)
+                if (ja[p] != i && v[ja[p]] < -1 && count < max_agg) {
+                    v[ja[p]] = na; --left; ++count;
+                }
+            ++na;
+        }
+        if (left == before) break;   /* the reference would loop forever */
+    }
+    for (int i = 0; i < n; ++i) if (v[i] < 0) v[i] = -1;
+    free(t); free(cnt);
+    return na;
+}
+
+int or_vmb_agg(int n, const int *ia, const int *ja, const double *a,
+               double theta, int max_agg, int *agg)
+{
+    int nnz = ia[n];
+    int *nia = (int *)malloc(sizeof(int) * (n + 1));
+    int *nja = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    double *nv = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    or_strength(n, ia, ja, a, theta, nia, nja, nv);
+    int nc = or_vmb(n, nia, nja, max_agg, agg);
+    free(nia); free(nja); free(nv);
+    return nc;
+}
+
 static ocsr g_rap;
 int or_rap(int n, const int *ia, const int *ja, const double *a, int nc,
            const int *agg, int *rap_ia, int *rap_ja, double *rap_val)

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|layout]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|layout]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -305,6 +305,48 @@ def sa_cases(R):
     np.savez_compressed(os.path.join(HERE, "sa.npz"), **out)
 
 
+VMB_VARIANTS = {
+    "fix/vmb": ("fix", dict(coarse_dof=100)),
+    "fix/vmb4": ("fix", dict(coarse_dof=100, max_aggregation=4)),
+    "kuhn/vmb": ("kuhn", {}),
+    "kuhn/vmb_t": ("kuhn", dict(strong_coupled=0.08)),
+    "kuhn/vmb_w": ("kuhn", dict(cycle_type=2, max_aggregation=9)),
+}
+
+
+def vmb_cases(R):
+    """VMB aggregation (aggregation_type 1, aggregation_vmb) on the matrices
+    of gmres.npz: level sizes, every aggregate map, SHA-256 digests of every
+    coarse operator, the adapted threshold, PCG iterations and solutions."""
+    out = {}
+    g = np.load(os.path.join(HERE, "gmres.npz"))
+    bases = {"fix": {}, "kuhn": dict(smoother=10, presmooth_iter=2, postsmooth_iter=2,
+                                     coarse_dof=100)}
+    for key, (name, over) in VMB_VARIANTS.items():
+        cia, cja, cval = g[f"{name}/A_ia"], g[f"{name}/A_ja"], g[f"{name}/A_val"]
+        cb = g[f"{name}/b"]
+        kw = dict(bases[name])
+        kw.update(over)
+        kw["aggregation_type"] = 1
+        prm = oracle.AMGParams(**kw)
+        assert R.setup(cia, cja, cval, prm) == 0
+        nl = R.num_levels()
+        out[key + "/params"] = np.array(prm.arrays()[0][:], np.int64)
+        out[key + "/dparams"] = np.array(prm.arrays()[1][:])
+        out[key + "/info"] = np.array([R.level_info(l)[:3] for l in range(nl)], np.int64)
+        out[key + "/theta_after"] = np.float64(R.strong_coupled())
+        for l in range(nl):
+            out[f"{key}/A{l}_sha"] = np.array([sha(a) for a in R.level_A(l)])
+            if l < nl - 1:
+                out[f"{key}/agg{l}"] = R.level_agg(l)
+        it, x, hist = R.pcg(cb, None, 1e-8, 300, 1)
+        out[key + "/pcg/iters"] = np.int64(it)
+        out[key + "/pcg/x"] = x
+        print("vmb", key, out[key + "/info"][:, 0], it)
+        R.free()
+    np.savez_compressed(os.path.join(HERE, "vmb.npz"), **out)
+
+
 BSR_VARIANTS = {
     "kuhn/gs": ("kuhn", {}),
     "kuhn/jac": ("kuhn", dict(smoother=1, presmooth_iter=2, postsmooth_iter=2)),
@@ -313,6 +355,7 @@ BSR_VARIANTS = {
     "kuhn/cs": ("kuhn", dict(coarse_scaling=1)),
     "kuhn/m2": ("kuhn", dict(maxit=2)),
     "kuhn/t": ("kuhn", dict(strong_coupled=0.08)),
+    "kuhn/vmb": ("kuhn", dict(aggregation_type=1)),
     "fix/gs": ("fix", {}),
 }
 BSR_NB = {"kuhn": 3, "fix": 2}
@@ -384,6 +427,9 @@ def main():
         return
     if only == "sa":
         sa_cases(R)
+        return
+    if only == "vmb":
+        vmb_cases(R)
         return
     if only == "bsr":
         bsr_cases(R)

@@ -6,7 +6,7 @@ GMRES(25) and flexible GMRES(25) iteration counts and solutions.  Matrices:
 problems.block_system of the Kuhn P1 matrix of gmres.npz with 3 x 3 blocks
 and of the 5-point matrix with 2 x 2 blocks.  Variants: block Gauss-Seidel,
 Jacobi (two sweeps), symmetric Gauss-Seidel, the W-cycle, coarse scaling, two
-cycles per application, a threshold that drops couplings."""
+cycles per application, a threshold that drops couplings, VMB aggregation."""
 import hashlib
 
 import numpy as np
@@ -25,7 +25,7 @@ pytestmark = pytest.mark.gpu
 ZTOL = 1e-10        # one preconditioner application, relative to max |z|
 XTOL = 1e-9         # solutions, relative to max |x|
 VARIANTS = ["kuhn/gs", "kuhn/jac", "kuhn/sgs", "kuhn/w", "kuhn/cs", "kuhn/m2", "kuhn/t",
-            "fix/gs"]
+            "kuhn/vmb", "fix/gs"]
 NB = {"kuhn": 3, "fix": 2}
 SEED = {"kuhn": 31, "fix": 32}
 KRYLOV = {"pcg": hz.SOLVER_CG, "gmres": hz.SOLVER_VGMRES, "fgmres": hz.SOLVER_VFGMRES}
