@@ -306,6 +306,20 @@ struct BsrHier {
     }
 };
 
+// device temporaries of one setup step, freed (stream-ordered) with it
+struct Scratch {
+    std::vector<void *> p;
+    template <typename T>
+    int get(T **x, size_t n) {
+        const int rc = dalloc(x, n);
+        if (rc == SUCCESS) p.push_back((void *)*x);
+        return rc;
+    }
+    ~Scratch() {
+        for (void *q : p) cudaFreeAsync(q, cur_stream());
+    }
+};
+
 void bsr_release(hzb_solver *S) {
     if (!S->bsr) return;
     S->bsr->release();
@@ -365,20 +379,24 @@ static int bsr_build(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia,
     const bool vmb = S->amg.aggregation_type == VMB;
     const bool par = !vmb && (S->bp.matching == HZB_MATCH_PARALLEL ||
                               S->amg.aggregation_type == HEC);
-    int *bad = nullptr, *tmp = nullptr;
-    HZB_TRY(dalloc(&bad, 1));
     int lvl = 0, rc = SUCCESS;
     for (;;) {
+        // device temporaries of this level, freed when the step ends (also on
+        // the early returns)
+        Scratch tmpv;
         BsrLevel &L = H.lv[lvl];
         if ((rc = expand(L, s))) break;
         if (!(L.nrow > min_cdof && lvl < max_levels - 1)) break;
         // the diagonal inverses of the levels that get a coarser one (the
         // smoothed levels); a near-zero pivot ends the process in the
         // reference, an error here
-        if ((rc = dalloc(&L.dinv, (size_t)L.nrow * nb2))) break;
+        const int m = L.nrow;
+        int *bad = nullptr, *tmp = nullptr;
+        if ((rc = dalloc(&L.dinv, (size_t)m * nb2)) || (rc = tmpv.get(&bad, 1)) ||
+            (rc = tmpv.get(&tmp, scan_tmp_size(m + 2))))
+            break;
         HZB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
-        k_bsr_diaginv<<<grid_for(L.nrow), 128, 0, s>>>(L.nrow, nb, L.ia, L.ja, L.val, L.dinv,
-                                                        bad);
+        k_bsr_diaginv<<<grid_for(m), 128, 0, s>>>(m, nb, L.ia, L.ja, L.val, L.dinv, bad);
         count_launch();
         int hbad = 0;
         HZB_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -388,32 +406,28 @@ static int bsr_build(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia,
             rc = ERROR_DATA_ZERODIAG;
             break;
         }
-        // condensed scalar matrix, then heavy edge matching on it
-        const int m = L.nrow;
+        // condensed scalar matrix, then the aggregation on its strength graph
         int *cnt = nullptr, *pia = nullptr, *pja = nullptr, *nia = nullptr, *nja = nullptr,
             *work = nullptr, pnnz = 0, nnnz = 0, nagg = 0;
         double *pval = nullptr, *nval = nullptr;
-        dfree(tmp);
-        if ((rc = dalloc(&tmp, scan_tmp_size(m + 2))) || (rc = dalloc(&cnt, m)) ||
-            (rc = dalloc(&pia, m + 1)))
-            break;
+        if ((rc = tmpv.get(&cnt, m)) || (rc = tmpv.get(&pia, m + 1))) break;
         k_bsr_condense_count<<<grid_for(m), 256, 0, s>>>(m, nb, L.ia, L.ja, L.val, cnt);
         count_launch();
         if ((rc = scan_exclusive(cnt, pia, m, tmp, s))) break;
         HZB_CUDA(cudaMemcpyAsync(&pnnz, pia + m, sizeof(int), cudaMemcpyDeviceToHost, s));
         HZB_CUDA(cudaStreamSynchronize(s));
-        dfree(cnt);
-        if ((rc = dalloc(&pja, pnnz > 0 ? pnnz : 1)) || (rc = dalloc(&pval, pnnz > 0 ? pnnz : 1)))
+        if ((rc = tmpv.get(&pja, pnnz > 0 ? pnnz : 1)) ||
+            (rc = tmpv.get(&pval, pnnz > 0 ? pnnz : 1)))
             break;
         k_bsr_condense_fill<<<grid_for(m), 256, 0, s>>>(m, nb, L.ia, L.ja, L.val, pia, pja, pval);
         count_launch();
         DCsr<double> PP;
         PP.n = m; PP.nnz = pnnz; PP.ia = pia; PP.ja = pja; PP.val = pval;
         if ((rc = bundle_capacity(m, pia, s, &PP.bundle_cap))) break;
-        if ((rc = dalloc(&nia, m + 1)) || (rc = dalloc(&nja, pnnz > 0 ? pnnz : 1)) ||
-            (rc = dalloc(&nval, pnnz > 0 ? pnnz : 1)) || (rc = dalloc(&L.agg, m)) ||
-            (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8
-                                    : (size_t)(vmb ? 2 : 1) * m)))
+        if ((rc = tmpv.get(&nia, m + 1)) || (rc = tmpv.get(&nja, pnnz > 0 ? pnnz : 1)) ||
+            (rc = tmpv.get(&nval, pnnz > 0 ? pnnz : 1)) || (rc = dalloc(&L.agg, m)) ||
+            (rc = tmpv.get(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8
+                                      : (size_t)(vmb ? 2 : 1) * m)))
             break;
         rc = strength_graph(PP, S->amg.strong_coupled, nia, nja, nval, &nnnz, tmp, s);
         if (!rc) {
@@ -422,67 +436,54 @@ static int bsr_build(hzb_solver *S, int nrow, int nnzb, int nb, const int *d_ia,
             else if (par) rc = hem_parallel(m, nia, nja, nval, L.agg, &nagg, work, s);
             else rc = hem_exact(m, nia, nja, nval, L.agg, &nagg, work, s);
         }
-        dfree(pia); dfree(pja); dfree(pval); dfree(nia); dfree(nja); dfree(nval); dfree(work);
         if (rc) break;
-        if (nagg < 1) break;
+        if (nagg < 1) break;   // the reference stops coarsening here
         L.nc = nagg;
         // R (block pattern, fine rows ascending) and the scalar aggregate maps
-        int *ria = nullptr, *rja = nullptr;
-        if ((rc = dalloc(&ria, nagg + 1)) || (rc = dalloc(&rja, m))) break;
+        int *ria = nullptr, *rja = nullptr, *stmp = nullptr;
+        if ((rc = tmpv.get(&ria, nagg + 1)) || (rc = tmpv.get(&rja, m))) break;
         if ((rc = restriction_pattern(m, nagg, L.agg, ria, rja, tmp, s))) break;
         Level &E = L.s;
         E.nc = nagg * nb;
         if ((rc = dalloc(&E.agg, E.n))) break;
         k_bsr_scalar_agg<<<grid_for(E.n), 256, 0, s>>>(m, nb, L.agg, E.agg);
         count_launch();
-        int *stmp = nullptr;
         if ((rc = dalloc(&E.ria, E.nc + 1)) || (rc = dalloc(&E.rja, E.n)) ||
-            (rc = dalloc(&stmp, scan_tmp_size(E.n + 1))))
+            (rc = tmpv.get(&stmp, scan_tmp_size(E.n + 1))) ||
+            (rc = restriction_pattern(E.n, E.nc, E.agg, E.ria, E.rja, stmp, s)))
             break;
-        rc = restriction_pattern(E.n, E.nc, E.agg, E.ria, E.rja, stmp, s);
-        dfree(stmp);
-        if (rc) break;
-        // coarse blocks: count (row lengths bounded by a table per row), fill
-        int *ccnt = nullptr, *cia = nullptr, *list = nullptr, *err = nullptr, cnnz = 0, herr = 0;
-        int cap = 64;
-        for (;;) {
-            dfree(list);
-            if ((rc = dalloc(&ccnt, nagg)) || (rc = dalloc(&list, (size_t)nagg * cap)) ||
-                (rc = dalloc(&err, 1)))
-                break;
+        // coarse blocks per row: distinct aggregates met, in a table per row
+        // that grows when a row overflows it
+        int *ccnt = nullptr, *list = nullptr, *err = nullptr, herr = 0;
+        if ((rc = tmpv.get(&ccnt, nagg)) || (rc = tmpv.get(&err, 1))) break;
+        for (int cap = std::min(64, nagg);; cap = std::min(cap * 4, nagg)) {
+            if ((rc = tmpv.get(&list, (size_t)nagg * cap))) break;
             HZB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
             k_bsr_rap_count<<<grid_for(nagg), 128, 0, s>>>(nagg, ria, rja, L.ia, L.ja, L.agg,
                                                             ccnt, list, cap, err);
             count_launch();
             HZB_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
             HZB_CUDA(cudaStreamSynchronize(s));
-            dfree(err);
             if (!herr || cap >= nagg) break;
-            dfree(ccnt);
-            cap = std::min(cap * 4, nagg);
         }
-        dfree(list);
         if (rc) break;
-        if ((rc = dalloc(&cia, nagg + 1)) || (rc = scan_exclusive(ccnt, cia, nagg, tmp, s)))
-            break;
-        dfree(ccnt);
-        HZB_CUDA(cudaMemcpyAsync(&cnnz, cia + nagg, sizeof(int), cudaMemcpyDeviceToHost, s));
-        HZB_CUDA(cudaStreamSynchronize(s));
+        // the coarse level joins the hierarchy before its arrays exist, so a
+        // failure from here on is released with it
         H.lv.emplace_back();
         BsrLevel &C = H.lv.back();
         BsrLevel &Lf = H.lv[lvl];   // re-bind: emplace_back may move the levels
-        C.nrow = nagg; C.nnzb = cnnz; C.nb = nb; C.ia = cia;
-        if ((rc = dalloc(&C.ja, cnnz)) || (rc = dalloc(&C.val, (size_t)cnnz * nb2))) break;
+        C.nrow = nagg; C.nb = nb;
+        if ((rc = dalloc(&C.ia, nagg + 1)) || (rc = scan_exclusive(ccnt, C.ia, nagg, tmp, s)))
+            break;
+        HZB_CUDA(cudaMemcpyAsync(&C.nnzb, C.ia + nagg, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HZB_CUDA(cudaStreamSynchronize(s));
+        if ((rc = dalloc(&C.ja, C.nnzb)) || (rc = dalloc(&C.val, (size_t)C.nnzb * nb2))) break;
         k_bsr_rap_fill<<<grid_for(nagg), 128, 0, s>>>(nagg, nb, ria, rja, Lf.ia, Lf.ja, Lf.val,
-                                                       Lf.agg, cia, C.ja, C.val);
+                                                       Lf.agg, C.ia, C.ja, C.val);
         count_launch();
         HZB_LAUNCH_CHECK();
-        dfree(ria);
-        dfree(rja);
         ++lvl;
     }
-    dfree(bad);
-    dfree(tmp);
     if (rc) return rc;
     H.nl = lvl + 1;
     // Gauss-Seidel level sets of the block pattern on the smoothed levels
