@@ -23,6 +23,13 @@ region).  The plain FP64 drop-in (exact HEM, FP64 cycle, same smoother) is
 timed beside it (`plain_fp64`).  The stored matrix (2.97 GB) is far larger
 than the 126 MB L2, so no flush is needed between steps.
 
+Workload bsr: the block (BSR) path, linear_solver_dbsr_krylov_amg's pieces on
+the device: problems.block_system of the 64^3-cube Kuhn matrix (sigma 1,
+seeds 2/3) with 3 x 3 blocks (250,047 block rows, 750,141 dofs), one step =
+amg_setup_ua_bsr (HEM, coarse_dof 100) + CG preconditioned by
+precond_dbsr_amg (block Gauss-Seidel V(1,1), coarsest level by GMRES(25)) to
+1e-8; the reference's BSR solver on the same system is the CPU baseline.
+
 Workload c3: 512 independent SPD systems (2D/3D anisotropic P1 diffusion,
 1k-200k dofs log-uniform, seed 11) solved together (hzb_batch_*); one step
 = batch setup + batch solve; reports the batch time and the p50/p99 of the
@@ -168,8 +175,61 @@ def time_reference(ia, ja, val, b):
     return t, int(it), kind
 
 
+BSR_NB = 3
+
+
+def bsr_case(N: int):
+    """The block system of the bsr workload on N^3 cubes: (ia, ja, val, b)."""
+    kia, kja, kval = P.kuhn3d_p1(N, P.lognormal_field(N, 1.0, 8.0, 2))
+    ia, ja, val = P.block_system(kia, kja, kval, BSR_NB, 31)
+    return ia, ja, val, P.rhs_uniform((len(ia) - 1) * BSR_NB, 3)
+
+
+def bsr_amg(hz):
+    return hz.survey_amg(coarse_dof=100, coarse_solver=0)
+
+
+def time_reference_bsr(ia, ja, val, b):
+    """One linear_solver_dbsr_krylov_amg (setup + CG) by the reference
+    compiled from its sources, single-threaded."""
+    import oracle
+    R = oracle.ref()
+    prm = oracle.AMGParams(coarse_dof=100, coarse_solver=0)
+    t0 = time.perf_counter()
+    it, _ = R.bsr_krylov_amg(BSR_NB, ia, ja, val, b, 1, tol=1e-8, maxit=500, params=prm)
+    return time.perf_counter() - t0, int(it), "reference"
+
+
 def run_reference(args):
     name = args.workload
+    if name == "bsr":
+        import oracle
+        if not oracle.ref_available():
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference library (oracle/_ref) was not built"}))
+            return
+        wia, wja, wval, wb = bsr_case(16)
+        sia, sja, sval, sb = bsr_case(64)
+        times, iters = [], 0
+        for step in range(args.warmup + args.steps):
+            if step < args.warmup:   # the same code on the 16^3 instance, untimed
+                time_reference_bsr(wia, wja, wval, wb)
+                continue
+            t, iters, _ = time_reference_bsr(sia, sja, sval, sb)
+            times.append(t)
+        v = statistics.mean(times)
+        what = "reference BSR setup+CG of the full workload"
+        line = {"metric": "BSR UA-AMG-PCG time to 1e-8 (setup + solve)", "value": v,
+                "unit": "s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "iterations": int(iters), "config": workload_desc("bsr"),
+                "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
+                                 "sample": what},
+                "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
     if name == "c3":
         systems, _ = P.batch_anisotropic(512, 11)
         rng = np.random.default_rng(5)
@@ -213,6 +273,12 @@ def run_reference(args):
 
 
 def workload_desc(name):
+    if name == "bsr":
+        return {"workload": "block system K (x) B + seeded SPD diagonal blocks, K the 3D P1 "
+                            "log-normal diffusion on the Kuhn mesh of 64^3 cubes (sigma 1), "
+                            "3 x 3 blocks", "block_rows": 63 ** 3, "dofs": 63 ** 3 * BSR_NB,
+                "solver": "amg_setup_ua_bsr (HEM, coarse_dof 100), CG with "
+                          "precond_dbsr_amg (block GS V(1,1), GMRES(25) coarsest)"}
     if name == "c3":
         return {"workload": "512 independent 2D/3D anisotropic P1 diffusion systems, "
                             "1k-200k dofs log-uniform (seed 11)"}
@@ -229,7 +295,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c5", choices=["c1", "c2", "c5", "c3"])
+    ap.add_argument("--workload", default="c5", choices=["c1", "c2", "c5", "c3", "bsr"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -253,6 +319,8 @@ def main():
     try:
         if args.workload == "c3":
             run_batch(args, rank, world, local, dist)
+        elif args.workload == "bsr":
+            run_bsr(args, rank, world, local, dist)
         else:
             run_single(args, rank, world, local, dist)
     finally:
@@ -486,6 +554,112 @@ def assembly_leg(hz, torch, name, dja, dval, n, nnz, dev, peak):
 # The 256^3 launches run the same kernels over 8.1x the entries, and their
 # traffic is this ratio times their algorithmic bytes.
 TRAFFIC_PER_BYTE = {"l1_32": 143.73e6 / 146709388.0, "spmv64": 404.52e6 / 405049716.0}
+
+
+def run_bsr(args, rank, world, local, dist):
+    import torch
+    import hazmath_b200 as hz
+    ia, ja, val, b = bsr_case(64)
+    nrow, nnzb, n = len(ia) - 1, int(ia[-1]), len(b)
+    dev = f"cuda:{local}"
+    dia, dja = torch.from_numpy(ia).to(dev), torch.from_numpy(ja).to(dev)
+    dval, db = torch.from_numpy(val).to(dev), torch.from_numpy(b).to(dev)
+    dx = torch.zeros_like(db)
+    p = lambda t: t.data_ptr()  # noqa: E731
+    it_par = itparam(hz)
+    S = hz.Solver(bsr_amg(hz), it_par, hz.b200_param(device=local))
+
+    def check(rc, what):
+        if rc < 0:
+            raise RuntimeError(f"{what} failed {rc}: {hz.last_error()}")
+        return rc
+
+    def step():
+        dx.zero_()
+        check(S.setup_bsr_device(nrow, nnzb, BSR_NB, p(dia), p(dja), p(dval)), "bsr setup")
+        return check(S.bsr_solve_device(p(db), p(dx)), "bsr solve")
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    setup_s, solve_s, launches, iters = [], [], 0, 0
+    ev0.record()
+    for _ in range(args.steps):
+        iters = step()
+        st = S.stats()
+        setup_s.append(st.setup_seconds)
+        solve_s.append(st.solve_seconds)
+        launches += st.launches
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_s = max_over_ranks(dist, ev0.elapsed_time(ev1) * 1e-3 / args.steps, dev)
+    x = dx.cpu().numpy()
+    import scipy.sparse as sp
+    sia, sja, sval = P.bsr_to_csr(ia, ja, val, BSR_NB)
+    A = sp.csr_matrix((sval, sja, sia), shape=(n, n))
+    relres = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+    peak, peak_kind = hbm_peak()
+    gs_ms, gs_by = S.time_kernel(hz.HZB_K_BSR_GS, 0, 20)
+    res_ms, res_by = S.time_kernel(hz.HZB_K_BSR_RES, 0, 50)
+    gs_gbs = gs_by / (gs_ms * 1e-3) / 1e9
+    res_gbs = res_by / (res_ms * 1e-3) / 1e9
+    # e2e through the host entry points (matrix and vectors copied in, the
+    # solution out, inside the timed region)
+    Se = hz.Solver(bsr_amg(hz), it_par, hz.b200_param(device=local))
+    xh = np.zeros(n)
+    e2e = []
+    for k in range(1 + min(args.steps, 3)):
+        xh[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        check(Se.setup_bsr_host(BSR_NB, ia, ja, val), "bsr setup_host")
+        check(Se.bsr_solve_host(b, xh), "bsr solve_host")
+        if k:
+            e2e.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(dist, statistics.mean(e2e), dev)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            t, it_ref, kind = time_reference_bsr(ia, ja, val, b)
+            cpu = {"value": t, "unit": "s", "cores": 1, "kind": kind,
+                   "sample": f"reference BSR setup+CG of the full workload "
+                             f"({it_ref} iterations)"}
+    if rank == 0:
+        line = {
+            "metric": "BSR UA-AMG-PCG time to 1e-8 (setup + solve)", "value": step_s,
+            "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_desc("bsr"), nnz_blocks=nnzb, parallelism="replicas",
+                           l2="inputs larger than L2 (no flush)"),
+            "iterations": int(iters), "final_relres": relres,
+            "setup_s": statistics.mean(setup_s), "solve_s": statistics.mean(solve_s),
+            "dof_per_s": n / statistics.mean(solve_s),
+            "roofline": {"bound": "hbm", "kernel": "level-0 ascending block Gauss-Seidel "
+                         "sweep (k_bsr_gs_set<3> / k_bsr_gs_run<3> over the level sets)",
+                         "achieved": gs_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gs_gbs / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": gs_by, "ms_per_launch": gs_ms, "traffic": None},
+            "block_residual": {"kernel": "k_bsr_residual<3>, level 0", "achieved": res_gbs,
+                               "frac": res_gbs / peak, "bytes_per_launch": res_by,
+                               "ms_per_launch": res_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s",
+                    "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + val.nbytes + b.nbytes
+                                              + xh.nbytes),
+                    "d2h_bytes_per_step": int(xh.nbytes)},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    S.close()
+    Se.close()
 
 
 def run_batch(args, rank, world, local, dist):

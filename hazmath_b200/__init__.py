@@ -54,6 +54,7 @@ HZB_GS_EXACT, HZB_GS_MULTICOLOR = 0, 1
 HZB_MATCH_EXACT, HZB_MATCH_PARALLEL = 0, 1
 # kernels hzb_time_kernel can time
 HZB_K_SPMV64, HZB_K_SPMV32, HZB_K_RES64, HZB_K_L1_32, HZB_K_L1_64 = 0, 1, 2, 3, 4
+HZB_K_BSR_RES, HZB_K_BSR_JAC, HZB_K_BSR_GS = 5, 6, 7
 MAX_AMG_LVL = 20
 
 
@@ -179,6 +180,8 @@ def lib() -> C.CDLL:
                                              C.c_void_p, P(INT)]
         L.hzb_destroy.argtypes = [C.c_void_p]
         L.hzb_bsr_setup_host.argtypes = [C.c_void_p, P(dBSRmat)]
+        L.hzb_bsr_setup_device.argtypes = [C.c_void_p, INT, INT, INT, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]
         L.hzb_bsr_level.argtypes = [C.c_void_p, INT, P(dBSRmat), C.c_void_p]
         for name in ("hzb_bsr_precond_device", "hzb_bsr_precond_host", "hzb_bsr_solve_device",
                      "hzb_bsr_solve_host"):
@@ -602,6 +605,17 @@ class Solver:
         """amg_setup_ua_bsr on the device for a host block matrix."""
         self._keep_bsr = _HostBSR(nb, ia, ja, val)
         return lib().hzb_bsr_setup_host(self.h, C.byref(self._keep_bsr.mat))
+
+    def setup_bsr_device(self, nrow, nnzb, nb, ia_ptr, ja_ptr, val_ptr) -> int:
+        return lib().hzb_bsr_setup_device(self.h, nrow, nnzb, nb, ia_ptr, ja_ptr, val_ptr)
+
+    def time_kernel(self, which: int, level: int, reps: int):
+        """(ms per launch, algorithmic bytes per launch) of hzb_time_kernel."""
+        ms, by = REAL(), REAL()
+        rc = lib().hzb_time_kernel(self.h, which, level, reps, C.byref(ms), C.byref(by))
+        if rc:
+            raise RuntimeError(f"hzb_time_kernel: {rc} {last_error()}")
+        return ms.value, by.value
 
     def bsr_level(self, l: int):
         """Block matrix of level l as (ia, ja, val) and its block

@@ -374,6 +374,11 @@ extern "C" INT hzb_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z) {
 
 extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
                                REAL *ms_per_launch, REAL *bytes_per_launch) {
+    if (S && which >= HZB_K_BSR_RES && which <= HZB_K_BSR_GS) {
+        cudaSetDevice(S->bp.device);
+        StreamScope scope_(S->s);
+        return hzb::bsr_time_kernel(S, which, level, reps, ms_per_launch, bytes_per_launch);
+    }
     if (!S || level < 0 || level >= S->nl || reps < 1) return ERROR_INPUT_PAR;
     cudaSetDevice(S->bp.device);
     StreamScope scope_(S->s);
@@ -1046,6 +1051,16 @@ extern "C" INT hzb_bsr_setup_host(hzb_solver *S, const dBSRmat *A) {
     StreamScope scope_(S->s);
     S->bsr_cyc = bsr_cycle_param_of(S->amg);
     return hzb::bsr_setup(S, A->ROW, A->NNZ, A->nb, A->IA, A->JA, A->val);
+}
+
+extern "C" INT hzb_bsr_setup_device(hzb_solver *S, INT nrow, INT nnzb, INT nb,
+                                    const INT *d_ia, const INT *d_ja, const REAL *d_val) {
+    if (!S || !d_ia || !d_ja || !d_val) return ERROR_INPUT_PAR;
+    if (nrow <= 0 || nnzb <= 0) return ERROR_MAT_SIZE;
+    cudaSetDevice(S->bp.device);
+    StreamScope scope_(S->s);
+    S->bsr_cyc = bsr_cycle_param_of(S->amg);
+    return hzb::bsr_setup(S, nrow, nnzb, nb, d_ia, d_ja, d_val);
 }
 
 extern "C" INT hzb_bsr_level(const hzb_solver *S, INT l, dBSRmat *out, INT *agg) {

@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 namespace hzb {
@@ -208,72 +209,114 @@ __global__ void k_bsr_rap_fill(int nc, int nb, const int *__restrict__ ria,
     }
 }
 
-// w = b - A x on the scalar expansion with the subtractions in row order:
-// dbsr_aAxpy(-1, A, x, w) on w = b negates w, adds the products and negates
-// back, which rounds as the sequential subtraction
-__global__ void k_bsr_residual(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                               const double *__restrict__ val, const double *__restrict__ b,
-                               const double *__restrict__ x, double *__restrict__ w) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double v = b[i];
-        for (int p = ia[i]; p < ia[i + 1]; ++p) v -= val[p] * x[ja[p]];
-        w[i] = v;
+// w = b - A x for block row I, the subtractions in row order (blocks in
+// order, a block's columns in order): dbsr_aAxpy(-1, A, x, w) on w = b
+// negates w, adds the products and negates back, which rounds as this
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_bsr_residual(int nrow, const int *__restrict__ ia, const int *__restrict__ ja,
+               const double *__restrict__ val, const double *__restrict__ b,
+               const double *__restrict__ x, double *__restrict__ w) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nrow; I += gridDim.x * blockDim.x) {
+        double t[NB];
+#pragma unroll
+        for (int r = 0; r < NB; ++r) t[r] = b[I * NB + r];
+        for (int k = ia[I]; k < ia[I + 1]; ++k) {
+            const double *a = val + (size_t)k * (NB * NB);
+            const int J = ja[k];
+            double xj[NB];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) xj[c] = x[J * NB + c];
+#pragma unroll
+            for (int r = 0; r < NB; ++r)
+#pragma unroll
+                for (int c = 0; c < NB; ++c) t[r] -= a[r * NB + c] * xj[c];
+        }
+#pragma unroll
+        for (int r = 0; r < NB; ++r) w[I * NB + r] = t[r];
     }
 }
 
 // one block row of Jacobi / Gauss-Seidel: x_I = D_I^{-1} (b_I - sum_{J != I}
 // A_IJ x_J), reading x from xin and writing xout (the same array for GS)
-__device__ __forceinline__ void bsr_relax_row(int I, int nb, const int *__restrict__ ia,
+template <int NB>
+__device__ __forceinline__ void bsr_relax_row(int I, const int *__restrict__ ia,
                                               const int *__restrict__ ja,
                                               const double *__restrict__ val,
                                               const double *__restrict__ dinv,
                                               const double *__restrict__ b, const double *xin,
                                               double *xout) {
-    const int nb2 = nb * nb;
-    double t[BSR_MAXNB];
-    for (int r = 0; r < nb; ++r) t[r] = b[I * nb + r];
+    double t[NB];
+#pragma unroll
+    for (int r = 0; r < NB; ++r) t[r] = b[I * NB + r];
     for (int k = ia[I]; k < ia[I + 1]; ++k) {
         const int J = ja[k];
         if (J == I) continue;
-        const double *a = val + (size_t)k * nb2;
-        for (int r = 0; r < nb; ++r)
-            for (int c = 0; c < nb; ++c) t[r] -= a[r * nb + c] * xin[J * nb + c];
+        const double *a = val + (size_t)k * (NB * NB);
+        double xj[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) xj[c] = xin[J * NB + c];
+#pragma unroll
+        for (int r = 0; r < NB; ++r)
+#pragma unroll
+            for (int c = 0; c < NB; ++c) t[r] -= a[r * NB + c] * xj[c];
     }
-    const double *d = dinv + (size_t)I * nb2;
-    for (int r = 0; r < nb; ++r) {
+    const double *d = dinv + (size_t)I * (NB * NB);
+#pragma unroll
+    for (int r = 0; r < NB; ++r) {
         double v = 0.0;
-        for (int c = 0; c < nb; ++c) v += d[r * nb + c] * t[c];
-        xout[I * nb + r] = v;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) v += d[r * NB + c] * t[c];
+        xout[I * NB + r] = v;
     }
 }
 
-__global__ void k_bsr_jacobi(int nrow, int nb, const int *__restrict__ ia,
-                             const int *__restrict__ ja, const double *__restrict__ val,
-                             const double *__restrict__ dinv, const double *__restrict__ b,
-                             const double *__restrict__ x, double *__restrict__ xn) {
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_bsr_jacobi(int nrow, const int *__restrict__ ia, const int *__restrict__ ja,
+             const double *__restrict__ val, const double *__restrict__ dinv,
+             const double *__restrict__ b, const double *__restrict__ x,
+             double *__restrict__ xn) {
     for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nrow; I += gridDim.x * blockDim.x)
-        bsr_relax_row(I, nb, ia, ja, val, dinv, b, x, xn);
+        bsr_relax_row<NB>(I, ia, ja, val, dinv, b, x, xn);
 }
 
 // the rows of one level set, in parallel
-__global__ void k_bsr_gs_set(const int *__restrict__ rows, int cnt, int nb,
-                             const int *__restrict__ ia, const int *__restrict__ ja,
-                             const double *__restrict__ val, const double *__restrict__ dinv,
-                             const double *__restrict__ b, double *x) {
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_bsr_gs_set(const int *__restrict__ rows, int cnt, const int *__restrict__ ia,
+             const int *__restrict__ ja, const double *__restrict__ val,
+             const double *__restrict__ dinv, const double *__restrict__ b, double *x) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x)
-        bsr_relax_row(rows[q], nb, ia, ja, val, dinv, b, x, x);
+        bsr_relax_row<NB>(rows[q], ia, ja, val, dinv, b, x, x);
 }
 
 // a run of small level sets [first, last) by one CTA, sets in order
-__global__ void k_bsr_gs_run(const int *__restrict__ rows, const int *__restrict__ set_ptr,
-                             int first, int last, int nb, const int *__restrict__ ia,
-                             const int *__restrict__ ja, const double *__restrict__ val,
-                             const double *__restrict__ dinv, const double *__restrict__ b,
-                             double *x) {
+template <int NB>
+__global__ void __launch_bounds__(256)
+k_bsr_gs_run(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first,
+             int last, const int *__restrict__ ia, const int *__restrict__ ja,
+             const double *__restrict__ val, const double *__restrict__ dinv,
+             const double *__restrict__ b, double *x) {
     for (int k = first; k < last; ++k) {
         for (int q = set_ptr[k] + threadIdx.x; q < set_ptr[k + 1]; q += blockDim.x)
-            bsr_relax_row(rows[q], nb, ia, ja, val, dinv, b, x, x);
+            bsr_relax_row<NB>(rows[q], ia, ja, val, dinv, b, x, x);
         __syncthreads();
+    }
+}
+
+// f(std::integral_constant<int, nb>) for the block sizes the kernels hold
+template <typename F>
+void with_nb(int nb, F &&f) {
+    switch (nb) {
+    case 1: f(std::integral_constant<int, 1>()); break;
+    case 2: f(std::integral_constant<int, 2>()); break;
+    case 3: f(std::integral_constant<int, 3>()); break;
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 5: f(std::integral_constant<int, 5>()); break;
+    case 6: f(std::integral_constant<int, 6>()); break;
+    case 7: f(std::integral_constant<int, 7>()); break;
+    default: f(std::integral_constant<int, 8>()); break;
     }
 }
 }  // namespace
@@ -541,8 +584,11 @@ static int bsr_smooth(hzb_solver *S, BsrLevel &L, int kind, int sweeps) {
     Level &E = L.s;
     for (int it = 0; it < sweeps; ++it) {
         if (kind == 0) {   // Jacobi: a new iterate from the old one
-            k_bsr_jacobi<<<grid_for(L.nrow), 128, 0, s>>>(L.nrow, L.nb, L.ia, L.ja, L.val, L.dinv,
-                                                          E.b, E.x, E.t);
+            with_nb(L.nb, [&](auto c) {
+                constexpr int NB = decltype(c)::value;
+                k_bsr_jacobi<NB><<<grid_for(L.nrow, 128), 128, 0, s>>>(L.nrow, L.ia, L.ja, L.val,
+                                                                       L.dinv, E.b, E.x, E.t);
+            });
             count_launch();
             HZB_TRY(vcopy<double>(E.n, E.t, E.x, s));
             continue;
@@ -550,19 +596,33 @@ static int bsr_smooth(hzb_solver *S, BsrLevel &L, int kind, int sweeps) {
         const Schedule &sc = kind == 1 ? L.asc : L.desc;
         for (size_t q = 0; q < sc.run_first.size(); ++q) {
             const int f = sc.run_first[q], l = sc.run_last[q];
-            if (l < 0) {
-                const int cnt = sc.h_ptr[f + 1] - sc.h_ptr[f];
-                k_bsr_gs_set<<<grid_for(cnt), 128, 0, s>>>(sc.rows + sc.h_ptr[f], cnt, L.nb, L.ia,
-                                                           L.ja, L.val, L.dinv, E.b, E.x);
-            } else {
-                k_bsr_gs_run<<<1, 256, 0, s>>>(sc.rows, sc.set_ptr, f, l, L.nb, L.ia, L.ja, L.val,
-                                               L.dinv, E.b, E.x);
-            }
+            with_nb(L.nb, [&](auto c) {
+                constexpr int NB = decltype(c)::value;
+                if (l < 0) {
+                    const int cnt = sc.h_ptr[f + 1] - sc.h_ptr[f];
+                    k_bsr_gs_set<NB><<<grid_for(cnt, 128), 128, 0, s>>>(
+                        sc.rows + sc.h_ptr[f], cnt, L.ia, L.ja, L.val, L.dinv, E.b, E.x);
+                } else {
+                    k_bsr_gs_run<NB><<<1, 256, 0, s>>>(sc.rows, sc.set_ptr, f, l, L.ia, L.ja,
+                                                        L.val, L.dinv, E.b, E.x);
+                }
+            });
             count_launch();
         }
     }
     HZB_LAUNCH_CHECK();
     return SUCCESS;
+}
+
+// w = b - A x on level L (block residual of mgcycle_bsr)
+static void bsr_residual(BsrLevel &L, const double *b, const double *x, double *w,
+                         cudaStream_t s) {
+    with_nb(L.nb, [&](auto c) {
+        constexpr int NB = decltype(c)::value;
+        k_bsr_residual<NB><<<grid_for(L.nrow, 128), 128, 0, s>>>(L.nrow, L.ia, L.ja, L.val, b,
+                                                                 x, w);
+    });
+    count_launch();
 }
 
 // the smoothing of mgcycle_bsr: Jacobi, GS (ascending before, descending
@@ -596,8 +656,7 @@ forward:
         Level &E = L.s;
         nu[l]++;
         HZB_TRY(bsr_smoothing(S, L, cyc, true));
-        k_bsr_residual<<<grid_for(E.n), 256, 0, s>>>(E.n, E.ia, E.ja, E.val, E.b, E.x, E.w);
-        count_launch();
+        bsr_residual(L, E.b, E.x, E.w, s);
         Level &Cn = H.lv[l + 1].s;
         HZB_TRY(restrict_agg<double>(E.nc, E.ria, E.rja, E.w, Cn.b, s));
         ++l;
@@ -639,6 +698,55 @@ forward:
         nu[l] = 0;
     }
     if (l > 0) goto forward;
+    return SUCCESS;
+}
+
+// reps launches of one block kernel on level l between the handle's events:
+// the residual (x, b -> w), a Jacobi sweep (x -> t) or an ascending
+// Gauss-Seidel sweep over the level sets (x in place); algorithmic bytes per
+// launch: blocks, block columns, row pointers (+ the diagonal inverses for a
+// sweep) and three n-vectors
+int bsr_time_kernel(hzb_solver *S, int which, int l, int reps, double *ms_per_launch,
+                    double *bytes_per_launch) {
+    if (!S->bsr || l < 0 || l >= S->bsr->nl || reps < 1) return ERROR_INPUT_PAR;
+    BsrLevel &L = S->bsr->lv[l];
+    Level &E = L.s;
+    const bool sweep = which == HZB_K_BSR_JAC || which == HZB_K_BSR_GS;
+    if (which != HZB_K_BSR_RES && !sweep) return ERROR_INPUT_PAR;
+    if (sweep && !L.dinv) return ERROR_INPUT_PAR;   // the coarsest level is not smoothed
+    if (which == HZB_K_BSR_GS && L.asc.run_first.empty()) return ERROR_INPUT_PAR;
+    const double nb2 = (double)L.nb * L.nb;
+    double bytes = L.nnzb * (8.0 * nb2 + 4.0) + 4.0 * (L.nrow + 1) + 3.0 * 8.0 * E.n;
+    if (sweep) bytes += 8.0 * nb2 * L.nrow;
+    cudaStream_t s = S->s;
+    HZB_TRY(vzero<double>(E.n, E.x, s));
+    auto launch = [&]() -> int {
+        if (which == HZB_K_BSR_RES) {
+            bsr_residual(L, E.b, E.x, E.w, s);
+            HZB_LAUNCH_CHECK();
+            return SUCCESS;
+        }
+        if (which == HZB_K_BSR_JAC) {
+            with_nb(L.nb, [&](auto c) {
+                constexpr int NB = decltype(c)::value;
+                k_bsr_jacobi<NB><<<grid_for(L.nrow, 128), 128, 0, s>>>(L.nrow, L.ia, L.ja, L.val,
+                                                                       L.dinv, E.b, E.x, E.t);
+            });
+            count_launch();
+            HZB_LAUNCH_CHECK();
+            return SUCCESS;
+        }
+        return bsr_smooth(S, L, 1, 1);
+    };
+    HZB_TRY(launch());
+    HZB_CUDA(cudaEventRecord(S->e0, s));
+    for (int r = 0; r < reps; ++r) HZB_TRY(launch());
+    HZB_CUDA(cudaEventRecord(S->e1, s));
+    HZB_CUDA(cudaEventSynchronize(S->e1));
+    float ms = 0.f;
+    HZB_CUDA(cudaEventElapsedTime(&ms, S->e0, S->e1));
+    *ms_per_launch = ms / reps;
+    *bytes_per_launch = bytes;
     return SUCCESS;
 }
 

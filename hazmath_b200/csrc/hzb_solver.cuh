@@ -257,4 +257,7 @@ int bsr_block_size(const hzb_solver *S);
 int bsr_level_copy(const hzb_solver *S, int l, int *nrow, int *nnzb, int *ia, int *ja,
                    double *val, int *agg);
 void bsr_release(hzb_solver *S);
+// hzb_time_kernel's block kernels (HZB_K_BSR_*)
+int bsr_time_kernel(hzb_solver *S, int which, int l, int reps, double *ms_per_launch,
+                    double *bytes_per_launch);
 }  // namespace hzb

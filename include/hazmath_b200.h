@@ -532,6 +532,9 @@ INT  hzb_level_copy(const hzb_solver *s, INT l, INT *ia, INT *ja, REAL *val,
  * or host vectors; the handle's Krylov type (1, 3, 4) preconditioned by it,
  * x holding the initial guess. */
 INT  hzb_bsr_setup_host(hzb_solver *s, const dBSRmat *A);
+/* the same from device arrays (row pointers, block columns, blocks) */
+INT  hzb_bsr_setup_device(hzb_solver *s, INT nrow, INT nnzb, INT nb, const INT *d_ia,
+                          const INT *d_ja, const REAL *d_val);
 INT  hzb_bsr_level(const hzb_solver *s, INT l, dBSRmat *out, INT *agg);
 INT  hzb_bsr_precond_device(hzb_solver *s, const REAL *d_r, REAL *d_z);
 INT  hzb_bsr_precond_host(hzb_solver *s, const REAL *r, REAL *z);
@@ -591,12 +594,18 @@ INT  hzb_learn_select_omega(hzb_solver *s, hzb_gnn *g, INT ns,
  * index per entry, row pointers, and each vector once).  which:
  *   HZB_K_SPMV64  y = A x, FP64        HZB_K_SPMV32  y = A x, FP32
  *   HZB_K_RES64   w = b - A x, FP64    HZB_K_L1_32   l1-Jacobi sweep, FP32
- *   HZB_K_L1_64   l1-Jacobi sweep, FP64                                    */
+ *   HZB_K_L1_64   l1-Jacobi sweep, FP64
+ * and on a block (BSR) hierarchy of the handle:
+ *   HZB_K_BSR_RES  w = b - A x         HZB_K_BSR_JAC  block Jacobi sweep
+ *   HZB_K_BSR_GS   ascending block Gauss-Seidel sweep (all level sets)     */
 #define HZB_K_SPMV64 0
 #define HZB_K_SPMV32 1
 #define HZB_K_RES64  2
 #define HZB_K_L1_32  3
 #define HZB_K_L1_64  4
+#define HZB_K_BSR_RES 5
+#define HZB_K_BSR_JAC 6
+#define HZB_K_BSR_GS  7
 INT hzb_time_kernel(hzb_solver *s, INT which, INT level, INT reps,
                     REAL *ms_per_launch, REAL *bytes_per_launch);
 
