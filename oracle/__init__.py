@@ -234,6 +234,21 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def srand(self, seed: int) -> None:
+        """Seed the oracle's restatement of the C library's rand() stream."""
+        self.lib.or_srand(ctypes.c_uint(seed))
+
+    def rand(self) -> int:
+        return self.lib.or_rand()
+
+    def hec(self, ia, ja, val, theta=0.0):
+        """aggregation_hec on the strength graph of (ia, ja, val), its row order
+        drawn from the rand() stream (continuing from the last call)."""
+        n = len(ia) - 1
+        agg = np.empty(n, np.int32)
+        nc = self.lib.or_hec_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
+        return nc, agg
+
     def vmb(self, ia, ja, val, theta=0.0, max_aggregation=20):
         """aggregation_vmb on the strength graph of (ia, ja, val)."""
         n = len(ia) - 1
@@ -342,6 +357,10 @@ class Ref(_Backend):
         self.lib.ref_free()
 
     # -- block (BSR) matrices: amg_setup_ua_bsr, precond_dbsr_amg ----------
+    def srand(self, seed: int) -> None:
+        """srand() in the reference's process (its HEC draws from rand())."""
+        self.lib.ref_srand(ctypes.c_uint(seed))
+
     def bsr_setup(self, nb, ia, ja, val, params: AMGParams | None = None) -> int:
         params = params or AMGParams()
         ia = np.ascontiguousarray(ia, np.int32)

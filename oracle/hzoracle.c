@@ -878,6 +878,89 @@ int or_vmb_agg(int n, const int *ia, const int *ja, const double *a,
     return nc;
 }
 
+/* The C library's rand() as the reference's HEC draws it (iarray_shuffle,
+ * array.c:302-315).  glibc's rand() is random() of the TYPE_3 additive
+ * feedback generator (published in glibc's random_r.c; the same since the
+ * BSD random(3)): srand(s) fills r[0..30] by r[i] = 16807 r[i-1] mod
+ * (2^31 - 1) from r[0] = s (s = 0 counts as 1), copies r[31..33] = r[0..2],
+ * discards 310 outputs of r[i] = r[i-31] + r[i-3] (mod 2^32), and returns
+ * r[i] >> 1.  A test checks this against the system's rand(). */
+static struct { uint32_t r[34]; int i; } g_rand;
+
+void or_srand(unsigned seed)
+{
+    int32_t r[34];
+    r[0] = (int32_t)(seed ? seed : 1);
+    for (int i = 1; i < 31; ++i) {
+        long long w = (16807LL * r[i - 1]) % 2147483647LL;
+        if (w < 0) w += 2147483647LL;
+        r[i] = (int32_t)w;
+    }
+    for (int i = 31; i < 34; ++i) r[i] = r[i - 31];
+    for (int i = 0; i < 34; ++i) g_rand.r[i] = (uint32_t)r[i];
+    g_rand.i = 34;
+    for (int k = 0; k < 310; ++k) {
+        uint32_t v = g_rand.r[(g_rand.i - 31) % 34] + g_rand.r[(g_rand.i - 3) % 34];
+        g_rand.r[g_rand.i % 34] = v;
+        ++g_rand.i;
+    }
+}
+
+int or_rand(void)
+{
+    uint32_t v = g_rand.r[(g_rand.i - 31) % 34] + g_rand.r[(g_rand.i - 3) % 34];
+    g_rand.r[g_rand.i % 34] = v;
+    ++g_rand.i;
+    if (g_rand.i >= 34 * 1024) g_rand.i -= 34 * 1000;   /* keep the index small */
+    return (int)(v >> 1);
+}
+
+/* aggregation_hec amg_setup_ua.c:752-845 on the strength graph: rows in the
+ * order of iarray_shuffle's permutation (drawn from the stream above, which
+ * continues across calls as the process-wide rand() does); each row pairs
+ * with its most strongly coupled neighbour (first maximum of |a| off the
+ * diagonal) when that one is unvisited, else joins its aggregate.  Returns
+ * the number of aggregates, -1 where the reference exits (a row of length > 1
+ * with no off-diagonal entry). */
+static int or_hec(int n, const int *ia, const int *ja, const double *a, int *v)
+{
+    int *perm = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) { perm[i] = i; v[i] = -2; }
+    for (int i = 0; i < n - 1; ++i) {
+        int j = i + or_rand() / (2147483647 / (n - i) + 1);
+        int t = perm[j]; perm[j] = perm[i]; perm[i] = t;
+    }
+    int na = 0;
+    for (int q = 0; q < n; ++q) {
+        int i = perm[q];
+        if (ia[i + 1] - ia[i] == 1) { v[i] = -1; continue; }
+        int k = -1;
+        double mx = -1.0;
+        for (int p = ia[i]; p < ia[i + 1]; ++p)
+            if (ja[p] != i && fabs(a[p]) > mx) { k = p; mx = fabs(a[p]); }
+        if (k < 0) { free(perm); return -1; }
+        int j = ja[k];
+        if (v[j] < -1) { v[j] = na; v[i] = na; ++na; }
+        else v[i] = v[j];
+    }
+    for (int i = 0; i < n; ++i) if (v[i] < 0) v[i] = -1;
+    free(perm);
+    return na;
+}
+
+int or_hec_agg(int n, const int *ia, const int *ja, const double *a, double theta,
+               int *agg)
+{
+    int nnz = ia[n];
+    int *nia = (int *)malloc(sizeof(int) * (n + 1));
+    int *nja = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    double *nv = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    or_strength(n, ia, ja, a, theta, nia, nja, nv);
+    int nc = or_hec(n, nia, nja, nv, agg);
+    free(nia); free(nja); free(nv);
+    return nc;
+}
+
 static ocsr g_rap;
 int or_rap(int n, const int *ia, const int *ja, const double *a, int nc,
            const int *agg, int *rap_ia, int *rap_ja, double *rap_val)

@@ -360,6 +360,10 @@ int ref_rap_agg(int n, int nnz, int *ia, int *ja, double *val, int nc,
     return g_rap.nnz;
 }
 
+/* srand() in this process: the reference's HEC aggregation draws its row
+ * order from rand() (iarray_shuffle, array.c:302) */
+void ref_srand(unsigned seed) { srand(seed); }
+
 /* ---- UA-AMG for BSR matrices: amg_setup_ua_bsr (amg_setup_ua.c:145),
  * precond_dbsr_amg (precond.c:1311) and linear_solver_dbsr_krylov_amg
  * (itsolver.c:2104), on one global hierarchy.  ip/dp as fill_param.       */

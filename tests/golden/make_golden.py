@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|layout]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|hec|layout]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -347,6 +347,28 @@ def vmb_cases(R):
     np.savez_compressed(os.path.join(HERE, "vmb.npz"), **out)
 
 
+def hec_cases(R):
+    """HEC aggregation (aggregation_type 4, the reference's default) with the
+    process's rand() seeded 1 (a fresh process), on the matrices of gmres.npz:
+    every level's aggregate map and the adapted threshold."""
+    out = {}
+    g = np.load(os.path.join(HERE, "gmres.npz"))
+    for name in ("fix", "kuhn"):
+        prm = oracle.AMGParams(aggregation_type=4, strong_coupled=0.04, coarse_dof=100)
+        R.srand(1)
+        assert R.setup(g[f"{name}/A_ia"], g[f"{name}/A_ja"], g[f"{name}/A_val"], prm) == 0
+        nl = R.num_levels()
+        out[f"{name}/info"] = np.array([R.level_info(l)[:3] for l in range(nl)], np.int64)
+        out[f"{name}/theta_after"] = np.float64(R.strong_coupled())
+        for l in range(nl):
+            out[f"{name}/A{l}_sha"] = np.array([sha(a) for a in R.level_A(l)])
+            if l < nl - 1:
+                out[f"{name}/agg{l}"] = R.level_agg(l)
+        print("hec", name, out[f"{name}/info"][:, 0])
+        R.free()
+    np.savez_compressed(os.path.join(HERE, "hec.npz"), **out)
+
+
 BSR_VARIANTS = {
     "kuhn/gs": ("kuhn", {}),
     "kuhn/jac": ("kuhn", dict(smoother=1, presmooth_iter=2, postsmooth_iter=2)),
@@ -427,6 +449,9 @@ def main():
         return
     if only == "sa":
         sa_cases(R)
+        return
+    if only == "hec":
+        hec_cases(R)
         return
     if only == "vmb":
         vmb_cases(R)
