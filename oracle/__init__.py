@@ -234,6 +234,31 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def bsr_hierarchy(self, nb, ia, ja, val, theta=0.0, coarse_dof=2000, max_levels=20,
+                      aggregation_type=5, max_aggregation=20):
+        """The block hierarchy of amg_setup_ua_bsr: a list of (ia, ja, val) per
+        level and the block aggregate maps of the levels below the coarsest."""
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        nl = self.lib.or_bsr_setup(len(ia) - 1, int(ia[-1]), nb, _p(ia), _p(ja), _p(val),
+                                   ctypes.c_double(theta), coarse_dof, max_levels,
+                                   aggregation_type, max_aggregation)
+        levels, aggs = [], []
+        for l in range(nl):
+            out = (ctypes.c_int * 2)()
+            self.lib.or_bsr_level_info(l, out)
+            lia = np.empty(out[0] + 1, np.int32)
+            lja = np.empty(out[1], np.int32)
+            lval = np.empty(out[1] * nb * nb)
+            self.lib.or_bsr_level_A(l, _p(lia), _p(lja), _p(lval))
+            levels.append((lia, lja, lval))
+            if l < nl - 1:
+                agg = np.empty(out[0], np.int32)
+                self.lib.or_bsr_level_agg(l, _p(agg))
+                aggs.append(agg)
+        return levels, aggs
+
     def srand(self, seed: int) -> None:
         """Seed the oracle's restatement of the C library's rand() stream."""
         self.lib.or_srand(ctypes.c_uint(seed))

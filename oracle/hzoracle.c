@@ -961,6 +961,158 @@ int or_hec_agg(int n, const int *ia, const int *ja, const double *a, double thet
     return nc;
 }
 
+/* ---- UA-AMG setup for block (BSR) matrices --------------------------------
+ * amg_setup_unsmoothP_unsmoothR_bsr (amg_setup_ua.c:2183-2425) without the
+ * smoother data: per level while the level has more than max(coarse_dof, 50)
+ * block rows and fewer than max_levels levels exist, the condensed matrix
+ * (condenseBSRLinf, sparse.c:6223: each block's max row sum of |a|, negated
+ * off the diagonal, entries <= 1e-8 dropped as dcsr_compress_inplace does),
+ * HEM or VMB on its strength graph (no threshold adaptation on this path; an
+ * aggregation failure stops coarsening), and the block Galerkin product
+ * dbsr_rap (sparse.c:5840-5980) with identity blocks in P and R: coarse row C
+ * reserves its diagonal block (0.0, accumulated), then blocks in first-
+ * encounter order over (fine rows of R row C ascending) x (A row order); a new
+ * block takes ddense_mul's sums, which start from 0.0 (so -0.0 becomes +0.0),
+ * a known block adds them.  Blocks are nb x nb, row-major. */
+typedef struct { int nrow, nnzb; int *ia, *ja, *agg; double *val; } obsr;
+static struct { int nl, nb; obsr lv[32]; } g_bsr;
+
+static void or_bsr_free(void)
+{
+    for (int l = 0; l < g_bsr.nl; ++l) {
+        free(g_bsr.lv[l].ia); free(g_bsr.lv[l].ja); free(g_bsr.lv[l].val);
+        free(g_bsr.lv[l].agg);
+    }
+    memset(&g_bsr, 0, sizeof(g_bsr));
+}
+
+static double ddense_linf(const double *b, int nb)
+{
+    double norm = 0.0;
+    for (int r = 0; r < nb; ++r) {
+        double v = 0.0;
+        for (int c = 0; c < nb; ++c) v = v + fabs(b[r * nb + c]);
+        norm = norm > v ? norm : v;
+    }
+    return norm;
+}
+
+int or_bsr_setup(int nrow, int nnzb, int nb, const int *ia, const int *ja, const double *val,
+                 double theta, int coarse_dof, int max_levels, int agg_type, int max_agg)
+{
+    or_bsr_free();
+    const int nb2 = nb * nb;
+    const int min_cdof = coarse_dof > 50 ? coarse_dof : 50;
+    if (max_levels > 32) max_levels = 32;
+    g_bsr.nb = nb;
+    obsr *L = &g_bsr.lv[0];
+    L->nrow = nrow; L->nnzb = nnzb;
+    L->ia = (int *)malloc(sizeof(int) * (nrow + 1));
+    L->ja = (int *)malloc(sizeof(int) * (nnzb > 0 ? nnzb : 1));
+    L->val = (double *)malloc(sizeof(double) * (size_t)(nnzb > 0 ? nnzb : 1) * nb2);
+    memcpy(L->ia, ia, sizeof(int) * (nrow + 1));
+    memcpy(L->ja, ja, sizeof(int) * nnzb);
+    memcpy(L->val, val, sizeof(double) * (size_t)nnzb * nb2);
+    int lvl = 0;
+    while (g_bsr.lv[lvl].nrow > min_cdof && lvl < max_levels - 1) {
+        L = &g_bsr.lv[lvl];
+        const int m = L->nrow;
+        /* condensed matrix, compressed */
+        int *pia = (int *)malloc(sizeof(int) * (m + 1));
+        int *pja = (int *)malloc(sizeof(int) * (L->nnzb > 0 ? L->nnzb : 1));
+        double *pv = (double *)malloc(sizeof(double) * (L->nnzb > 0 ? L->nnzb : 1));
+        int q = 0;
+        pia[0] = 0;
+        for (int i = 0; i < m; ++i) {
+            for (int k = L->ia[i]; k < L->ia[i + 1]; ++k) {
+                double v = ddense_linf(L->val + (size_t)k * nb2, nb);
+                if (L->ja[k] != i) v = -v;
+                if (fabs(v) > 1e-8) { pja[q] = L->ja[k]; pv[q] = v; ++q; }
+            }
+            pia[i + 1] = q;
+        }
+        int *nia = (int *)malloc(sizeof(int) * (m + 1));
+        int *nja = (int *)malloc(sizeof(int) * (q > 0 ? q : 1));
+        double *nv = (double *)malloc(sizeof(double) * (q > 0 ? q : 1));
+        or_strength(m, pia, pja, pv, theta, nia, nja, nv);
+        L->agg = (int *)malloc(sizeof(int) * m);
+        int nc = agg_type == 1 ? or_vmb(m, nia, nja, max_agg, L->agg)
+                               : or_hem(m, nia, nja, nv, L->agg);
+        free(pia); free(pja); free(pv); free(nia); free(nja); free(nv);
+        if (nc < 1) { free(L->agg); L->agg = NULL; break; }
+        /* R pattern (fine rows ascending) and the block Galerkin product */
+        int *ria = (int *)malloc(sizeof(int) * (nc + 1));
+        int *rja = (int *)malloc(sizeof(int) * m);
+        or_trans_agg(m, nc, L->agg, ria, rja);
+        int *slot = (int *)malloc(sizeof(int) * nc);
+        for (int c = 0; c < nc; ++c) slot[c] = -1;
+        int cap = 16 * nc + 16, cnnz = 0;
+        int *cia = (int *)malloc(sizeof(int) * (nc + 1));
+        int *cja = (int *)malloc(sizeof(int) * cap);
+        double *cv = (double *)malloc(sizeof(double) * (size_t)cap * nb2);
+        for (int C = 0; C < nc; ++C) {
+            cia[C] = cnnz;
+            const int base = cnnz;
+#define OR_BSR_GROW()                                                              \
+            if (cnnz >= cap) {                                                     \
+                cap *= 2;                                                          \
+                cja = (int *)realloc(cja, sizeof(int) * cap);                      \
+                cv = (double *)realloc(cv, sizeof(double) * (size_t)cap * nb2);    \
+            }
+            OR_BSR_GROW();
+            cja[cnnz] = C; slot[C] = cnnz;
+            for (int t = 0; t < nb2; ++t) cv[(size_t)cnnz * nb2 + t] = 0.0;
+            ++cnnz;
+            for (int r1 = ria[C]; r1 < ria[C + 1]; ++r1) {
+                const int I = rja[r1];
+                for (int k = L->ia[I]; k < L->ia[I + 1]; ++k) {
+                    const int D = L->agg[L->ja[k]];
+                    if (D < 0) continue;
+                    const double *src = L->val + (size_t)k * nb2;
+                    if (slot[D] < base) {
+                        OR_BSR_GROW();
+                        slot[D] = cnnz; cja[cnnz] = D;
+                        for (int t = 0; t < nb2; ++t)
+                            cv[(size_t)cnnz * nb2 + t] = src[t] + 0.0;
+                        ++cnnz;
+                    } else {
+                        for (int t = 0; t < nb2; ++t)
+                            cv[(size_t)slot[D] * nb2 + t] += src[t] + 0.0;
+                    }
+                }
+            }
+#undef OR_BSR_GROW
+        }
+        cia[nc] = cnnz;
+        free(ria); free(rja); free(slot);
+        obsr *Cl = &g_bsr.lv[lvl + 1];
+        Cl->nrow = nc; Cl->nnzb = cnnz; Cl->ia = cia; Cl->ja = cja; Cl->val = cv;
+        ++lvl;
+    }
+    g_bsr.nl = lvl + 1;
+    return g_bsr.nl;
+}
+
+/* out: nrow, nnzb of level l */
+void or_bsr_level_info(int l, int *out)
+{
+    out[0] = g_bsr.lv[l].nrow;
+    out[1] = g_bsr.lv[l].nnzb;
+}
+
+void or_bsr_level_A(int l, int *ia, int *ja, double *val)
+{
+    const obsr *L = &g_bsr.lv[l];
+    memcpy(ia, L->ia, sizeof(int) * (L->nrow + 1));
+    memcpy(ja, L->ja, sizeof(int) * L->nnzb);
+    memcpy(val, L->val, sizeof(double) * (size_t)L->nnzb * g_bsr.nb * g_bsr.nb);
+}
+
+void or_bsr_level_agg(int l, int *agg)
+{
+    memcpy(agg, g_bsr.lv[l].agg, sizeof(int) * g_bsr.lv[l].nrow);
+}
+
 static ocsr g_rap;
 int or_rap(int n, const int *ia, const int *ja, const double *a, int nc,
            const int *agg, int *rap_ia, int *rap_ja, double *rap_val)

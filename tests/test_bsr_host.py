@@ -1,8 +1,9 @@
 """CPU checks of the block (BSR) path: the fixture matrices are what
 problems.block_system makes, the scalar expansion is the block matrix, the
-reference (where it is built here) still produces the committed hierarchy,
-and linear_solver_dbsr_krylov_amg rejects malformed input before it touches
-a device."""
+oracle's restatement of amg_setup_ua_bsr gives the reference's hierarchies
+bit for bit, the reference (where it is built here) still produces the
+committed hierarchy, and linear_solver_dbsr_krylov_amg rejects malformed
+input before it touches a device."""
 import ctypes as C
 import hashlib
 
@@ -73,6 +74,31 @@ def test_reference_still_gives_committed_hierarchy(golden):
         assert [sha(a) for a in R.bsr_level_A(l, 3)] == list(v[f"A{l}_sha"])
     np.testing.assert_array_equal(R.bsr_precond(z["kuhn/b"]), v["z"])
     R.bsr_free()
+
+
+BSR_VARIANTS = ["kuhn/gs", "kuhn/jac", "kuhn/sgs", "kuhn/w", "kuhn/cs", "kuhn/m2", "kuhn/t",
+                "kuhn/vmb", "fix/gs"]
+
+
+@pytest.mark.parametrize("key", BSR_VARIANTS)
+def test_oracle_bsr_hierarchy_matches_reference(golden, port, key):
+    """The oracle's restatement of amg_setup_ua_bsr (condensation, HEM or
+    VMB, dbsr_rap) against the reference's hierarchy digests."""
+    case = key.split("/")[0]
+    g = small_case(golden("gmres.npz"), case)
+    ia, ja, val = P.block_system(g["A_ia"], g["A_ja"], g["A_val"], NB[case], SEED[case])
+    v = small_case(golden("bsr.npz"), key)
+    ip = [int(t) for t in v["params"]]
+    levels, aggs = port.bsr_hierarchy(NB[case], ia, ja, val, theta=float(v["dparams"][0]),
+                                      coarse_dof=ip[1], max_levels=ip[0],
+                                      aggregation_type=ip[7], max_aggregation=ip[8])
+    info = v["info"]
+    assert len(levels) == len(info)
+    for l, (lia, lja, lval) in enumerate(levels):
+        assert (len(lia) - 1, len(lja)) == tuple(info[l]), l
+        assert [sha(lia), sha(lja), sha(lval)] == list(v[f"A{l}_sha"]), l
+    for l, agg in enumerate(aggs):
+        np.testing.assert_array_equal(agg, v[f"agg{l}"])
 
 
 def _mat(ia, ja, val, nb, manner=0, nnz=None):
