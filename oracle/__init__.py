@@ -234,6 +234,34 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def sa_hierarchy(self, ia, ja, val, theta=0.0, coarse_dof=2000, max_levels=20,
+                     aggregation_type=5, max_aggregation=20, smooth_filter=1,
+                     tentative_smooth=0.67, coarse_solver=32):
+        """The hierarchy of amg_setup_sa: a list of A per level, a list of the
+        smoothed P per level below the coarsest, and the adapted threshold."""
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        th = ctypes.c_double()
+        nl = self.lib.or_sa_setup(len(ia) - 1, int(ia[-1]), _p(ia), _p(ja), _p(val),
+                                  ctypes.c_double(theta), coarse_dof, max_levels,
+                                  aggregation_type, max_aggregation, int(smooth_filter == 1),
+                                  ctypes.c_double(tentative_smooth), coarse_solver,
+                                  ctypes.byref(th))
+        As, Ps = [], []
+        for l in range(nl):
+            out = (ctypes.c_int * 3)()
+            self.lib.or_sa_level_info(l, out)
+            a = (np.empty(out[0] + 1, np.int32), np.empty(out[1], np.int32), np.empty(out[1]))
+            self.lib.or_sa_level_A(l, *(_p(x) for x in a))
+            As.append(a)
+            if l < nl - 1:
+                pp = (np.empty(out[0] + 1, np.int32), np.empty(out[2], np.int32),
+                      np.empty(out[2]))
+                self.lib.or_sa_level_P(l, *(_p(x) for x in pp))
+                Ps.append(pp)
+        return As, Ps, th.value
+
     def bsr_hierarchy(self, nb, ia, ja, val, theta=0.0, coarse_dof=2000, max_levels=20,
                       aggregation_type=5, max_aggregation=20):
         """The block hierarchy of amg_setup_ua_bsr: a list of (ia, ja, val) per

@@ -1113,6 +1113,207 @@ void or_bsr_level_agg(int l, int *agg)
     memcpy(agg, g_bsr.lv[l].agg, sizeof(int) * g_bsr.lv[l].nrow);
 }
 
+/* ---- smoothed aggregation: amg_setup_smoothP_smoothR ---------------------
+ * (amg_setup_ua.c:1461-1700) -- the aggregates of the UA setup (same adaptive
+ * threshold), P = S P_tent with S = I - omega D^{-1} N (smooth_aggregation_p,
+ * :472-560: N the strength graph with its diagonal corrected by the dropped
+ * row sum when smooth_filter is on, else A; D its first diagonal entries,
+ * |d| < 1e-6 -> 1; S's diagonal 1 - omega n_ii / d_i, off-diagonal
+ * (-omega) n_ij / d_i), dcsr_mxm (sparse.c:1832-1917: columns in first-
+ * encounter order, each value summed from 0.0 in (S entry, P entry) order),
+ * R = P^T (dcsr_trans, rows ascending), A_c = dcsr_rap (sparse.c:2401-2520:
+ * diagonal slot first from 0.0, new columns in first-encounter order, values
+ * (r a) p added in traversal order; a fine column seen before in the coarse
+ * row only adds).  With the direct coarse solver the coarsest matrix is
+ * replaced by its transpose (:1631-1640). */
+static struct { int nl; ocsr A[32], P[32]; } g_sa;
+
+static void or_sa_free(void)
+{
+    for (int l = 0; l < 32; ++l) { ocsr_free(&g_sa.A[l]); ocsr_free(&g_sa.P[l]); }
+    g_sa.nl = 0;
+}
+
+/* dcsr_trans of an n x m CSR with values: rows of T list rows of A ascending */
+static void or_trans_full(int n, int m, const int *ia, const int *ja, const double *v,
+                          ocsr *T)
+{
+    const int nnz = ia[n];
+    T->n = m; T->m = n; T->nnz = nnz;
+    T->ia = (int *)calloc(m + 1, sizeof(int));
+    T->ja = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    T->val = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    for (int k = 0; k < nnz; ++k) T->ia[ja[k] + 1]++;
+    for (int c = 0; c < m; ++c) T->ia[c + 1] += T->ia[c];
+    int *pos = (int *)malloc(sizeof(int) * (m > 0 ? m : 1));
+    memcpy(pos, T->ia, sizeof(int) * m);
+    for (int i = 0; i < n; ++i)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+            int q = pos[ja[k]]++;
+            T->ja[q] = i; T->val[q] = v[k];
+        }
+    free(pos);
+}
+
+int or_sa_setup(int n, int nnz, const int *ia, const int *ja, const double *val,
+                double theta, int coarse_dof, int max_levels, int agg_type, int max_agg,
+                int filter, double omega, int csolver, double *theta_out)
+{
+    or_sa_free();
+    if (max_levels > 32) max_levels = 32;
+    const int min_cdof = coarse_dof > 1 ? coarse_dof : 1;
+    ocsr *A0 = &g_sa.A[0];
+    A0->n = A0->m = n; A0->nnz = nnz;
+    A0->ia = (int *)malloc(sizeof(int) * (n + 1));
+    A0->ja = (int *)malloc(sizeof(int) * nnz);
+    A0->val = (double *)malloc(sizeof(double) * nnz);
+    memcpy(A0->ia, ia, sizeof(int) * (n + 1));
+    memcpy(A0->ja, ja, sizeof(int) * nnz);
+    memcpy(A0->val, val, sizeof(double) * nnz);
+    int lvl = 0;
+    while (g_sa.A[lvl].n > min_cdof && lvl < max_levels - 1) {
+        ocsr *A = &g_sa.A[lvl];
+        const int m = A->n;
+        int *nia = (int *)malloc(sizeof(int) * (m + 1));
+        int *nja = (int *)malloc(sizeof(int) * (A->nnz > 0 ? A->nnz : 1));
+        double *nv = (double *)malloc(sizeof(double) * (A->nnz > 0 ? A->nnz : 1));
+        or_strength(m, A->ia, A->ja, A->val, theta, nia, nja, nv);
+        int *agg = (int *)malloc(sizeof(int) * m);
+        int nc = agg_type == 1 ? or_vmb(m, nia, nja, max_agg, agg)
+                               : or_hem(m, nia, nja, nv, agg);
+        if (nc * 4 > m) theta /= 2;
+        else if (nc * 1.25 < m) theta *= 2;
+        if (nc < 1) { free(nia); free(nja); free(nv); free(agg); break; }
+        /* the smoother's matrix: the filtered strength graph, or A */
+        const int *sia = A->ia, *sja = A->ja;
+        const double *sv = A->val;
+        if (filter) {
+            for (int i = 0; i < m; ++i) {
+                double rsa = 0.0, rsn = 0.0;
+                for (int k = A->ia[i]; k < A->ia[i + 1]; ++k)
+                    if (A->ja[k] != i) rsa += A->val[k];
+                for (int k = nia[i]; k < nia[i + 1]; ++k)
+                    if (nja[k] != i) rsn += nv[k];
+                for (int k = nia[i]; k < nia[i + 1]; ++k)
+                    if (nja[k] == i) nv[k] += rsa - rsn;
+            }
+            sia = nia; sja = nja; sv = nv;
+        }
+        double *d = (double *)malloc(sizeof(double) * m);
+        or_getdiag(m, sia, sja, sv, d);
+        for (int i = 0; i < m; ++i) if (fabs(d[i]) < 1e-6) d[i] = 1.0;
+        const int snnz = sia[m];
+        double *S = (double *)malloc(sizeof(double) * (snnz > 0 ? snnz : 1));
+        for (int i = 0; i < m; ++i)
+            for (int k = sia[i]; k < sia[i + 1]; ++k)
+                S[k] = sja[k] == i ? 1 - omega * sv[k] / d[i] : -omega * sv[k] / d[i];
+        /* P = S P_tent: a column per aggregate met, first encounter first */
+        ocsr *P = &g_sa.P[lvl];
+        P->n = m; P->m = nc;
+        P->ia = (int *)malloc(sizeof(int) * (m + 1));
+        int pcap = snnz > 0 ? snnz : 1, q = 0;
+        P->ja = (int *)malloc(sizeof(int) * pcap);
+        P->val = (double *)malloc(sizeof(double) * pcap);
+        for (int i = 0; i < m; ++i) {
+            P->ia[i] = q;
+            for (int k = sia[i]; k < sia[i + 1]; ++k) {
+                const int c = agg[sja[k]];
+                if (c < 0) continue;
+                int j = P->ia[i];
+                while (j < q && P->ja[j] != c) ++j;
+                if (j == q) { P->ja[q] = c; P->val[q] = 0.0; ++q; }
+            }
+            for (int j = P->ia[i]; j < q; ++j)
+                for (int k = sia[i]; k < sia[i + 1]; ++k)
+                    if (agg[sja[k]] == P->ja[j]) P->val[j] += S[k] * 1.0;
+        }
+        P->ia[m] = q; P->nnz = q;
+        free(S); free(d); free(nia); free(nja); free(nv); free(agg);
+        /* R = P^T, A_c = R A P */
+        ocsr R;
+        or_trans_full(m, nc, P->ia, P->ja, P->val, &R);
+        ocsr *Ac = &g_sa.A[lvl + 1];
+        int *ps = (int *)malloc(sizeof(int) * nc);
+        int *as = (int *)malloc(sizeof(int) * m);
+        for (int c = 0; c < nc; ++c) ps[c] = -1;
+        for (int i = 0; i < m; ++i) as[i] = -1;
+        int ccap = 64 + 8 * nc, cc = 0;
+        Ac->n = Ac->m = nc;
+        Ac->ia = (int *)malloc(sizeof(int) * (nc + 1));
+        Ac->ja = (int *)malloc(sizeof(int) * ccap);
+        Ac->val = (double *)malloc(sizeof(double) * ccap);
+        for (int ic = 0; ic < nc; ++ic) {
+            const int row0 = cc;
+            Ac->ia[ic] = cc;
+            if (cc >= ccap) {
+                ccap *= 2;
+                Ac->ja = (int *)realloc(Ac->ja, sizeof(int) * ccap);
+                Ac->val = (double *)realloc(Ac->val, sizeof(double) * ccap);
+            }
+            ps[ic] = cc; Ac->ja[cc] = ic; Ac->val[cc] = 0.0; ++cc;
+            for (int j1 = R.ia[ic]; j1 < R.ia[ic + 1]; ++j1) {
+                const double re = R.val[j1];
+                const int i1 = R.ja[j1];
+                for (int j2 = A->ia[i1]; j2 < A->ia[i1 + 1]; ++j2) {
+                    const double ra = re * A->val[j2];
+                    const int i2 = A->ja[j2];
+                    const int first = as[i2] != ic;
+                    as[i2] = ic;
+                    for (int j3 = P->ia[i2]; j3 < P->ia[i2 + 1]; ++j3) {
+                        const double rap = ra * P->val[j3];
+                        const int i3 = P->ja[j3];
+                        if (first && ps[i3] < row0) {
+                            if (cc >= ccap) {
+                                ccap *= 2;
+                                Ac->ja = (int *)realloc(Ac->ja, sizeof(int) * ccap);
+                                Ac->val = (double *)realloc(Ac->val, sizeof(double) * ccap);
+                            }
+                            ps[i3] = cc; Ac->ja[cc] = i3; Ac->val[cc] = rap; ++cc;
+                        } else {
+                            Ac->val[ps[i3]] += rap;
+                        }
+                    }
+                }
+            }
+        }
+        Ac->ia[nc] = cc; Ac->nnz = cc;
+        free(ps); free(as); ocsr_free(&R);
+        ++lvl;
+    }
+    g_sa.nl = lvl + 1;
+    if (csolver == 32) {
+        ocsr *C = &g_sa.A[lvl], T;
+        or_trans_full(C->n, C->n, C->ia, C->ja, C->val, &T);
+        ocsr_free(C);
+        *C = T;
+    }
+    if (theta_out) *theta_out = theta;
+    return g_sa.nl;
+}
+
+/* out: rows, stored entries of A, and of P (0 on the coarsest level) */
+void or_sa_level_info(int l, int *out)
+{
+    out[0] = g_sa.A[l].n; out[1] = g_sa.A[l].nnz;
+    out[2] = l < g_sa.nl - 1 ? g_sa.P[l].nnz : 0;
+}
+
+void or_sa_level_A(int l, int *ia, int *ja, double *val)
+{
+    const ocsr *A = &g_sa.A[l];
+    memcpy(ia, A->ia, sizeof(int) * (A->n + 1));
+    memcpy(ja, A->ja, sizeof(int) * A->nnz);
+    memcpy(val, A->val, sizeof(double) * A->nnz);
+}
+
+void or_sa_level_P(int l, int *ia, int *ja, double *val)
+{
+    const ocsr *P = &g_sa.P[l];
+    memcpy(ia, P->ia, sizeof(int) * (P->n + 1));
+    memcpy(ja, P->ja, sizeof(int) * P->nnz);
+    memcpy(val, P->val, sizeof(double) * P->nnz);
+}
+
 static ocsr g_rap;
 int or_rap(int n, const int *ia, const int *ja, const double *a, int nc,
            const int *agg, int *rap_ia, int *rap_ja, double *rap_val)
