@@ -1214,19 +1214,20 @@ int or_sa_setup(int n, int nnz, const int *ia, const int *ja, const double *val,
         int pcap = snnz > 0 ? snnz : 1, q = 0;
         P->ja = (int *)malloc(sizeof(int) * pcap);
         P->val = (double *)malloc(sizeof(double) * pcap);
+        /* each column's sum gets its products in S-row order, as dcsr_mxm's
+         * per-entry loop over the row gives them */
+        int *cslot = (int *)malloc(sizeof(int) * nc);
+        for (int c = 0; c < nc; ++c) cslot[c] = -1;
         for (int i = 0; i < m; ++i) {
             P->ia[i] = q;
             for (int k = sia[i]; k < sia[i + 1]; ++k) {
                 const int c = agg[sja[k]];
                 if (c < 0) continue;
-                int j = P->ia[i];
-                while (j < q && P->ja[j] != c) ++j;
-                if (j == q) { P->ja[q] = c; P->val[q] = 0.0; ++q; }
+                if (cslot[c] < P->ia[i]) { cslot[c] = q; P->ja[q] = c; P->val[q] = 0.0; ++q; }
+                P->val[cslot[c]] += S[k] * 1.0;
             }
-            for (int j = P->ia[i]; j < q; ++j)
-                for (int k = sia[i]; k < sia[i + 1]; ++k)
-                    if (agg[sja[k]] == P->ja[j]) P->val[j] += S[k] * 1.0;
         }
+        free(cslot);
         P->ia[m] = q; P->nnz = q;
         free(S); free(d); free(nia); free(nja); free(nv); free(agg);
         /* R = P^T, A_c = R A P */
