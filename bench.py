@@ -30,6 +30,13 @@ amg_setup_ua_bsr (HEM, coarse_dof 100) + CG preconditioned by
 precond_dbsr_amg (block Gauss-Seidel V(1,1), coarsest level by GMRES(25)) to
 1e-8; the reference's BSR solver on the same system is the CPU baseline.
 
+--variant NAME (workloads c1, c2) times one of the drop-in's other
+configurations instead, FP64 as linear_solver_dcsr_krylov_amg runs it: the
+W, AMLI, nonlinear AMLI and additive cycles, GMRES / flexible GMRES /
+MINRES, smoothed aggregation, VMB aggregation (table VARIANTS); one step =
+setup + solve to 1e-8, the reference running the same configuration beside
+it.
+
 Workload c3: 512 independent SPD systems (2D/3D anisotropic P1 diffusion,
 1k-200k dofs log-uniform, seed 11) solved together (hzb_batch_*); one step
 = batch setup + batch solve; reports the batch time and the p50/p99 of the
@@ -91,10 +98,24 @@ def workload(name: str):
     return kuhn_case(*CASES[name])
 
 
-def cpu_sample(name: str):
+def cpu_sample(name: str, variant: str = ""):
     """The bounded CPU sample of a workload and its scale to the full one:
     the 128^3 instance of the same family for c5 (about 30 s single-threaded),
-    the workload itself otherwise."""
+    for smoothed aggregation (whose coarse levels fill in) the 127^2 Poisson
+    problem for c1 and the 32^3 Kuhn instance for c2, the workload itself
+    otherwise."""
+    if variant == "sa" and name in ("c1", "c2"):
+        if name == "c1":
+            ia, ja, val = P.poisson2d_5pt(127)
+            b = P.rhs_uniform(len(ia) - 1, 1)
+            what = "2D Poisson 127^2 dofs (16,129)"
+        else:
+            ia, ja, val, b, _ = kuhn_case(32, 1.0, (2, 3))
+            what = "the 32^3-cube instance (29,791 dofs)"
+        full = 65025 if name == "c1" else 2048383
+        scale = full / (len(ia) - 1)
+        return ia, ja, val, b, scale, (f"reference setup+solve of {what}, scaled by the "
+                                       f"dof ratio {scale:.2f}")
     if name == "c5":
         N, sigma, seeds = CASES["c5"]
         ia, ja, val, b, _ = kuhn_case(128, sigma, seeds)
@@ -175,6 +196,154 @@ def time_reference(ia, ja, val, b):
     return t, int(it), kind
 
 
+# --variant: (what, AMG_param fields over the survey setting, Krylov method)
+VARIANTS = {
+    "w": ("W-cycle, PCG", dict(cycle_type=2), "pcg"),
+    "amli": ("AMLI cycle of degree 2, PCG", dict(cycle_type=3), "pcg"),
+    "nlamli": ("nonlinear AMLI cycle (flexible GMRES on the coarse levels), "
+               "flexible GMRES(100)", dict(cycle_type=4), "fgmres"),
+    "add": ("additive cycle, flexible GMRES(100)", dict(cycle_type=5), "fgmres"),
+    "gmres": ("V-cycle, GMRES(25)", {}, "gmres"),
+    "fgmres": ("V-cycle, flexible GMRES(100)", {}, "fgmres"),
+    "minres": ("V-cycle, MINRES", {}, "minres"),
+    "sa": ("smoothed aggregation, V-cycle, PCG", dict(AMG_type=2), "pcg"),
+    "vmb": ("VMB aggregation, V-cycle, PCG", dict(aggregation_type=1), "pcg"),
+}
+KRYLOV_TYPE = {"pcg": 1, "minres": 2, "gmres": 3, "fgmres": 4}
+RESTART = {"gmres": 25, "fgmres": 100}
+
+
+def variant_metric(name):
+    return (f"UA-AMG drop-in, {VARIANTS[name][0]}: time to 1e-8 FP64 residual "
+            f"(setup + solve)")
+
+
+def time_reference_variant(ia, ja, val, b, name):
+    """One setup + solve of a variant by the reference compiled from its
+    sources, single-threaded."""
+    import oracle
+    _, over, method = VARIANTS[name]
+    R = oracle.ref()
+    prm = oracle.AMGParams(amli_degree=2, nl_amli_krylov_type=4, **over)
+    t0 = time.perf_counter()
+    assert R.setup(ia, ja, val, prm) == 0
+    if method == "pcg":
+        it = R.pcg(b, None, 1e-8, 500, 1)[0]
+    elif method == "minres":
+        it = R.minres(b, tol=1e-8, maxit=500)[0]
+    else:
+        it = R.gmres(b, tol=1e-8, maxit=500, restart=RESTART[method],
+                     flexible=method == "fgmres")[0]
+    t = time.perf_counter() - t0
+    R.free()
+    return t, int(it), "reference"
+
+
+def run_variant(args, rank, world, local, dist):
+    import torch
+    import hazmath_b200 as hz
+    name = args.variant
+    what, over, method = VARIANTS[name]
+    ia, ja, val, b, desc = workload(args.workload)
+    n, nnz = len(b), int(ia[-1])
+    dev = f"cuda:{local}"
+    dia, dja = torch.from_numpy(ia).to(dev), torch.from_numpy(ja).to(dev)
+    dval, db = torch.from_numpy(val).to(dev), torch.from_numpy(b).to(dev)
+    dx = torch.zeros_like(db)
+    p = lambda t: t.data_ptr()  # noqa: E731
+    amg = hz.survey_amg(amli_degree=2, nl_amli_krylov_type=4, **over)
+    it_par = hz.itsolver_param(linear_itsolver_type=KRYLOV_TYPE[method],
+                               linear_precond_type=hz.PREC_AMG, linear_tol=1e-8,
+                               linear_maxit=500, linear_stop_type=hz.STOP_REL_RES,
+                               linear_restart=RESTART.get(method, 100))
+
+    def check(rc, what_):
+        if rc < 0:
+            raise RuntimeError(f"{what_} failed {rc}: {hz.last_error()}")
+        return rc
+
+    S = hz.Solver(amg, it_par, hz.b200_param(device=local))
+
+    def step():
+        dx.zero_()
+        check(S.setup_device(n, nnz, p(dia), p(dja), p(dval)), "setup")
+        return check(S.solve_device(p(db), p(dx)), "solve")
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    setup_s, solve_s, launches, iters = [], [], 0, 0
+    ev0.record()
+    for _ in range(args.steps):
+        iters = step()
+        st = S.stats()
+        setup_s.append(st.setup_seconds)
+        solve_s.append(st.solve_seconds)
+        launches += st.launches
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_s = max_over_ranks(dist, ev0.elapsed_time(ev1) * 1e-3 / args.steps, dev)
+    x = dx.cpu().numpy()
+    import scipy.sparse as sp
+    A = sp.csr_matrix((val, ja, ia), shape=(n, n))
+    relres = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+    peak, peak_kind = hbm_peak()
+    sp_ms, sp_by = S.time_kernel(hz.HZB_K_SPMV64, 0, 50)
+    sp_gbs = sp_by / (sp_ms * 1e-3) / 1e9
+    Se = hz.Solver(amg, it_par, hz.b200_param(device=local))
+    xh = np.zeros(n)
+    e2e = []
+    for k in range(1 + min(args.steps, 3)):
+        xh[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        check(Se.setup_host(ia, ja, val), "setup_host")
+        check(Se.solve_host(b, xh), "solve_host")
+        if k:
+            e2e.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(dist, statistics.mean(e2e), dev)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            sia, sja, sval, sb, scale, sample = cpu_sample(args.workload, name)
+            t, it_ref, kind = time_reference_variant(sia, sja, sval, sb, name)
+            cpu = {"value": t * scale, "unit": "s", "cores": 1, "kind": kind,
+                   "sample": f"{sample} ({it_ref} iterations)"}
+    if rank == 0:
+        line = {
+            "metric": variant_metric(name), "value": step_s, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": dict(desc, variant=name, solver=what, parallelism="replicas",
+                           l2="inputs larger than L2 (no flush)" if nnz > 10_000_000
+                           else "inputs smaller than L2, resident between steps"),
+            "iterations": int(iters), "final_relres": relres,
+            "setup_s": statistics.mean(setup_s), "solve_s": statistics.mean(solve_s),
+            "roofline": {"bound": "hbm", "kernel": "level-0 FP64 SpMV of the drop-in "
+                         "(k_spmv_bundle<double>)", "achieved": sp_gbs, "peak": peak,
+                         "unit": "GB/s", "frac": sp_gbs / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": sp_by, "ms_per_launch": sp_ms,
+                         "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s",
+                    "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + val.nbytes + b.nbytes
+                                              + xh.nbytes),
+                    "d2h_bytes_per_step": int(xh.nbytes)},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    S.close()
+    Se.close()
+
+
 BSR_NB = 3
 
 
@@ -202,6 +371,35 @@ def time_reference_bsr(ia, ja, val, b):
 
 def run_reference(args):
     name = args.workload
+    if args.variant:
+        import oracle
+        if not oracle.ref_available():
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference library (oracle/_ref) was not built"}))
+            return
+        wia, wja, wval, wb, _ = kuhn_case(12, 1.0, (2, 3))
+        sia, sja, sval, sb, scale, sample = cpu_sample(name, args.variant)
+        times, iters = [], 0
+        for step in range(args.warmup + args.steps):
+            if step < args.warmup:   # the same code on a small instance, untimed
+                time_reference_variant(wia, wja, wval, wb, args.variant)
+                continue
+            t, iters, _ = time_reference_variant(sia, sja, sval, sb, args.variant)
+            times.append(t * scale)
+        v = statistics.mean(times)
+        line = {"metric": variant_metric(args.variant), "value": v, "unit": "s",
+                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "iterations": int(iters),
+                "config": dict(workload_desc(name), variant=args.variant,
+                               solver=VARIANTS[args.variant][0]),
+                "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
     if name == "bsr":
         import oracle
         if not oracle.ref_available():
@@ -297,8 +495,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c5", choices=["c1", "c2", "c5", "c3", "bsr"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", default="", choices=[""] + sorted(VARIANTS))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.variant and args.workload not in ("c1", "c2"):
+        ap.error("--variant runs on the c1 and c2 workloads")
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -317,7 +518,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if args.workload == "c3":
+        if args.variant:
+            run_variant(args, rank, world, local, dist)
+        elif args.workload == "c3":
             run_batch(args, rank, world, local, dist)
         elif args.workload == "bsr":
             run_bsr(args, rank, world, local, dist)

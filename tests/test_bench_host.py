@@ -1,0 +1,52 @@
+"""bench.py's reference arm and argument checks on CPU: the JSON line of the
+contract (metric, value, unit, impl, cpu_baseline, e2e) for a --variant of
+the drop-in and for the bsr workload, and the variants' workload rule."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+import oracle
+from conftest import ROOT
+
+KEYS = {"metric", "value", "unit", "impl", "n_gpus", "steps", "warmup", "ms_per_step",
+        "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+        "cpu_baseline", "e2e"}
+
+
+def _bench(*args, timeout=600):
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT,
+                          capture_output=True, text=True, timeout=timeout)
+
+
+def _line(r):
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    return json.loads(lines[0])
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("variant", ["gmres", "w"])
+def test_reference_arm_variant_line(variant):
+    d = _line(_bench("--impl", "reference", "--workload", "c1", "--variant", variant,
+                     "--steps", "1", "--warmup", "3"))
+    assert KEYS <= set(d)
+    assert d["impl"] == "reference" and d["config"]["variant"] == variant
+    assert d["value"] > 0 and d["iterations"] > 0
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["cores"] == 1
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_reference_arm_bsr_line():
+    d = _line(_bench("--impl", "reference", "--workload", "bsr", "--steps", "1",
+                     "--warmup", "3"))
+    assert KEYS <= set(d)
+    assert d["iterations"] == 9 and d["config"]["dofs"] == 750141
+
+
+def test_variant_needs_c1_or_c2():
+    r = _bench("--impl", "reference", "--workload", "c5", "--variant", "gmres", timeout=120)
+    assert r.returncode == 2 and "c1 and c2" in r.stderr
