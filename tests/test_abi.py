@@ -87,3 +87,24 @@ def test_amg_data_create_free(lib):
     assert mgl[0].max_levels == 5 and mgl[4].max_levels == 5 and mgl[0].num_levels == 0
     p = hz.amg_param()
     lib.amg_data_free(mgl, C.byref(p))
+
+
+def test_entry_points_fail_loudly_without_a_device(lib):
+    """On a machine without a usable GPU the drop-in entry points return
+    ERROR_SOLVER_MISC with the CUDA error text: there is no CPU path to fall
+    back on."""
+    import numpy as np
+    import torch
+    from hazmath_b200 import problems as P
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    ia, ja, val = P.poisson2d_5pt(16)
+    b = np.ones(len(ia) - 1)
+    x = np.zeros_like(b)
+    it = hz.itsolver_param(linear_itsolver_type=hz.SOLVER_CG)
+    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.survey_amg()) == \
+        hz.ERROR_SOLVER_MISC
+    assert "CUDA" in hz.last_error()
+    assert hz.linear_solver_dbsr_krylov_amg(1, ia, ja, val, b, x, it, hz.survey_amg()) == \
+        hz.ERROR_SOLVER_MISC
+    assert not x.any()
