@@ -340,7 +340,7 @@ struct BsrLevel {
 struct BsrHier {
     std::vector<BsrLevel> lv;
     int nl = 0, nb = 1;
-    KrylovWork kwc;   // coarse GMRES runs on its own scratch
+    KrylovWork kwc;   // inner products of the coarse scaling (level-0 length)
     void release() {
         for (auto &L : lv) L.release();
         lv.clear();
