@@ -234,6 +234,18 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def precond_cycle(self, kind, r, coef=None, tol=1e-6):
+        """z = B r with maxit AMLI (kind 3, polynomial coefficients coef) or
+        additive (kind 5) cycles of the last setup's hierarchy."""
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros_like(r)
+        c = np.ascontiguousarray(coef if coef is not None else [1.0], np.float64)
+        rc = self.lib.or_precond_cycle(kind, _p(c), len(c) - 1, ctypes.c_double(tol), _p(r),
+                                       _p(z))
+        if rc:
+            raise ValueError(f"cycle kind {kind}: {rc}")
+        return z
+
     def sa_hierarchy(self, ia, ja, val, theta=0.0, coarse_dof=2000, max_levels=20,
                      aggregation_type=5, max_aggregation=20, smooth_filter=1,
                      tentative_smooth=0.67, coarse_solver=32):

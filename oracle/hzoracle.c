@@ -586,6 +586,7 @@ void or_set_omega(const float *omega) { g_or.omega = omega; }
 static int or_pcg_core(const ocsr *A, const double *b, double *u, int use_pc,
                        double tol, int maxit, int stop_type, double *hist,
                        int hist_cap, int *nhist);
+static double or_dot(int n, const double *x, const double *y);
 
 /* coarse_itsolver mgcycle.c:34-52: unpreconditioned CG to ctol, maxit 20n */
 static void or_coarse_cg(const ocsr *A, const double *b, double *x, double ctol)
@@ -662,6 +663,124 @@ void or_cycle_from(int l0, const double *b, double *x)
         or_mgcycle_from(l0);
     }
     memcpy(x, g_or.x[l0], sizeof(double) * m);
+}
+
+/* the coarsest-level solve of the recursive cycles: the direct solver, or
+ * coarse_itsolver to ctol */
+static void or_coarse_solve(int l, double ctol)
+{
+    ocsr *C = &g_or.A[l];
+    if (g_or.coarse_solver == 32) or_chol_solve(C->n, g_or.Lc, g_or.b[l], g_or.x[l]);
+    else or_coarse_cg(C, g_or.b[l], g_or.x[l], ctol);
+}
+
+/* sum_i x_i (A x)_i, dcsr_vmv sparse.c:1797-1815 */
+static double or_vmv(const ocsr *A, const double *x)
+{
+    double den = 0.0;
+    for (int i = 0; i < A->n; ++i) {
+        double t = 0.0;
+        for (int k = A->ia[i]; k < A->ia[i + 1]; ++k) t += A->val[k] * x[A->ja[k]];
+        den += x[i] * t;
+    }
+    return den;
+}
+
+/* amli mgcycle.c:430-555 from `level` with b, x of that level in place:
+ * smoothing, residual, restriction, then degree + 1 recursive coarse cycles
+ * combined by the polynomial's coefficients (b1 = A1 e1 + (c_{d-i}/c_d) r1),
+ * e1 scaled by c_d, optional scaling alpha <= 2, prolongation, smoothing.
+ * r1[l] keeps the restricted residual of level l. */
+static double *g_r1[OR_MAXLVL];
+
+static void or_amli(int level, const double *coef, int degree, double tol)
+{
+    or_amg *G = &g_or;
+    ocsr *A0 = &G->A[level];
+    if (level >= G->nl - 1) { or_coarse_solve(level, tol * 1e-4); return; }
+    ocsr *A1 = &G->A[level + 1];
+    const int m0 = A0->n, m1 = A1->n;
+    double *b0 = G->b[level], *e0 = G->x[level], *r = G->w[level];
+    double *b1 = G->b[level + 1], *e1 = G->x[level + 1];
+    double *r1 = g_r1[level + 1];
+    or_smooth(G->smoother, 1, G->pre, G->relaxation, m0, A0->ia, A0->ja, A0->val, b0, e0,
+              level == 0 ? G->omega : NULL);
+    memcpy(r, b0, sizeof(double) * m0);
+    or_aAxpy(-1.0, m0, A0->ia, A0->ja, A0->val, e0, r);
+    or_restrict(G->nc[level], G->ria[level], G->rja[level], r, b1);
+    memcpy(r1, b1, sizeof(double) * m1);
+    for (int i = 1; i <= degree; ++i) {
+        memset(e1, 0, sizeof(double) * m1);
+        or_amli(level + 1, coef, degree, tol);
+        or_mxv(m1, A1->ia, A1->ja, A1->val, e1, b1);
+        const double c = coef[degree - i] / coef[degree];   /* array_axpy array.c:357 */
+        if (c == 1.0) for (int k = 0; k < m1; ++k) b1[k] += r1[k];
+        else if (c == -1.0) for (int k = 0; k < m1; ++k) b1[k] -= r1[k];
+        else for (int k = 0; k < m1; ++k) b1[k] += c * r1[k];
+    }
+    memset(e1, 0, sizeof(double) * m1);
+    or_amli(level + 1, coef, degree, tol);
+    for (int k = 0; k < m1; ++k) e1[k] *= coef[degree];   /* array_ax */
+    double alpha = 1.0;
+    if (G->coarse_scaling == 1) {
+        alpha = or_dot(m1, e1, r1) / or_vmv(A1, e1);
+        if (alpha > 2.0) alpha = 2.0;
+    }
+    or_prolong(alpha, m0, G->agg[level], e1, e0);
+    or_smooth(G->smoother, 0, G->post, G->relaxation, m0, A0->ia, A0->ja, A0->val, b0, e0,
+              level == 0 ? G->omega : NULL);
+}
+
+/* mgcycle_add mgcycle.c:700-820: the fine residual first (from x), then on
+ * every level smoothing and restriction of the fine residual / the level's
+ * b, the coarsest solve, and prolongations only (no post-smoothing) */
+static void or_add_cycle(double tol)
+{
+    or_amg *G = &g_or;
+    const int nl = G->nl;
+    ocsr *A0 = &G->A[0];
+    memcpy(G->w[0], G->b[0], sizeof(double) * A0->n);
+    or_aAxpy(-1.0, A0->n, A0->ia, A0->ja, A0->val, G->x[0], G->w[0]);
+    int l = 0;
+    while (l < nl - 1) {
+        ocsr *A = &G->A[l];
+        or_smooth(G->smoother, 1, G->pre, G->relaxation, A->n, A->ia, A->ja, A->val,
+                  G->b[l], G->x[l], l == 0 ? G->omega : NULL);
+        or_restrict(G->nc[l], G->ria[l], G->rja[l], l == 0 ? G->w[0] : G->b[l], G->b[l + 1]);
+        ++l;
+        memset(G->x[l], 0, sizeof(double) * G->A[l].n);
+    }
+    or_coarse_solve(nl - 1, tol * 1e-2);
+    while (l > 0) {
+        --l;
+        double alpha = 1.0;
+        if (G->coarse_scaling == 1) {
+            ocsr *Ac = &G->A[l + 1];
+            alpha = or_dot(Ac->n, G->x[l + 1], G->b[l + 1]) / or_vmv(Ac, G->x[l + 1]);
+            if (alpha > 2.0) alpha = 2.0;
+        }
+        or_prolong(alpha, G->A[l].n, G->agg[l], G->x[l + 1], G->x[l]);
+    }
+}
+
+/* precond_amli / precond_amg_add precond.c:232-250, 336-355: maxit cycles
+ * of the kind (3 AMLI, 5 additive) from x = 0 on b = r */
+int or_precond_cycle(int kind, const double *coef, int degree, double tol, const double *r,
+                     double *z)
+{
+    const int m = g_or.A[0].n;
+    if (kind != 3 && kind != 5) return -1;
+    for (int l = 1; l < g_or.nl; ++l)
+        g_r1[l] = (double *)malloc(sizeof(double) * (g_or.A[l].n > 0 ? g_or.A[l].n : 1));
+    memcpy(g_or.b[0], r, sizeof(double) * m);
+    memset(g_or.x[0], 0, sizeof(double) * m);
+    for (int i = 0; i < g_or.amg_maxit; ++i) {
+        if (kind == 3) or_amli(0, coef, degree, tol);
+        else or_add_cycle(tol);
+    }
+    memcpy(z, g_or.x[0], sizeof(double) * m);
+    for (int l = 1; l < g_or.nl; ++l) { free(g_r1[l]); g_r1[l] = NULL; }
+    return 0;
 }
 
 int or_hier_level(int l, int *n, const int **ia, const int **ja, const double **a,

@@ -51,3 +51,38 @@ def test_cycle_fixture_covers_every_variant(golden):
             v = small_case(z, f"{case}/{var}")
             assert int(v["params"][2]) in (3, 4, 5)
             assert "pcg/iters" in v and "fgmres/iters" in v and "gcg/iters" in v
+
+
+ORACLE_CYCLES = [("fix", "a2"), ("fix", "d"), ("kuhn", "a1"), ("kuhn", "a2"), ("kuhn", "a3"),
+                 ("kuhn", "a2s"), ("kuhn", "a2i"), ("kuhn", "a2d"), ("kuhn", "d"),
+                 ("kuhn", "ds"), ("kuhn", "di")]
+
+
+@pytest.mark.parametrize("case,var", ORACLE_CYCLES)
+def test_oracle_amli_and_additive_cycles_match_reference(golden, port, case, var):
+    """The oracle's restatement of amli / mgcycle_add (oracle/hzoracle.c
+    or_amli, or_add_cycle) against one application of the reference's
+    precond_amli / precond_amg_add: bit for bit with the iterative coarse
+    solver, to 1e-13 of max |z| with the direct one (dense Cholesky here,
+    the reference's sparse LDL^T there)."""
+    import oracle
+    A = small_case(golden("gmres.npz"), case)
+    z = golden("cycles.npz")
+    v = small_case(z, f"{case}/{var}")
+    names = ["max_levels", "coarse_dof", "cycle_type", "smoother", "presmooth_iter",
+             "postsmooth_iter", "coarse_solver", "aggregation_type", "max_aggregation",
+             "coarse_scaling", "print_level", "maxit", "amli_degree", "nl_amli_krylov_type"]
+    ip = [int(t) for t in v["params"]]
+    dp = [float(t) for t in v["dparams"]]
+    kw = dict(zip(names, ip[:14]))
+    kw.update(strong_coupled=dp[0], relaxation=dp[1], tol=dp[2])
+    prm = oracle.AMGParams(**kw)
+    assert port.setup(A["A_ia"], A["A_ja"], A["A_val"], prm) == 0
+    assert port.num_levels() == int(v["levels"])
+    kind = 3 if var.startswith("a") else 5
+    coef = z[f"amli_coef/{prm.amli_degree}"] if kind == 3 else None
+    got = port.precond_cycle(kind, A["b"], coef, prm.tol)
+    if prm.coarse_solver != 32:
+        assert got.tobytes() == v["z"].tobytes()
+    else:
+        np.testing.assert_allclose(got, v["z"], rtol=0, atol=1e-13 * np.abs(v["z"]).max())
