@@ -234,6 +234,20 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def gcg(self, b, kind=1, coef=None, amg_tol=1e-6, tol=1e-8, maxit=100, hist_cap=1024):
+        """dcsr_pgcg from x = 0 with the cycle of the last setup (kind 1
+        V/W, 3 AMLI with coef, 5 additive): (iterations, x, ||r|| at each
+        preconditioner call)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b)
+        c = np.ascontiguousarray(coef if coef is not None else [1.0], np.float64)
+        hist = np.zeros(hist_cap)
+        nh = ctypes.c_int()
+        it = self.lib.or_gcg(_p(b), _p(x), ctypes.c_double(tol), maxit, kind, _p(c),
+                             len(c) - 1, ctypes.c_double(amg_tol), _p(hist), hist_cap,
+                             ctypes.byref(nh))
+        return it, x, hist[: min(nh.value, hist_cap)].copy()
+
     def precond_cycle(self, kind, r, coef=None, tol=1e-6):
         """z = B r with maxit AMLI (kind 3, polynomial coefficients coef) or
         additive (kind 5) cycles of the last setup's hierarchy."""

@@ -587,6 +587,8 @@ static int or_pcg_core(const ocsr *A, const double *b, double *u, int use_pc,
                        double tol, int maxit, int stop_type, double *hist,
                        int hist_cap, int *nhist);
 static double or_dot(int n, const double *x, const double *y);
+static double or_norm2(int n, const double *x);
+void or_precond(const double *r, double *z);
 
 /* coarse_itsolver mgcycle.c:34-52: unpreconditioned CG to ctol, maxit 20n */
 static void or_coarse_cg(const ocsr *A, const double *b, double *x, double ctol)
@@ -781,6 +783,70 @@ int or_precond_cycle(int kind, const double *coef, int degree, double tol, const
     memcpy(z, g_or.x[0], sizeof(double) * m);
     for (int l = 1; l < g_or.nl; ++l) { free(g_r1[l]); g_r1[l] = NULL; }
     return 0;
+}
+
+/* y' A x, dcsr_vmv sparse.c:1797-1815 */
+static double or_vmv2(const ocsr *A, const double *x, const double *y)
+{
+    double value = 0.0;
+    for (int i = 0; i < A->n; ++i) {
+        double t = 0.0;
+        for (int k = A->ia[i]; k < A->ia[i + 1]; ++k) t += A->val[k] * x[A->ja[k]];
+        value += y[i] * t;
+    }
+    return value;
+}
+
+/* dcsr_pgcg krylov.c:2309-2420 with the preconditioner of the last setup's
+ * cycle type (1 V/W, 3 AMLI with coef, 5 additive): a steepest-descent
+ * step, then each new direction B r A-orthogonalised against all earlier
+ * ones (beta_i = -(p_i' A Br) / (p_i' A p_i)); the relative residual is
+ * ||r|| / ||b||, checked from the second step on.  hist: ||r|| handed to each
+ * preconditioner call. */
+int or_gcg(const double *b, double *u, double tol, int maxit, int kind, const double *coef,
+           int degree, double amg_tol, double *hist, int hist_cap, int *nhist)
+{
+    const ocsr *A = &g_or.A[0];
+    const int m = A->n;
+    int nh = 0, iter = 0;
+    double *r = (double *)malloc(sizeof(double) * m);
+    double *Br = (double *)malloc(sizeof(double) * m);
+    double *p = (double *)malloc(sizeof(double) * (size_t)m * (maxit > 0 ? maxit : 1));
+    double *beta = (double *)malloc(sizeof(double) * (maxit > 0 ? maxit : 1));
+#define OR_GCG_PC(in, out)                                                      \
+    do {                                                                         \
+        if (hist && nh < hist_cap) hist[nh] = or_norm2(m, in);                  \
+        ++nh;                                                                    \
+        if (kind == 1) or_precond(in, out);                                      \
+        else or_precond_cycle(kind, coef, degree, amg_tol, in, out);            \
+    } while (0)
+    const double normb = or_norm2(m, b);
+    memcpy(r, b, sizeof(double) * m);
+    or_aAxpy(-1.0, m, A->ia, A->ja, A->val, u, r);
+    OR_GCG_PC(r, p);
+    double alpha = or_dot(m, r, p) / or_vmv2(A, p, p);
+    for (int i = 0; i < m; ++i) u[i] += alpha * p[i];
+    or_aAxpy(-1.0 * alpha, m, A->ia, A->ja, A->val, p, r);
+    double relres = or_norm2(m, r) / normb;
+    for (iter = 1; iter < maxit; ++iter) {
+        OR_GCG_PC(r, Br);
+        double *pk = p + (size_t)iter * m;
+        memcpy(pk, Br, sizeof(double) * m);
+        for (int i = 0; i < iter; ++i) {
+            const double *pi = p + (size_t)i * m;
+            beta[i] = (-1.0) * (or_vmv2(A, Br, pi) / or_vmv2(A, pi, pi));
+            for (int k = 0; k < m; ++k) pk[k] += beta[i] * pi[k];   /* array_axpy */
+        }
+        alpha = or_dot(m, r, pk) / or_vmv2(A, pk, pk);
+        for (int k = 0; k < m; ++k) u[k] += alpha * pk[k];
+        or_aAxpy(-1.0 * alpha, m, A->ia, A->ja, A->val, pk, r);
+        relres = or_norm2(m, r) / normb;
+        if (relres < tol) break;
+    }
+#undef OR_GCG_PC
+    free(r); free(Br); free(p); free(beta);
+    if (nhist) *nhist = nh;
+    return iter > maxit ? -48 : iter;
 }
 
 int or_hier_level(int l, int *n, const int **ia, const int **ja, const double **a,

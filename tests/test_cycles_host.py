@@ -86,3 +86,40 @@ def test_oracle_amli_and_additive_cycles_match_reference(golden, port, case, var
         assert got.tobytes() == v["z"].tobytes()
     else:
         np.testing.assert_allclose(got, v["z"], rtol=0, atol=1e-13 * np.abs(v["z"]).max())
+
+
+GCG_CASES = [(c, v) for c in ("fix", "kuhn")
+             for v in ("v", "a1", "a2", "a3", "a2s", "a2i", "a2d", "d", "ds", "di")]
+
+
+@pytest.mark.parametrize("case,var", GCG_CASES)
+def test_oracle_gcg_matches_reference(golden, port, case, var):
+    """The oracle's dcsr_pgcg (or_gcg) with the cycle type's preconditioner
+    against the reference's run: the same iteration count, the residual norm
+    at every preconditioner call to 1e-13 of the largest (bit for bit with the
+    iterative coarse solver), the solution to 1e-13 of max |x| where stored."""
+    import oracle
+    A = small_case(golden("gmres.npz"), case)
+    z = golden("cycles.npz")
+    v = small_case(z, f"{case}/{var}")
+    names = ["max_levels", "coarse_dof", "cycle_type", "smoother", "presmooth_iter",
+             "postsmooth_iter", "coarse_solver", "aggregation_type", "max_aggregation",
+             "coarse_scaling", "print_level", "maxit", "amli_degree", "nl_amli_krylov_type"]
+    ip = [int(t) for t in v["params"]]
+    dp = [float(t) for t in v["dparams"]]
+    kw = dict(zip(names, ip[:14]))
+    kw.update(strong_coupled=dp[0], relaxation=dp[1], tol=dp[2])
+    prm = oracle.AMGParams(**kw)
+    assert port.setup(A["A_ia"], A["A_ja"], A["A_val"], prm) == 0
+    kind = {1: 1, 2: 1, 3: 3, 5: 5}[prm.cycle_type]
+    coef = z[f"amli_coef/{prm.amli_degree}"] if kind == 3 else None
+    it, x, hist = port.gcg(A["b"], kind, coef, prm.tol, tol=1e-8, maxit=100)
+    assert it == int(v["gcg/iters"])
+    rh = v["gcg/hist"]
+    assert len(hist) == len(rh)
+    if prm.coarse_solver != 32:
+        assert hist.tobytes() == rh.tobytes()
+    else:
+        np.testing.assert_allclose(hist, rh, rtol=0, atol=1e-13 * rh.max())
+    if "gcg/x" in v:
+        np.testing.assert_allclose(x, v["gcg/x"], rtol=0, atol=1e-13 * np.abs(v["gcg/x"]).max())
