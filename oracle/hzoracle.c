@@ -849,6 +849,190 @@ int or_gcg(const double *b, double *u, double tol, int maxit, int kind, const do
     return iter > maxit ? -48 : iter;
 }
 
+/* array_axpy array.c:357-373: y += a x with a = +-1 as plain sums (x may be y) */
+static void or_axpy(int n, double a, const double *x, double *y)
+{
+    if (a == 1.0) for (int i = 0; i < n; ++i) y[i] += x[i];
+    else if (a == -1.0) for (int i = 0; i < n; ++i) y[i] -= x[i];
+    else for (int i = 0; i < n; ++i) y[i] += a * x[i];
+}
+
+/* dcsr_pvgmres krylov.c:4612-4930 (flexible = 0) and dcsr_pvfgmres
+ * krylov.c:5974-6280 (flexible = 1), right-preconditioned by the V/W cycle
+ * of the last setup: restart cycles of modified Gram-Schmidt Arnoldi with
+ * Givens rotations; the restart length shrinks by 3 (not below 3) while the
+ * last cycle's convergence rate is in [0.174, 0.99], returns to `restart`
+ * otherwise; a converged cycle is checked on the true residual and
+ * restarted from it if that check fails.  hist: ||v|| of every vector handed
+ * to the preconditioner. */
+int or_gmres(int flexible, const double *b, double *x, double tol, int MaxIt, int restart,
+             int stop_type, double *hist, int hist_cap, int *nhist)
+{
+    const ocsr *A = &g_or.A[0];
+    const int n = A->n;
+    const double cr_max = 0.99, cr_min = 0.174, epsmac = SMALLREAL;
+    int nh = 0, iter = 0, i = 0, Restart = restart;
+    const int R1 = restart + 1;
+    double *r = (double *)calloc(n, sizeof(double));
+    double *w = (double *)calloc(n, sizeof(double));
+    double *rs = (double *)calloc(R1, sizeof(double));
+    double *c = (double *)calloc(R1, sizeof(double));
+    double *sn = (double *)calloc(R1, sizeof(double));
+    double *pv = (double *)calloc((size_t)R1 * n, sizeof(double));
+    double *zv = (double *)calloc((size_t)R1 * n, sizeof(double));
+    double *hh = (double *)calloc((size_t)R1 * R1, sizeof(double));
+#define P(k) (pv + (size_t)(k) * n)
+#define Z(k) (zv + (size_t)(k) * n)
+#define H(a, b_) hh[(size_t)(a) * R1 + (b_)]
+#define OR_PC(in, out)                                                          \
+    do {                                                                         \
+        if (hist && nh < hist_cap) hist[nh] = or_norm2(n, in);                  \
+        ++nh;                                                                    \
+        or_precond(in, out);                                                     \
+    } while (0)
+    double cr = 1.0, r_norm_old = 0.0, r_norm, relres = BIGREAL, absres0 = BIGREAL;
+    double absres, normu, den_norm = 1.0, epsilon = 0.0, b_norm = 0.0;
+    memcpy(P(0), b, sizeof(double) * n);
+    or_aAxpy(-1.0, n, A->ia, A->ja, A->val, x, P(0));
+    if (flexible) {
+        b_norm = or_norm2(n, b);
+        r_norm = or_norm2(n, P(0));
+        den_norm = b_norm > 0.0 ? b_norm : r_norm;
+        epsilon = tol * den_norm;
+        if (r_norm < epsilon || r_norm < 1e-3 * tol) goto done;
+    } else {
+        r_norm = or_norm2(n, P(0));
+        switch (stop_type) {
+        case 1: absres0 = r_norm > SMALLREAL ? r_norm : SMALLREAL; relres = r_norm / absres0;
+            break;
+        case 2: {
+            OR_PC(P(0), r);
+            double rb = sqrt(or_dot(n, P(0), r));
+            absres0 = rb > SMALLREAL ? rb : SMALLREAL;
+            relres = rb / absres0;
+            break;
+        }
+        default:
+            normu = or_norm2(n, x);
+            if (normu < SMALLREAL) normu = SMALLREAL;
+            absres0 = r_norm;
+            relres = absres0 / normu;
+        }
+        if (relres < tol || absres0 < 1e-3 * tol) goto done;
+    }
+    while (iter < MaxIt) {
+        rs[0] = r_norm_old = r_norm;
+        if (flexible && r_norm == 0.0) goto done;
+        if (cr > cr_max || iter == 0) Restart = restart;
+        else if (cr < cr_min) { /* keep */ }
+        else Restart = (Restart - 3 > 3) ? Restart - 3 : restart;
+        const double t0 = 1.0 / r_norm;
+        for (int k = 0; k < n; ++k) P(0)[k] *= t0;
+        i = 0;
+        while (i < Restart && iter < MaxIt) {
+            ++i; ++iter;
+            double *zi = flexible ? Z(i - 1) : r;
+            OR_PC(P(i - 1), zi);
+            or_mxv(n, A->ia, A->ja, A->val, zi, P(i));
+            for (int j = 0; j < i; ++j) {
+                H(j, i - 1) = or_dot(n, P(j), P(i));
+                or_axpy(n, -H(j, i - 1), P(j), P(i));
+            }
+            double t = or_norm2(n, P(i));
+            H(i, i - 1) = t;
+            if (t != 0.0) {
+                t = 1.0 / t;
+                for (int k = 0; k < n; ++k) P(i)[k] *= t;
+            }
+            for (int j = 1; j < i; ++j) {
+                t = H(j - 1, i - 1);
+                H(j - 1, i - 1) = sn[j - 1] * H(j, i - 1) + c[j - 1] * t;
+                H(j, i - 1) = -sn[j - 1] * t + c[j - 1] * H(j, i - 1);
+            }
+            t = H(i, i - 1) * H(i, i - 1);
+            t += H(i - 1, i - 1) * H(i - 1, i - 1);
+            double gamma = sqrt(t);
+            if (gamma == 0.0) gamma = epsmac;
+            c[i - 1] = H(i - 1, i - 1) / gamma;
+            sn[i - 1] = H(i, i - 1) / gamma;
+            rs[i] = -sn[i - 1] * rs[i - 1];
+            rs[i - 1] = c[i - 1] * rs[i - 1];
+            H(i - 1, i - 1) = sn[i - 1] * H(i, i - 1) + c[i - 1] * H(i - 1, i - 1);
+            if (flexible) {
+                r_norm = fabs(rs[i]);
+                if (r_norm <= epsilon) break;
+            } else {
+                absres = r_norm = fabs(rs[i]);
+                relres = absres / absres0;
+                if (relres < tol) break;
+            }
+        }
+        rs[i - 1] = rs[i - 1] / H(i - 1, i - 1);
+        for (int k = i - 2; k >= 0; --k) {
+            double t = 0.0;
+            for (int j = k + 1; j < i; ++j) t -= H(k, j) * rs[j];
+            t += rs[k];
+            rs[k] = t / H(k, k);
+        }
+        int conv;
+        if (flexible) {
+            memcpy(r, Z(i - 1), sizeof(double) * n);
+            for (int k = 0; k < n; ++k) r[k] *= rs[i - 1];
+            for (int j = i - 2; j >= 0; --j) or_axpy(n, rs[j], Z(j), r);
+            or_axpy(n, 1.0, r, x);
+            conv = r_norm <= epsilon;
+        } else {
+            memcpy(w, P(i - 1), sizeof(double) * n);
+            for (int k = 0; k < n; ++k) w[k] *= rs[i - 1];
+            for (int j = i - 2; j >= 0; --j) or_axpy(n, rs[j], P(j), w);
+            OR_PC(w, r);
+            or_axpy(n, 1.0, r, x);
+            conv = relres < tol;
+        }
+        if (conv) {
+            memcpy(r, b, sizeof(double) * n);
+            or_aAxpy(-1.0, n, A->ia, A->ja, A->val, x, r);
+            r_norm = or_norm2(n, r);
+            double dn = flexible ? den_norm : absres0;
+            switch (stop_type) {
+            case 1: relres = r_norm / dn; break;
+            case 2: {
+                double *dst = flexible ? P(0) : w;
+                OR_PC(r, dst);
+                relres = sqrt(or_dot(n, dst, r)) / dn;
+                break;
+            }
+            default:
+                normu = or_norm2(n, x);
+                if (normu < SMALLREAL) normu = SMALLREAL;
+                relres = r_norm / normu;
+            }
+            if (flexible ? relres <= tol : relres < tol) break;
+            memcpy(P(0), r, sizeof(double) * n);
+            i = 0;
+        }
+        for (int j = i; j > 0; --j) {
+            rs[j - 1] = -sn[j - 1] * rs[j];
+            rs[j] = c[j - 1] * rs[j];
+        }
+        if (i) or_axpy(n, rs[i] - 1.0, P(i), P(i));
+        for (int j = i - 1; j > 0; --j) or_axpy(n, rs[j], P(j), P(i));
+        if (i) {
+            or_axpy(n, rs[0] - 1.0, P(0), P(0));
+            or_axpy(n, 1.0, P(i), P(0));
+        }
+        cr = r_norm / r_norm_old;
+    }
+done:
+#undef P
+#undef Z
+#undef H
+#undef OR_PC
+    free(r); free(w); free(rs); free(c); free(sn); free(pv); free(zv); free(hh);
+    if (nhist) *nhist = nh;
+    return iter >= MaxIt ? -48 : iter;
+}
+
 int or_hier_level(int l, int *n, const int **ia, const int **ja, const double **a,
                   const int **agg, const int **ria, const int **rja, int *nc)
 {
