@@ -172,7 +172,7 @@ def hbm_peak():
 
 
 def amg_l1(hz):
-    return hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    return hz.bench_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
 
 
 def itparam(hz, maxit=500):
@@ -196,7 +196,7 @@ def time_reference(ia, ja, val, b):
     return t, int(it), kind
 
 
-# --variant: (what, AMG_param fields over the survey setting, Krylov method)
+# --variant: (what, AMG_param fields over bench_amg's setting, Krylov method)
 VARIANTS = {
     "w": ("W-cycle, PCG", dict(cycle_type=2), "pcg"),
     "amli": ("AMLI cycle of degree 2, PCG", dict(cycle_type=3), "pcg"),
@@ -251,7 +251,7 @@ def run_variant(args, rank, world, local, dist):
     dval, db = torch.from_numpy(val).to(dev), torch.from_numpy(b).to(dev)
     dx = torch.zeros_like(db)
     p = lambda t: t.data_ptr()  # noqa: E731
-    amg = hz.survey_amg(amli_degree=2, nl_amli_krylov_type=4, **over)
+    amg = hz.bench_amg(amli_degree=2, nl_amli_krylov_type=4, **over)
     it_par = hz.itsolver_param(linear_itsolver_type=KRYLOV_TYPE[method],
                                linear_precond_type=hz.PREC_AMG, linear_tol=1e-8,
                                linear_maxit=500, linear_stop_type=hz.STOP_REL_RES,
@@ -355,7 +355,7 @@ def bsr_case(N: int):
 
 
 def bsr_amg(hz):
-    return hz.survey_amg(coarse_dof=100, coarse_solver=0)
+    return hz.bench_amg(coarse_dof=100, coarse_solver=0)
 
 
 def time_reference_bsr(ia, ja, val, b):

@@ -273,7 +273,7 @@ def b200_param(**kw) -> hzb_param:
     return p
 
 
-def survey_amg(**kw) -> AMG_param:
+def bench_amg(**kw) -> AMG_param:
     """The UA-AMG setting of the benchmark configurations: HEM, theta = 0,
     V(1,1) Gauss-Seidel, coarse direct solve at <= 2000 rows."""
     base = dict(AMG_type=UA_AMG, cycle_type=V_CYCLE, smoother=SMOOTHER_GS,
@@ -510,7 +510,7 @@ class Solver:
 
     def __init__(self, amg: AMG_param | None = None, it: linear_itsolver_param | None = None,
                  b200: hzb_param | None = None):
-        self.amg = amg or survey_amg()
+        self.amg = amg or bench_amg()
         self.it = it or itsolver_param(linear_itsolver_type=SOLVER_CG,
                                        linear_precond_type=PREC_AMG, linear_tol=1e-8,
                                        linear_maxit=500)

@@ -29,7 +29,7 @@ import numpy as np
 
 from . import (HZB_K_L1_32, HZB_K_L1_64, HZB_K_RES64, HZB_K_SPMV32, HZB_K_SPMV64,
                HZB_MATCH_EXACT, HZB_MATCH_PARALLEL, HZB_PREC_FP64, HZB_PREC_MIXED,
-               SMOOTHER_L1DIAG, Solver, b200_param, last_error, lib, survey_amg)
+               SMOOTHER_L1DIAG, Solver, b200_param, last_error, lib, bench_amg)
 from . import problems as P
 
 KERNELS = {"spmv64": HZB_K_SPMV64, "spmv32": HZB_K_SPMV32, "res64": HZB_K_RES64,
@@ -56,7 +56,7 @@ def main():
     ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, sigma, 8.0, seed))
     n = len(ia) - 1
     dia, dja, dval = (torch.from_numpy(v).cuda() for v in (ia, ja, val))
-    amg = survey_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    amg = bench_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
     prec = HZB_PREC_MIXED if a.precision == "mixed" else HZB_PREC_FP64
     match = HZB_MATCH_PARALLEL if a.matching == "parallel" else HZB_MATCH_EXACT
     S = Solver(amg, None, b200_param(precision=prec, matching=match))

@@ -25,7 +25,7 @@ import numpy as np
 
 from . import problems as P
 from . import (HZB_MATCH_PARALLEL, HZB_PREC_FP64, SMOOTHER_L1DIAG, Solver, b200_param, lib,
-               last_error, survey_amg)
+               last_error, bench_amg)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "gnn_weights.npy")
@@ -154,7 +154,7 @@ def training_problem(rng: np.random.Generator, small: bool = False):
 
 
 def l1_solver(device: int = 0) -> Solver:
-    amg = survey_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2,
+    amg = bench_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2,
                      coarse_dof=400)
     return Solver(amg, None, b200_param(precision=HZB_PREC_FP64, matching=HZB_MATCH_PARALLEL,
                                         device=device))
@@ -235,7 +235,7 @@ def evaluate(gnn: GNN, problems, precision: int | None = None, device: int = 0,
         tia, tja = torch.from_numpy(ia).to(dev), torch.from_numpy(ja).to(dev)
         tval, tb = torch.from_numpy(val).to(dev), torch.from_numpy(b).to(dev)
         x = torch.zeros_like(tb)
-        amg = survey_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+        amg = bench_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
         it = itsolver_param(linear_itsolver_type=SOLVER_CG, linear_precond_type=PREC_AMG,
                             linear_tol=1e-8, linear_maxit=1000,
                             linear_stop_type=STOP_REL_RES)

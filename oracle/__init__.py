@@ -39,7 +39,7 @@ def build(ref: bool = True) -> None:
 @dataclass
 class AMGParams:
     """The AMG_param fields this path reads (include/param.h of the reference),
-    with the survey configuration's values as defaults: UA, HEM, theta = 0,
+    with the benchmark configurations' values as defaults: UA, HEM, theta = 0,
     V(1,1) Gauss-Seidel, coarse direct solve below 2000 rows."""
 
     max_levels: int = 20

@@ -102,9 +102,9 @@ def test_entry_points_fail_loudly_without_a_device(lib):
     b = np.ones(len(ia) - 1)
     x = np.zeros_like(b)
     it = hz.itsolver_param(linear_itsolver_type=hz.SOLVER_CG)
-    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.survey_amg()) == \
+    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.bench_amg()) == \
         hz.ERROR_SOLVER_MISC
     assert "CUDA" in hz.last_error()
-    assert hz.linear_solver_dbsr_krylov_amg(1, ia, ja, val, b, x, it, hz.survey_amg()) == \
+    assert hz.linear_solver_dbsr_krylov_amg(1, ia, ja, val, b, x, it, hz.bench_amg()) == \
         hz.ERROR_SOLVER_MISC
     assert not x.any()

@@ -91,7 +91,7 @@ def test_assembled_matrix_solves_like_host_one():
                            linear_tol=1e-8, linear_maxit=200)
     out = []
     for arrs in ((ia, ja, val), P.kuhn3d_p1(N, k)):
-        S = hz.Solver(hz.survey_amg(), it)
+        S = hz.Solver(hz.bench_amg(), it)
         assert S.setup_host(*arrs) == 0
         x = np.zeros(len(b))
         out.append((S.solve_host(b, x), x))

@@ -16,7 +16,7 @@ torch = pytest.importorskip("torch")
 
 
 def _amg():
-    return hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    return hz.bench_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
 
 
 def _it(tol=1e-8):

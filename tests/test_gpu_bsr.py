@@ -38,7 +38,7 @@ def sha(a):
 def amg_of(v):
     ip = [int(t) for t in v["params"]]
     dp = [float(t) for t in v["dparams"]]
-    return hz.survey_amg(max_levels=ip[0], coarse_dof=ip[1], cycle_type=ip[2], smoother=ip[3],
+    return hz.bench_amg(max_levels=ip[0], coarse_dof=ip[1], cycle_type=ip[2], smoother=ip[3],
                          presmooth_iter=ip[4], postsmooth_iter=ip[5], coarse_solver=ip[6],
                          aggregation_type=ip[7], max_aggregation=ip[8], coarse_scaling=ip[9],
                          maxit=ip[11], strong_coupled=dp[0], relaxation=dp[1], tol=dp[2])

@@ -19,7 +19,7 @@ OFF_WO = 160 + 3 * 3200
 
 
 def solver_for(ia, ja, val, coarse_dof=50):
-    amg = hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2,
+    amg = hz.bench_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2,
                         coarse_dof=coarse_dof)
     S = hz.Solver(amg)   # exact HEM: the same hierarchy as the oracle
     assert S.setup_host(ia, ja, val) == 0, hz.last_error()
@@ -140,7 +140,7 @@ def test_training_reduces_contraction_and_fallback():
     assert after[:, 1].mean() < after[:, 0].mean(), after
     ia, ja, val = P.aniso2d_p1(120, 1e-3, 0.9)
     b = P.rhs_uniform(len(ia) - 1, 6)
-    amg = hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    amg = hz.bench_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
     S0 = hz.Solver(amg)
     assert S0.setup_host(ia, ja, val) == 0
     x = np.zeros(len(b))

@@ -19,7 +19,7 @@ BASES = {"fix": {}, "kuhn": dict(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2,
 
 
 def amg(case):
-    return hz.survey_amg(**BASES[case])
+    return hz.bench_amg(**BASES[case])
 
 
 def check(it, x, g):

@@ -27,7 +27,7 @@ def sha(a):
 def amg_of(v):
     ip = [int(t) for t in v["params"]]
     dp = [float(t) for t in v["dparams"]]
-    return hz.survey_amg(max_levels=ip[0], coarse_dof=ip[1], cycle_type=ip[2], smoother=ip[3],
+    return hz.bench_amg(max_levels=ip[0], coarse_dof=ip[1], cycle_type=ip[2], smoother=ip[3],
                          presmooth_iter=ip[4], postsmooth_iter=ip[5], coarse_solver=ip[6],
                          aggregation_type=ip[7], max_aggregation=ip[8], coarse_scaling=ip[9],
                          maxit=ip[11], amli_degree=ip[12], nl_amli_krylov_type=ip[13],

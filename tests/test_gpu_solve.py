@@ -24,7 +24,7 @@ def sha(a):
 def amg_from_case(c):
     ip = [int(v) for v in c["params"]]
     dp = [float(v) for v in c["dparams"]]
-    return hz.survey_amg(max_levels=ip[0], coarse_dof=ip[1], cycle_type=ip[2], smoother=ip[3],
+    return hz.bench_amg(max_levels=ip[0], coarse_dof=ip[1], cycle_type=ip[2], smoother=ip[3],
                          presmooth_iter=ip[4], postsmooth_iter=ip[5], coarse_solver=ip[6],
                          aggregation_type=ip[7], max_aggregation=ip[8], coarse_scaling=ip[9],
                          maxit=ip[11], strong_coupled=dp[0], relaxation=dp[1], tol=dp[2])
@@ -74,7 +74,7 @@ def test_fixture128_drop_in(golden):
     ia, ja, val = P.poisson2d_5pt(128)
     it = hz.itsolver_param(linear_itsolver_type=1, linear_precond_type=2, linear_tol=1e-8,
                            linear_maxit=500, linear_stop_type=1)
-    amg = hz.survey_amg()
+    amg = hz.bench_amg()
     x = np.zeros(len(ia) - 1)
     n_it = hz.linear_solver_dcsr_krylov_amg(ia, ja, val, g["b"], x, it, amg)
     assert n_it == int(g["iters"]) == 15
@@ -125,7 +125,7 @@ def test_amg_setup_precond_pcg_pieces(golden):
     HAZNICS' create_precond_amg assembles the preconditioner."""
     g = golden("fixture128.npz")
     ia, ja, val = P.poisson2d_5pt(128)
-    H = hz.AMGHierarchy(ia, ja, val, hz.survey_amg())
+    H = hz.AMGHierarchy(ia, ja, val, hz.bench_amg())
     assert H.status == 0
     assert H.num_levels == len(g["info"])
     for l in range(H.num_levels - 1):
@@ -148,7 +148,7 @@ def test_linear_solver_amg_converges():
     ia, ja, val = P.poisson2d_5pt(64)
     b = P.rhs_uniform(len(ia) - 1, 5)
     x = np.zeros(len(b))
-    it = hz.linear_solver_amg(ia, ja, val, b, x, hz.survey_amg(maxit=100, tol=1e-8))
+    it = hz.linear_solver_amg(ia, ja, val, b, x, hz.bench_amg(maxit=100, tol=1e-8))
     assert 0 < it <= 100
     r = b - _spmv(ia, ja, val, x)
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-8
@@ -165,10 +165,10 @@ def test_error_codes():
     ia, ja, val = P.poisson2d_5pt(20)
     x = np.zeros(400)
     b = np.ones(400)
-    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.survey_amg()) \
+    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.bench_amg()) \
         == hz.ERROR_SOLVER_TYPE
     it = hz.itsolver_param(linear_itsolver_type=1, linear_tol=1e-8, linear_maxit=2)
-    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.survey_amg(
+    assert hz.linear_solver_dcsr_krylov_amg(ia, ja, val, b, x, it, hz.bench_amg(
         coarse_dof=10)) == hz.ERROR_SOLVER_MAXIT
 
 
@@ -194,12 +194,12 @@ def test_mixed_precision_kuhn():
     N = 24
     ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, 1.0, 8.0, 2))
     b = P.rhs_uniform(len(ia) - 1, 3)
-    amg = hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    amg = hz.bench_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
     S64 = hz.Solver(amg)
     assert S64.setup_host(ia, ja, val) == 0
     x64 = np.zeros(len(b))
     it64 = S64.solve_host(b, x64)
-    S32 = hz.Solver(hz.survey_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2,
+    S32 = hz.Solver(hz.bench_amg(smoother=hz.SMOOTHER_L1DIAG, presmooth_iter=2,
                                   postsmooth_iter=2),
                     b200=hz.b200_param(precision=hz.HZB_PREC_MIXED))
     assert S32.setup_host(ia, ja, val) == 0
