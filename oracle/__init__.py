@@ -325,6 +325,17 @@ class Port(_Backend):
                 aggs.append(agg)
         return levels, aggs
 
+    def bsr_precond(self, r, cycle_type=1, smoother=2, presmooth_iter=1, coarse_scaling=0,
+                    maxit=1):
+        """z = B r of precond_dbsr_amg on the last bsr_hierarchy."""
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros_like(r)
+        rc = self.lib.or_bsr_precond(cycle_type, smoother, presmooth_iter, coarse_scaling,
+                                     maxit, _p(r), _p(z))
+        if rc:
+            raise ValueError(f"or_bsr_precond: {rc}")
+        return z
+
     def srand(self, seed: int) -> None:
         """Seed the oracle's restatement of the C library's rand() stream."""
         self.lib.or_srand(ctypes.c_uint(seed))

@@ -865,10 +865,33 @@ static void or_axpy(int n, double a, const double *x, double *y)
  * otherwise; a converged cycle is checked on the true residual and
  * restarted from it if that check fails.  hist: ||v|| of every vector handed
  * to the preconditioner. */
+/* r = b - A x: CSR (dcsr_aAxpy(-1): the row sum subtracted) or, for the
+ * scalar expansion of a block matrix, the products subtracted one by one
+ * (dbsr_aAxpy(-1) negates, adds and negates back) */
+static void or_resid_of(const ocsr *A, int block, const double *b, const double *x,
+                        double *r)
+{
+    memcpy(r, b, sizeof(double) * A->n);
+    if (!block) { or_aAxpy(-1.0, A->n, A->ia, A->ja, A->val, x, r); return; }
+    for (int i = 0; i < A->n; ++i)
+        for (int k = A->ia[i]; k < A->ia[i + 1]; ++k) r[i] -= A->val[k] * x[A->ja[k]];
+}
+
+static int or_gmres_on(int flexible, const ocsr *A, int block, int use_pc, const double *b,
+                       double *x, double tol, int MaxIt, int restart, int stop_type,
+                       double *hist, int hist_cap, int *nhist);
+
 int or_gmres(int flexible, const double *b, double *x, double tol, int MaxIt, int restart,
              int stop_type, double *hist, int hist_cap, int *nhist)
 {
-    const ocsr *A = &g_or.A[0];
+    return or_gmres_on(flexible, &g_or.A[0], 0, 1, b, x, tol, MaxIt, restart, stop_type, hist,
+                       hist_cap, nhist);
+}
+
+static int or_gmres_on(int flexible, const ocsr *A, int block, int use_pc, const double *b,
+                       double *x, double tol, int MaxIt, int restart, int stop_type,
+                       double *hist, int hist_cap, int *nhist)
+{
     const int n = A->n;
     const double cr_max = 0.99, cr_min = 0.174, epsmac = SMALLREAL;
     int nh = 0, iter = 0, i = 0, Restart = restart;
@@ -888,12 +911,12 @@ int or_gmres(int flexible, const double *b, double *x, double tol, int MaxIt, in
     do {                                                                         \
         if (hist && nh < hist_cap) hist[nh] = or_norm2(n, in);                  \
         ++nh;                                                                    \
-        or_precond(in, out);                                                     \
+        if (use_pc) or_precond(in, out);                                         \
+        else memcpy(out, in, sizeof(double) * n);                                \
     } while (0)
     double cr = 1.0, r_norm_old = 0.0, r_norm, relres = BIGREAL, absres0 = BIGREAL;
     double absres, normu, den_norm = 1.0, epsilon = 0.0, b_norm = 0.0;
-    memcpy(P(0), b, sizeof(double) * n);
-    or_aAxpy(-1.0, n, A->ia, A->ja, A->val, x, P(0));
+    or_resid_of(A, block, b, x, P(0));
     if (flexible) {
         b_norm = or_norm2(n, b);
         r_norm = or_norm2(n, P(0));
@@ -990,8 +1013,7 @@ int or_gmres(int flexible, const double *b, double *x, double tol, int MaxIt, in
             conv = relres < tol;
         }
         if (conv) {
-            memcpy(r, b, sizeof(double) * n);
-            or_aAxpy(-1.0, n, A->ia, A->ja, A->val, x, r);
+            or_resid_of(A, block, b, x, r);
             r_norm = or_norm2(n, r);
             double dn = flexible ? den_norm : absres0;
             switch (stop_type) {
@@ -1343,14 +1365,22 @@ int or_hec_agg(int n, const int *ia, const int *ja, const double *a, double thet
  * encounter order over (fine rows of R row C ascending) x (A row order); a new
  * block takes ddense_mul's sums, which start from 0.0 (so -0.0 becomes +0.0),
  * a known block adds them.  Blocks are nb x nb, row-major. */
-typedef struct { int nrow, nnzb; int *ia, *ja, *agg; double *val; } obsr;
+typedef struct {
+    int nrow, nnzb; int *ia, *ja, *agg; double *val;
+    /* the cycle's data: scalar expansion, diagonal-block inverses, scalar
+     * aggregate map and its R pattern, level vectors */
+    ocsr E; double *dinv; int *sagg, *sria, *srja, snc; double *b, *x, *w, *t1, *t2;
+} obsr;
 static struct { int nl, nb; obsr lv[32]; } g_bsr;
 
 static void or_bsr_free(void)
 {
-    for (int l = 0; l < g_bsr.nl; ++l) {
-        free(g_bsr.lv[l].ia); free(g_bsr.lv[l].ja); free(g_bsr.lv[l].val);
-        free(g_bsr.lv[l].agg);
+    for (int l = 0; l < 32; ++l) {
+        obsr *L = &g_bsr.lv[l];
+        free(L->ia); free(L->ja); free(L->val); free(L->agg);
+        ocsr_free(&L->E);
+        free(L->dinv); free(L->sagg); free(L->sria); free(L->srja);
+        free(L->b); free(L->x); free(L->w); free(L->t1); free(L->t2);
     }
     memset(&g_bsr, 0, sizeof(g_bsr));
 }
@@ -1459,7 +1489,172 @@ int or_bsr_setup(int nrow, int nnzb, int nb, const int *ia, const int *ja, const
         ++lvl;
     }
     g_bsr.nl = lvl + 1;
+    /* the cycle's data (dbsr_getdiaginv sparse.c:6122 on the smoothed levels:
+     * the row's last diagonal block inverted by ddense_inv_inplace's
+     * Gauss-Jordan, dense.c:1266; 1/a for nb = 1) */
+    for (int l = 0; l < g_bsr.nl; ++l) {
+        obsr *L = &g_bsr.lv[l];
+        const int n = L->nrow * nb;
+        ocsr *E = &L->E;
+        E->n = E->m = n; E->nnz = L->nnzb * nb2;
+        E->ia = (int *)malloc(sizeof(int) * (n + 1));
+        E->ja = (int *)malloc(sizeof(int) * (E->nnz > 0 ? E->nnz : 1));
+        E->val = (double *)malloc(sizeof(double) * (E->nnz > 0 ? E->nnz : 1));
+        int q = 0;
+        for (int I = 0; I < L->nrow; ++I)
+            for (int r = 0; r < nb; ++r) {
+                E->ia[I * nb + r] = q;
+                for (int k = L->ia[I]; k < L->ia[I + 1]; ++k)
+                    for (int c = 0; c < nb; ++c, ++q) {
+                        E->ja[q] = L->ja[k] * nb + c;
+                        E->val[q] = L->val[(size_t)k * nb2 + r * nb + c];
+                    }
+            }
+        E->ia[n] = q;
+        L->b = (double *)calloc(n, sizeof(double));
+        L->x = (double *)calloc(n, sizeof(double));
+        L->w = (double *)calloc(n, sizeof(double));
+        L->t1 = (double *)calloc(n, sizeof(double));
+        L->t2 = (double *)calloc(n, sizeof(double));
+        if (l == g_bsr.nl - 1) continue;
+        L->dinv = (double *)calloc((size_t)L->nrow * nb2, sizeof(double));
+        for (int i = 0; i < L->nrow; ++i) {
+            double *a = L->dinv + (size_t)i * nb2;
+            for (int k = L->ia[i]; k < L->ia[i + 1]; ++k)
+                if (L->ja[k] == i) memcpy(a, L->val + (size_t)k * nb2, sizeof(double) * nb2);
+            if (nb == 1) { a[0] = 1.0 / a[0]; continue; }
+            for (int k = 0; k < nb; ++k) {
+                const int kn = k * nb, ll = kn + k;
+                const double alinv = 1.0 / a[ll];
+                a[ll] = alinv;
+                for (int j = 0; j < k; ++j) a[kn + j] *= alinv;
+                for (int j = k + 1; j < nb; ++j) a[kn + j] *= alinv;
+                for (int r = 0; r < k; ++r)
+                    for (int j = 0; j < nb; ++j) if (j != k) a[r * nb + j] -= a[r * nb + k] * a[kn + j];
+                for (int r = k + 1; r < nb; ++r)
+                    for (int j = 0; j < nb; ++j) if (j != k) a[r * nb + j] -= a[r * nb + k] * a[kn + j];
+                for (int r = 0; r < k; ++r) a[r * nb + k] *= -alinv;
+                for (int r = k + 1; r < nb; ++r) a[r * nb + k] *= -alinv;
+            }
+        }
+        const int nc = g_bsr.lv[l + 1].nrow;
+        L->snc = nc * nb;
+        L->sagg = (int *)malloc(sizeof(int) * n);
+        for (int i = 0; i < n; ++i) {
+            const int a = L->agg[i / nb];
+            L->sagg[i] = a < 0 ? -1 : a * nb + i % nb;
+        }
+        L->sria = (int *)malloc(sizeof(int) * (L->snc + 1));
+        L->srja = (int *)malloc(sizeof(int) * n);
+        or_trans_agg(n, L->snc, L->sagg, L->sria, L->srja);
+    }
     return g_bsr.nl;
+}
+
+/* block relaxation of row i: x_i = D_i^{-1} (b_i - sum_{j != i} A_ij x_j)
+ * (smoother_dbsr_gs_ascend / _descend, smoother.c:904-1040: ddense_ymAx per
+ * block, ddense_mxv from 0.0; nb = 1: (b - sum) * diaginv) */
+static void or_bsr_relax(const obsr *L, int nb, int i, const double *b, const double *xin,
+                         double *xout, double *bt)
+{
+    const int nb2 = nb * nb;
+    for (int r = 0; r < nb; ++r) bt[r] = b[i * nb + r];
+    for (int k = L->ia[i]; k < L->ia[i + 1]; ++k) {
+        const int j = L->ja[k];
+        if (j == i) continue;
+        const double *a = L->val + (size_t)k * nb2;
+        for (int r = 0; r < nb; ++r)
+            for (int c = 0; c < nb; ++c) bt[r] -= a[r * nb + c] * xin[j * nb + c];
+    }
+    const double *d = L->dinv + (size_t)i * nb2;
+    if (nb == 1) { xout[i] = bt[0] * d[0]; return; }
+    for (int r = 0; r < nb; ++r) {
+        double t = 0.0;
+        for (int c = 0; c < nb; ++c) t += d[r * nb + c] * bt[c];
+        xout[i * nb + r] = t;
+    }
+}
+
+/* smoother_dbsr_jacobi (all rows from the old iterate) and the Gauss-Seidel
+ * sweeps (kind 1 ascending, 2 descending) */
+static void or_bsr_sweep(obsr *L, int nb, int kind)
+{
+    double bt[64];
+    if (kind == 0) {
+        for (int i = 0; i < L->nrow; ++i) or_bsr_relax(L, nb, i, L->b, L->x, L->t1, bt);
+        memcpy(L->x, L->t1, sizeof(double) * L->E.n);
+    } else if (kind == 1) {
+        for (int i = 0; i < L->nrow; ++i) or_bsr_relax(L, nb, i, L->b, L->x, L->x, bt);
+    } else {
+        for (int i = L->nrow - 1; i >= 0; --i) or_bsr_relax(L, nb, i, L->b, L->x, L->x, bt);
+    }
+}
+
+static void or_bsr_smoothing(obsr *L, int nb, int smoother, int steps, int pre)
+{
+    for (int k = 0; k < steps; ++k) {
+        if (smoother == 1) or_bsr_sweep(L, nb, 0);
+        else if (smoother == 2) or_bsr_sweep(L, nb, pre ? 1 : 2);
+        else { or_bsr_sweep(L, nb, 1); or_bsr_sweep(L, nb, 2); }
+    }
+}
+
+/* mgcycle_bsr mgcycle.c:952-1160 as precond_dbsr_amg runs it
+ * (precond.c:1311-1339): presmooth_iter sweeps before and after the coarse
+ * correction, the coarsest level by GMRES(25) without preconditioner to
+ * 1e-6 with at most min(n^2, 200) steps, the coarse scaling of its PeH / Aeh
+ * form (alpha <= 1); maxit cycles from x = 0 */
+int or_bsr_precond(int cycle_type, int smoother, int steps, int coarse_scaling, int maxit,
+                   const double *r, double *z)
+{
+    const int nl = g_bsr.nl, nb = g_bsr.nb;
+    if (nb > 8 || nl < 1) return -1;
+    obsr *L0 = &g_bsr.lv[0];
+    memcpy(L0->b, r, sizeof(double) * L0->E.n);
+    memset(L0->x, 0, sizeof(double) * L0->E.n);
+    for (int it = 0; it < maxit; ++it) {
+        int nu[32] = {0};
+        int l = 0;
+forward:
+        while (l < nl - 1) {
+            obsr *L = &g_bsr.lv[l];
+            nu[l]++;
+            or_bsr_smoothing(L, nb, smoother, steps, 1);
+            or_resid_of(&L->E, 1, L->b, L->x, L->w);
+            or_restrict(L->snc, L->sria, L->srja, L->w, g_bsr.lv[l + 1].b);
+            ++l;
+            memset(g_bsr.lv[l].x, 0, sizeof(double) * g_bsr.lv[l].E.n);
+        }
+        {
+            obsr *C = &g_bsr.lv[nl - 1];
+            const long long cs = C->E.n;
+            const int cmaxit = cs * cs < 200 ? (int)(cs * cs) : 200;
+            or_gmres_on(0, &C->E, 1, 0, C->b, C->x, 1e-6, cmaxit, 25, 1, NULL, 0, NULL);
+        }
+        while (l > 0) {
+            --l;
+            obsr *L = &g_bsr.lv[l];
+            obsr *Cn = &g_bsr.lv[l + 1];
+            const int n = L->E.n;
+            if (coarse_scaling == 1) {
+                double *peh = L->t1, *aeh = L->t2;
+                memset(peh, 0, sizeof(double) * n);
+                or_prolong(1.0, n, L->sagg, Cn->x, peh);
+                or_mxv(n, L->E.ia, L->E.ja, L->E.val, peh, aeh);
+                double alpha = or_dot(n, aeh, L->w) / or_dot(n, aeh, aeh);
+                if (alpha > 1.0) alpha = 1.0;
+                or_axpy(n, alpha, peh, L->x);
+            } else {
+                or_prolong(1.0, n, L->sagg, Cn->x, L->x);
+            }
+            or_bsr_smoothing(L, nb, smoother, steps, 0);
+            if (nu[l] < cycle_type) break;
+            nu[l] = 0;
+        }
+        if (l > 0) goto forward;
+    }
+    memcpy(z, L0->x, sizeof(double) * L0->E.n);
+    return 0;
 }
 
 /* out: nrow, nnzb of level l */

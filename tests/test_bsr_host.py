@@ -125,3 +125,21 @@ def test_drop_in_rejects_malformed_input_on_the_host():
     assert call(_mat(ia, ja, val, 2, nnz=3)) == hz.ERROR_DATA_STRUCTURE
     assert call(_mat(ia, ja, val, 2), np.ones(3)) == hz.ERROR_MAT_SIZE
     assert L.linear_solver_dbsr_krylov_amg(None, None, None, None, None) == hz.ERROR_INPUT_PAR
+
+
+@pytest.mark.parametrize("key", BSR_VARIANTS)
+def test_oracle_bsr_precond_bit_exact(golden, port, key):
+    """The oracle's restatement of precond_dbsr_amg / mgcycle_bsr (block
+    smoothers, sequential residuals, the coarsest GMRES(25) without
+    preconditioner, coarse scaling) gives the reference's z bit for bit."""
+    case = key.split("/")[0]
+    g = small_case(golden("gmres.npz"), case)
+    ia, ja, val = P.block_system(g["A_ia"], g["A_ja"], g["A_val"], NB[case], SEED[case])
+    z = golden("bsr.npz")
+    v = small_case(z, key)
+    ip = [int(t) for t in v["params"]]
+    port.bsr_hierarchy(NB[case], ia, ja, val, theta=float(v["dparams"][0]), coarse_dof=ip[1],
+                       max_levels=ip[0], aggregation_type=ip[7], max_aggregation=ip[8])
+    got = port.bsr_precond(z[f"{case}/b"], cycle_type=ip[2], smoother=ip[3],
+                           presmooth_iter=ip[4], coarse_scaling=ip[9], maxit=ip[11])
+    assert got.tobytes() == v["z"].tobytes()
