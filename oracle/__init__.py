@@ -260,6 +260,14 @@ class Port(_Backend):
                              ctypes.byref(nh))
         return it, x, hist[: min(nh.value, hist_cap)].copy()
 
+    def precond_nl_amli(self, r, degree=2, krylov=4, tol=1e-6):
+        """z = B r with maxit nonlinear AMLI cycles of the last setup
+        (coarse-level Krylov: 5 GCG, else flexible GMRES(30))."""
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros_like(r)
+        self.lib.or_precond_nl_amli(degree, krylov, ctypes.c_double(tol), _p(r), _p(z))
+        return z
+
     def precond_cycle(self, kind, r, coef=None, tol=1e-6):
         """z = B r with maxit AMLI (kind 3, polynomial coefficients coef) or
         additive (kind 5) cycles of the last setup's hierarchy."""

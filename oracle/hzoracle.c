@@ -31,6 +31,9 @@ typedef struct {
     double *val;
 } ocsr;
 
+/* a preconditioner z = B r for the Krylov restatements (NULL: B = I) */
+typedef void (*or_pcfn)(const double *in, double *out, void *ctx);
+
 static void ocsr_free(ocsr *A)
 {
     free(A->ia); free(A->ja); free(A->val);
@@ -803,10 +806,28 @@ static double or_vmv2(const ocsr *A, const double *x, const double *y)
  * ones (beta_i = -(p_i' A Br) / (p_i' A p_i)); the relative residual is
  * ||r|| / ||b||, checked from the second step on.  hist: ||r|| handed to each
  * preconditioner call. */
+typedef struct { int kind, degree; const double *coef; double amg_tol; } or_cycle_pc;
+
+static void or_pc_cycle(const double *in, double *out, void *ctx)
+{
+    const or_cycle_pc *c = (const or_cycle_pc *)ctx;
+    if (c->kind == 1) or_precond(in, out);
+    else or_precond_cycle(c->kind, c->coef, c->degree, c->amg_tol, in, out);
+}
+
+static int or_gcg_on(const ocsr *A, or_pcfn pc, void *pcctx, const double *b, double *u,
+                     double tol, int maxit, double *hist, int hist_cap, int *nhist);
+
 int or_gcg(const double *b, double *u, double tol, int maxit, int kind, const double *coef,
            int degree, double amg_tol, double *hist, int hist_cap, int *nhist)
 {
-    const ocsr *A = &g_or.A[0];
+    or_cycle_pc c = {kind, degree, coef, amg_tol};
+    return or_gcg_on(&g_or.A[0], or_pc_cycle, &c, b, u, tol, maxit, hist, hist_cap, nhist);
+}
+
+static int or_gcg_on(const ocsr *A, or_pcfn pc, void *pcctx, const double *b, double *u,
+                     double tol, int maxit, double *hist, int hist_cap, int *nhist)
+{
     const int m = A->n;
     int nh = 0, iter = 0;
     double *r = (double *)malloc(sizeof(double) * m);
@@ -817,8 +838,8 @@ int or_gcg(const double *b, double *u, double tol, int maxit, int kind, const do
     do {                                                                         \
         if (hist && nh < hist_cap) hist[nh] = or_norm2(m, in);                  \
         ++nh;                                                                    \
-        if (kind == 1) or_precond(in, out);                                      \
-        else or_precond_cycle(kind, coef, degree, amg_tol, in, out);            \
+        if (pc) pc(in, out, pcctx);                                              \
+        else memcpy(out, in, sizeof(double) * m);                                \
     } while (0)
     const double normb = or_norm2(m, b);
     memcpy(r, b, sizeof(double) * m);
@@ -877,20 +898,26 @@ static void or_resid_of(const ocsr *A, int block, const double *b, const double 
         for (int k = A->ia[i]; k < A->ia[i + 1]; ++k) r[i] -= A->val[k] * x[A->ja[k]];
 }
 
-static int or_gmres_on(int flexible, const ocsr *A, int block, int use_pc, const double *b,
-                       double *x, double tol, int MaxIt, int restart, int stop_type,
-                       double *hist, int hist_cap, int *nhist);
+static void or_pc_vcycle(const double *in, double *out, void *ctx)
+{
+    (void)ctx;
+    or_precond(in, out);
+}
+
+static int or_gmres_on(int flexible, const ocsr *A, int block, or_pcfn pc, void *pcctx,
+                       const double *b, double *x, double tol, int MaxIt, int restart,
+                       int stop_type, double *hist, int hist_cap, int *nhist);
 
 int or_gmres(int flexible, const double *b, double *x, double tol, int MaxIt, int restart,
              int stop_type, double *hist, int hist_cap, int *nhist)
 {
-    return or_gmres_on(flexible, &g_or.A[0], 0, 1, b, x, tol, MaxIt, restart, stop_type, hist,
-                       hist_cap, nhist);
+    return or_gmres_on(flexible, &g_or.A[0], 0, or_pc_vcycle, NULL, b, x, tol, MaxIt, restart,
+                       stop_type, hist, hist_cap, nhist);
 }
 
-static int or_gmres_on(int flexible, const ocsr *A, int block, int use_pc, const double *b,
-                       double *x, double tol, int MaxIt, int restart, int stop_type,
-                       double *hist, int hist_cap, int *nhist)
+static int or_gmres_on(int flexible, const ocsr *A, int block, or_pcfn pc, void *pcctx,
+                       const double *b, double *x, double tol, int MaxIt, int restart,
+                       int stop_type, double *hist, int hist_cap, int *nhist)
 {
     const int n = A->n;
     const double cr_max = 0.99, cr_min = 0.174, epsmac = SMALLREAL;
@@ -911,7 +938,7 @@ static int or_gmres_on(int flexible, const ocsr *A, int block, int use_pc, const
     do {                                                                         \
         if (hist && nh < hist_cap) hist[nh] = or_norm2(n, in);                  \
         ++nh;                                                                    \
-        if (use_pc) or_precond(in, out);                                         \
+        if (pc) pc(in, out, pcctx);                                              \
         else memcpy(out, in, sizeof(double) * n);                                \
     } while (0)
     double cr = 1.0, r_norm_old = 0.0, r_norm, relres = BIGREAL, absres0 = BIGREAL;
@@ -1053,6 +1080,78 @@ done:
     free(r); free(w); free(rs); free(c); free(sn); free(pv); free(zv); free(hh);
     if (nhist) *nhist = nh;
     return iter >= MaxIt ? -48 : iter;
+}
+
+/* nl_amli mgcycle.c:561-690 from absolute level a with nrem levels left
+ * (the reference shifts mgl and counts levels from there): smoothing,
+ * residual, restriction; below the second-coarsest level the coarse
+ * correction is amli_degree + 1 steps of GCG (nl_amli_krylov_type 5) or
+ * flexible GMRES(30) on the next level, to tol 1e-4 * amg tol, from zero,
+ * preconditioned by precond_nl_amli there (one cycle); the second-coarsest
+ * level calls the cycle once on the coarsest, which solves directly or by
+ * coarse_itsolver to the same tolerance */
+typedef struct { int a, nrem, degree, krylov; double tol; } or_nl_ctx;
+static double *g_uH[OR_MAXLVL], *g_bH[OR_MAXLVL];
+
+static void or_nl_amli(int a, int nrem, int degree, int krylov, double tol);
+
+static void or_pc_nl_amli(const double *in, double *out, void *ctx)
+{
+    const or_nl_ctx *c = (const or_nl_ctx *)ctx;
+    const int m = g_or.A[c->a].n;
+    memcpy(g_or.b[c->a], in, sizeof(double) * m);
+    memset(g_or.x[c->a], 0, sizeof(double) * m);
+    or_nl_amli(c->a, c->nrem, c->degree, c->krylov, c->tol);
+    memcpy(out, g_or.x[c->a], sizeof(double) * m);
+}
+
+static void or_nl_amli(int a, int nrem, int degree, int krylov, double tol)
+{
+    or_amg *G = &g_or;
+    const double ktol = tol * 1e-4;
+    if (!(0 < nrem - 1)) { or_coarse_solve(a, ktol); return; }
+    ocsr *A0 = &G->A[a], *A1 = &G->A[a + 1];
+    const int m0 = A0->n, m1 = A1->n;
+    or_smooth(G->smoother, 1, G->pre, G->relaxation, m0, A0->ia, A0->ja, A0->val, G->b[a],
+              G->x[a], a == 0 ? G->omega : NULL);
+    memcpy(G->w[a], G->b[a], sizeof(double) * m0);
+    or_aAxpy(-1.0, m0, A0->ia, A0->ja, A0->val, G->x[a], G->w[a]);
+    or_restrict(G->nc[a], G->ria[a], G->rja[a], G->w[a], G->b[a + 1]);
+    memset(G->x[a + 1], 0, sizeof(double) * m1);
+    if (nrem - 2 == 0) {
+        or_nl_amli(a + 1, nrem - 1, degree, krylov, tol);
+    } else {
+        double *bH = g_bH[a + 1], *uH = g_uH[a + 1];
+        memcpy(bH, G->b[a + 1], sizeof(double) * m1);
+        memcpy(uH, G->x[a + 1], sizeof(double) * m1);
+        or_nl_ctx c = {a + 1, nrem - 1, degree, krylov, tol};
+        if (krylov == 5)
+            or_gcg_on(A1, or_pc_nl_amli, &c, bH, uH, ktol, degree + 1, NULL, 0, NULL);
+        else
+            or_gmres_on(1, A1, 0, or_pc_nl_amli, &c, bH, uH, ktol, degree + 1, 30, 1, NULL, 0,
+                        NULL);
+        memcpy(G->b[a + 1], bH, sizeof(double) * m1);
+        memcpy(G->x[a + 1], uH, sizeof(double) * m1);
+    }
+    or_prolong(1.0, m0, G->agg[a], G->x[a + 1], G->x[a]);
+    or_smooth(G->smoother, 0, G->post, G->relaxation, m0, A0->ia, A0->ja, A0->val, G->b[a],
+              G->x[a], a == 0 ? G->omega : NULL);
+}
+
+/* precond_nl_amli precond.c:301-320: maxit cycles from x = 0 */
+int or_precond_nl_amli(int degree, int krylov, double tol, const double *r, double *z)
+{
+    const int m = g_or.A[0].n;
+    for (int l = 1; l < g_or.nl; ++l) {
+        g_uH[l] = (double *)calloc(g_or.A[l].n > 0 ? g_or.A[l].n : 1, sizeof(double));
+        g_bH[l] = (double *)calloc(g_or.A[l].n > 0 ? g_or.A[l].n : 1, sizeof(double));
+    }
+    memcpy(g_or.b[0], r, sizeof(double) * m);
+    memset(g_or.x[0], 0, sizeof(double) * m);
+    for (int i = 0; i < g_or.amg_maxit; ++i) or_nl_amli(0, g_or.nl, degree, krylov, tol);
+    memcpy(z, g_or.x[0], sizeof(double) * m);
+    for (int l = 1; l < g_or.nl; ++l) { free(g_uH[l]); free(g_bH[l]); g_uH[l] = g_bH[l] = NULL; }
+    return 0;
 }
 
 int or_hier_level(int l, int *n, const int **ia, const int **ja, const double **a,
@@ -1629,7 +1728,8 @@ forward:
             obsr *C = &g_bsr.lv[nl - 1];
             const long long cs = C->E.n;
             const int cmaxit = cs * cs < 200 ? (int)(cs * cs) : 200;
-            or_gmres_on(0, &C->E, 1, 0, C->b, C->x, 1e-6, cmaxit, 25, 1, NULL, 0, NULL);
+            or_gmres_on(0, &C->E, 1, NULL, NULL, C->b, C->x, 1e-6, cmaxit, 25, 1, NULL, 0,
+                        NULL);
         }
         while (l > 0) {
             --l;

@@ -123,3 +123,34 @@ def test_oracle_gcg_matches_reference(golden, port, case, var):
         np.testing.assert_allclose(hist, rh, rtol=0, atol=1e-13 * rh.max())
     if "gcg/x" in v:
         np.testing.assert_allclose(x, v["gcg/x"], rtol=0, atol=1e-13 * np.abs(v["gcg/x"]).max())
+
+
+NL_CASES = [("fix", "n"), ("kuhn", "n"), ("kuhn", "ng"), ("kuhn", "nd"), ("kuhn", "ngd"),
+            ("kuhn", "ni")]
+
+
+@pytest.mark.parametrize("case,var", NL_CASES)
+def test_oracle_nl_amli_matches_reference(golden, port, case, var):
+    """The oracle's nonlinear AMLI cycle (or_nl_amli: flexible GMRES(30) or
+    GCG on the coarse levels, preconditioned by the cycle one level down)
+    against one application of the reference's precond_nl_amli: bit for bit
+    with the iterative coarse solver, to 1e-13 of max |z| with the direct
+    one."""
+    import oracle
+    A = small_case(golden("gmres.npz"), case)
+    v = small_case(golden("cycles.npz"), f"{case}/{var}")
+    names = ["max_levels", "coarse_dof", "cycle_type", "smoother", "presmooth_iter",
+             "postsmooth_iter", "coarse_solver", "aggregation_type", "max_aggregation",
+             "coarse_scaling", "print_level", "maxit", "amli_degree", "nl_amli_krylov_type"]
+    ip = [int(t) for t in v["params"]]
+    dp = [float(t) for t in v["dparams"]]
+    kw = dict(zip(names, ip[:14]))
+    kw.update(strong_coupled=dp[0], relaxation=dp[1], tol=dp[2])
+    prm = oracle.AMGParams(**kw)
+    assert port.setup(A["A_ia"], A["A_ja"], A["A_val"], prm) == 0
+    assert port.num_levels() == int(v["levels"])
+    got = port.precond_nl_amli(A["b"], prm.amli_degree, prm.nl_amli_krylov_type, prm.tol)
+    if prm.coarse_solver != 32:
+        assert got.tobytes() == v["z"].tobytes()
+    else:
+        np.testing.assert_allclose(got, v["z"], rtol=0, atol=1e-13 * np.abs(v["z"]).max())
