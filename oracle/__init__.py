@@ -234,6 +234,17 @@ class Port(_Backend):
         nc = self.lib.or_hem_agg(n, _p(ia), _p(ja), _p(val), ctypes.c_double(theta), _p(agg))
         return nc, agg
 
+    def minres_port(self, b, tol=1e-8, maxit=500, stop_type=1, use_pc=True, hist_cap=1024):
+        """dcsr_pminres from x = 0 with the V/W cycle of the last setup (or
+        none): (iterations, x, ||v|| of every vector preconditioned)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b)
+        hist = np.zeros(hist_cap)
+        nh = ctypes.c_int()
+        it = self.lib.or_minres(_p(b), _p(x), ctypes.c_double(tol), maxit, stop_type,
+                                int(use_pc), _p(hist), hist_cap, ctypes.byref(nh))
+        return it, x, hist[: min(nh.value, hist_cap)].copy()
+
     def gmres_port(self, b, tol=1e-8, maxit=500, restart=25, flexible=True, stop_type=1,
                    hist_cap=1024):
         """dcsr_pvgmres / dcsr_pvfgmres from x = 0 with the V/W cycle of the

@@ -591,6 +591,7 @@ static int or_pcg_core(const ocsr *A, const double *b, double *u, int use_pc,
                        int hist_cap, int *nhist);
 static double or_dot(int n, const double *x, const double *y);
 static double or_norm2(int n, const double *x);
+static double or_norminf(int n, const double *x);
 void or_precond(const double *r, double *z);
 
 /* coarse_itsolver mgcycle.c:34-52: unpreconditioned CG to ctol, maxit 20n */
@@ -1080,6 +1081,154 @@ done:
     free(r); free(w); free(rs); free(c); free(sn); free(pv); free(zv); free(hh);
     if (nhist) *nhist = nh;
     return iter >= MaxIt ? -48 : iter;
+}
+
+/* dcsr_pminres krylov.c:2449-2840: preconditioned MINRES by the three-term
+ * recurrence of A-orthonormal directions p (with t = A p, z = B A p), with
+ * the reference's checks: a zero solution (ERROR_SOLVER_SOLSTAG), stagnation
+ * (restart from the true residual, at most 20 times, ERROR_SOLVER_STAG) and
+ * false convergence (restart, at most 20 times, ERROR_SOLVER_TOLSMALL).
+ * hist: ||v|| of every vector preconditioned. */
+static int or_minres_on(const ocsr *A, or_pcfn pc, void *pcctx, const double *b, double *u,
+                        double tol, int MaxIt, int stop_type, double *hist, int hist_cap,
+                        int *nhist)
+{
+    const int m = A->n;
+    const double maxdiff = tol * 1e-4;
+    int iter = 0, stag = 1, more_step = 1, nh = 0;
+    double absres0 = BIGREAL, absres = BIGREAL, normr0 = BIGREAL, relres = BIGREAL;
+    double normu2 = 0.0, normp, alpha = 0.0;
+    double *w = (double *)calloc((size_t)11 * m, sizeof(double));
+    double *p0 = w, *p1 = w + m, *p2 = p1 + m, *z0 = p2 + m, *z1 = z0 + m;
+    double *t0 = z1 + m, *t1 = t0 + m, *t = t1 + m, *tp = t + m, *tz = tp + m, *r = tz + m;
+#define OR_M_PC(in, out)                                                        \
+    do {                                                                         \
+        if (hist && nh < hist_cap) hist[nh] = or_norm2(m, in);                  \
+        ++nh;                                                                    \
+        if (pc) pc(in, out, pcctx);                                              \
+        else memcpy(out, in, sizeof(double) * m);                                \
+    } while (0)
+#define OR_M_MEASURE()                                                          \
+    do {                                                                         \
+        if (stop_type == 2) {                                                    \
+            OR_M_PC(r, t);                                                       \
+            absres = sqrt(fabs(or_dot(m, r, t)));                                \
+            relres = absres / normr0;                                            \
+        } else {                                                                 \
+            absres = sqrt(or_dot(m, r, r));                                      \
+            relres = absres / (stop_type == 3 ? normu2 : normr0);                \
+        }                                                                        \
+    } while (0)
+#define OR_M_RESTART(use_abs)                                                   \
+    do {                                                                         \
+        memset(p0, 0, sizeof(double) * m);                                       \
+        OR_M_PC(r, p1);                                                          \
+        or_mxv(m, A->ia, A->ja, A->val, p1, tp);                                 \
+        OR_M_PC(tp, tz);                                                         \
+        normp = or_dot(m, tz, tp);                                               \
+        normp = sqrt((use_abs) ? fabs(normp) : normp);                           \
+        memcpy(t, p1, sizeof(double) * m);                                       \
+        memset(t0, 0, sizeof(double) * m);                                       \
+        memset(z0, 0, sizeof(double) * m);                                       \
+        memset(t1, 0, sizeof(double) * m);                                       \
+        memset(z1, 0, sizeof(double) * m);                                       \
+        memset(p1, 0, sizeof(double) * m);                                       \
+        or_axpy(m, 1 / normp, t, p1);                                            \
+        or_axpy(m, 1 / normp, tp, t1);                                           \
+        or_axpy(m, 1 / normp, tz, z1);                                           \
+    } while (0)
+    or_resid_of(A, 0, b, u, r);
+    OR_M_PC(r, p1);
+    if (stop_type == 2) {
+        absres0 = sqrt(or_dot(m, r, p1));
+        normr0 = absres0 > SMALLREAL ? absres0 : SMALLREAL;
+        relres = absres0 / normr0;
+    } else if (stop_type == 3) {
+        absres0 = or_norm2(m, r);
+        normu2 = or_norm2(m, u);
+        if (normu2 < SMALLREAL) normu2 = SMALLREAL;
+        relres = absres0 / normu2;
+    } else {
+        absres0 = or_norm2(m, r);
+        normr0 = absres0 > SMALLREAL ? absres0 : SMALLREAL;
+        relres = absres0 / normr0;
+    }
+    if (relres < tol || absres0 < 1e-3 * tol) goto done;
+    or_mxv(m, A->ia, A->ja, A->val, p1, tp);
+    OR_M_PC(tp, tz);
+    normp = sqrt(fabs(or_dot(m, tz, tp)));
+    memcpy(t, p1, sizeof(double) * m);
+    memset(p1, 0, sizeof(double) * m);
+    or_axpy(m, 1 / normp, t, p1);
+    memset(t0, 0, sizeof(double) * m);
+    memcpy(z0, t0, sizeof(double) * m);
+    memcpy(t1, t0, sizeof(double) * m);
+    memcpy(z1, t0, sizeof(double) * m);
+    or_axpy(m, 1.0 / normp, tp, t1);
+    or_axpy(m, 1.0 / normp, tz, z1);
+    while (iter++ < MaxIt) {
+        alpha = or_dot(m, r, z1);
+        or_axpy(m, alpha, p1, u);
+        or_axpy(m, -alpha, t1, r);
+        or_mxv(m, A->ia, A->ja, A->val, z1, t);
+        const double alpha1 = or_dot(m, z1, t);
+        or_mxv(m, A->ia, A->ja, A->val, z0, t);
+        const double alpha0 = or_dot(m, z1, t);
+        memcpy(p2, z1, sizeof(double) * m);
+        or_axpy(m, -alpha1, p1, p2);
+        or_axpy(m, -alpha0, p0, p2);
+        or_mxv(m, A->ia, A->ja, A->val, p2, tp);
+        OR_M_PC(tp, tz);
+        normp = sqrt(fabs(or_dot(m, tz, tp)));
+        if (normp < 1e-14) { iter--; break; }
+        memcpy(t, p2, sizeof(double) * m);
+        memset(p2, 0, sizeof(double) * m);
+        or_axpy(m, 1 / normp, t, p2);
+        memcpy(p0, p1, sizeof(double) * m);
+        memcpy(p1, p2, sizeof(double) * m);
+        memcpy(t0, t1, sizeof(double) * m);
+        memcpy(z0, z1, sizeof(double) * m);
+        memset(t1, 0, sizeof(double) * m);
+        memcpy(z1, t1, sizeof(double) * m);
+        or_axpy(m, 1 / normp, tp, t1);
+        or_axpy(m, 1 / normp, tz, z1);
+        normu2 = or_norm2(m, u);
+        OR_M_MEASURE();
+        if (or_norminf(m, u) <= SMALLREAL) { iter = -43; break; }
+        double normuu = or_norm2(m, p1);
+        normuu = fabs(alpha) * (normuu / normu2);
+        if (normuu < maxdiff) {
+            or_resid_of(A, 0, b, u, r);
+            OR_M_MEASURE();
+            if (relres < tol) break;
+            if (stag >= 20) { iter = -42; break; }
+            ++stag;
+            OR_M_RESTART(1);
+        }
+        if (relres < tol) {
+            or_resid_of(A, 0, b, u, r);
+            OR_M_MEASURE();
+            if (relres < tol) break;
+            if (more_step >= 20) { iter = -44; break; }
+            ++more_step;
+            OR_M_RESTART(0);
+        }
+        absres0 = absres;
+    }
+done:
+#undef OR_M_PC
+#undef OR_M_MEASURE
+#undef OR_M_RESTART
+    free(w);
+    if (nhist) *nhist = nh;
+    return iter > MaxIt ? -48 : iter;
+}
+
+int or_minres(const double *b, double *x, double tol, int maxit, int stop_type, int use_pc,
+              double *hist, int hist_cap, int *nhist)
+{
+    return or_minres_on(&g_or.A[0], use_pc ? or_pc_vcycle : NULL, NULL, b, x, tol, maxit,
+                        stop_type, hist, hist_cap, nhist);
 }
 
 /* nl_amli mgcycle.c:561-690 from absolute level a with nrem levels left

@@ -38,3 +38,31 @@ def test_oracle_gmres_matches_reference(golden, port, case):
         if key + "/x" in A:
             np.testing.assert_allclose(x, A[key + "/x"], rtol=0,
                                        atol=1e-9 * np.abs(A[key + "/x"]).max(), err_msg=key)
+
+
+BASES = {"fix": {}, "kuhn": dict(smoother=10, presmooth_iter=2, postsmooth_iter=2,
+                                 coarse_dof=100)}
+
+
+@pytest.mark.parametrize("case", ["fix", "kuhn"])
+def test_oracle_minres_matches_reference(golden, port, case):
+    """dcsr_pminres restated (or_minres) against the reference's runs in
+    tests/golden/minres.npz: the same iteration counts and preconditioner
+    calls for the three stopping types with the V-cycle, histories and
+    solutions to 1e-13; without a preconditioner (139 steps on the Kuhn
+    matrix) the solution bit for bit."""
+    A = small_case(golden("gmres.npz"), case)
+    z = golden("minres.npz")
+    assert port.setup(A["A_ia"], A["A_ja"], A["A_val"], oracle.AMGParams(**BASES[case])) == 0
+    for stop in (1, 2, 3):
+        v = small_case(z, f"{case}/s{stop}")
+        it, x, hist = port.minres_port(A["b"], tol=1e-8, maxit=500, stop_type=stop)
+        assert it == int(v["iters"]), stop
+        assert len(hist) == len(v["hist"]), stop
+        np.testing.assert_allclose(hist, v["hist"], rtol=0, atol=1e-13 * v["hist"].max())
+        np.testing.assert_allclose(x, v["x"], rtol=0, atol=1e-13 * np.abs(v["x"]).max())
+    if case == "kuhn":
+        v = small_case(z, "kuhn/nopc")
+        it, x, _ = port.minres_port(A["b"], tol=1e-6, maxit=2000, stop_type=1, use_pc=False)
+        assert it == int(v["iters"])
+        assert x.tobytes() == v["x"].tobytes()
