@@ -3,7 +3,11 @@
  *
  * A plain-C restatement of HAZmath's UA-AMG preconditioned CG path, written
  * from the reference's behaviour (each function cites the reference
- * file:line it follows).  It is the checker for the CUDA library: only the
+ * file:line it follows), and of the configurations around it: VMB and HEC
+ * aggregation (with the C library's rand() stream), smoothed aggregation,
+ * the block (BSR) setup and cycle, the AMLI / nonlinear AMLI / additive
+ * cycles, GCG, MINRES and (flexible) GMRES.  It is the checker for the CUDA
+ * library: only the
  * tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
  * It is pinned against the reference itself (oracle/_ref, built by
  * oracle/build_ref.sh) through the golden fixtures in tests/golden/.
