@@ -54,7 +54,7 @@ HZB_GS_EXACT, HZB_GS_MULTICOLOR = 0, 1
 HZB_MATCH_EXACT, HZB_MATCH_PARALLEL = 0, 1
 # kernels hzb_time_kernel can time
 HZB_K_SPMV64, HZB_K_SPMV32, HZB_K_RES64, HZB_K_L1_32, HZB_K_L1_64 = 0, 1, 2, 3, 4
-HZB_K_BSR_RES, HZB_K_BSR_JAC, HZB_K_BSR_GS = 5, 6, 7
+HZB_K_BSR_RES, HZB_K_BSR_JAC, HZB_K_BSR_GS, HZB_K_GS64 = 5, 6, 7, 8
 MAX_AMG_LVL = 20
 
 

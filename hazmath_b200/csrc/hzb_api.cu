@@ -393,6 +393,10 @@ extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
     case HZB_K_SPMV64: case HZB_K_SPMV32: bytes += 2 * vb * n; break;     // x, y
     case HZB_K_RES64: bytes += 3 * vb * n; break;                        // x, b, w
     case HZB_K_L1_32: case HZB_K_L1_64: bytes += 3 * vb * n; break;      // x, b, xn
+    case HZB_K_GS64:
+        if (level >= S->nl - 1) return ERROR_INPUT_PAR;   // the coarsest is not smoothed
+        bytes += 4 * vb * n;                                // b, 1/d, x read and written
+        break;
     default: return ERROR_INPUT_PAR;
     }
     auto launch = [&]() -> int {
@@ -405,6 +409,8 @@ extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
             return spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, S->s);
         case HZB_K_L1_32:
             return l1_sweep<float>(L.A32(), L.b32, L.x32, L.t32, nullptr, S->s);
+        case HZB_K_GS64:
+            return time_gs_sweep(S, level);
         default:
             return l1_sweep<double>(L.A64(), L.b, L.x, L.t, nullptr, S->s);
         }

@@ -139,6 +139,14 @@ static int gs_sweep(hzb_solver *S, Level &L, int kind, bool forward, double w) {
     return run_sets(S, A, forward ? L.fwd : L.bwd, kind, d, w, L.b, L.x, false);
 }
 
+// one forward Gauss-Seidel sweep of level l as the cycle runs it (the level's
+// schedule, exact or multicolour), for hzb_time_kernel
+int time_gs_sweep(hzb_solver *S, int l) {
+    Level &L = S->lv[l];
+    if (!L.d_gs_f) return ERROR_INPUT_PAR;   // the smoother of the setup is not GS
+    return gs_sweep(S, L, 0, true, 1.0);
+}
+
 int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc) {
     Level &L = S->lv[l];
     const int sweeps = pre ? cyc.presmooth_iter : cyc.postsmooth_iter;

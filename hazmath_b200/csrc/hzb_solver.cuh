@@ -232,6 +232,8 @@ int learn_loss_grad(hzb_solver *S, const float *omega, int ns, const double *E, 
 // dcsr_aAxpy)
 int restrict_level(hzb_solver *S, int l, const double *w, double *bc);
 int prolong_level(hzb_solver *S, int l, const double *xc, double *x, double alpha);
+// one forward Gauss-Seidel sweep of level l on its schedule (level b, x)
+int time_gs_sweep(hzb_solver *S, int l);
 // smoothing of level l as mgcycle's pre (pre = true) / post smoothing calls
 int smooth64(hzb_solver *S, int l, bool pre, const AMG_param &cyc);
 // diagonals and sweep schedules the configured smoother needs on level L

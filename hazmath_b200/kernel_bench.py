@@ -1,13 +1,15 @@
 """Level-kernel timing on a workload's hierarchy.
 
-    python -m hazmath_b200.kernel_bench [--case c2|c5] [--levels 0,1,2]
-        [--kernels spmv64,spmv32,res64,l1_32,l1_64] [--reps 50]
-        [--precision mixed|fp64] [--matching parallel|exact]
+    python -m hazmath_b200.kernel_bench [--case c1|c2|c5] [--levels 0,1,2]
+        [--kernels spmv64,spmv32,res64,l1_32,l1_64,gs64] [--reps 50]
+        [--precision mixed|fp64] [--matching parallel|exact] [--smoother l1|gs]
     python -m hazmath_b200.kernel_bench --assemble [--case c2|c5] [--reps 20]
 
-Builds the UA-AMG hierarchy (l1-Jacobi V(2,2) settings) of the 3D P1
-log-normal diffusion problem on the Kuhn mesh of 128^3 (c2, sigma 1) or
-256^3 (c5, sigma 1.5) cubes, then times each requested kernel on each
+Builds the UA-AMG hierarchy (l1-Jacobi V(2,2) settings, or Gauss-Seidel
+V(1,1) with --smoother gs, whose sweep gs64 times on the level schedules) of
+the 3D P1 log-normal diffusion problem on the Kuhn mesh of 128^3 (c2,
+sigma 1) or 256^3 (c5, sigma 1.5) cubes, or of the 2D 255^2 Poisson problem
+(c1), then times each requested kernel on each
 requested level with hzb_time_kernel: `reps` back-to-back launches on the
 handle's stream between CUDA events, after one warm-up launch.  Prints
 achieved GB/s from the kernel's algorithmic bytes and the fraction of the
@@ -27,14 +29,15 @@ import os
 
 import numpy as np
 
-from . import (HZB_K_L1_32, HZB_K_L1_64, HZB_K_RES64, HZB_K_SPMV32, HZB_K_SPMV64,
+from . import (HZB_K_GS64, HZB_K_L1_32, HZB_K_L1_64, HZB_K_RES64, HZB_K_SPMV32, HZB_K_SPMV64,
                HZB_MATCH_EXACT, HZB_MATCH_PARALLEL, HZB_PREC_FP64, HZB_PREC_MIXED,
-               SMOOTHER_L1DIAG, Solver, b200_param, last_error, lib, bench_amg)
+               SMOOTHER_GS, SMOOTHER_L1DIAG, Solver, b200_param, last_error, lib,
+               bench_amg)
 from . import problems as P
 
 KERNELS = {"spmv64": HZB_K_SPMV64, "spmv32": HZB_K_SPMV32, "res64": HZB_K_RES64,
-           "l1_32": HZB_K_L1_32, "l1_64": HZB_K_L1_64}
-CASES = {"c2": (128, 1.0, 2), "c5": (256, 1.5, 7)}
+           "l1_32": HZB_K_L1_32, "l1_64": HZB_K_L1_64, "gs64": HZB_K_GS64}
+CASES = {"c1": None, "c2": (128, 1.0, 2), "c5": (256, 1.5, 7)}
 PEAKS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
                      "MEASURED_PEAKS.json")
 
@@ -48,15 +51,22 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--matching", default="parallel", choices=["parallel", "exact"])
     ap.add_argument("--assemble", action="store_true")
+    ap.add_argument("--smoother", default="l1", choices=["l1", "gs"])
     a = ap.parse_args()
+    if a.assemble and a.case == "c1":
+        ap.error("--assemble times the Kuhn-mesh cases c2 and c5")
     import torch
     if a.assemble:
         return assemble(a, torch)
-    N, sigma, seed = CASES[a.case]
-    ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, sigma, 8.0, seed))
+    if a.case == "c1":
+        ia, ja, val = P.poisson2d_5pt(255)
+    else:
+        N, sigma, seed = CASES[a.case]
+        ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, sigma, 8.0, seed))
     n = len(ia) - 1
     dia, dja, dval = (torch.from_numpy(v).cuda() for v in (ia, ja, val))
-    amg = bench_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2)
+    amg = bench_amg(smoother=SMOOTHER_L1DIAG, presmooth_iter=2, postsmooth_iter=2) \
+        if a.smoother == "l1" else bench_amg(smoother=SMOOTHER_GS)
     prec = HZB_PREC_MIXED if a.precision == "mixed" else HZB_PREC_FP64
     match = HZB_MATCH_PARALLEL if a.matching == "parallel" else HZB_MATCH_EXACT
     S = Solver(amg, None, b200_param(precision=prec, matching=match))

@@ -594,7 +594,8 @@ INT  hzb_learn_select_omega(hzb_solver *s, hzb_gnn *g, INT ns,
  * index per entry, row pointers, and each vector once).  which:
  *   HZB_K_SPMV64  y = A x, FP64        HZB_K_SPMV32  y = A x, FP32
  *   HZB_K_RES64   w = b - A x, FP64    HZB_K_L1_32   l1-Jacobi sweep, FP32
- *   HZB_K_L1_64   l1-Jacobi sweep, FP64
+ *   HZB_K_L1_64   l1-Jacobi sweep, FP64  HZB_K_GS64    forward Gauss-Seidel sweep
+ *                                        on the level's schedule (GS setups)
  * and on a block (BSR) hierarchy of the handle:
  *   HZB_K_BSR_RES  w = b - A x         HZB_K_BSR_JAC  block Jacobi sweep
  *   HZB_K_BSR_GS   ascending block Gauss-Seidel sweep (all level sets)     */
@@ -606,6 +607,7 @@ INT  hzb_learn_select_omega(hzb_solver *s, hzb_gnn *g, INT ns,
 #define HZB_K_BSR_RES 5
 #define HZB_K_BSR_JAC 6
 #define HZB_K_BSR_GS  7
+#define HZB_K_GS64    8
 INT hzb_time_kernel(hzb_solver *s, INT which, INT level, INT reps,
                     REAL *ms_per_launch, REAL *bytes_per_launch);
 
