@@ -1186,6 +1186,10 @@ extern "C" INT linear_solver_dbsr_krylov_amg(dBSRmat *A, dvector *b, dvector *x,
     krylov_banner(prtlvl, type);
     const INT it = hzb_bsr_solve_host(S, b->val, x->val);
     if (type == SOLVER_CG) printf("Estimated condition number = %13.6e\n", S->st.condest);
+    if (prtlvl >= PRINT_SOME && it >= 0) {   // itsolver.c:298-303
+        printf("Iterative method costs %.4f seconds.\n", S->st.solve_seconds);
+        printf("**********************************************************\n");
+    }
     if (prtlvl >= PRINT_MIN)
         printf("BSR Krylov method costs %.4f seconds.\n",
                S->st.setup_seconds + S->st.solve_seconds);
