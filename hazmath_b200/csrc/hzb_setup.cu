@@ -983,6 +983,57 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
 }
 
 // ---------------------------------------------------------------------------
+// Caller-supplied Galerkin inputs, checked before any kernel indexes by them
+// (read-only): aggregate ids in [-1, nc), row pointers non-decreasing from 0
+// to nnz, column indices in [0, n).  Bits of *bad: 1 aggregate id, 2 row
+// pointers, 4 column index.
+// ---------------------------------------------------------------------------
+__global__ void k_check_rap_inputs(int n, int nnz, const int *__restrict__ ia,
+                                   const int *__restrict__ ja, int nc,
+                                   const int *__restrict__ agg, int *bad) {
+    int b = 0;
+    const int m = n > nnz ? n : nnz;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += gridDim.x * blockDim.x) {
+        if (i < n) {
+            const int c = agg[i];
+            if (c < -1 || c >= nc) b |= 1;
+            if (ia[i + 1] < ia[i]) b |= 2;
+        }
+        if (i < nnz) {
+            const int j = ja[i];
+            if (j < 0 || j >= n) b |= 4;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (ia[0] != 0 || ia[n] != nnz)) b |= 2;
+    if (b) atomicOr(bad, b);
+}
+
+int check_rap_inputs(int n, int nnz, const int *ia, const int *ja, int nc, const int *agg,
+                     int *d_bad, cudaStream_t s) {
+    HZB_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+    k_check_rap_inputs<<<grid_for(n > nnz ? n : nnz), 256, 0, s>>>(n, nnz, ia, ja, nc, agg,
+                                                                    d_bad);
+    count_launch();
+    int bad = 0;
+    HZB_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HZB_CUDA(cudaStreamSynchronize(s));
+    if (bad & 1) {
+        set_error_msg("Galerkin product: an aggregate id lies outside [-1, nc)");
+        return ERROR_INPUT_PAR;
+    }
+    if (bad & 2) {
+        set_error_msg("Galerkin product: row pointers do not rise from 0 to nnz");
+        return ERROR_INPUT_PAR;
+    }
+    if (bad & 4) {
+        set_error_msg("Galerkin product: a column index lies outside [0, n)");
+        return ERROR_INPUT_PAR;
+    }
+    return SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
 // R = P^T pattern with ascending fine indices per row
 // ---------------------------------------------------------------------------
 __global__ void k_agg_count(int n, const int *__restrict__ agg, int *cnt) {
@@ -1549,24 +1600,26 @@ done:
 // ---------------------------------------------------------------------------
 // Galerkin product without device allocation.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is
-// being captured into a graph, processes whose device memory is reserved up
-// front by their own allocator, and library code that must not trigger the
-// implicit device synchronisation of cudaMalloc/cudaFree.  For them the
-// product's scratch (restriction pattern, per-row bounds, slot lists, scan
-// partials) lives in one file-scope device array of fixed size, held by every
-// device that loads this library until the process exits.  Its size bounds
-// the problem: n <= HZB_NOALLOC_MAX_ROWS fine rows and nnz <=
-// HZB_NOALLOC_MAX_NNZ stored entries.
+// Some callers cannot call cudaMalloc: processes whose device memory is
+// reserved up front by their own allocator (a framework's caching pool, an
+// embedded solver with a fixed memory budget), and library code that must
+// not trigger the implicit device synchronisation that cudaMalloc and
+// cudaFree bring.  For them the product's scratch (restriction pattern,
+// per-row bounds, slot lists, scan partials, an error flag) lives in one
+// file-scope device array of fixed size, held by every device that loads
+// this library until the process exits.  Its size bounds the problem:
+// n <= HZB_NOALLOC_MAX_ROWS fine rows and nnz <= HZB_NOALLOC_MAX_NNZ stored
+// entries.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr size_t NA_ROWS = HZB_NOALLOC_MAX_ROWS;
 constexpr size_t NA_NNZ = HZB_NOALLOC_MAX_NNZ;
 constexpr size_t NA_TMP = (NA_ROWS + 1 + 2047) / 2048 + 8;
-// int words: cnt, ria, rja, ub, off, rowcnt, scan tmp, scol
-constexpr size_t NA_INTS = 6 * (NA_ROWS + 1) + NA_TMP + (NA_NNZ + NA_ROWS);
+constexpr size_t NA_SLOTS = NA_NNZ + NA_ROWS;   // slot lists: nc + sum of row lengths
+// int words: cnt, ria, rja, ub, off, rowcnt, scan tmp, error flag (padded), scol
+constexpr size_t NA_INTS = 6 * (NA_ROWS + 1) + NA_TMP + 4 + NA_SLOTS;
 constexpr size_t NA_INT_WORDS = (NA_INTS + 1) / 2;   // in 8-byte words
-constexpr size_t NA_WORDS = NA_INT_WORDS + (NA_NNZ + NA_ROWS);   // + sval
+constexpr size_t NA_WORDS = NA_INT_WORDS + NA_SLOTS;   // + sval
 }  // namespace
 
 static __device__ __align__(256) double g_noalloc_scratch[NA_WORDS];
@@ -1595,7 +1648,9 @@ static int noalloc_scratch(double **p) {
 
 // The same kernels, in the same order, as hzb_rap_agg_device, so the result
 // is identical bit for bit; only the scratch comes from the static array and
-// the outputs from the caller.
+// the outputs from the caller.  The inputs are checked on the device before
+// any kernel indexes by them, and the slot lists' total against the array
+// before they are written.
 extern "C" INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const INT *ja,
                                           const REAL *val, INT nc, const INT *agg,
                                           INT cap_nnz, INT *rap_ia, INT *rap_ja,
@@ -1605,6 +1660,10 @@ extern "C" INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const I
         set_error_msg("hzb_rap_agg_device_noalloc: sizes beyond HZB_NOALLOC_MAX_ROWS / "
                       "HZB_NOALLOC_MAX_NNZ");
         return ERROR_MAT_SIZE;
+    }
+    if (!ia || !ja || !val || !agg || !rap_ia || !rap_nnz || cap_nnz < 0) {
+        set_error_msg("hzb_rap_agg_device_noalloc: null array or negative capacity");
+        return ERROR_INPUT_PAR;
     }
     double *base = nullptr;
     HZB_TRY(noalloc_scratch(&base));
@@ -1616,10 +1675,12 @@ extern "C" INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const I
     int *off = ip;                       ip += NA_ROWS + 1;
     int *rowcnt = ip;                    ip += NA_ROWS + 1;
     int *tmp = ip;                       ip += NA_TMP;
+    int *bad = ip;                       ip += 4;
     int *scol = ip;
     double *sval = base + NA_INT_WORDS;
     cudaStream_t s = 0;
     const int gn = grid_for(n), gc = grid_for(nc);
+    HZB_TRY(check_rap_inputs(n, nnz, ia, ja, nc, agg, bad, s));
     // R = P^T (counts start at zero: the array keeps the previous call's data)
     HZB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * nc, s));
     k_agg_count<<<gn, 256, 0, s>>>(n, agg, cnt);
@@ -1632,6 +1693,13 @@ extern "C" INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const I
     k_rap_bound<<<gc, 256, 0, s>>>(nc, ria, rja, ia, ub);
     count_launch(3);
     HZB_TRY(scan_exclusive(ub, off, nc, tmp, s));
+    int slots = 0;
+    HZB_CUDA(cudaMemcpyAsync(&slots, off + nc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HZB_CUDA(cudaStreamSynchronize(s));
+    if (slots < 0 || (size_t)slots > NA_SLOTS) {
+        set_error_msg("hzb_rap_agg_device_noalloc: the slot lists exceed the static scratch");
+        return ERROR_MAT_SIZE;
+    }
     k_rap_build<<<gc, 128, 0, s>>>(nc, ria, rja, ia, ja, val, agg, off, scol, sval, rowcnt);
     count_launch();
     HZB_TRY(scan_exclusive(rowcnt, rap_ia, nc, tmp, s));
@@ -1642,6 +1710,10 @@ extern "C" INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const I
     if (total > cap_nnz) {
         set_error_msg("hzb_rap_agg_device_noalloc: output capacity too small (*rap_nnz "
                       "holds the size needed)");
+        return ERROR_INPUT_PAR;
+    }
+    if (total > 0 && (!rap_ja || !rap_val)) {
+        set_error_msg("hzb_rap_agg_device_noalloc: null output array");
         return ERROR_INPUT_PAR;
     }
     k_rap_compact<<<gc, 256, 0, s>>>(nc, off, rap_ia, scol, sval, rap_ja, rap_val);

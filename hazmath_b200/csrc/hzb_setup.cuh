@@ -34,6 +34,13 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
 int vmb_aggregate(int n, const int *nia, const int *nja, int max_agg, int *agg, int *nagg,
                   int *work, cudaStream_t s);
 
+// A caller's Galerkin inputs checked on the device before any kernel indexes
+// by them (aggregate ids in [-1, nc), row pointers rising from 0 to nnz,
+// columns in [0, n)); d_bad is one device int of scratch.  Synchronises s;
+// ERROR_INPUT_PAR with a message on bad input.
+int check_rap_inputs(int n, int nnz, const int *ia, const int *ja, int nc, const int *agg,
+                     int *d_bad, cudaStream_t s);
+
 // R = P^T: rows of R list fine indices ascending (dcsr_trans, sparse.c:770).
 int restriction_pattern(int n, int nc, const int *agg, int *ria, int *rja,
                         int *tmp, cudaStream_t s);

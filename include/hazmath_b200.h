@@ -595,7 +595,14 @@ INT  hzb_learn_select_omega(hzb_solver *s, hzb_gnn *g, INT ns,
  *   HZB_K_SPMV64  y = A x, FP64        HZB_K_SPMV32  y = A x, FP32
  *   HZB_K_RES64   w = b - A x, FP64    HZB_K_L1_32   l1-Jacobi sweep, FP32
  *   HZB_K_L1_64   l1-Jacobi sweep, FP64  HZB_K_GS64    forward Gauss-Seidel sweep
- *                                        on the level's schedule (GS setups)
+ *                                        on the level's schedule; needs a
+ *                                        setup with a Gauss-Seidel smoother
+ *                                        (ERROR_INPUT_PAR otherwise)
+ * HZB_K_L1_32 on level 0 runs with the learned weights (and counts their
+ * 4 bytes per row) when the handle's solve uses them.
+ * The byte counts are single-pass lower bounds: the exact Gauss-Seidel
+ * schedule's level sets and the multicolour schedule's colours re-read x,
+ * which the count leaves out.
  * and on a block (BSR) hierarchy of the handle:
  *   HZB_K_BSR_RES  w = b - A x         HZB_K_BSR_JAC  block Jacobi sweep
  *   HZB_K_BSR_GS   ascending block Gauss-Seidel sweep (all level sets)     */
@@ -630,7 +637,9 @@ INT hzb_aggregation_hem_device(INT n, INT nnz, const INT *ia, const INT *ja,
                                INT *agg, INT *num_aggregates);
 /* Galerkin product for an aggregate map; the device pattern (int32) and the
  * values are written to freshly allocated device arrays returned through
- * rap_*; free them with hzb_free_device. */
+ * rap_*; free them with hzb_free_device.  The inputs are checked on the
+ * device first (agg in [-1, nc), ia rising from 0 to nnz, ja in [0, n)); a
+ * violation returns ERROR_INPUT_PAR before any kernel indexes by them. */
 INT hzb_rap_agg_device(INT n, INT nnz, const INT *ia, const INT *ja,
                        const REAL *val, INT nc, const INT *agg,
                        INT *rap_nnz, INT **rap_ia, INT **rap_ja,
@@ -659,24 +668,31 @@ INT hzb_assemble_p1_kuhn_device(INT N, const REAL *d_kcell, const REAL *K, INT *
 INT hzb_copy_to_host(void *dst, const void *src_device, size_t bytes);
 
 /* Galerkin product that allocates nothing.  No counterpart in the
- * reference.  It serves callers that cannot call cudaMalloc: code running
- * while a stream is captured into a CUDA graph, processes whose device
- * memory is reserved up front by their own allocator, and library code that
- * must not trigger the implicit device synchronisation of cudaMalloc or
- * cudaFree.  The result equals hzb_rap_agg_device's bit for bit.
+ * reference.  It serves callers that cannot call cudaMalloc: processes whose
+ * device memory is reserved up front by their own allocator (a caching pool
+ * that owns the whole budget, an embedded solver with a fixed footprint),
+ * and library code that must not trigger the implicit device
+ * synchronisation of cudaMalloc or cudaFree.  The result equals
+ * hzb_rap_agg_device's bit for bit.
  *  - Inputs and outputs are the caller's device arrays: rap_ia (nc+1 ints),
  *    rap_ja (cap_nnz ints) and rap_val (cap_nnz doubles); *rap_nnz receives
  *    the product's entry count, also when it exceeds cap_nnz (then the call
  *    returns ERROR_INPUT_PAR and fills only rap_ia).
+ *  - The inputs are checked on the device before any kernel indexes by them:
+ *    agg in [-1, nc), ia rising from 0 to nnz, ja in [0, n); a violation
+ *    returns ERROR_INPUT_PAR and writes nothing.
  *  - Scratch is one file-scope device array of about 15 MB, held by every
  *    device that loads the library until the process exits.  It limits the
  *    fine matrix to n <= HZB_NOALLOC_MAX_ROWS rows and nnz <=
  *    HZB_NOALLOC_MAX_NNZ entries; larger sizes return ERROR_MAT_SIZE.
  *  - The first call on a device looks up the array's device address (with
  *    that device current); make that first call before any stream capture.
- *  - Every call shares the array: calls that overlap on the GPU (several
- *    host threads or streams at once) race.  Runs on the legacy default
- *    stream and synchronises before returning. */
+ *  - Every call shares the array, which keeps the last call's contents (the
+ *    call clears what must start at zero): calls that overlap on the GPU
+ *    (several host threads or streams at once) race.  Runs on the legacy
+ *    default stream; it waits for the device three times (after the input
+ *    check, to read the slot-list total, to read the entry count) and once
+ *    more before returning. */
 #define HZB_NOALLOC_MAX_ROWS 65536
 #define HZB_NOALLOC_MAX_NNZ  1048576
 INT hzb_rap_agg_device_noalloc(INT n, INT nnz, const INT *ia, const INT *ja,
