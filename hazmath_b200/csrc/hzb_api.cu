@@ -399,6 +399,11 @@ extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
         break;
     default: return ERROR_INPUT_PAR;
     }
+    // the FP32 sweep of level 0 runs with the learned weights when the
+    // solve does (as smooth32 passes them), and reads them
+    const float *om = (which == HZB_K_L1_32 && level == 0 && S->omega_active) ? S->omega
+                                                                             : nullptr;
+    if (om) bytes += 4.0 * n;
     auto launch = [&]() -> int {
         switch (which) {
         case HZB_K_SPMV64:
@@ -408,7 +413,7 @@ extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
         case HZB_K_RES64:
             return spmv<double>(L.A64(), SPMV_RES, L.x, L.b, L.w, 1.0, nullptr, S->s);
         case HZB_K_L1_32:
-            return l1_sweep<float>(L.A32(), L.b32, L.x32, L.t32, nullptr, S->s);
+            return l1_sweep<float>(L.A32(), L.b32, L.x32, L.t32, om, S->s);
         case HZB_K_GS64:
             return time_gs_sweep(S, level);
         default:
@@ -1450,9 +1455,14 @@ extern "C" INT hzb_rap_agg_device(INT n, INT nnz, const INT *ia, const INT *ja,
     int rc = SUCCESS;
     DCsr<double> A;
     A.n = n; A.nnz = nnz; A.ia = ia; A.ja = ja; A.val = val;
+    if (n < 1 || nnz < 0 || nc < 1 || nc > n || !ia || !ja || !val || !agg) {
+        set_error_msg("hzb_rap_agg_device: need n >= 1, nnz >= 0, 1 <= nc <= n");
+        return ERROR_INPUT_PAR;
+    }
     if ((rc = dalloc(&ria, nc + 1)) || (rc = dalloc(&rja, n)) ||
         (rc = dalloc(&tmp, scan_tmp_size(n + 1)))) goto done;
-    rc = restriction_pattern(n, nc, agg, ria, rja, tmp, s);
+    rc = check_rap_inputs(n, nnz, ia, ja, nc, agg, ria, s);
+    if (!rc) rc = restriction_pattern(n, nc, agg, ria, rja, tmp, s);
     if (!rc) rc = rap_agg(A, nc, agg, ria, rja, rap_ia, rap_ja, rap_val, rap_nnz, s);
 done:
     dfree(ria); dfree(rja); dfree(tmp);

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|hec|layout]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|hec|layout|c2|c5]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -33,7 +33,9 @@ from hazmath_b200 import problems as P  # noqa: E402
 
 ARGS = [a for i, a in enumerate(sys.argv[1:], 1)
         if a != "--only" and sys.argv[i - 1] != "--only"]
-REF = ARGS[0] if ARGS else os.environ.get("HAZ_REF", "/root/reference")
+REF = ARGS[0] if ARGS else os.environ.get("HAZ_REF", "")
+if not os.path.isdir(os.path.join(REF, "src")):
+    sys.exit("make_golden.py: give the reference's source tree as REFERENCE_DIR or $HAZ_REF")
 
 
 def sha(a) -> str:
@@ -430,11 +432,72 @@ def bsr_cases(R):
     np.savez_compressed(os.path.join(HERE, "bsr.npz"), **out)
 
 
+# The benchmark configurations' 3D instances: (cubes per edge, sigma, field
+# seed, rhs seed, stride of the solution sample, smoothers recorded)
+BIG = {
+    "c2": (128, 1.0, 2, 3, 97, ("l1", "gs")),
+    "c5": (256, 1.5, 7, 8, 797, ("l1",)),
+}
+BIG_SMOOTHERS = {"l1": dict(smoother=10, presmooth_iter=2, postsmooth_iter=2), "gs": {}}
+
+
+def big_cases(R, name):
+    """The FP64 drop-in at a benchmark configuration's full size: the 3D P1
+    log-normal diffusion on the Kuhn mesh of N^3 cubes (128^3: sigma 1,
+    seeds 2/3; 256^3: sigma 1.5, seeds 7/8), UA-AMG with HEM, theta 0,
+    coarse_dof 2000, direct coarsest solve, with l1-Jacobi V(2,2) (and, at
+    128^3, Gauss-Seidel V(1,1)); PCG to 1e-8 from x0 = 0.  Stored: level
+    sizes, SHA-256 digests of every coarse operator and aggregate map, the
+    adapted threshold, PCG iterations, the residual at every preconditioner
+    call, a strided sample of the solution, the reference's own setup and
+    solve seconds on this machine, and a strided sample of the l1-Jacobi
+    solve tightened to 1e-12 (the FP64 oracle solve that the mixed-precision
+    error is stated against)."""
+    N, sigma, fseed, bseed, stride, smoothers = BIG[name]
+    k = P.lognormal_field(N, sigma, 8.0, fseed)
+    ia, ja, val = P.kuhn3d_p1(N, k)
+    b = P.rhs_uniform(len(ia) - 1, bseed)
+    out = {"A_sha": np.array([sha(ia), sha(ja), sha(val)]), "b_sha": np.array([sha(b)]),
+           "stride": np.int64(stride)}
+    for sm in smoothers:
+        prm = oracle.AMGParams(**BIG_SMOOTHERS[sm])
+        assert R.setup(ia, ja, val, prm) == 0
+        nl = R.num_levels()
+        out[f"{sm}/params"] = np.array(prm.arrays()[0][:], np.int64)
+        out[f"{sm}/dparams"] = np.array(prm.arrays()[1][:])
+        out[f"{sm}/info"] = np.array([R.level_info(l)[:3] for l in range(nl)], np.int64)
+        out[f"{sm}/theta_after"] = np.float64(R.strong_coupled())
+        for l in range(nl):
+            out[f"{sm}/A{l}_sha"] = np.array([sha(a) for a in R.level_A(l)])
+            if l < nl - 1:
+                out[f"{sm}/agg{l}_sha"] = np.array([sha(R.level_agg(l))])
+        it, x, hist = R.pcg(b, None, 1e-8, 500, 1)
+        setup_s, solve_s = R.timings()
+        out[f"{sm}/iters"] = np.int64(it)
+        out[f"{sm}/hist"] = hist
+        out[f"{sm}/x_sample"] = x[::stride].copy()
+        out[f"{sm}/x_norm"] = np.float64(np.linalg.norm(x))
+        out[f"{sm}/seconds"] = np.array([setup_s, solve_s])
+        print(name, sm, "levels", out[f"{sm}/info"][:, 0], "iters", it,
+              f"setup {setup_s:.1f} s solve {solve_s:.1f} s", flush=True)
+        if sm == "l1":
+            it12, x12, _ = R.pcg(b, None, 1e-12, 1000, 1)
+            out["l1/tight/iters"] = np.int64(it12)
+            out["l1/tight/x_sample"] = x12[::stride].copy()
+            out["l1/tight/x_norm"] = np.float64(np.linalg.norm(x12))
+            print(name, "tight iters", it12, flush=True)
+        R.free()
+    np.savez_compressed(os.path.join(HERE, f"{name}_kuhn.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
     R = oracle.ref()
     only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if only in BIG:
+        big_cases(R, only)
+        return
     if only == "gmres":
         gmres_cases(R)
         return
