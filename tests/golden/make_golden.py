@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|hec|layout|c2|c5]
+    python tests/golden/make_golden.py [REFERENCE_DIR] [--only gmres|cycles|cube|minres|sa|bsr|vmb|hec|layout|c2|c5|batch]
 
 Runs the reference HAZmath library compiled from its own sources
 (oracle/build_ref.sh -> oracle/_ref/libhazref.so) on seeded synthetic inputs
@@ -490,6 +490,34 @@ def big_cases(R, name):
     np.savez_compressed(os.path.join(HERE, f"{name}_kuhn.npz"), **out)
 
 
+BATCH = (24, 3, 500, 30000)   # systems, seed, dof range of problems.batch_anisotropic
+BATCH_STRIDE = 4
+
+
+def batch_cases(R):
+    """Each system of the GPU tests' batch (problems.batch_anisotropic(24,
+    seed 3, 500-30000 dofs)) solved on its own by the reference: UA-AMG with
+    HEM, theta 0, coarse_dof 2000, l1-Jacobi V(2,2), PCG to 1e-8 (iterations)
+    and to 1e-12 (every 4th entry of the solution: the FP64 oracle the
+    batch's answers are compared with)."""
+    systems, _ = P.batch_anisotropic(BATCH[0], BATCH[1], BATCH[2], BATCH[3])
+    out = {"stride": np.int64(BATCH_STRIDE)}
+    prm = oracle.AMGParams(smoother=10, presmooth_iter=2, postsmooth_iter=2)
+    for k, (ia, ja, val, b) in enumerate(systems):
+        assert R.setup(ia, ja, val, prm) == 0
+        out[f"{k}/A_sha"] = np.array([sha(ia), sha(ja), sha(val)])
+        out[f"{k}/levels"] = np.int64(R.num_levels())
+        it, _, _ = R.pcg(b, None, 1e-8, 500, 1)
+        out[f"{k}/iters"] = np.int64(it)
+        it12, x12, _ = R.pcg(b, None, 1e-12, 1000, 1)
+        out[f"{k}/tight_iters"] = np.int64(it12)
+        out[f"{k}/x_sample"] = x12[::BATCH_STRIDE].copy()
+        out[f"{k}/x_norm"] = np.float64(np.linalg.norm(x12))
+        print("batch", k, len(b), R.num_levels(), it, it12)
+        R.free()
+    np.savez_compressed(os.path.join(HERE, "batch.npz"), **out)
+
+
 def main():
     if not oracle.ref_available():
         oracle.build(ref=True)
@@ -497,6 +525,9 @@ def main():
     only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
     if only in BIG:
         big_cases(R, only)
+        return
+    if only == "batch":
+        batch_cases(R)
         return
     if only == "gmres":
         gmres_cases(R)
