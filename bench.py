@@ -14,13 +14,26 @@ configurations' shapes.
 
 One step = one solve of that system from x0 = 0 to 1e-8 FP64 relative
 residual as a user pays for it: UA-AMG setup (parallel matching, Galerkin
-products, coarse factorisation), the learned weights (network inference
-and the measured-contraction fallback check), and flexible CG with the FP32
-V-cycle (l1-Jacobi V(2,2)).  `value` is that time with the inputs resident
-in HBM; `e2e` is the same through the handle API with host arrays (matrix
-and vectors copied in, the solution copied out, all inside the timed
-region).  The plain FP64 drop-in (exact HEM, FP64 cycle, same smoother) is
-timed beside it (`plain_fp64`).  The stored matrix (2.97 GB) is far larger
+products, coarse factorisation) and flexible CG with the FP32 V-cycle
+(l1-Jacobi V(2,2)).  `value` is that time with the inputs resident in HBM;
+`e2e` is the same through the handle API with host arrays (matrix and
+vectors copied in, the solution copied out, all inside the timed region).
+Beside it: the plain FP64 drop-in (exact HEM, FP64 cycle, same smoother;
+`plain_fp64`, with its level sizes and iterations against the reference's
+on the same system), the same step with the learned smoother weights
+(network inference, the measured-contraction fallback check, the solve;
+`mixed_learned`, with the iterations of uniform weights 0.7 and 1.3, which
+bound what per-row weights can change on this problem) and the learned
+weights on unseen 1024^2-vertex anisotropic problems of their training
+class (`learned_c4`), and the other configurations as short legs on the
+same box (`configs`: c1 the 2D FP64 Gauss-Seidel drop-in with the
+reference timed beside it, c2 the 128^3 mixed-vs-plain comparison with its
+parity and oracle errors, c3 the 512-system batch).  Every level of both
+hierarchies is timed
+(`levels_mixed`, `levels_fp64`), the solve as a whole against the HBM
+roofline from its algorithmic bytes (`solve_roofline`), and both solutions
+against the reference's FP64 solve tightened to 1e-12 (`error_vs_oracle`,
+from tests/golden/c5_kuhn.npz).  The stored matrix (2.97 GB) is far larger
 than the 126 MB L2, so no flush is needed between steps.
 
 Workload bsr: the block (BSR) path, linear_solver_dbsr_krylov_amg's pieces on
@@ -43,8 +56,13 @@ Workload c3: 512 independent SPD systems (2D/3D anisotropic P1 diffusion,
 per-system solve times.
 
 --impl reference times the reference HAZmath implementation (compiled from
-its own C sources, single-threaded -- the reference has no threading) on a
-bounded sample of the same workload, scaled to it by the dof count.
+its own C sources, single-threaded -- the reference has no threading): on
+c5 one measured setup + PCG solve of the full 256^3 system (minutes on one
+core, so exactly one is timed whatever --steps asks; the line reports
+steps = 1 and steps_requested), on c1/c2 the full workload every step, on
+c3 a sample of the systems scaled by the dof count.  The b200 line's
+cpu_baseline is a bounded sample (the 128^3 instance, scaled by the dof
+ratio).
 Multi-GPU: the path does not shard; N ranks run N independent replicas.
 """
 from __future__ import annotations
@@ -70,12 +88,11 @@ FALLBACK_HBM = 6650.0
 METRIC = "AMG-PCG time to 1e-8 FP64 residual: mixed+learned vs plain on B200; SpMV GB/s"
 
 
-_FIELD = {}   # the last per-cube coefficient field generated, by N
+_FIELD = {}   # the per-cube coefficient field of each instance generated, by N
 
 
 def kuhn_case(N: int, sigma: float, seeds):
     k = P.lognormal_field(N, sigma, 8.0, seeds[0])
-    _FIELD.clear()
     _FIELD[N] = k
     ia, ja, val = P.kuhn3d_p1(N, k)
     b = P.rhs_uniform(len(ia) - 1, seeds[1])
@@ -190,14 +207,20 @@ def time_reference(ia, ja, val, b):
     prm = oracle.AMGParams(smoother=10, presmooth_iter=2, postsmooth_iter=2)
     t0 = time.perf_counter()
     assert R.setup(ia, ja, val, prm) == 0
+    t1 = time.perf_counter()
     it, _, _ = R.pcg(b, None, 1e-8, 500, 1)
     t = time.perf_counter() - t0
     R.free()
+    LAST_REFERENCE.update(setup_s=t1 - t0, solve_s=t - (t1 - t0))
     return t, int(it), kind
+
+
+LAST_REFERENCE = {}   # setup / solve seconds of the last time_reference call
 
 
 # --variant: (what, AMG_param fields over bench_amg's setting, Krylov method)
 VARIANTS = {
+    "v": ("V-cycle, PCG", {}, "pcg"),
     "w": ("W-cycle, PCG", dict(cycle_type=2), "pcg"),
     "amli": ("AMLI cycle of degree 2, PCG", dict(cycle_type=3), "pcg"),
     "nlamli": ("nonlinear AMLI cycle (flexible GMRES on the coarse levels), "
@@ -277,6 +300,7 @@ def run_variant(args, rank, world, local, dist):
     clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     setup_s, solve_s, launches, iters = [], [], 0, 0
+    torch.cuda.profiler.start()
     ev0.record()
     for _ in range(args.steps):
         iters = step()
@@ -286,6 +310,7 @@ def run_variant(args, rank, world, local, dist):
         launches += st.launches
     ev1.record()
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     clk = clocks.stop()
     step_s = max_over_ranks(dist, ev0.elapsed_time(ev1) * 1e-3 / args.steps, dev)
     x = dx.cpu().numpy()
@@ -439,13 +464,24 @@ def run_reference(args):
                 f"({sample} of {total} dofs), scaled by the dof ratio {scale:.2f}")
         warm = [systems[pick[0]]]
         work = [systems[k] for k in pick]
+    elif name == "c5":
+        # the full 256^3 system: one reference solve takes minutes on one
+        # core, so exactly one is timed whatever --steps asks for (the line
+        # says so: steps = 1, steps_requested = K)
+        ia, ja, val, b, desc = workload(name)
+        scale, what = 1.0, ("reference setup+solve of the full 256^3 system (16,581,375 dofs), "
+                            "measured, one timed solve")
+        wia, wja, wval, wb, _ = kuhn_case(48, 1.0, (2, 3))
+        warm = [(wia, wja, wval, wb)]
+        work = [(ia, ja, val, b)]
     else:
         ia, ja, val, b, scale, what = cpu_sample(name)
         wia, wja, wval, wb, _ = kuhn_case(48, 1.0, (2, 3))
         warm = [(wia, wja, wval, wb)]
         work = [(ia, ja, val, b)]
+    timed_steps = 1 if name == "c5" else args.steps
     times, iters, kind = [], 0, "reference"
-    for step in range(args.warmup + args.steps):
+    for step in range(args.warmup + timed_steps):
         # warm-up steps run the same code on a small instance (untimed)
         batch = warm if step < args.warmup else work
         t = 0.0
@@ -458,7 +494,8 @@ def run_reference(args):
     desc = workload_desc(name)
     line = {"metric": METRIC if name != "c3" else "batched UA-AMG-PCG: 512 systems, batch time",
             "value": v, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+            "steps": timed_steps, "steps_requested": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "iterations": int(iters),
             "config": dict(desc, smoother="l1-Jacobi V(2,2), HEM, coarse direct, FP64 CG",
@@ -467,6 +504,8 @@ def run_reference(args):
                              "sample": what},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if name != "c3":
+        line["setup_s"], line["solve_s"] = LAST_REFERENCE["setup_s"], LAST_REFERENCE["solve_s"]
     print(json.dumps(line))
 
 
@@ -495,6 +534,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c5", choices=["c1", "c2", "c5", "c3", "bsr"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the c1/c2/c3 legs of the default c5 run")
+    ap.add_argument("--steps-only", action="store_true",
+                    help="run the warm-up and timed steps only, print a short line (for "
+                         "launch lists taken under a profiler; not a bench line)")
     ap.add_argument("--variant", default="", choices=[""] + sorted(VARIANTS))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -577,23 +621,25 @@ def run_single(args, rank, world, local, dist):
         it = check(S.solve_device(p(db), p(dx)), "solve")
         return it, sel
 
+    # the headline step: the mixed solve with plain l1-Jacobi weights (the
+    # learned weights, which do not reduce this problem's iteration count,
+    # are measured beside it below)
     S = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
     for _ in range(args.warmup):
-        step(S, True)
+        step(S, False)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    setup_s, solve_s, select_s, launches, iters, sel = [], [], [], 0, 0, None
+    setup_s, solve_s, launches, iters = [], [], 0, 0
     torch.cuda.profiler.start()
     ev0.record()
     for _ in range(args.steps):
-        iters, sel = step(S, True)
+        iters, _ = step(S, False)
         st = S.stats()
         setup_s.append(st.setup_seconds)
         solve_s.append(st.solve_seconds)
-        select_s.append(sel["select_s"])
         launches += st.launches
     ev1.record()
     torch.cuda.synchronize()
@@ -604,12 +650,42 @@ def run_single(args, rank, world, local, dist):
     import scipy.sparse as sp
     A = sp.csr_matrix((val, ja, ia), shape=(n, n))
     relres = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+    if args.steps_only:   # the timed steps alone (for launch lists under a profiler)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": step_s, "unit": "s",
+                              "steps_only": True, "iterations": int(iters),
+                              "final_relres": relres, "config": desc}))
+        S.close()
+        gnn.close()
+        return
 
-    # the mixed cycle with plain weights, for the learned part's share
-    Sp = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
-    step(Sp, False)
-    it_mp = step(Sp, False)[0]
-    st_mp = Sp.stats()
+    # the same step with the learned weights: network inference and the
+    # measured-contraction fallback check, then the solve (one warm-up step,
+    # one timed between CUDA events); then the solve with uniform weights,
+    # which shows how far any per-row weights can move this problem
+    Sl = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
+    step(Sl, True)
+    torch.cuda.synchronize()
+    ev0.record()
+    it_l, sel = step(Sl, True)
+    ev1.record()
+    torch.cuda.synchronize()
+    st_l = Sl.stats()
+    learned = dict(sel, ns=NS_SELECT, step_s=ev0.elapsed_time(ev1) * 1e-3,
+                   iterations=int(it_l), setup_s=st_l.setup_seconds,
+                   solve_s=st_l.solve_seconds)
+    om = torch.empty(n, dtype=torch.float32, device=dev)
+    uniform = {}
+    for w in (0.7, 1.3):
+        om.fill_(w)
+        check(Sl.set_omega_device(p(om)), "set_omega")
+        dx.zero_()
+        uniform[str(w)] = int(check(Sl.solve_device(p(db), p(dx)), "solve"))
+    check(Sl.set_omega_device(None), "set_omega")
+    learned["iterations_uniform_omega"] = uniform
+    del om
+    c4 = c4_leg(gnn, local)
+    legs = config_legs(local) if args.workload == "c5" and not args.no_legs else None
 
     # plain FP64 drop-in (exact HEM, FP64 V-cycle, same smoother) beside it
     S64 = hz.Solver(amg_l1(hz), itparam(hz), bp_plain)
@@ -621,20 +697,25 @@ def run_single(args, rank, world, local, dist):
     total64 = st64.setup_seconds + st64.solve_seconds
 
     # roofline of the step's dominant kernel (the level-0 FP32 l1-Jacobi
-    # sweep, a quarter of the step's device time) and of the drop-in's
-    # level-0 FP64 SpMV (the level SpMV the 70 % target names): each timed as
-    # 50 launches on the solver's stream between CUDA events
+    # sweep, with the weights the step ran) and of the drop-in's level-0 FP64
+    # SpMV (the level SpMV the 70 % target names): each timed as 50 launches
+    # on the solver's stream between CUDA events; then every level of both
+    # hierarchies, and the solve-level figure
     peak, peak_kind = hbm_peak()
 
-    def kernel(h, which):
+    def kernel(h, which, level=0, reps=50):
         ms, by = C.c_double(), C.c_double()
-        check(hz.lib().hzb_time_kernel(h, which, 0, 50, C.byref(ms), C.byref(by)),
+        check(hz.lib().hzb_time_kernel(h, which, level, reps, C.byref(ms), C.byref(by)),
               "time_kernel")
         return ms.value, by.value, by.value / (ms.value * 1e-3) / 1e9
 
     l1_ms, l1_by, l1_gbs = kernel(S.h, hz.HZB_K_L1_32)
     sp_ms, sp_by, spmv64_gbs = kernel(S64.h, hz.HZB_K_SPMV64)
     spmv32_gbs = kernel(S.h, hz.HZB_K_SPMV32)[2]
+    lv_mixed = level_table(S, kernel, hz.HZB_K_L1_32, peak, mixed=True)
+    lv_fp64 = level_table(S64, kernel, hz.HZB_K_SPMV64, peak, mixed=False)
+    solve_by = solve_bytes_mixed(lv_mixed, int(iters), False)
+    oracle_err = oracle_errors(args.workload, x, x64)
 
     # device assembly of the same matrix from the per-cube coefficients
     asm = assembly_leg(hz, torch, args.workload, dja, dval, n, nnz, dev, peak) \
@@ -649,7 +730,6 @@ def run_single(args, rank, world, local, dist):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         check(Se.setup_host(ia, ja, val), "setup_host")
-        gnn.select(Se, NS_SELECT, 99)
         check(Se.solve_host(b, xh), "solve_host")
         t = time.perf_counter() - t0
         if k:
@@ -670,28 +750,44 @@ def run_single(args, rank, world, local, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32-cycle/f64-outer", "data": "synthetic",
-            "config": dict(desc, solver="UA-AMG (parallel matching) V(2,2) l1-Jacobi with "
-                           "learned weights (fallback to plain), FP32 cycle in FP64 "
-                           "flexible CG", parallelism="replicas",
-                           l2="inputs larger than L2 (no flush)"),
+            "config": dict(desc, solver="UA-AMG (parallel matching) V(2,2) l1-Jacobi, FP32 "
+                           "cycle in FP64 flexible CG; the learned weights with their "
+                           "fallback check are timed beside it (mixed_learned)",
+                           parallelism="replicas", l2="inputs larger than L2 (no flush)"),
             "iterations": int(iters), "final_relres": relres,
-            "setup_s": statistics.mean(setup_s), "learned_select_s": statistics.mean(select_s),
+            "setup_s": statistics.mean(setup_s),
             "solve_s": solve_ml, "dof_per_s": n / solve_ml,
-            "learned": dict(sel, ns=NS_SELECT),
-            "mixed_plain_weights": {"iterations": int(it_mp), "solve_s": st_mp.solve_seconds},
+            "mixed_learned": learned,
+            "learned_c4": c4,
+            "configs": legs,
             "plain_fp64": {"iterations": int(it64), "setup_s": st64.setup_seconds,
-                           "solve_s": st64.solve_seconds, "total_s": total64},
+                           "solve_s": st64.solve_seconds, "total_s": total64,
+                           "parity": parity_vs_fixture(args.workload, st64, it64)},
             "speedup_vs_plain": total64 / step_s,
             "speedup_solve_vs_plain": st64.solve_seconds / solve_ml,
             "err_vs_fp64": err_vs_fp64,
             "roofline": {"bound": "hbm", "kernel": "level-0 FP32 l1-Jacobi sweep of the "
-                         "mixed cycle (k_l1_vec / k_l1_bundle<float>, autotuned)",
-                         "achieved": l1_gbs, "peak": peak, "unit": "GB/s",
-                         "frac": l1_gbs / peak, "peak_kind": peak_kind,
+                         "mixed cycle (k_l1_vec / k_l1_bundle<float>, autotuned), with the "
+                         "weights the step ran", "achieved": l1_gbs, "peak": peak,
+                         "unit": "GB/s", "frac": l1_gbs / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": l1_by, "ms_per_launch": l1_ms,
                          "traffic": TRAFFIC_PER_BYTE["l1_32"] * l1_by,
-                         "traffic_source": "ncu DRAM bytes per algorithmic byte on the "
-                         "128^3 case (profiles/l1_32_level0_c2.md), times this launch's bytes"},
+                         "traffic_source": "ncu DRAM bytes per algorithmic byte of this "
+                         "kernel on the 128^3 case, times this launch's bytes"},
+            "solve_roofline": {"bound": "hbm", "bytes": solve_by,
+                               "seconds": solve_ml, "achieved": solve_by / solve_ml / 1e9,
+                               "peak": peak, "unit": "GB/s",
+                               "frac": solve_by / solve_ml / 1e9 / peak,
+                               "model": "per V-cycle and level: first sweep from x = 0 "
+                               "(12n), 3 l1 sweeps (8 nnz32 + 4(n+1) + 12n [+4n weights]), "
+                               "residual (8 nnz32 + 4(n+1) + 12n), restriction (4(nc+1) + "
+                               "8n + 4nc), prolongation (12n + 4nc); coarsest 8 nc^2 + 8 nc; "
+                               "per iteration the FP64 SpMV with its dot (12 nnz + 4(n+1) "
+                               "+ 16n) and 112n of flexible-CG vector work and precision "
+                               "conversions; iterations + 1 cycles, 2 extra residuals"},
+            "levels_mixed": lv_mixed,
+            "levels_fp64": lv_fp64,
+            "error_vs_oracle": oracle_err,
             "drop_in_spmv64": {"kernel": "level-0 FP64 SpMV of the drop-in "
                                "(k_spmv_bundle<double>)", "achieved": spmv64_gbs,
                                "peak": peak, "unit": "GB/s", "frac": spmv64_gbs / peak,
@@ -708,7 +804,7 @@ def run_single(args, rank, world, local, dist):
             "clocks": clk,
         }
         print(json.dumps(line))
-    for h in (S, Sp, S64, Se):
+    for h in (S, Sl, S64, Se):
         h.close()
     gnn.close()
 
@@ -748,6 +844,234 @@ def assembly_leg(hz, torch, name, dja, dval, n, nnz, dev, peak):
            "frac": by / t / 1e9 / peak, "matches_host_generator": same}
     del kd, ia, ja, va
     return out
+
+
+def _timed_steps(torch, step, steps):
+    """steps calls of step() between CUDA events after one warm-up call:
+    seconds per call and the last call's result."""
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        out = step()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / steps, out
+
+
+def config_legs(device, steps=3):
+    """The other configurations of the benchmark, each as its own short leg
+    of the default run (same clock and box as the headline):
+    c1 -- the FP64 drop-in as configured there (2D 255^2 Poisson, HEM, GS
+          V(1,1), PCG), with the reference timed on the same system;
+    c2 -- the 128^3 Kuhn system (sigma 1): mixed solve against the FP64
+          drop-in, the drop-in's level sizes and iterations against the
+          reference's, both errors against the reference's 1e-12 solve;
+    c3 -- 512 independent systems (~20M dofs) solved as one batch."""
+    import torch
+    import hazmath_b200 as hz
+    dev = f"cuda:{device}"
+    p = lambda t: t.data_ptr()  # noqa: E731
+    out = {}
+
+    def up(*arrs):
+        return [torch.from_numpy(a).to(dev) for a in arrs]
+
+    # c1
+    ia, ja, val, b, _ = workload("c1")
+    dia, dja, dval, db = up(ia, ja, val, b)
+    dx = torch.zeros_like(db)
+    S = hz.Solver(hz.bench_amg(), itparam(hz), hz.b200_param(device=device))
+
+    def c1_step():
+        dx.zero_()
+        assert S.setup_device(len(b), len(ja), p(dia), p(dja), p(dval)) == 0, hz.last_error()
+        return S.solve_device(p(db), p(dx))
+
+    t, it = _timed_steps(torch, c1_step, steps)
+    st = S.stats()
+    S.close()
+    leg = {"workload": "2D P1 Poisson 257^2 vertices (65,025 dofs), FP64 drop-in, HEM, GS "
+                       "V(1,1), coarse direct, PCG to 1e-8", "step_s": t, "iterations": int(it),
+           "setup_s": st.setup_seconds, "solve_s": st.solve_seconds, "steps": steps}
+    import oracle
+    if oracle.ref_available():
+        tr, itr, _ = time_reference_variant(ia, ja, val, b, "v")
+        leg["reference"] = {"step_s": tr, "iterations": itr, "cores": 1,
+                            "kind": "reference", "measured": "this run, this host"}
+    out["c1"] = leg
+    del dia, dja, dval, db, dx
+
+    # c2
+    ia, ja, val, b, _ = workload("c2")
+    n = len(b)
+    dia, dja, dval, db = up(ia, ja, val, b)
+    dx = torch.zeros_like(db)
+    leg = {"workload": "3D P1 log-normal diffusion, Kuhn mesh 128^3 cubes (sigma 1; "
+                       "2,048,383 dofs), l1-Jacobi V(2,2), to 1e-8", "steps": steps}
+    for tag, bp in (("mixed", hz.b200_param(precision=hz.HZB_PREC_MIXED,
+                                            matching=hz.HZB_MATCH_PARALLEL, device=device)),
+                    ("plain_fp64", hz.b200_param(device=device))):
+        S = hz.Solver(amg_l1(hz), itparam(hz), bp)
+
+        def c2_step():
+            dx.zero_()
+            assert S.setup_device(n, len(ja), p(dia), p(dja), p(dval)) == 0, hz.last_error()
+            return S.solve_device(p(db), p(dx))
+
+        t, it = _timed_steps(torch, c2_step, steps if tag == "mixed" else 1)
+        st = S.stats()
+        x = dx.cpu().numpy()
+        leg[tag] = {"step_s": t, "iterations": int(it), "setup_s": st.setup_seconds,
+                    "solve_s": st.solve_seconds}
+        if tag == "plain_fp64":
+            leg[tag]["parity"] = parity_vs_fixture("c2", st, it)
+        g = fixture("c2")
+        if g is not None:
+            xt = g["l1/tight/x_sample"]
+            leg[tag]["error_vs_oracle"] = float(np.linalg.norm(x[::int(g["stride"])] - xt)
+                                                / np.linalg.norm(xt))
+        S.close()
+    leg["speedup_vs_plain"] = leg["plain_fp64"]["step_s"] / leg["mixed"]["step_s"]
+    leg["speedup_solve_vs_plain"] = leg["plain_fp64"]["solve_s"] / leg["mixed"]["solve_s"]
+    g = fixture("c2")
+    if g is not None:
+        leg["reference_recorded"] = {"setup_s": float(g["l1/seconds"][0]),
+                                     "solve_s": float(g["l1/seconds"][1]), "cores": 1,
+                                     "measured": "tests/golden/make_golden.py, build container"}
+    out["c2"] = leg
+    del dia, dja, dval, db, dx
+
+    # c3
+    systems, (off, ia, ja, val, b) = P.batch_anisotropic(512, 11)
+    dia, dja, dval, db = up(ia, ja, val, b)
+    dx = torch.zeros_like(db)
+    bp = hz.b200_param(precision=hz.HZB_PREC_MIXED, matching=hz.HZB_MATCH_PARALLEL,
+                       device=device)
+    S = hz.Solver(amg_l1(hz), itparam(hz, 1000), bp)
+
+    def c3_step():
+        dx.zero_()
+        assert S.batch_setup_device(off, int(ia[-1]), p(dia), p(dja), p(dval)) == 0
+        rc, its, rel, sec = S.batch_solve_device(p(db), p(dx))
+        assert rc > 0, hz.last_error()
+        return its, rel, sec
+
+    t, (its, rel, sec) = _timed_steps(torch, c3_step, steps)
+    out["c3"] = {"workload": "512 independent 2D/3D anisotropic P1 systems, 1k-200k dofs "
+                             f"log-uniform (seed 11), {len(b)} dofs", "batch_s": t,
+                 "steps": steps, "per_system_solve_s": {
+                     "p50": float(np.percentile(sec, 50)), "p99": float(np.percentile(sec, 99))},
+                 "iterations": {"p50": float(np.percentile(its, 50)), "max": int(its.max())},
+                 "worst_relres": float(rel.max())}
+    S.close()
+    return out
+
+
+def c4_leg(gnn, device, count=4):
+    """The learned weights on unseen problems of their training class: 2D
+    anisotropic P1 diffusion on 1024^2-vertex meshes (epsilon log-uniform in
+    [1e-4, 1], random rotation; learn.eval_problem, seed 20260), plain
+    l1-Jacobi weights against the learned ones with their fallback check, in
+    the mixed solve to 1e-8: iterations, solve and selection seconds."""
+    from hazmath_b200 import learn
+    rng = np.random.default_rng(20260)
+    rows = learn.evaluate(gnn, [learn.eval_problem(rng) for _ in range(count)],
+                          device=device, ns=2)
+    keep = ("eps", "angle", "dofs", "plain_iters", "learned_iters", "plain_solve_s",
+            "learned_solve_s", "select_s", "learned_used", "rho_plain", "rho_learned")
+    rows = [{k: r[k] for k in keep} for r in rows]
+    return {"problems": rows,
+            "plain_iters": sum(r["plain_iters"] for r in rows),
+            "learned_iters": sum(r["learned_iters"] for r in rows),
+            "plain_solve_s": sum(r["plain_solve_s"] for r in rows),
+            "learned_solve_plus_select_s": sum(r["learned_solve_s"] + r["select_s"]
+                                               for r in rows)}
+
+
+def level_table(S, kernel, which, peak, mixed):
+    """Per level of a hierarchy: rows, stored entries (the FP32 copy's,
+    without exact zeros, for the mixed cycle), and the GB/s of its l1 sweep
+    (mixed) or FP64 SpMV (drop-in) against the HBM peak; levels whose data
+    fit twice into the 126 MB L2 are marked (they run from L2)."""
+    st = S.stats()
+    out = []
+    for l in range(st.num_levels):
+        n = st.rows[l]
+        if mixed and l == st.num_levels - 1:
+            out.append({"level": l, "rows": n, "coarsest": True})
+            break
+        reps = 50 if n > 100000 else 200
+        ms, by, gbs = kernel(S.h, which, l, reps)
+        sp_by = kernel(S.h, hz_const("HZB_K_SPMV32"), l, 1)[1] if mixed else None
+        row = {"level": l, "rows": n, "nnz": st.nnz[l], "bytes": by, "ms": ms, "gbs": gbs,
+               "frac": gbs / peak, "l2_resident": by < 63e6}
+        if mixed:
+            row["nnz32"] = int(round((sp_by - 4.0 * (n + 1) - 8.0 * n) / 8.0))
+        out.append(row)
+    return out
+
+
+def hz_const(name):
+    import hazmath_b200 as hz
+    return getattr(hz, name)
+
+
+def solve_bytes_mixed(levels, iters, omega):
+    """Algorithmic bytes of one mixed solve (FP64 flexible CG around the
+    FP32 V(2,2) l1-Jacobi cycle) from the level sizes; the terms are listed
+    in the bench line's solve_roofline.model."""
+    n0, nnz0 = levels[0]["rows"], levels[0]["nnz"]
+    outer = 12.0 * nnz0 + 4.0 * (n0 + 1) + 16.0 * n0 + 112.0 * n0
+    cyc = 0.0
+    for l in range(len(levels) - 1):
+        n, nz, nc = levels[l]["rows"], levels[l]["nnz32"], levels[l + 1]["rows"]
+        w = 4.0 * n if (omega and l == 0) else 0.0
+        sweep = 8.0 * nz + 4.0 * (n + 1) + 12.0 * n + w
+        first = 12.0 * n + w
+        res = 8.0 * nz + 4.0 * (n + 1) + 12.0 * n
+        restr = 4.0 * (nc + 1) + 8.0 * n + 4.0 * nc
+        prol = 12.0 * n + 4.0 * nc
+        cyc += first + 3.0 * sweep + res + restr + prol
+    nc = levels[-1]["rows"]
+    cyc += 8.0 * nc * nc + 8.0 * nc
+    res0 = 12.0 * nnz0 + 4.0 * (n0 + 1) + 24.0 * n0
+    return iters * outer + (iters + 1) * cyc + 2.0 * res0
+
+
+def fixture(name):
+    path = os.path.join(ROOT, "tests", "golden", f"{name}_kuhn.npz")
+    return np.load(path) if os.path.exists(path) else None
+
+
+def oracle_errors(name, x_mixed, x_fp64):
+    """Errors of the mixed and of the FP64 (1e-8) solutions against the
+    reference's FP64 solve tightened to 1e-12 (a strided sample of it,
+    recorded by tests/golden/make_golden.py)."""
+    g = fixture(name)
+    if g is None:
+        return None
+    st = int(g["stride"])
+    xt = g["l1/tight/x_sample"]
+    nt = np.linalg.norm(xt)
+    return {"mixed": float(np.linalg.norm(x_mixed[::st] - xt) / nt),
+            "plain_fp64": float(np.linalg.norm(x_fp64[::st] - xt) / nt),
+            "oracle": f"reference FP64 PCG to 1e-12 ({int(g['l1/tight/iters'])} iterations), "
+                      f"every {st}th entry ({len(xt)} entries)"}
+
+
+def parity_vs_fixture(name, st, iters):
+    """The drop-in's level sizes and PCG iterations against the reference's
+    on the same system (the full digests are compared by the GPU tests)."""
+    g = fixture(name)
+    if g is None:
+        return None
+    info = g["l1/info"]
+    sizes = [(st.rows[l], st.nnz[l]) for l in range(st.num_levels)]
+    return {"levels_equal": sizes == [(int(r[0]), int(r[1])) for r in info],
+            "iterations": int(iters), "reference_iterations": int(g["l1/iters"]),
+            "theta_equal": st.strong_coupled == float(g["l1/theta_after"])}
 
 
 # DRAM bytes (read + written) per algorithmic byte of one launch, measured by

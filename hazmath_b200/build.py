@@ -34,6 +34,7 @@ SOURCES = [
     ("hzb_sa.cu", False),
     ("hzb_bsr.cu", False),
     ("hzb_vmb.cu", False),
+    ("hzb_hec.cu", False),
     ("hzb_assemble.cu", False),
     ("hzb_learn.cu", False),
     ("hzb_gnn.cu", True),

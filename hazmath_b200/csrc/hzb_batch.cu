@@ -29,6 +29,7 @@
 namespace hzb {
 
 constexpr int BAT_CHUNK = 4096;     // rows per work item
+constexpr int BAT_TERM_ROWS = 128;  // a system's coarsening ends at this many rows
 constexpr int BAT_THREADS = 256;
 enum BatState { BAT_DONE = 0, BAT_ACTIVE = 1, BAT_CHECK = 2, BAT_FAILED = 3 };
 // per-system scalars, sc[k * nsys + s]
@@ -53,8 +54,29 @@ struct Batch {
     int **d_sys = nullptr;          // device copies of the per-level pointers
     unsigned char **d_act = nullptr;
     int *d_nrows = nullptr, *d_blkoff = nullptr;   // rows, first block per level
+    // Terminal levels: a system stops coarsening once it has at most
+    // BAT_TERM_ROWS rows; on that level its block is solved with its dense
+    // inverse (row-major, FP64 and an FP32 copy), and its rows leave the
+    // coarser levels.  Per level: the blocks ending there.
+    std::vector<unsigned char> done;          // host, per system: has its terminal block
+    unsigned char *d_done = nullptr;          // device copy
+    int *d_cnt = nullptr;                     // per-system row counts of a level
+    std::vector<int> tl_n;                    // blocks per level
+    std::vector<int *> tl_row0, tl_m;         // device: first row and size of each block
+    std::vector<long long *> tl_off;          // device: offset of its inverse
+    std::vector<double *> tl_inv;             // inverses of the level's blocks
+    std::vector<float *> tl_inv32;
     void release() {
         g_iter.release();
+        for (auto p : tl_row0) dfree(p);
+        for (auto p : tl_m) dfree(p);
+        for (auto p : tl_off) dfree(p);
+        for (auto p : tl_inv) dfree(p);
+        for (auto p : tl_inv32) dfree(p);
+        tl_row0.clear(); tl_m.clear(); tl_off.clear(); tl_inv.clear(); tl_inv32.clear();
+        tl_n.clear();
+        done.clear();
+        dfree(d_done); dfree(d_cnt);
         dfree(item_lo); dfree(item_hi); dfree(item_sys); dfree(sys_item);
         dfree(state); dfree(iters); dfree(sc); dfree(part);
         dfree(t_done); dfree(t_start); dfree(queue); dfree(nactive);
@@ -272,6 +294,271 @@ __global__ void k_bat_activity(int nlev, int nblk_all, const int *__restrict__ b
 
 static int bat_grid(int nitems) { return std::max(1, std::min(nitems, sm_count() * 8)); }
 
+// rows of every system on a level
+__global__ void k_bat_count(int n, const int *__restrict__ sys, int *cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(cnt + sys[i], 1);
+}
+
+// Dense inverse of each terminal block (one CTA per block, the block in
+// shared memory): the block's CSR rows [row0, row0 + m) scattered into an
+// m x m matrix (its columns lie in the same range: systems do not couple),
+// then Gauss-Jordan elimination in place without pivoting (the block is
+// SPD): for each k the pivot row is scaled by 1 / a_kk with a_kk replaced by
+// 1, and every other row subtracts its column-k multiple of it with its
+// column-k entry replaced by 0; after m steps the array holds the inverse.
+// A pivot that is not positive and finite sets *bad.
+__global__ void __launch_bounds__(256)
+k_bat_term_inverse(int nblk, const int *__restrict__ row0, const int *__restrict__ msz,
+                   const long long *__restrict__ off, const int *__restrict__ ia,
+                   const int *__restrict__ ja, const double *__restrict__ val,
+                   double *inv, float *inv32, int *bad) {
+    extern __shared__ double sa[];
+    const int blk = blockIdx.x;
+    if (blk >= nblk) return;
+    const int m = msz[blk], r0 = row0[blk];
+    double *A = sa;               // m x m, row-major
+    double *colk = sa + m * m;    // column k before the step
+    for (int q = threadIdx.x; q < m * m; q += blockDim.x) A[q] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        for (int p = ia[r0 + i]; p < ia[r0 + i + 1]; ++p) {
+            const int j = ja[p] - r0;
+            if (j >= 0 && j < m) A[i * m + j] += val[p];
+        }
+    bool ok = true;
+    for (int k = 0; k < m; ++k) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) colk[i] = A[i * m + k];
+        __syncthreads();
+        const double piv = colk[k];
+        if (!(piv > 0.0) || !isfinite(piv)) { ok = false; break; }
+        for (int j = threadIdx.x; j < m; j += blockDim.x)
+            A[k * m + j] = (j == k ? 1.0 : A[k * m + j]) / piv;
+        __syncthreads();
+        for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+            const int i = q / m, j = q - i * m;
+            if (i != k) A[q] = (j == k ? 0.0 : A[q]) - colk[i] * A[k * m + j];
+        }
+    }
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(bad, 1);
+        return;
+    }
+    __syncthreads();
+    double *out = inv + off[blk];
+    float *out32 = inv32 + off[blk];
+    for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+        out[q] = A[q];
+        out32[q] = (float)A[q];
+    }
+}
+
+// x = inverse * b on every terminal block of a level (one CTA per block, a
+// warp per row, lanes over the row's columns, fixed-order lane sums)
+template <typename T, typename V>
+__global__ void __launch_bounds__(256)
+k_bat_term_solve(int nblk, const int *__restrict__ row0, const int *__restrict__ msz,
+                 const long long *__restrict__ off, const V *__restrict__ inv,
+                 const T *__restrict__ b, T *__restrict__ x) {
+    __shared__ T sb[BAT_TERM_ROWS];
+    const int blk = blockIdx.x;
+    const int m = msz[blk], r0 = row0[blk];
+    for (int j = threadIdx.x; j < m; j += blockDim.x) sb[j] = b[r0 + j];
+    __syncthreads();
+    const V *M = inv + off[blk];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = warp; i < m; i += nw) {
+        T acc = T(0);
+        for (int j = lane; j < m; j += 32) acc += T(M[(size_t)i * m + j]) * sb[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) x[r0 + i] = acc;
+    }
+}
+
+// terminal systems' rows leave the next level; the surviving aggregates are
+// renumbered in order (the rows of a system stay contiguous)
+__global__ void k_bat_mask(int n, const int *__restrict__ sys,
+                           const unsigned char *__restrict__ done, int *agg, int *kept) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (agg[i] < 0) continue;
+        if (done[sys[i]]) agg[i] = UNPT;
+        else kept[agg[i]] = 1;
+    }
+}
+__global__ void k_bat_renumber(int n, const int *__restrict__ pos, int *agg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (agg[i] >= 0) agg[i] = pos[agg[i]];
+}
+
+// Which systems end their coarsening on level lvl (at most BAT_TERM_ROWS
+// rows there, or every system left when force is set), their dense
+// inverses, and the rows of the systems that go on (*live).
+int batch_level_begin(hzb_solver *S, int lvl, bool force, int *live) {
+    Batch &B = *S->batch;
+    cudaStream_t s = S->s;
+    const Level &L = S->lv[lvl];
+    if (lvl == 0) {
+        B.sysmap.clear();
+        B.sysmap.push_back(nullptr);
+        HZB_TRY(dalloc(&B.sysmap[0], std::max(1, L.n)));
+        k_bat_sys0<<<bat_grid(B.nitems), 256, 0, s>>>(B.nitems, B.item_lo, B.item_hi,
+                                                      B.item_sys, B.sysmap[0]);
+        count_launch();
+        B.done.assign(B.nsys, 0);
+        if (!B.d_done) HZB_TRY(dalloc(&B.d_done, B.nsys));
+        if (!B.d_cnt) HZB_TRY(dalloc(&B.d_cnt, B.nsys));
+    }
+    if ((int)B.tl_n.size() <= lvl) {
+        B.tl_n.resize(lvl + 1, 0);
+        B.tl_row0.resize(lvl + 1, nullptr);
+        B.tl_m.resize(lvl + 1, nullptr);
+        B.tl_off.resize(lvl + 1, nullptr);
+        B.tl_inv.resize(lvl + 1, nullptr);
+        B.tl_inv32.resize(lvl + 1, nullptr);
+    }
+    HZB_CUDA(cudaMemsetAsync(B.d_cnt, 0, sizeof(int) * B.nsys, s));
+    if (L.n > 0) {
+        k_bat_count<<<grid_for(L.n), 256, 0, s>>>(L.n, B.sysmap[lvl], B.d_cnt);
+        count_launch();
+    }
+    std::vector<int> cnt(B.nsys);
+    HZB_CUDA(cudaMemcpyAsync(cnt.data(), B.d_cnt, sizeof(int) * B.nsys, cudaMemcpyDeviceToHost,
+                             s));
+    HZB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> row0, msz;
+    std::vector<long long> off;
+    long long words = 0;
+    int r = 0, mmax = 0;
+    *live = 0;
+    for (int k = 0; k < B.nsys; ++k) {
+        const int c = cnt[k];
+        if (c > 0 && !B.done[k]) {
+            if (c <= BAT_TERM_ROWS || force) {
+                if (c > BAT_TERM_ROWS) {
+                    set_error_msg("batch: a system still has more rows than its terminal "
+                                  "block may hold on the last level (raise max_levels)");
+                    return ERROR_AMG_COARSEING;
+                }
+                row0.push_back(r);
+                msz.push_back(c);
+                off.push_back(words);
+                words += (long long)c * c;
+                mmax = std::max(mmax, c);
+                B.done[k] = 1;
+            } else {
+                *live += c;
+            }
+        }
+        r += c;
+    }
+    if (r != L.n) {
+        set_error_msg("batch: the rows of a level do not add up over the systems");
+        return ERROR_SOLVER_MISC;
+    }
+    const int nb = (int)row0.size();
+    B.tl_n[lvl] = nb;
+    HZB_CUDA(cudaMemcpyAsync(B.d_done, B.done.data(), B.nsys, cudaMemcpyHostToDevice, s));
+    if (nb == 0) return SUCCESS;
+    int *bad = B.d_cnt;   // the counts are on the host now
+    HZB_TRY(dalloc(&B.tl_row0[lvl], nb));
+    HZB_TRY(dalloc(&B.tl_m[lvl], nb));
+    HZB_TRY(dalloc(&B.tl_off[lvl], nb));
+    HZB_TRY(dalloc(&B.tl_inv[lvl], (size_t)words));
+    HZB_TRY(dalloc(&B.tl_inv32[lvl], (size_t)words));
+    HZB_CUDA(cudaMemcpyAsync(B.tl_row0[lvl], row0.data(), sizeof(int) * nb,
+                             cudaMemcpyHostToDevice, s));
+    HZB_CUDA(cudaMemcpyAsync(B.tl_m[lvl], msz.data(), sizeof(int) * nb, cudaMemcpyHostToDevice,
+                             s));
+    HZB_CUDA(cudaMemcpyAsync(B.tl_off[lvl], off.data(), sizeof(long long) * nb,
+                             cudaMemcpyHostToDevice, s));
+    HZB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    const size_t smem = sizeof(double) * ((size_t)mmax * mmax + mmax);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_bat_term_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * (BAT_TERM_ROWS * BAT_TERM_ROWS +
+                                                     BAT_TERM_ROWS)));
+        attr = true;
+    }
+    k_bat_term_inverse<<<nb, 256, smem, s>>>(nb, B.tl_row0[lvl], B.tl_m[lvl], B.tl_off[lvl],
+                                             L.ia, L.ja, L.val, B.tl_inv[lvl],
+                                             B.tl_inv32[lvl], bad);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    int hbad = 0;
+    HZB_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HZB_CUDA(cudaStreamSynchronize(s));
+    if (hbad) {
+        set_error_msg("batch: a system's terminal block has a non-positive pivot");
+        return ERROR_DATA_ZERODIAG;
+    }
+    return SUCCESS;
+}
+
+// After level lvl's aggregation: rows of systems that ended here leave the
+// coarser levels, the other aggregates are renumbered in order; the row ->
+// system map of the next level.  *nagg becomes the surviving count.
+int batch_level_end(hzb_solver *S, int lvl, int *agg, int *nagg) {
+    Batch &B = *S->batch;
+    cudaStream_t s = S->s;
+    const int n = S->lv[lvl].n;
+    int *kept = nullptr, *pos = nullptr, *tmp = nullptr;
+    int rc = SUCCESS;
+    if ((rc = dalloc(&kept, std::max(1, *nagg))) || (rc = dalloc(&pos, *nagg + 1)) ||
+        (rc = dalloc(&tmp, scan_tmp_size(*nagg + 1)))) {
+        dfree(kept); dfree(pos); dfree(tmp);
+        return rc;
+    }
+    int total = 0;
+    cudaMemsetAsync(kept, 0, sizeof(int) * std::max(1, *nagg), s);
+    k_bat_mask<<<grid_for(n), 256, 0, s>>>(n, B.sysmap[lvl], B.d_done, agg, kept);
+    count_launch();
+    rc = scan_exclusive(kept, pos, *nagg, tmp, s);
+    if (!rc) {
+        k_bat_renumber<<<grid_for(n), 256, 0, s>>>(n, pos, agg);
+        count_launch();
+        if (cudaMemcpyAsync(&total, pos + *nagg, sizeof(int), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            rc = ERROR_SOLVER_MISC;
+    }
+    dfree(kept); dfree(pos); dfree(tmp);
+    if (rc) return rc;
+    *nagg = total;
+    if (total > 0) {
+        int *sc = nullptr;
+        HZB_TRY(dalloc(&sc, total));
+        B.sysmap.push_back(sc);
+        k_bat_sys_down<<<grid_for(n), 256, 0, s>>>(n, agg, B.sysmap[lvl], sc);
+        count_launch();
+    }
+    return SUCCESS;
+}
+
+// x = A_T^{-1} b on the terminal blocks of level lvl (no-op without any)
+int batch_terminal_solve(hzb_solver *S, int lvl, bool fp32) {
+    Batch &B = *S->batch;
+    if (lvl >= (int)B.tl_n.size() || B.tl_n[lvl] == 0) return SUCCESS;
+    const Level &L = S->lv[lvl];
+    if (fp32)
+        k_bat_term_solve<float, float><<<B.tl_n[lvl], 256, 0, S->s>>>(
+            B.tl_n[lvl], B.tl_row0[lvl], B.tl_m[lvl], B.tl_off[lvl], B.tl_inv32[lvl], L.b32,
+            L.x32);
+    else
+        k_bat_term_solve<double, double><<<B.tl_n[lvl], 256, 0, S->s>>>(
+            B.tl_n[lvl], B.tl_row0[lvl], B.tl_m[lvl], B.tl_off[lvl], B.tl_inv[lvl], L.b, L.x);
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+bool batch_has_terminal(const hzb_solver *S, int lvl) {
+    const Batch *B = S->batch;
+    return B && lvl < (int)B->tl_n.size() && B->tl_n[lvl] > 0;
+}
+
 static int bat_activity(hzb_solver *S, Batch &B) {
     if (B.nblk_all == 0) return SUCCESS;
     k_bat_activity<<<grid_for(32LL * B.nblk_all), 256, 0, S->s>>>(
@@ -420,27 +707,23 @@ int batch_setup(hzb_solver *S, int nsys, const int *off, int n, int nnz, const i
         return rc;
     }
     if (S->bp.precision == HZB_PREC_MIXED) HZB_TRY(ensure_fp32(S));
-    // per-level row -> system maps and activity blocks
+    // activity blocks per level (the row -> system maps were built by the
+    // setup's level loop along with the terminal blocks)
     B->nlev = S->nl;
+    if ((int)B->sysmap.size() != S->nl) {
+        set_error_msg("batch: row -> system maps missing for a level");
+        batch_release(S);
+        return ERROR_SOLVER_MISC;
+    }
     std::vector<int> nrows(S->nl), blkoff(S->nl + 1, 0);
-    B->sysmap.assign(S->nl, nullptr);
     B->actv.assign(S->nl, nullptr);
     for (int l = 0; l < S->nl; ++l) {
         const int nl_rows = S->lv[l].n;
         nrows[l] = nl_rows;
         blkoff[l + 1] = blkoff[l] + (nl_rows + ACT_ROWS - 1) / ACT_ROWS;
-        HZB_TRY(dalloc(&B->sysmap[l], std::max(1, nl_rows)));
         HZB_TRY(dalloc(&B->actv[l], std::max(1, blkoff[l + 1] - blkoff[l])));
     }
     B->nblk_all = blkoff[S->nl];
-    k_bat_sys0<<<bat_grid(B->nitems), 256, 0, s>>>(B->nitems, B->item_lo, B->item_hi,
-                                                   B->item_sys, B->sysmap[0]);
-    count_launch();
-    for (int l = 0; l + 1 < S->nl; ++l) {
-        k_bat_sys_down<<<grid_for(S->lv[l].n), 256, 0, s>>>(S->lv[l].n, S->lv[l].agg,
-                                                            B->sysmap[l], B->sysmap[l + 1]);
-        count_launch();
-    }
     HZB_TRY(dalloc(&B->d_sys, S->nl));
     HZB_TRY(dalloc(&B->d_act, S->nl));
     HZB_TRY(dalloc(&B->d_nrows, S->nl));
@@ -484,11 +767,10 @@ int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit
     HZB_TRY(vcopy<double>(B->n, w.z, w.p, s));
     HZB_TRY(bat_vec<OP_ZTR>(S, *B, q + 6, b, x, w.r, w.p, w.z, w.t));
     HZB_TRY(bat_final<FIN_ZR0>(S, *B));
-    // the FP64 cycle is capturable only with the dense coarse solve
+    // the FP64 cycle is capturable without coarse scaling (its coarsest
+    // solves are the systems' dense terminal blocks)
     const bool graph = S->bp.use_graph &&
-                       (S->bp.precision == HZB_PREC_MIXED ||
-                        (S->amg.coarse_solver == SOLVER_UMFPACK && S->Ainv &&
-                         S->amg.coarse_scaling != ON));
+                       (S->bp.precision == HZB_PREC_MIXED || S->amg.coarse_scaling != ON);
     int iter = 0;
     for (;;) {
         const long long tag = ((long long)S->omega_active << 1) | (S->bp.precision & 1);

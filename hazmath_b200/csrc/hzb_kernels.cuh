@@ -123,6 +123,8 @@ int csr_val_d2f(int nnz, const double *x, float *y, cudaStream_t s);
 // entries != 0 per row, and the FP32 copy of those entries (row pointer ia32
 // from a scan of the counts)
 int csr_nonzero_count(int n, const int *ia, const double *a, int *cnt, cudaStream_t s);
+int csr_nonzero_fill64(int n, const int *ia, const double *a, const int *ia32, double *a64,
+                       cudaStream_t s);
 int csr_nonzero_fill(int n, const int *ia, const int *ja, const double *a, const int *ia32,
                      int *ja32, float *a32, cudaStream_t s);
 

@@ -1134,6 +1134,107 @@ __global__ void k_rap_build(int nc, const int *__restrict__ ria,
     }
 }
 
+// The same slot lists with a warp per coarse row, for rows whose bound ub
+// (1 + the fine rows' lengths) is at most 64: slot t lives in lane t % 32,
+// register t / 32.  The warp loads 32 entries of a fine row at a time (their
+// coarse columns in parallel), then takes the products one by one in CSR
+// order: a ballot finds the slot holding the column, whose lane adds the
+// value, or the next free slot takes it.  Every slot receives its values in
+// the same order as above, so the sums are the same bit for bit.  Rows with
+// a larger bound are left to k_rap_build (rowcnt untouched here).
+__global__ void __launch_bounds__(256)
+k_rap_build_warp(int nc, const int *__restrict__ ria, const int *__restrict__ rja,
+                 const int *__restrict__ ia, const int *__restrict__ ja,
+                 const double *__restrict__ a, const int *__restrict__ agg,
+                 const int *__restrict__ off, const int *__restrict__ ub, int *scol,
+                 double *sval, int *rowcnt, int *nbig) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += warps) {
+        if (ub[c] > 64) {
+            if (lane == 0) atomicAdd(nbig, 1);
+            continue;
+        }
+        int col0 = lane == 0 ? c : -1, col1 = -1;
+        double val0 = 0.0, val1 = 0.0;
+        int cnt = 1;
+        for (int q = ria[c]; q < ria[c + 1]; ++q) {
+            const int i = rja[q];
+            const int k0 = ia[i], k1 = ia[i + 1];
+            for (int kb = k0; kb < k1; kb += 32) {
+                const int k = kb + lane;
+                int cc_l = -1;
+                double v_l = 0.0;
+                if (k < k1) {
+                    cc_l = agg[ja[k]];
+                    v_l = a[k];
+                }
+                const int m = min(32, k1 - kb);
+                for (int j = 0; j < m; ++j) {
+                    const int cc = __shfl_sync(FULL, cc_l, j);
+                    const double v = __shfl_sync(FULL, v_l, j);
+                    if (cc < 0) continue;
+                    const unsigned h0 = __ballot_sync(FULL, col0 == cc);
+                    const unsigned h1 = __ballot_sync(FULL, col1 == cc);
+                    if (h0) {
+                        if (lane == __ffs(h0) - 1) val0 += v;
+                    } else if (h1) {
+                        if (lane == __ffs(h1) - 1) val1 += v;
+                    } else {
+                        if (lane == (cnt & 31)) {
+                            if (cnt < 32) { col0 = cc; val0 = v; }
+                            else { col1 = cc; val1 = v; }
+                        }
+                        ++cnt;
+                    }
+                }
+            }
+        }
+        int *cols = scol + off[c];
+        double *vals = sval + off[c];
+        if (lane < cnt) { cols[lane] = col0; vals[lane] = val0; }
+        if (lane + 32 < cnt) { cols[lane + 32] = col1; vals[lane + 32] = val1; }
+        if (lane == 0) rowcnt[c] = cnt;
+    }
+}
+
+// k_rap_build for the rows k_rap_build_warp left (bound above 64)
+__global__ void k_rap_build_big(int nc, const int *__restrict__ ria,
+                                const int *__restrict__ rja, const int *__restrict__ ia,
+                                const int *__restrict__ ja, const double *__restrict__ a,
+                                const int *__restrict__ agg, const int *__restrict__ off,
+                                const int *__restrict__ ub, int *scol, double *sval,
+                                int *rowcnt) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc;
+         c += gridDim.x * blockDim.x) {
+        if (ub[c] <= 64) continue;
+        int *cols = scol + off[c];
+        double *vals = sval + off[c];
+        int cnt = 1;
+        cols[0] = c;
+        vals[0] = 0.0;
+        for (int q = ria[c]; q < ria[c + 1]; ++q) {
+            const int i = rja[q];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                const int cc = agg[ja[k]];
+                if (cc < 0) continue;
+                int pos = -1;
+                for (int t = 0; t < cnt; ++t)
+                    if (cols[t] == cc) { pos = t; break; }
+                if (pos >= 0) {
+                    vals[pos] += a[k];
+                } else {
+                    cols[cnt] = cc;
+                    vals[cnt] = a[k];
+                    ++cnt;
+                }
+            }
+        }
+        rowcnt[c] = cnt;
+    }
+}
+
 __global__ void k_rap_compact(int nc, const int *__restrict__ off,
                               const int *__restrict__ cia,
                               const int *__restrict__ scol,
@@ -1172,9 +1273,25 @@ int rap_agg(const DCsr<double> &A, int nc, const int *agg, const int *ria,
     if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto fail; }
     if ((rc = dalloc(&scol, total))) goto fail;
     if ((rc = dalloc(&sval, total))) goto fail;
-    k_rap_build<<<g, 128, 0, s>>>(nc, ria, rja, A.ia, A.ja, A.val, agg, off, scol,
-                                  sval, rowcnt);
-    count_launch();
+    {
+        // a warp per coarse row; rows with a bound above 64 slots by a thread
+        int *nbig = tmp;   // the scan scratch is free until the next scan
+        e = cudaMemsetAsync(nbig, 0, sizeof(int), s);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto fail; }
+        k_rap_build_warp<<<grid_for(32LL * nc), 256, 0, s>>>(nc, ria, rja, A.ia, A.ja, A.val,
+                                                            agg, off, ub, scol, sval, rowcnt,
+                                                            nbig);
+        int hbig = 0;
+        e = cudaMemcpyAsync(&hbig, nbig, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto fail; }
+        count_launch();
+        if (hbig) {
+            k_rap_build_big<<<g, 128, 0, s>>>(nc, ria, rja, A.ia, A.ja, A.val, agg, off, ub,
+                                              scol, sval, rowcnt);
+            count_launch();
+        }
+    }
     if ((rc = scan_exclusive(rowcnt, cia, nc, tmp, s))) goto fail;
     e = cudaMemcpyAsync(cnnz, cia + nc, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1417,6 +1534,57 @@ __global__ void k_kahn_round(int head, int cnt, const int *__restrict__ ia,
     }
 }
 
+// Every round of Kahn's algorithm in one CTA: the frontier [head, cur) of the
+// queue releases the rows that depend on it; the queue end moves by a
+// shared-memory atomic and the rounds are separated by __syncthreads, so a
+// level of many small sets costs no launch or host round trip per set.
+// Each round removes at least one row, so at most n rounds run.  ptr
+// receives the set boundaries (n + 1 ints at most), *nsets their count.
+constexpr int KAHN_CTA_MAX_ROWS = 1 << 20;
+__global__ void __launch_bounds__(1024)
+k_kahn_all(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+           const int *__restrict__ tia, const int *__restrict__ tja, int backward,
+           int *indeg, int *rows, const int *__restrict__ tail0, int *ptr, int *nsets) {
+    __shared__ int s_tail, s_head, s_cur, s_ns;
+    if (threadIdx.x == 0) {
+        s_head = 0;
+        s_cur = *tail0;
+        s_tail = s_cur;
+        s_ns = 0;
+        ptr[0] = 0;
+    }
+    __syncthreads();
+    for (int round = 0; round < n; ++round) {
+        const int head = s_head, cur = s_cur;
+        if (cur <= head) break;
+        if (threadIdx.x == 0) ptr[++s_ns] = cur;
+        for (int q = head + threadIdx.x; q < cur; q += blockDim.x) {
+            const int i = rows[q];
+            for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                const int j = ja[k];
+                if (backward ? (j < i) : (j > i))
+                    if (atomicSub(indeg + j, 1) == 1) rows[atomicAdd(&s_tail, 1)] = j;
+            }
+            for (int k = tia[i]; k < tia[i + 1]; ++k) {
+                const int j = tja[k];
+                if (backward ? (j < i) : (j > i))
+                    if (atomicSub(indeg + j, 1) == 1) rows[atomicAdd(&s_tail, 1)] = j;
+            }
+        }
+        __threadfence_block();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_head = cur;
+            s_cur = s_tail;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        nsets[0] = s_ns;
+        nsets[1] = s_head;   // rows placed
+    }
+}
+
 static void make_runs(Schedule *sch) {
     const int ns = (int)sch->h_ptr.size() - 1;
     int k = 0;
@@ -1460,7 +1628,34 @@ int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,
     k_transpose_fill<<<g, 256, 0, s>>>(n, ia, ja, tia, fillc, tja);
     k_indeg<<<g, 256, 0, s>>>(n, ia, ja, tia, tja, backward, indeg, sch->rows, tail);
     count_launch(2);
-    {
+    if (n <= KAHN_CTA_MAX_ROWS) {
+        // one CTA runs every round; set boundaries and counts come back once
+        int *dptr = nullptr, *dns = nullptr;
+        if ((rc = dalloc(&dptr, n + 1)) || (rc = dalloc(&dns, 2))) {
+            dfree(dptr);
+            goto done;
+        }
+        k_kahn_all<<<1, 1024, 0, s>>>(n, ia, ja, tia, tja, backward, indeg, sch->rows, tail,
+                                       dptr, dns);
+        count_launch();
+        int hns[2] = {0, 0};
+        e = cudaMemcpyAsync(hns, dns, sizeof(hns), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && hns[1] == n) {
+            ptr.resize(hns[0] + 1);
+            e = cudaMemcpyAsync(ptr.data(), dptr, sizeof(int) * (hns[0] + 1),
+                                cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        }
+        dfree(dptr);
+        dfree(dns);
+        if (e != cudaSuccess) { set_error(e, __FILE__, __LINE__); rc = ERROR_SOLVER_MISC; goto done; }
+        if (hns[1] != n) {
+            set_error_msg("gs_schedule: incomplete level schedule");
+            rc = ERROR_DATA_STRUCTURE;
+            goto done;
+        }
+    } else {
         int head = 0, cur = 0;
         e = cudaMemcpyAsync(&cur, tail, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -34,6 +34,18 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
 int vmb_aggregate(int n, const int *nia, const int *nja, int max_agg, int *agg, int *nagg,
                   int *work, cudaStream_t s);
 
+// HEC aggregation (aggregation_hec, amg_setup_ua.c:752-845) in the
+// reference's order: rows visited in the permutation iarray_shuffle draws
+// from glibc's rand() (state: 35 device words, seeded by hec_seed and carried
+// across levels), each pairing with its strongest neighbour when that one is
+// unvisited, else joining its aggregate.  work: hec_work_ints(n) ints.
+// ERROR_AMG_COARSEING where the reference exits (a row of several entries
+// without an off-diagonal one).
+int hec_seed(unsigned *state, unsigned seed, cudaStream_t s);
+int hec_aggregate(int n, const int *nia, const int *nja, const double *nval, int *agg,
+                  int *nagg, unsigned *state, int *work, cudaStream_t s);
+size_t hec_work_ints(int n);
+
 // A caller's Galerkin inputs checked on the device before any kernel indexes
 // by them (aggregate ids in [-1, nc), row pointers rising from 0 to nnz,
 // columns in [0, n)); d_bad is one device int of scratch.  Synchronises s;

@@ -51,6 +51,7 @@ void Level::release() {
     if (own_A) { dfree(ia); dfree(ja); dfree(val); }
     ia = ja = nullptr; val = nullptr;
     dfree(val32);
+    dfree(val64nz);
     if (own32) { dfree(ia32); dfree(ja32); }
     ia32 = ja32 = nullptr;
     own32 = false;
@@ -273,13 +274,16 @@ forward:
         ++l;
         HZB_TRY(vzero<double>(S->lv[l].n, S->lv[l].x, S->s));
     }
-    HZB_TRY(coarse_solve64(S, cyc, cyc.tol * 1e-2));
+    if (S->batch) HZB_TRY(batch_terminal_solve(S, nl - 1, false));
+    else HZB_TRY(coarse_solve64(S, cyc, cyc.tol * 1e-2));
     while (l > l0) {
         --l;
         Level &L = S->lv[l];
         if (cyc.coarse_scaling == ON) HZB_TRY(coarse_alpha(S, l + 1, S->lv[l + 1].b, &alpha));
         HZB_TRY(prolong_level(S, l, S->lv[l + 1].x, L.x, alpha));
         HZB_TRY(smooth64(S, l, false, cyc));
+        // batched systems whose coarsening ended here: their block exactly
+        if (S->batch) HZB_TRY(batch_terminal_solve(S, l, false));
         if (num_lvl[l] < cyc.cycle_type) break;
         else num_lvl[l] = 0;
     }
@@ -375,7 +379,9 @@ forward:
         ++l;
         if (l < nl - 1) zero[l] = true;   // x_l = 0, folded into its first sweep
     }
-    {
+    if (S->batch) {
+        HZB_TRY(batch_terminal_solve(S, nl - 1, true));
+    } else {
         Level &C = S->lv[nl - 1];
         HZB_TRY(dense_gemv<float>(C.n, S->Ainv, C.b32, C.x32, S->s));
     }
@@ -384,6 +390,8 @@ forward:
         Level &L = S->lv[l];
         HZB_TRY(prolong_agg<float>(L.n, L.agg, S->lv[l + 1].x32, L.x32, 1.0f, S->s, L.act));
         HZB_TRY(smooth32(S, l, false, cyc, false));
+        // batched systems whose coarsening ended here: their block exactly
+        if (S->batch) HZB_TRY(batch_terminal_solve(S, l, true));
         if (num_lvl[l] < cyc.cycle_type) break;
         else num_lvl[l] = 0;
     }
@@ -420,6 +428,10 @@ int ensure_fp32(hzb_solver *S) {
                 HZB_TRY(dalloc(&L.val32, nz));
                 HZB_TRY(csr_nonzero_fill(L.n, L.ia, L.ja, L.val, L.ia32, L.ja32, L.val32, S->s));
                 L.own32 = true;
+                if (l == 0 && !S->batch) {   // the outer loop's operator
+                    HZB_TRY(dalloc(&L.val64nz, nz));
+                    HZB_TRY(csr_nonzero_fill64(L.n, L.ia, L.val, L.ia32, L.val64nz, S->s));
+                }
             }
             L.nnz32 = nz;
             HZB_TRY(bundle_capacity_rows(L.n, L.bundle_rows, L.ia32, S->s, &L.bundle_cap32));
@@ -529,7 +541,17 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
     int *tmp = nullptr;
     HZB_TRY(dalloc(&tmp, scan_tmp_size(n + 2)));
     int rc = SUCCESS;
-    while (S->lv[lvl].n > min_cdof && lvl < max_levels - 1) {
+    // batch mode: every system coarsens until its own terminal block (the
+    // union's size does not decide), see batch_level_begin
+    const bool batch = S->batch != nullptr;
+    int batch_begun = -1;   // the last level batch_level_begin has seen
+    while (lvl < max_levels - 1 && (batch || S->lv[lvl].n > min_cdof)) {
+        if (batch) {
+            int live = 0;
+            batch_begun = lvl;
+            if ((rc = batch_level_begin(S, lvl, false, &live))) break;
+            if (live == 0) break;   // every system ends on this level
+        }
         Level &L = S->lv[lvl];
         const int m = L.n;
         int *nia = nullptr, *nja = nullptr, *agg = nullptr, *work = nullptr;
@@ -539,19 +561,27 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
         // deterministic parallel matching (hzb_param.matching, and for HEC,
         // whose reference order comes from an unseeded rand())
         const bool vmb = S->amg.aggregation_type == VMB;
-        const bool par = !vmb && (S->bp.matching == HZB_MATCH_PARALLEL ||
-                                  S->amg.aggregation_type == HEC);
+        const bool par = !vmb && S->bp.matching == HZB_MATCH_PARALLEL;
+        const bool hec = !vmb && !par && S->amg.aggregation_type == HEC;
         if ((rc = dalloc(&nia, m + 1)) || (rc = dalloc(&nja, L.nnz)) ||
             (rc = dalloc(&nval, L.nnz)) || (rc = dalloc(&agg, m)) ||
             (rc = dalloc(&work, par ? (size_t)6 * m + scan_tmp_size(m + 1) + 8
-                                    : (size_t)(vmb ? 2 : 1) * m))) {
+                                : hec ? hec_work_ints(m)
+                                      : (size_t)(vmb ? 2 : 1) * m))) {
             dfree(nia); dfree(nja); dfree(nval); dfree(agg); dfree(work);
             break;
         }
-        rc = strength_graph(L.A64(), S->amg.strong_coupled, nia, nja, nval, &nnnz, tmp, s);
+        // HEC draws from rand() as a fresh process does: seeded 1 per setup
+        if (hec && lvl == 0) {
+            if (!S->hec_state) rc = dalloc(&S->hec_state, 35);
+            if (!rc) rc = hec_seed(S->hec_state, 1u, s);
+        }
+        if (!rc) rc = strength_graph(L.A64(), S->amg.strong_coupled, nia, nja, nval, &nnnz,
+                                     tmp, s);
         if (!rc) {
             if (vmb) rc = vmb_aggregate(m, nia, nja, S->amg.max_aggregation, agg, &nagg, work, s);
             else if (par) rc = hem_parallel(m, nia, nja, nval, agg, &nagg, work, s);
+            else if (hec) rc = hec_aggregate(m, nia, nja, nval, agg, &nagg, S->hec_state, work, s);
             else rc = hem_exact(m, nia, nja, nval, agg, &nagg, work, s);
         }
         dfree(work);
@@ -569,7 +599,11 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
         if (nagg * 4 > m) S->amg.strong_coupled /= 2;
         else if (nagg * 1.25 < m) S->amg.strong_coupled *= 2;
         if (S->caller_amg) S->caller_amg->strong_coupled = S->amg.strong_coupled;
-        if (nagg < MIN_CDOF) {
+        if (batch && (rc = batch_level_end(S, lvl, agg, &nagg))) {
+            dfree(agg);
+            break;
+        }
+        if (batch ? nagg == 0 : nagg < MIN_CDOF) {
             dfree(agg);
             if (sa) { dfree(nia); dfree(nja); dfree(nval); }
             break;
@@ -611,9 +645,15 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
     dfree(tmp);
     if (rc) return rc;
     S->nl = lvl + 1;
+    if (batch && batch_begun != lvl) {
+        // systems still coarsening when the level cap ends the loop end there
+        int live = 0;
+        HZB_TRY(batch_level_begin(S, lvl, true, &live));
+    }
     // coarsest level: dense inverse (coarse_solver 32, and always for the
-    // FP32 cycle)
-    if (S->amg.coarse_solver == SOLVER_UMFPACK || S->bp.precision == HZB_PREC_MIXED) {
+    // FP32 cycle); batched systems use their terminal blocks instead
+    if (!batch &&
+        (S->amg.coarse_solver == SOLVER_UMFPACK || S->bp.precision == HZB_PREC_MIXED)) {
         // amg_setup_ua.c:1392-1401: the coarsest matrix is transposed (columns
         // ascending) and that transpose is factored
         Level &C = S->lv[S->nl - 1];
@@ -1044,7 +1084,7 @@ int solver_precond(hzb_solver *S, const double *r, double *z) {
 int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
               int prtlvl, double *relres_out) {
     KrylovWork &w = S->kw;
-    const DCsr<double> A = S->lv[0].A64();
+    const DCsr<double> A = S->lv[0].A64outer();
     const int m = A.n;
     cudaStream_t s = S->s;
     const int G = reduce_blocks(m);
@@ -1113,6 +1153,7 @@ void destroy(hzb_solver *S) {
     S->lv.clear();
     dfree(S->Ainv);
     dfree(S->omega);
+    dfree(S->hec_state);
     dfree(S->pr);
     dfree(S->pz);
     S->kw.release();

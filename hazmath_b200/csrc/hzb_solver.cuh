@@ -24,6 +24,10 @@ struct Level {
     int *ia32 = nullptr, *ja32 = nullptr;
     float *val32 = nullptr;
     bool own32 = false;
+    // level 0 of the mixed solve with stored exact zeros: the FP64 values of
+    // the FP32 copy's pattern, for the outer Krylov loop's SpMV (a zero adds
+    // nothing to a row sum, so its result is the full matrix's)
+    double *val64nz = nullptr;
     // transfer to level + 1 (P = agg map, R = P^T with ascending rows);
     // smoothed aggregation keeps P as a CSR with values and R's values too
     int nc = 0;
@@ -63,6 +67,16 @@ struct Level {
     DCsr<double> A64() const {
         DCsr<double> m;
         m.n = n; m.nnz = nnz; m.ia = ia; m.ja = ja; m.val = val; m.bundle_cap = bundle_cap;
+        m.bundle_rows = bundle_rows;
+        m.act = act;
+        return m;
+    }
+    // the outer loop's FP64 operator: the zero-free copy when there is one
+    DCsr<double> A64outer() const {
+        if (!val64nz) return A64();
+        DCsr<double> m;
+        m.n = n; m.nnz = nnz32; m.ia = ia32; m.ja = ja32; m.val = val64nz;
+        m.bundle_cap = bundle_cap32;
         m.bundle_rows = bundle_rows;
         m.act = act;
         return m;
@@ -138,6 +152,7 @@ struct hzb_solver {
     // nonlinear AMLI cycle and the coarse GMRES fallback
     std::vector<hzb::GmresWork *> gm_ws;
     std::vector<hzb::GcgWork *> gcg_ws;
+    unsigned *hec_state = nullptr;    // rand() stream of HEC aggregation (35 words)
     float *omega = nullptr;           // learned fine-level weights (device)
     bool omega_active = false;
     hzb_stats st{};
@@ -245,6 +260,14 @@ int batch_setup(hzb_solver *S, int nsys, const int *off, int n, int nnz, const i
 int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit,
                 int *h_iters, double *h_relres, double *h_seconds);
 void batch_release(hzb_solver *S);
+// terminal levels of the batched systems, called by setup's level loop in
+// batch mode: which systems end on level lvl (their dense inverses; *live =
+// rows of the others), then after the aggregation the removal of their rows
+// from the coarser levels; and the solves of a level's terminal blocks
+int batch_level_begin(hzb_solver *S, int lvl, bool force, int *live);
+int batch_level_end(hzb_solver *S, int lvl, int *agg, int *nagg);
+int batch_terminal_solve(hzb_solver *S, int lvl, bool fp32);
+bool batch_has_terminal(const hzb_solver *S, int lvl);
 // UA-AMG of a block matrix (hzb_bsr.cu): amg_setup_ua_bsr on nrow block rows
 // of nb x nb blocks (row-major); z = B r of precond_dbsr_amg with the cycle
 // parameters S->bsr_cyc; the scalar expansion of the level-0 matrix (the

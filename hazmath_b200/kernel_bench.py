@@ -1,6 +1,6 @@
 """Level-kernel timing on a workload's hierarchy.
 
-    python -m hazmath_b200.kernel_bench [--case c1|c2|c5] [--levels 0,1,2]
+    python -m hazmath_b200.kernel_bench [--case c1|c2|c5] [--cubes N] [--levels 0,1,2]
         [--kernels spmv64,spmv32,res64,l1_32,l1_64,gs64] [--reps 50]
         [--precision mixed|fp64] [--matching parallel|exact] [--smoother l1|gs]
     python -m hazmath_b200.kernel_bench --assemble [--case c2|c5] [--reps 20]
@@ -9,7 +9,9 @@ Builds the UA-AMG hierarchy (l1-Jacobi V(2,2) settings, or Gauss-Seidel
 V(1,1) with --smoother gs, whose sweep gs64 times on the level schedules) of
 the 3D P1 log-normal diffusion problem on the Kuhn mesh of 128^3 (c2,
 sigma 1) or 256^3 (c5, sigma 1.5) cubes, or of the 2D 255^2 Poisson problem
-(c1), then times each requested kernel on each
+(c1) -- or, with --cubes N, of the c5 family (sigma 1.5) on N^3 cubes, a
+smaller instance whose levels still exceed the L2 -- then times each
+requested kernel on each
 requested level with hzb_time_kernel: `reps` back-to-back launches on the
 handle's stream between CUDA events, after one warm-up launch.  Prints
 achieved GB/s from the kernel's algorithmic bytes and the fraction of the
@@ -52,6 +54,7 @@ def main():
     ap.add_argument("--matching", default="parallel", choices=["parallel", "exact"])
     ap.add_argument("--assemble", action="store_true")
     ap.add_argument("--smoother", default="l1", choices=["l1", "gs"])
+    ap.add_argument("--cubes", type=int, default=0)
     a = ap.parse_args()
     if a.assemble and a.case == "c1":
         ap.error("--assemble times the Kuhn-mesh cases c2 and c5")
@@ -62,6 +65,8 @@ def main():
         ia, ja, val = P.poisson2d_5pt(255)
     else:
         N, sigma, seed = CASES[a.case]
+        if a.cubes:
+            N, sigma, seed = a.cubes, 1.5, 7
         ia, ja, val = P.kuhn3d_p1(N, P.lognormal_field(N, sigma, 8.0, seed))
     n = len(ia) - 1
     dia, dja, dval = (torch.from_numpy(v).cuda() for v in (ia, ja, val))

@@ -50,3 +50,33 @@ def test_reference_arm_bsr_line():
 def test_variant_needs_c1_or_c2():
     r = _bench("--impl", "reference", "--workload", "c5", "--variant", "gmres", timeout=120)
     assert r.returncode == 2 and "c1 and c2" in r.stderr
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_reference_arm_c1_line():
+    """c1: the full workload every timed step; setup and solve seconds of the
+    reference reported beside the total."""
+    d = _line(_bench("--impl", "reference", "--workload", "c1", "--steps", "2",
+                     "--warmup", "3"))
+    assert KEYS <= set(d)
+    assert d["steps"] == 2 and d["steps_requested"] == 2
+    assert d["iterations"] == 25   # l1-Jacobi V(2,2) on the 255^2 Poisson problem
+    assert d["setup_s"] > 0 and d["solve_s"] > 0
+
+
+def test_solve_bytes_model():
+    """The solve-level byte model of the mixed solve on a two-level
+    hierarchy, term by term."""
+    sys.path.insert(0, ROOT)
+    import bench
+    n0, nnz0, nz32, n1 = 1000, 7000, 5000, 400
+    levels = [{"rows": n0, "nnz": nnz0, "nnz32": nz32}, {"rows": n1}]
+    sweep = 8 * nz32 + 4 * (n0 + 1) + 12 * n0
+    cyc = 12 * n0 + 3 * sweep + sweep + (4 * (n1 + 1) + 8 * n0 + 4 * n1) \
+        + (12 * n0 + 4 * n1) + 8 * n1 * n1 + 8 * n1
+    outer = 12 * nnz0 + 4 * (n0 + 1) + 16 * n0 + 112 * n0
+    res0 = 12 * nnz0 + 4 * (n0 + 1) + 24 * n0
+    assert bench.solve_bytes_mixed(levels, 10, False) == 10 * outer + 11 * cyc + 2 * res0
+    # the learned weights add 4 bytes per fine row to the first and three full sweeps
+    assert bench.solve_bytes_mixed(levels, 10, True) - bench.solve_bytes_mixed(
+        levels, 10, False) == 11 * 4 * (4 * n0)

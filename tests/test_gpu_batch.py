@@ -1,8 +1,9 @@
 """Batched independent systems (hzb_batch_setup_device / hzb_batch_solve_device):
 every system reaches its own tolerance on its own true FP64 residual, each
-system's answer is the one an independent solve gives, one system alone
-takes the single-system path's iterations, and an entry that couples two
-systems is rejected."""
+system's answer is the one an independent solve gives and is within the
+tolerance's order of the reference's solve of that system alone, one system
+alone takes about the single-system path's iterations, and an entry that
+couples two systems is rejected."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -100,8 +101,10 @@ def test_single_system_batch_is_the_single_system_solve():
     assert S.setup_host(ia, ja, val) == 0
     it1 = S.solve_host(b, xs)
     S.close()
-    # same hierarchy and cycle; only the inner-product summation order differs
-    assert abs(int(its[0]) - it1) <= 1
+    # the batch ends a system's coarsening at 128 rows (a dense block solve),
+    # the single-system solve at coarse_dof = 2000 rows; the cycles differ
+    # below that, so the counts may differ by a few
+    assert abs(int(its[0]) - it1) <= 3, (int(its[0]), it1)
     assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-6
 
 
@@ -117,3 +120,35 @@ def test_batch_rejects_coupled_systems():
                               dval.data_ptr())
     S.close()
     assert rc == hz.ERROR_INPUT_PAR
+
+
+def test_batch_against_reference_per_system(golden):
+    """Each of the 24 systems solved by the batch (FP32 cycle, parallel
+    matching, per-system flexible CG to 1e-8) against the same system solved
+    on its own by the reference (tests/golden/batch.npz: FP64 UA-AMG with
+    HEM, l1-Jacobi V(2,2), PCG): the error against the reference's solve
+    tightened to 1e-12 is of the tolerance's order (below 1e-6 relative),
+    and the iteration counts are bounded against the reference's: a system
+    the reference coarsens (more than coarse_dof = 2000 rows) needs at most
+    2.5 times the reference's iterations; a smaller one the reference solves
+    directly (one iteration), while the batch runs it through the union's
+    hierarchy (at most 25 iterations)."""
+    g = golden("batch.npz")
+    systems, union = P.batch_anisotropic(24, seed=3, dof_lo=500, dof_hi=30000)
+    rc, its, rel, sec, x, _ = _batch_solve(union)
+    assert rc > 0, hz.last_error()
+    off = union[0]
+    st = int(g["stride"])
+    worst, rows = 0.0, []
+    for k in range(len(systems)):
+        xs = g[f"{k}/x_sample"]
+        xk = x[off[k]:off[k + 1]][::st]
+        err = np.linalg.norm(xk - xs) / np.linalg.norm(xs)
+        worst = max(worst, err)
+        rows.append((k, len(systems[k][3]), int(its[k]), int(g[f"{k}/iters"]), err))
+        assert err < 1e-6, (k, err)
+    print("system, dofs, batch its, reference its, error vs reference 1e-12 solve:")
+    for r in rows:
+        print("  %2d %6d %4d %4d %.2e" % r)
+    for k, n, ib, ir, _ in rows:
+        assert ib <= (2.5 * ir if n > 2000 else 25), (k, n, ib, ir)
