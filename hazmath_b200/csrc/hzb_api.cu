@@ -288,6 +288,10 @@ extern "C" INT hzb_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
     }
     HZB_CUDA(cudaEventRecord(S->e1, S->s));
     HZB_CUDA(cudaEventSynchronize(S->e1));
+    if (it >= 0) {
+        const int wc = check_waits(S);
+        if (wc) it = wc;
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, S->e0, S->e1);
     S->st.solve_seconds = ms * 1e-3;
@@ -369,7 +373,7 @@ extern "C" INT hzb_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z) {
     HZB_TRY(apply_precond(S, pc_kind_of_cycle(S->pc_cyc.cycle_type), nullptr, S->lv[0].n, d_r,
                           d_z));
     HZB_CUDA(cudaStreamSynchronize(S->s));
-    return SUCCESS;
+    return check_waits(S);
 }
 
 extern "C" INT hzb_time_kernel(hzb_solver *S, INT which, INT level, INT reps,
@@ -885,6 +889,10 @@ static INT krylov_host(dCSRmat *A, dvector *b, dvector *u, precond *pc, REAL tol
         else
             it = gmres(S, D, db, du, kind, &hp, tol, MaxIt, restart, stop_type, prtlvl,
                        type == SOLVER_VFGMRES, &rel);
+        if (it >= 0 && S->nl > 0) {
+            const int wc = check_waits(S);
+            if (wc) it = wc;
+        }
         if (it != ERROR_SOLVER_MISC) {
             cudaMemcpyAsync(u->val, du, sizeof(double) * A->row, cudaMemcpyDeviceToHost, S->s);
             if (cudaStreamSynchronize(S->s) != cudaSuccess) it = ERROR_SOLVER_MISC;
@@ -1123,6 +1131,10 @@ extern "C" INT hzb_bsr_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {
     }
     HZB_CUDA(cudaEventRecord(S->e1, S->s));
     HZB_CUDA(cudaEventSynchronize(S->e1));
+    if (it >= 0) {
+        const int wc = check_waits(S);
+        if (wc) it = wc;
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, S->e0, S->e1);
     S->st.solve_seconds = ms * 1e-3;

@@ -915,15 +915,15 @@ __global__ void k_gs_rows(int cnt, const int *__restrict__ rows,
 // (CSR order from b_i, the diagonal skipped), so the result is the same bit
 // for bit.
 constexpr int GS_PRE = 8;
-template <typename T>
+template <typename T, int P = GS_PRE>
 struct GsRowData {
     int i = -1, k0 = 0, k1 = 0;
-    int col[GS_PRE];
-    T val[GS_PRE];
+    int col[P];
+    T val[P];
     T bi = T(0), di = T(0);
 };
-template <typename T>
-__device__ __forceinline__ void gs_row_load(GsRowData<T> &r, const int *__restrict__ rows,
+template <typename T, int P>
+__device__ __forceinline__ void gs_row_load(GsRowData<T, P> &r, const int *__restrict__ rows,
                                             int q, int q1, const int *__restrict__ ia,
                                             const int *__restrict__ ja,
                                             const T *__restrict__ a,
@@ -934,7 +934,7 @@ __device__ __forceinline__ void gs_row_load(GsRowData<T> &r, const int *__restri
     r.k0 = ia[r.i];
     r.k1 = ia[r.i + 1];
 #pragma unroll
-    for (int u = 0; u < GS_PRE; ++u) {
+    for (int u = 0; u < P; ++u) {
         if (r.k0 + u < r.k1) {
             r.col[u] = ja[r.k0 + u];
             r.val[u] = a[r.k0 + u];
@@ -1016,6 +1016,154 @@ int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
+// ---------------------------------------------------------------------------
+// Consecutive large level sets in one cooperative launch, the sets separated
+// by a grid barrier.  The barrier is an arrival counter and a generation
+// word (bar[0], bar[1]; the last CTA to arrive resets the counter and bumps
+// the generation).  Its wait is bounded: after GRID_SPIN_LIMIT polls
+// (about half a second) the CTA raises *err and returns, and a CTA that sees
+// *err raised stops too, so a missing CTA ends the sweep with an error that
+// the host reads (the Krylov loops read *err with their scalars), never with
+// a hang.  Cooperative launch guarantees the CTAs are co-resident.  x is
+// read and written at L2 (ld/st.global.cg): the CTAs of other SMs wrote it.
+// ---------------------------------------------------------------------------
+constexpr unsigned GRID_SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err) {
+    __shared__ int s_bad;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        volatile int *verr = err;
+        const unsigned g = *gen;
+        int bad = 0;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            for (unsigned spin = 0; *gen == g; ++spin) {
+                if (*verr) { bad = 1; break; }
+                if (spin > GRID_SPIN_LIMIT) {
+                    atomicExch(err, 1);
+                    bad = 1;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        if (*verr) bad = 1;
+        s_bad = bad;
+    }
+    __syncthreads();
+    return !s_bad;
+}
+
+// One row per thread per set when the grid covers the largest set (the
+// launch sizes it so): the row data of the next set is loaded before each
+// barrier, as in k_gs_run; rows beyond the grid (a set larger than the
+// co-resident threads) are swept with plain loads.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_gs_sets_grid(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first,
+               int last, const int *__restrict__ ia, const int *__restrict__ ja,
+               const T *__restrict__ a, const T *__restrict__ d, int kind, T w,
+               const T *__restrict__ b, T *x, int skip, unsigned *bar, int *err) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthr = gridDim.x * blockDim.x;
+    constexpr int P = 16;
+    GsRowData<T, P> cur, nxt;
+    int q0 = set_ptr[first], q1 = set_ptr[first + 1];
+    gs_row_load(cur, rows, q0 + gtid, q1, ia, ja, a, d, b);
+    for (int sidx = first; sidx < last; ++sidx) {
+        const int i = cur.i;
+        if (i >= 0 && i != skip) {
+            T t = cur.bi;
+            T xv[P];
+#pragma unroll
+            for (int u = 0; u < P; ++u)
+                xv[u] = cur.k0 + u < cur.k1 ? __ldcg(x + cur.col[u]) : T(0);
+#pragma unroll
+            for (int u = 0; u < P; ++u)
+                if (cur.k0 + u < cur.k1 && cur.col[u] != i) t -= cur.val[u] * xv[u];
+            for (int k = cur.k0 + P; k < cur.k1; ++k) {
+                const int j = ja[k];
+                if (j != i) t -= a[k] * __ldcg(x + j);
+            }
+            const T di = cur.di;
+            if (kind == 0) {
+                __stcg(x + i, t * di);
+            } else if (kind == 1) {
+                if (fabs(di) > T(SMALLREAL)) __stcg(x + i, w * (t / di) + (1 - w) * __ldcg(x + i));
+            } else {
+                if (fabs(di) > T(SMALLREAL)) __stcg(x + i, t / di);
+            }
+        }
+        for (int q = q0 + gtid + nthr; q < q1; q += nthr) {   // beyond one row per thread
+            const int r = rows[q];
+            if (r == skip) continue;
+            T t = b[r];
+            for (int k = ia[r]; k < ia[r + 1]; ++k) {
+                const int j = ja[k];
+                if (j != r) t -= a[k] * __ldcg(x + j);
+            }
+            const T di = d[r];
+            if (kind == 0) {
+                __stcg(x + r, t * di);
+            } else if (kind == 1) {
+                if (fabs(di) > T(SMALLREAL)) __stcg(x + r, w * (t / di) + (1 - w) * __ldcg(x + r));
+            } else {
+                if (fabs(di) > T(SMALLREAL)) __stcg(x + r, t / di);
+            }
+        }
+        if (sidx + 1 < last) {
+            q0 = q1;
+            q1 = set_ptr[sidx + 2];
+            gs_row_load(nxt, rows, q0 + gtid, q1, ia, ja, a, d, b);
+            if (!grid_barrier(bar, gridDim.x, err)) return;
+            cur = nxt;
+        }
+    }
+}
+
+template <typename T>
+int gs_sets_grid(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr, int first,
+                 int last, int max_set, const T *d, T w, const T *b, T *x, unsigned *bar,
+                 int *err, cudaStream_t s) {
+    if (last <= first) return SUCCESS;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_sets_grid<T>, 256, 0) !=
+                cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    const int grid = std::max(1, std::min(per_sm * sm_count(), div_up(max_set, 256)));
+    const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
+    const int kd = kind & 15;
+    // every launch starts its barrier from zero (a wait that ran out may
+    // have left an arrival counted)
+    HZB_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HZB_CUDA(cudaLaunchKernelEx(&cfg, k_gs_sets_grid<T>, rows, set_ptr, first, last, A.ia,
+                                A.ja, A.val, d, kd, w, b, x, skip, bar, err));
+    count_launch();
+    return SUCCESS;
+}
+template int gs_sets_grid<double>(const DCsr<double> &, int, const int *, const int *, int,
+                                  int, int, const double *, double, const double *, double *,
+                                  unsigned *, int *, cudaStream_t);
+
 template int gs_rows<double>(const DCsr<double> &, int, const int *, int,
                              const double *, double, const double *, double *,
                              cudaStream_t);

@@ -84,6 +84,13 @@ constexpr int GS_SKIP_LAST = 16;
 template <typename T>
 int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt,
             const T *d, T w, const T *b, T *x, cudaStream_t s);
+// consecutive level sets [first, last) of up to max_set rows each in one
+// cooperative launch with a bounded grid barrier between sets (bar: 2
+// device words, zero at first use; err: raised if a barrier wait ran out)
+template <typename T>
+int gs_sets_grid(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr, int first,
+                 int last, int max_set, const T *d, T w, const T *b, T *x, unsigned *bar,
+                 int *err, cudaStream_t s);
 // One CTA runs level sets [first, last) back to back, __syncthreads between
 // sets (all sets of the run hold <= 1024 rows).
 template <typename T>

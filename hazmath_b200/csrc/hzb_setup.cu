@@ -851,15 +851,19 @@ __global__ void k_pm_accept(int n, int round, const int *__restrict__ ia,
 
 __global__ void k_pm_assign(int n, const int *__restrict__ acc,
                             const int *__restrict__ flag,
-                            const int *__restrict__ pos, int base, int *state) {
+                            const int *__restrict__ pos, const int *__restrict__ base,
+                            int *state) {
+    const int b = *base;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n;
          j += gridDim.x * blockDim.x)
         if (flag[j]) {
-            const int c = base + pos[j];
+            const int c = b + pos[j];
             state[j] = c;
             state[acc[j]] = c;
         }
 }
+// the aggregate count after a round: base += the round's pairs
+__global__ void k_pm_advance(int *base, const int *__restrict__ cnt) { *base += *cnt; }
 
 // Renumbering by leader: aggregate ids follow their smallest member vertex,
 // so coarse rows keep the fine ordering's locality (ids were handed out round
@@ -930,6 +934,7 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
     const int g = grid_for(n);
     k_pm_init<<<g, 256, 0, s>>>(n, nia, state);
     count_launch();
+    cudaMemsetAsync(dflag + 1, 0, sizeof(int), s);   // the aggregate count
     int nc = 0;
     int *acc = size;   // free during the rounds
     for (int round = 0, idle = 0; round < 96 && idle < 4; ++round) {
@@ -937,19 +942,18 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
         k_pm_propose<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr);
         k_pm_accept<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr, acc, flag, dflag);
         count_launch(2);
-        int any = 0, cnt = 0;
         int rc = scan_exclusive(flag, pos, n, tmp, s);
         if (rc) { dfree(dflag); return rc; }
-        cudaMemcpyAsync(&any, dflag, sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&cnt, pos + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+        k_pm_assign<<<g, 256, 0, s>>>(n, acc, flag, pos, dflag + 1, state);
+        k_pm_advance<<<1, 1, 0, s>>>(dflag + 1, pos + n);
+        count_launch(2);
+        int h[2];
+        cudaMemcpyAsync(h, dflag, sizeof(h), cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { dfree(dflag); set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
+        nc = h[1];
         // stop after a few rounds in a row without a new pair
-        if (!any) { ++idle; continue; }
-        idle = 0;
-        k_pm_assign<<<g, 256, 0, s>>>(n, acc, flag, pos, nc, state);
-        count_launch();
-        nc += cnt;
+        idle = h[0] ? 0 : idle + 1;
     }
     cudaMemsetAsync(size, 0, sizeof(int) * (nc > 0 ? nc : 1), s);
     k_pm_sizes<<<g, 256, 0, s>>>(n, state, size);
@@ -1472,6 +1476,7 @@ fail:
 void Schedule::release() {
     dfree(rows);
     dfree(set_ptr);
+    dfree(bar);
     h_ptr.clear();
     run_first.clear();
     run_last.clear();
@@ -1679,6 +1684,11 @@ int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,
         }
     }
     sch->h_ptr = ptr;
+    if ((rc = dalloc(&sch->bar, 2))) goto done;
+    if (cudaMemsetAsync(sch->bar, 0, 2 * sizeof(unsigned), s) != cudaSuccess) {
+        rc = ERROR_SOLVER_MISC;
+        goto done;
+    }
     if ((rc = dalloc(&sch->set_ptr, ptr.size()))) goto done;
     e = cudaMemcpyAsync(sch->set_ptr, ptr.data(), sizeof(int) * ptr.size(),
                         cudaMemcpyHostToDevice, s);

@@ -85,6 +85,7 @@ struct Schedule {
     std::vector<int> h_ptr;        // host copy of set_ptr
     std::vector<int> run_first;    // runs of small sets for one CTA: [first,last)
     std::vector<int> run_last;
+    unsigned *bar = nullptr;       // device, 2 words: grid barrier of gs_sets_grid
     void release();
 };
 int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,

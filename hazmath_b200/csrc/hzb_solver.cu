@@ -44,6 +44,65 @@ __global__ void k_fcg_p(int n, const double *__restrict__ zt,
 
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
 
+// The mixed solve's flexible-CG update: u += alpha p, r -= alpha t with
+// alpha = num / den (the products as k_pcg_update forms them), the partial
+// sums of (r, r), and the FP32 copy of r the cycle starts from.
+__global__ void k_fcg_update(int n, const double *__restrict__ num,
+                             const double *__restrict__ den, double *u, double *r,
+                             const double *__restrict__ p, const double *__restrict__ t,
+                             float *r32, double *part) {
+    __shared__ double sh[32];
+    const double alpha = num[0] / den[0];
+    double rr = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const double pi = p[i];
+        double ui = u[i];
+        if (alpha == 1.0) ui += pi;
+        else if (alpha == -1.0) ui -= pi;
+        else ui += alpha * pi;
+        const double ma = -alpha;
+        double ri = r[i];
+        const double ti = t[i];
+        if (ma == 1.0) ri += ti;
+        else if (ma == -1.0) ri -= ti;
+        else ri += ma * ti;
+        u[i] = ui;
+        r[i] = ri;
+        r32[i] = (float)ri;
+        rr += ri * ri;
+    }
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = rr;
+}
+
+// (z, t) and (z, r) with z the cycle's FP32 output widened to FP64 (the
+// values f2d would write), and p = z + beta p from the same z
+__global__ void k_dot2_partial_f(int n, const float *__restrict__ z,
+                                 const double *__restrict__ t,
+                                 const double *__restrict__ r, double *part) {
+    __shared__ double sh[32];
+    double a = 0.0, b = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const double zi = (double)z[i];
+        a += zi * t[i];
+        b += zi * r[i];
+    }
+    a = block_sum(a, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+    b = block_sum(b, sh);
+    if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = b;
+}
+__global__ void k_fcg_p_f(int n, const double *__restrict__ zt,
+                          const double *__restrict__ pap, const float *__restrict__ z,
+                          double *p) {
+    const double beta = -zt[0] / pap[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        p[i] = (double)z[i] + beta * p[i];
+}
+
 // ---------------------------------------------------------------------------
 // containers
 // ---------------------------------------------------------------------------
@@ -68,10 +127,12 @@ void Level::release() {
 }
 
 // scalar slots of KrylovWork::sc
+// SC_ERR: raised (as an int) by a device wait that ran out; read with the
+// scalars by every fetch
 enum { SC_T1 = 0, SC_T2 = 1, SC_RR = 2, SC_UM = 3, SC_UU = 4, SC_PP = 5,
-       SC_T3 = 6, SC_ZT = 7, SC_X = 8, SC_N = 16 };
+       SC_T3 = 6, SC_ZT = 7, SC_X = 8, SC_ERR = 15, SC_N = 16 };
 
-int KrylovWork::alloc(int nn) {
+int KrylovWork::alloc(int nn, cudaStream_t st) {
     release();
     n = nn;
     const int G = reduce_blocks(n);
@@ -82,6 +143,8 @@ int KrylovWork::alloc(int nn) {
     HZB_TRY(dalloc(&t, n));
     HZB_TRY(dalloc(&part, np));
     HZB_TRY(dalloc(&sc, SC_N));
+    // on the stream the allocations were made on (the entry point's)
+    HZB_CUDA(cudaMemsetAsync(sc, 0, SC_N * sizeof(double), st ? st : cur_stream()));
     HZB_CUDA(cudaMallocHost((void **)&h_sc, SC_N * sizeof(double)));
     return SUCCESS;
 }
@@ -96,6 +159,28 @@ static int fetch(hzb_solver *S, KrylovWork &w) {
     HZB_CUDA(cudaMemcpyAsync(w.h_sc, w.sc, SC_N * sizeof(double),
                              cudaMemcpyDeviceToHost, S->s));
     HZB_CUDA(cudaStreamSynchronize(S->s));
+    int e = 0;
+    memcpy(&e, w.h_sc + SC_ERR, sizeof(int));
+    if (e) {
+        cudaMemsetAsync(w.sc + SC_ERR, 0, sizeof(double), S->s);
+        set_error_msg("a grid barrier of a Gauss-Seidel sweep ran out of time");
+        return ERROR_SOLVER_MISC;
+    }
+    return SUCCESS;
+}
+
+// the word the cycle's device waits raise (for paths that do not fetch the
+// outer loop's scalars every step)
+int check_waits(hzb_solver *S) {
+    if (!S->kw.sc) return SUCCESS;
+    int e = 0;
+    HZB_CUDA(cudaMemcpyAsync(&e, S->kw.sc + SC_ERR, sizeof(int), cudaMemcpyDeviceToHost, S->s));
+    HZB_CUDA(cudaStreamSynchronize(S->s));
+    if (e) {
+        cudaMemsetAsync(S->kw.sc + SC_ERR, 0, sizeof(double), S->s);
+        set_error_msg("a grid barrier of a Gauss-Seidel sweep ran out of time");
+        return ERROR_SOLVER_MISC;
+    }
     return SUCCESS;
 }
 
@@ -111,12 +196,35 @@ static int run_sets(hzb_solver *S, const DCsr<double> &A, const Schedule &sc,
                     int kind, const double *d, double w, const double *b,
                     double *x, bool reverse) {
     const int ns = (int)sc.h_ptr.size() - 1;
+    // consecutive large sets go to one cooperative launch when the grid
+    // barrier has its words (exact schedules) and a place to report to;
+    // HZB_GS_GRID=0 launches them one by one instead (same results)
+    static const bool grid_ok = [] {
+        const char *e = getenv("HZB_GS_GRID");
+        return !(e && e[0] == '0');
+    }();
+    int *err = grid_ok && S->kw.sc ? reinterpret_cast<int *>(S->kw.sc + SC_ERR) : nullptr;
     if (!reverse) {
-        for (size_t q = 0; q < sc.run_first.size(); ++q) {
+        const size_t nr = sc.run_first.size();
+        for (size_t q = 0; q < nr; ++q) {
             const int f = sc.run_first[q], l = sc.run_last[q];
             if (l < 0) {
-                HZB_TRY(gs_rows<double>(A, kind, sc.rows + sc.h_ptr[f],
-                                        sc.h_ptr[f + 1] - sc.h_ptr[f], d, w, b, x, S->s));
+                size_t q2 = q;
+                int max_set = 0;
+                while (q2 < nr && sc.run_last[q2] < 0) {
+                    const int k = sc.run_first[q2];
+                    max_set = std::max(max_set, sc.h_ptr[k + 1] - sc.h_ptr[k]);
+                    ++q2;
+                }
+                if (sc.bar && err && q2 - q > 1) {
+                    const int f2 = sc.run_first[q2 - 1] + 1;
+                    HZB_TRY(gs_sets_grid<double>(A, kind, sc.rows, sc.set_ptr, f, f2, max_set,
+                                                 d, w, b, x, sc.bar, err, S->s));
+                    q = q2 - 1;
+                } else {
+                    HZB_TRY(gs_rows<double>(A, kind, sc.rows + sc.h_ptr[f],
+                                            sc.h_ptr[f + 1] - sc.h_ptr[f], d, w, b, x, S->s));
+                }
             } else {
                 HZB_TRY(gs_run<double>(A, kind, sc.rows, sc.set_ptr, f, l, d, w, b, x, S->s));
             }
@@ -499,6 +607,7 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
           const double *d_val, bool copy_in) {
     S->g64.release();
     S->g32.release();
+    S->g32c.release();
     S->gcyc.release();
     gmres_release(S);
     gcg_release(S);
@@ -675,9 +784,9 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
             L.bundle_cap = A.bundle_cap;
         }
     }
-    HZB_TRY(S->kw.alloc(n));
+    HZB_TRY(S->kw.alloc(n, s));
     if (S->amg.coarse_solver != SOLVER_UMFPACK)
-        HZB_TRY(S->kwc.alloc(S->lv[S->nl - 1].n));
+        HZB_TRY(S->kwc.alloc(S->lv[S->nl - 1].n, s));
     if (S->bp.precision == HZB_PREC_MIXED) HZB_TRY(ensure_fp32(S));
     HZB_CUDA(cudaEventRecord(S->e1, s));
     HZB_CUDA(cudaEventSynchronize(S->e1));
@@ -1046,6 +1155,17 @@ static int apply_pc32(hzb_solver *S, const double *r, double *z) {
                       [&]() { return apply_pc32_body(S, r, z); });
 }
 
+// the FP32 cycles alone: level 0's b32 is already the residual, the result
+// stays in level 0's x32
+static int cycles32(hzb_solver *S) {
+    Level &L0 = S->lv[0];
+    return with_graph(S, S->g32c, L0.b32, L0.x32, cycle_tag(S, S->amg), [&]() {
+        AMG_param cyc = S->amg;
+        for (int i = 0; i < std::max<int>(1, cyc.maxit); ++i) HZB_TRY(cycle32(S, cyc, i == 0));
+        return SUCCESS;
+    });
+}
+
 // The FP64 preconditioner is replayed from a graph unless a branch of the
 // cycle reads a device value on the host (coarse scaling, coarse CG).
 int precond64(hzb_solver *S, const double *r, double *z, const AMG_param &cyc) {
@@ -1105,10 +1225,16 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
     HZB_TRY(apply_pc32(S, w.r, w.z));
     HZB_TRY(vcopy<double>(m, w.z, w.p, s));
     HZB_TRY(dot(m, w.z, w.r, w.part, w.sc + SC_T1, s));
+    // the update writes the cycle's FP32 residual, and the cycle's FP32 output
+    // feeds the inner products and the new direction directly: z is never
+    // stored in FP64 (the values are the same as through d2f / f2d)
+    Level &L0 = S->lv[0];
     while (iter++ < maxit) {
         HZB_TRY(spmv<double>(A, SPMV_Y_DOT, w.p, nullptr, w.t, 1.0, partd, s));
         HZB_TRY(reduce_final(partd, spmv_blocks_rows(m, A.bundle_rows), w.sc + SC_T2, s));
-        HZB_TRY(pcg_update(m, w.sc + SC_T1, w.sc + SC_T2, x, w.r, w.p, w.t, part4, s));
+        k_fcg_update<<<G, 256, 0, s>>>(m, w.sc + SC_T1, w.sc + SC_T2, x, w.r, w.p, w.t,
+                                        L0.b32, part4);
+        count_launch();
         HZB_TRY(reduce_final(part4, G, w.sc + SC_RR, s));
         HZB_TRY(fetch(S, w));
         absres = sqrt(w.h_sc[SC_RR]);
@@ -1122,13 +1248,14 @@ int fcg_mixed(hzb_solver *S, const double *b, double *x, double tol, int maxit,
             HZB_TRY(fetch(S, w));
             relres = sqrt(w.h_sc[SC_X]) / normr0;
             if (relres < tol) break;
+            HZB_TRY(d2f(m, w.r, L0.b32, s));   // the cycle starts from the true residual
         }
-        HZB_TRY(apply_pc32(S, w.r, w.z));
-        k_dot2_partial<<<G, 256, 0, s>>>(m, w.z, w.t, w.r, part4);
+        HZB_TRY(cycles32(S));
+        k_dot2_partial_f<<<G, 256, 0, s>>>(m, L0.x32, w.t, w.r, part4);
         count_launch();
         HZB_TRY(reduce_final(part4, G, w.sc + SC_ZT, s));
         HZB_TRY(reduce_final(part4 + G, G, w.sc + SC_T3, s));
-        k_fcg_p<<<grid_for(m), 256, 0, s>>>(m, w.sc + SC_ZT, w.sc + SC_T2, w.z, w.p);
+        k_fcg_p_f<<<grid_for(m), 256, 0, s>>>(m, w.sc + SC_ZT, w.sc + SC_T2, L0.x32, w.p);
         k_copy_scalar<<<1, 1, 0, s>>>(w.sc + SC_T3, w.sc + SC_T1);
         count_launch(2);
         HZB_LAUNCH_CHECK();
@@ -1146,6 +1273,7 @@ void destroy(hzb_solver *S) {
     bsr_release(S);
     S->g64.release();
     S->g32.release();
+    S->g32c.release();
     S->gcyc.release();
     gmres_release(S);
     gcg_release(S);

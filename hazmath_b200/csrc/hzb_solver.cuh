@@ -100,7 +100,7 @@ struct KrylovWork {
     double *part = nullptr;   // 4 * reduce_blocks(n) + spmv_blocks(n)
     double *sc = nullptr;     // device scalars
     double *h_sc = nullptr;   // pinned host mirror
-    int alloc(int n);
+    int alloc(int n, cudaStream_t s = nullptr);   // scalars zeroed on s (or the current stream)
     void release();
 };
 
@@ -146,6 +146,7 @@ struct hzb_solver {
     hzb::KrylovWork kw;               // outer Krylov loop
     hzb::KrylovWork kwc;              // coarse-level CG (coarse_solver != 32)
     hzb::GraphCache g64, g32;         // captured FP64 / FP32 preconditioners
+    hzb::GraphCache g32c;             // the FP32 cycles alone (level-0 b32 given)
     hzb::GraphCache gcyc;             // captured AMLI / additive preconditioner
     std::vector<double> amli_coef;    // polynomial of the AMLI cycle (degree + 1)
     // Krylov work kept per level for the coarse-level solves of the
@@ -260,6 +261,8 @@ int batch_setup(hzb_solver *S, int nsys, const int *off, int n, int nnz, const i
 int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit,
                 int *h_iters, double *h_relres, double *h_seconds);
 void batch_release(hzb_solver *S);
+// ERROR_SOLVER_MISC if a device wait of the cycle (a grid barrier) ran out
+int check_waits(hzb_solver *S);
 // terminal levels of the batched systems, called by setup's level loop in
 // batch mode: which systems end on level lvl (their dense inverses; *live =
 // rows of the others), then after the aggregation the removal of their rows
