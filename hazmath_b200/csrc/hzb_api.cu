@@ -1100,7 +1100,7 @@ extern "C" INT hzb_bsr_precond_device(hzb_solver *S, const REAL *d_r, REAL *d_z)
     StreamScope scope_(S->s);
     HZB_TRY(hzb::bsr_precond(S, d_r, d_z));
     HZB_CUDA(cudaStreamSynchronize(S->s));
-    return SUCCESS;
+    return hzb::check_waits(S);
 }
 
 extern "C" INT hzb_bsr_solve_device(hzb_solver *S, const REAL *d_b, REAL *d_x) {

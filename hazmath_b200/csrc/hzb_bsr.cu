@@ -238,8 +238,17 @@ k_bsr_residual(int nrow, const int *__restrict__ ia, const int *__restrict__ ja,
 }
 
 // one block row of Jacobi / Gauss-Seidel: x_I = D_I^{-1} (b_I - sum_{J != I}
-// A_IJ x_J), reading x from xin and writing xout (the same array for GS)
-template <int NB>
+// A_IJ x_J), reading x from xin and writing xout (the same array for GS);
+// CG: x read and written at L2 (other SMs wrote it in the same launch)
+template <bool CG>
+__device__ __forceinline__ double ldx(const double *p) { return CG ? __ldcg(p) : *p; }
+template <bool CG>
+__device__ __forceinline__ void stx(double *p, double v) {
+    if (CG) __stcg(p, v);
+    else *p = v;
+}
+
+template <int NB, bool CG = false>
 __device__ __forceinline__ void bsr_relax_row(int I, const int *__restrict__ ia,
                                               const int *__restrict__ ja,
                                               const double *__restrict__ val,
@@ -249,13 +258,37 @@ __device__ __forceinline__ void bsr_relax_row(int I, const int *__restrict__ ia,
     double t[NB];
 #pragma unroll
     for (int r = 0; r < NB; ++r) t[r] = b[I * NB + r];
-    for (int k = ia[I]; k < ia[I + 1]; ++k) {
+    const int k1 = ia[I + 1];
+    int k = ia[I];
+    // U blocks at a time: their column indices, then their x gathers, are
+    // issued together before the products (same order of subtractions)
+    constexpr int U = NB <= 2 ? 8 : 4;
+    for (; k + U <= k1; k += U) {
+        int J[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) J[u] = ja[k + u];
+        double xj[U][NB];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int c = 0; c < NB; ++c) xj[u][c] = J[u] == I ? 0.0 : ldx<CG>(xin + J[u] * NB + c);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (J[u] == I) continue;
+            const double *a = val + (size_t)(k + u) * (NB * NB);
+#pragma unroll
+            for (int r = 0; r < NB; ++r)
+#pragma unroll
+                for (int c = 0; c < NB; ++c) t[r] -= a[r * NB + c] * xj[u][c];
+        }
+    }
+    for (; k < k1; ++k) {
         const int J = ja[k];
         if (J == I) continue;
         const double *a = val + (size_t)k * (NB * NB);
         double xj[NB];
 #pragma unroll
-        for (int c = 0; c < NB; ++c) xj[c] = xin[J * NB + c];
+        for (int c = 0; c < NB; ++c) xj[c] = ldx<CG>(xin + J * NB + c);
 #pragma unroll
         for (int r = 0; r < NB; ++r)
 #pragma unroll
@@ -267,7 +300,7 @@ __device__ __forceinline__ void bsr_relax_row(int I, const int *__restrict__ ia,
         double v = 0.0;
 #pragma unroll
         for (int c = 0; c < NB; ++c) v += d[r * NB + c] * t[c];
-        xout[I * NB + r] = v;
+        stx<CG>(xout + I * NB + r, v);
     }
 }
 
@@ -303,6 +336,49 @@ k_bsr_gs_run(const int *__restrict__ rows, const int *__restrict__ set_ptr, int 
             bsr_relax_row<NB>(rows[q], ia, ja, val, dinv, b, x, x);
         __syncthreads();
     }
+}
+
+// consecutive large level sets [first, last) in one cooperative launch,
+// the sets separated by the bounded grid barrier
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_bsr_gs_sets_grid(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first,
+                   int last, const int *__restrict__ ia, const int *__restrict__ ja,
+                   const double *__restrict__ val, const double *__restrict__ dinv,
+                   const double *__restrict__ b, double *x, unsigned *bar, int *err) {
+    const int nthr = gridDim.x * blockDim.x;
+    for (int k = first; k < last; ++k) {
+        const int q1 = set_ptr[k + 1];
+        for (int q = set_ptr[k] + blockIdx.x * blockDim.x + threadIdx.x; q < q1; q += nthr)
+            bsr_relax_row<NB, true>(rows[q], ia, ja, val, dinv, b, x, x);
+        if (k + 1 < last && !grid_barrier(bar, gridDim.x, err)) return;
+    }
+}
+
+template <int NB>
+int bsr_gs_sets_grid(const int *rows, const int *set_ptr, int first, int last, int max_set,
+                     const int *ia, const int *ja, const double *val, const double *dinv,
+                     const double *b, double *x, unsigned *bar, int *err, cudaStream_t s) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bsr_gs_sets_grid<NB>, 128,
+                                                          0) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    const int grid = std::max(1, std::min(per_sm * sm_count(), div_up(max_set, 128)));
+    HZB_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HZB_CUDA(cudaLaunchKernelEx(&cfg, k_bsr_gs_sets_grid<NB>, rows, set_ptr, first, last, ia,
+                                ja, val, dinv, b, x, bar, err));
+    return SUCCESS;
 }
 
 // f(std::integral_constant<int, nb>) for the block sizes the kernels hold
@@ -594,11 +670,25 @@ static int bsr_smooth(hzb_solver *S, BsrLevel &L, int kind, int sweeps) {
             continue;
         }
         const Schedule &sc = kind == 1 ? L.asc : L.desc;
-        for (size_t q = 0; q < sc.run_first.size(); ++q) {
+        int *err = wait_err(S);
+        const size_t nr = sc.run_first.size();
+        for (size_t q = 0; q < nr; ++q) {
             const int f = sc.run_first[q], l = sc.run_last[q];
+            // consecutive large sets: one cooperative launch when the
+            // barrier has its words and a place to report to
+            size_t q2 = q;
+            while (l < 0 && q2 < nr && sc.run_last[q2] < 0) ++q2;
+            int rc = SUCCESS;
             with_nb(L.nb, [&](auto c) {
                 constexpr int NB = decltype(c)::value;
-                if (l < 0) {
+                if (l < 0 && sc.bar && err && q2 - q > 1) {
+                    int max_set = 0;
+                    for (size_t r = q; r < q2; ++r) max_set = std::max(max_set, sc.run_max[r]);
+                    rc = bsr_gs_sets_grid<NB>(sc.rows, sc.set_ptr, f, sc.run_first[q2 - 1] + 1,
+                                              max_set, L.ia, L.ja, L.val, L.dinv, E.b, E.x,
+                                              sc.bar, err, s);
+                    q = q2 - 1;
+                } else if (l < 0) {
                     const int cnt = sc.h_ptr[f + 1] - sc.h_ptr[f];
                     k_bsr_gs_set<NB><<<grid_for(cnt, 128), 128, 0, s>>>(
                         sc.rows + sc.h_ptr[f], cnt, L.ia, L.ja, L.val, L.dinv, E.b, E.x);
@@ -607,6 +697,7 @@ static int bsr_smooth(hzb_solver *S, BsrLevel &L, int kind, int sweeps) {
                                                         L.val, L.dinv, E.b, E.x);
                 }
             });
+            HZB_TRY(rc);
             count_launch();
         }
     }

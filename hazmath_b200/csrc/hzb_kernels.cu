@@ -906,16 +906,11 @@ __global__ void k_gs_rows(int cnt, const int *__restrict__ rows,
         gs_row<T>(rows[q], kind, ia, ja, a, d, w, b, x, skip);
 }
 
-// A run of small level sets (at most 1024 rows each, so a thread has at
-// most one row per set) in one CTA.  Everything a row needs except x --
-// its index, column indices, values (up to GS_PRE entries), b_i and d_i --
-// does not depend on the sweep, so the thread loads it for its row of the
-// next set before the barrier that ends the current one; only the x gathers
-// remain between barriers.  The row sum runs in the same order as gs_row's
-// (CSR order from b_i, the diagonal skipped), so the result is the same bit
-// for bit.
-constexpr int GS_PRE = 8;
-template <typename T, int P = GS_PRE>
+// Row data of one thread's row in a level set: its index, bounds, the first
+// P column indices and values, b_i and d_i -- all independent of the sweep,
+// so a kernel loads them for its next set before the barrier that ends the
+// current one.
+template <typename T, int P>
 struct GsRowData {
     int i = -1, k0 = 0, k1 = 0;
     int col[P];
@@ -943,53 +938,121 @@ __device__ __forceinline__ void gs_row_load(GsRowData<T, P> &r, const int *__res
     r.bi = b[r.i];
     r.di = d[r.i];
 }
-template <typename T>
-__device__ __forceinline__ void gs_row_apply(const GsRowData<T> &r, int kind,
-                                             const int *__restrict__ ja,
-                                             const T *__restrict__ a, T w, T *x, int skip) {
-    const int i = r.i;
-    if (i < 0 || i == skip) return;
-    T t = r.bi;
-#pragma unroll
-    for (int u = 0; u < GS_PRE; ++u) {
-        if (r.k0 + u < r.k1) {
-            const int j = r.col[u];
-            if (j != i) t -= r.val[u] * x[j];
+// A run of small level sets (at most NT rows each, so a thread has at most
+// one row per set) in one CTA of NT threads, the sets separated by
+// __syncthreads.  Everything a row needs except x is independent of the
+// sweep and is loaded ahead in a three-deep pipeline: while set s is swept,
+// a thread loads its row index in set s+3, the bounds, b_i and d_i of its
+// row in set s+2 and the first P column indices and values of its row in
+// set s+1, each from values that arrived during the previous set, so the
+// chain set pointer -> row -> row bounds -> entries costs no barrier period
+// of its own.  Only the x gathers remain between barriers.  The run's set
+// pointers sit in shared memory, and so does x when the level fits (XS): the
+// run then reads x once, sweeps in shared memory and writes x back.  The row
+// sum runs in CSR order from b_i with the diagonal skipped, as gs_row's.
+template <typename T, int NT, int P, bool XS>
+__global__ void __launch_bounds__(NT)
+k_gs_pipe(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first, int last,
+          int n, const int *__restrict__ ia, const int *__restrict__ ja,
+          const T *__restrict__ a, const T *__restrict__ d, int kind, T w,
+          const T *__restrict__ b, T *xg, int skip) {
+    extern __shared__ __align__(16) unsigned char gs_smem[];
+    const int ns = last - first;
+    int *sp = reinterpret_cast<int *>(gs_smem);
+    T *xs = reinterpret_cast<T *>(gs_smem + gs_sp_bytes(ns));
+    for (int k = threadIdx.x; k <= ns; k += NT) sp[k] = set_ptr[first + k];
+    if (XS) {
+#pragma unroll 4
+        for (int k = threadIdx.x; k < n; k += NT) xs[k] = xg[k];
+    }
+    __syncthreads();
+    T *x = XS ? xs : xg;
+    const int t = threadIdx.x;
+    auto row_of = [&](int r) -> int {   // this thread's row in set r of the run, or -1
+        if (r >= ns) return -1;
+        const int q = sp[r] + t;
+        return q < sp[r + 1] ? __ldg(rows + q) : -1;
+    };
+    auto bounds = [&](int i, int &k0, int &k1, T &bi, T &di) {
+        k0 = k1 = 0;
+        bi = di = T(0);
+        if (i >= 0) {
+            k0 = __ldg(ia + i);
+            k1 = __ldg(ia + i + 1);
+            bi = __ldg(b + i);
+            di = __ldg(d + i);
         }
-    }
-    for (int k = r.k0 + GS_PRE; k < r.k1; ++k) {
-        const int j = ja[k];
-        if (j != i) t -= a[k] * x[j];
-    }
-    const T di = r.di;
-    if (kind == 0) {
-        x[i] = t * di;
-    } else if (kind == 1) {
-        if (fabs(di) > T(SMALLREAL)) x[i] = w * (t / di) + (1 - w) * x[i];
-    } else {
-        if (fabs(di) > T(SMALLREAL)) x[i] = t / di;
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(1024)
-k_gs_run(const int *__restrict__ rows, const int *__restrict__ set_ptr,
-         int first, int last, const int *__restrict__ ia,
-         const int *__restrict__ ja, const T *__restrict__ a,
-         const T *__restrict__ d, int kind, T w, const T *__restrict__ b, T *x,
-         int skip) {
-    GsRowData<T> cur, nxt;
-    int q0 = set_ptr[first], q1 = set_ptr[first + 1];
-    gs_row_load(cur, rows, q0 + (int)threadIdx.x, q1, ia, ja, a, d, b);
-    for (int sidx = first; sidx < last; ++sidx) {
-        gs_row_apply(cur, kind, ja, a, w, x, skip);
-        if (sidx + 1 < last) {
-            q0 = q1;
-            q1 = set_ptr[sidx + 2];
-            gs_row_load(nxt, rows, q0 + (int)threadIdx.x, q1, ia, ja, a, d, b);
+    };
+    auto entries = [&](int k0, int k1, int *col, T *val) {
+#pragma unroll
+        for (int u = 0; u < P; ++u) {
+            col[u] = 0;
+            val[u] = T(0);
+            if (k0 + u < k1) {
+                col[u] = __ldg(ja + k0 + u);
+                val[u] = __ldg(a + k0 + u);
+            }
+        }
+    };
+    // pipeline registers: suffix 0 = set s, 1 = set s+1, 2 = set s+2
+    int i0 = row_of(0), i1 = row_of(1), i2 = row_of(2);
+    int k00, k10, k01, k11;
+    T b0, d0, b1, d1;
+    bounds(i0, k00, k10, b0, d0);
+    bounds(i1, k01, k11, b1, d1);
+    int c0[P];
+    T v0[P];
+    entries(k00, k10, c0, v0);
+    for (int s = 0; s < ns; ++s) {
+        // loads for the next sets first, so that they overlap the gathers
+        int c1[P];
+        T v1[P];
+        entries(k01, k11, c1, v1);
+        int k02, k12;
+        T b2, d2;
+        bounds(i2, k02, k12, b2, d2);
+        const int i3 = row_of(s + 3);
+        if (i0 >= 0 && i0 != skip) {
+            T xv[P];
+#pragma unroll
+            for (int u = 0; u < P; ++u) xv[u] = k00 + u < k10 ? x[c0[u]] : T(0);
+            T tv = b0;
+#pragma unroll
+            for (int u = 0; u < P; ++u)
+                if (k00 + u < k10 && c0[u] != i0) tv -= v0[u] * xv[u];
+            for (int k = k00 + P; k < k10; ++k) {
+                const int j = __ldg(ja + k);
+                if (j != i0) tv -= __ldg(a + k) * x[j];
+            }
+            if (kind == 0) {
+                x[i0] = tv * d0;
+            } else if (kind == 1) {
+                if (fabs(d0) > T(SMALLREAL)) x[i0] = w * (tv / d0) + (1 - w) * x[i0];
+            } else {
+                if (fabs(d0) > T(SMALLREAL)) x[i0] = tv / d0;
+            }
         }
         __syncthreads();
-        cur = nxt;
+        i0 = i1;
+        i1 = i2;
+        i2 = i3;
+        k00 = k01;
+        k10 = k11;
+        b0 = b1;
+        d0 = d1;
+        k01 = k02;
+        k11 = k12;
+        b1 = b2;
+        d1 = d2;
+#pragma unroll
+        for (int u = 0; u < P; ++u) {
+            c0[u] = c1[u];
+            v0[u] = v1[u];
+        }
+    }
+    if (XS) {
+#pragma unroll 4
+        for (int k = threadIdx.x; k < n; k += NT) xg[k] = xs[k];
     }
 }
 
@@ -1004,63 +1067,51 @@ int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt, const T *d,
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
-template <typename T>
-int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
-           int first, int last, const T *d, T w, const T *b, T *x,
-           cudaStream_t s) {
-    if (last <= first) return SUCCESS;
-    const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
-    k_gs_run<T><<<1, 1024, 0, s>>>(rows, set_ptr, first, last, A.ia, A.ja,
-                                   A.val, d, kind & 15, w, b, x, skip);
+template <typename T, int NT, int P>
+static int gs_pipe_launch(const DCsr<T> &A, int kd, const int *rows, const int *set_ptr,
+                          int first, int last, const T *d, T w, const T *b, T *x, int skip,
+                          cudaStream_t s) {
+    const size_t spb = gs_sp_bytes(last - first);
+    const size_t xsb = sizeof(T) * (size_t)A.n;
+    if (spb + xsb <= GS_SMEM_MAX) {
+        static bool done = false;   // per instantiation: raise the limit once
+        if (!done) {
+            cudaFuncSetAttribute(k_gs_pipe<T, NT, P, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GS_SMEM_MAX);
+            done = true;
+        }
+        k_gs_pipe<T, NT, P, true><<<1, NT, spb + xsb, s>>>(rows, set_ptr, first, last, A.n,
+                                                           A.ia, A.ja, A.val, d, kd, w, b, x,
+                                                           skip);
+    } else {
+        k_gs_pipe<T, NT, P, false><<<1, NT, spb, s>>>(rows, set_ptr, first, last, A.n, A.ia,
+                                                      A.ja, A.val, d, kd, w, b, x, skip);
+    }
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
+
+template <typename T>
+int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
+           int first, int last, int max_set, const T *d, T w, const T *b, T *x,
+           cudaStream_t s) {
+    if (last <= first) return SUCCESS;
+    if (last - first > GS_RUN_SETS || max_set > GS_SMALL_SET) return ERROR_INPUT_PAR;
+    const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
+    const int kd = kind & 15;
+    // 4 entries per row ahead at 1024 threads (64 registers a thread), 16 below
+    if (max_set <= 128)
+        return gs_pipe_launch<T, 128, 16>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+    if (max_set <= 256)
+        return gs_pipe_launch<T, 256, 16>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+    return gs_pipe_launch<T, 1024, 4>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+}
 // ---------------------------------------------------------------------------
 // Consecutive large level sets in one cooperative launch, the sets separated
-// by a grid barrier.  The barrier is an arrival counter and a generation
-// word (bar[0], bar[1]; the last CTA to arrive resets the counter and bumps
-// the generation).  Its wait is bounded: after GRID_SPIN_LIMIT polls
-// (about half a second) the CTA raises *err and returns, and a CTA that sees
-// *err raised stops too, so a missing CTA ends the sweep with an error that
-// the host reads (the Krylov loops read *err with their scalars), never with
-// a hang.  Cooperative launch guarantees the CTAs are co-resident.  x is
-// read and written at L2 (ld/st.global.cg): the CTAs of other SMs wrote it.
+// by grid_barrier (hzb_kernels.cuh).  x is read and written at L2
+// (ld/st.global.cg): the CTAs of other SMs wrote it.
 // ---------------------------------------------------------------------------
-constexpr unsigned GRID_SPIN_LIMIT = 1u << 22;
-
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err) {
-    __shared__ int s_bad;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
-        volatile int *verr = err;
-        const unsigned g = *gen;
-        int bad = 0;
-        __threadfence();
-        if (atomicAdd(bar, 1u) == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            for (unsigned spin = 0; *gen == g; ++spin) {
-                if (*verr) { bad = 1; break; }
-                if (spin > GRID_SPIN_LIMIT) {
-                    atomicExch(err, 1);
-                    bad = 1;
-                    break;
-                }
-                __nanosleep(100);
-            }
-        }
-        __threadfence();
-        if (*verr) bad = 1;
-        s_bad = bad;
-    }
-    __syncthreads();
-    return !s_bad;
-}
-
 // One row per thread per set when the grid covers the largest set (the
 // launch sizes it so): the row data of the next set is loaded before each
 // barrier, as in k_gs_run; rows beyond the grid (a set larger than the
@@ -1171,10 +1222,10 @@ template int gs_rows<float>(const DCsr<float> &, int, const int *, int,
                             const float *, float, const float *, float *,
                             cudaStream_t);
 template int gs_run<double>(const DCsr<double> &, int, const int *, const int *,
-                            int, int, const double *, double, const double *,
+                            int, int, int, const double *, double, const double *,
                             double *, cudaStream_t);
 template int gs_run<float>(const DCsr<float> &, int, const int *, const int *,
-                           int, int, const float *, float, const float *,
+                           int, int, int, const float *, float, const float *,
                            float *, cudaStream_t);
 
 // ---------------------------------------------------------------------------

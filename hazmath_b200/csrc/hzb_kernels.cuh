@@ -84,6 +84,48 @@ constexpr int GS_SKIP_LAST = 16;
 template <typename T>
 int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt,
             const T *d, T w, const T *b, T *x, cudaStream_t s);
+// Grid barrier of the cooperative level-set sweeps: an arrival counter and a
+// generation word (bar[0], bar[1]; the last CTA to arrive resets the counter
+// and bumps the generation).  Its wait is bounded: after GRID_SPIN_LIMIT
+// polls (about half a second) the CTA raises *err and returns false, and a
+// CTA that sees *err raised returns false too, so a missing CTA ends the
+// sweep with an error that the host reads, never with a hang.  Cooperative
+// launch guarantees the CTAs are co-resident.  The host zeroes bar before
+// every launch.
+constexpr unsigned GRID_SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err) {
+    __shared__ int s_bad;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        volatile int *verr = err;
+        const unsigned g = *gen;
+        int bad = 0;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            for (unsigned spin = 0; *gen == g; ++spin) {
+                if (*verr) { bad = 1; break; }
+                if (spin > GRID_SPIN_LIMIT) {
+                    atomicExch(err, 1);
+                    bad = 1;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        if (*verr) bad = 1;
+        s_bad = bad;
+    }
+    __syncthreads();
+    return !s_bad;
+}
+
 // consecutive level sets [first, last) of up to max_set rows each in one
 // cooperative launch with a bounded grid barrier between sets (bar: 2
 // device words, zero at first use; err: raised if a barrier wait ran out)
@@ -92,10 +134,18 @@ int gs_sets_grid(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr
                  int last, int max_set, const T *d, T w, const T *b, T *x, unsigned *bar,
                  int *err, cudaStream_t s);
 // One CTA runs level sets [first, last) back to back, __syncthreads between
-// sets (all sets of the run hold <= 1024 rows).
+// sets: at most GS_RUN_SETS sets of at most GS_SMALL_SET rows each (max_set:
+// the run's largest set), else ERROR_INPUT_PAR.  x lives in shared memory
+// for the run when the level fits GS_SMEM_MAX.
+constexpr int GS_SMALL_SET = 1024;
+constexpr int GS_RUN_SETS = 4096;
+constexpr size_t GS_SMEM_MAX = 220 * 1024;
+__host__ __device__ constexpr size_t gs_sp_bytes(int nsets) {
+    return (sizeof(int) * (size_t)(nsets + 1) + 15) / 16 * 16;
+}
 template <typename T>
 int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
-           int first, int last, const T *d, T w, const T *b, T *x,
+           int first, int last, int max_set, const T *d, T w, const T *b, T *x,
            cudaStream_t s);
 
 // Deterministic reductions: partial sums per block, then an ordered final

@@ -1480,6 +1480,7 @@ void Schedule::release() {
     h_ptr.clear();
     run_first.clear();
     run_last.clear();
+    run_max.clear();
 }
 
 __global__ void k_transpose_count(int n, const int *__restrict__ ia,
@@ -1595,14 +1596,21 @@ static void make_runs(Schedule *sch) {
     int k = 0;
     while (k < ns) {
         int k2 = k;
-        while (k2 < ns && sch->h_ptr[k2 + 1] - sch->h_ptr[k2] <= 1024) ++k2;
+        int mx = 0;
+        while (k2 < ns && k2 - k < GS_RUN_SETS &&
+               sch->h_ptr[k2 + 1] - sch->h_ptr[k2] <= GS_SMALL_SET) {
+            mx = std::max(mx, sch->h_ptr[k2 + 1] - sch->h_ptr[k2]);
+            ++k2;
+        }
         if (k2 > k) {   // run of small sets
             sch->run_first.push_back(k);
             sch->run_last.push_back(k2);
+            sch->run_max.push_back(mx);
             k = k2;
         } else {        // one large set: a grid-wide launch (marked by -1)
             sch->run_first.push_back(k);
             sch->run_last.push_back(-1);
+            sch->run_max.push_back(sch->h_ptr[k + 1] - sch->h_ptr[k]);
             ++k;
         }
     }

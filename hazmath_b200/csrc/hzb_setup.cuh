@@ -84,7 +84,8 @@ struct Schedule {
     int *set_ptr = nullptr;        // device, nsets+1
     std::vector<int> h_ptr;        // host copy of set_ptr
     std::vector<int> run_first;    // runs of small sets for one CTA: [first,last)
-    std::vector<int> run_last;
+    std::vector<int> run_last;     // (-1: one large set)
+    std::vector<int> run_max;      // the run's largest set
     unsigned *bar = nullptr;       // device, 2 words: grid barrier of gs_sets_grid
     void release();
 };

@@ -184,6 +184,10 @@ int check_waits(hzb_solver *S) {
     return SUCCESS;
 }
 
+int *wait_err(hzb_solver *S) {
+    return S->kw.sc ? reinterpret_cast<int *>(S->kw.sc + SC_ERR) : nullptr;
+}
+
 // ||x||^2 into sc[slot] (deterministic)
 static int norm2sq(hzb_solver *S, KrylovWork &w, int n, const double *x, int slot) {
     return dot(n, x, x, w.part, w.sc + slot, S->s);
@@ -203,7 +207,7 @@ static int run_sets(hzb_solver *S, const DCsr<double> &A, const Schedule &sc,
         const char *e = getenv("HZB_GS_GRID");
         return !(e && e[0] == '0');
     }();
-    int *err = grid_ok && S->kw.sc ? reinterpret_cast<int *>(S->kw.sc + SC_ERR) : nullptr;
+    int *err = grid_ok ? wait_err(S) : nullptr;
     if (!reverse) {
         const size_t nr = sc.run_first.size();
         for (size_t q = 0; q < nr; ++q) {
@@ -226,7 +230,8 @@ static int run_sets(hzb_solver *S, const DCsr<double> &A, const Schedule &sc,
                                             sc.h_ptr[f + 1] - sc.h_ptr[f], d, w, b, x, S->s));
                 }
             } else {
-                HZB_TRY(gs_run<double>(A, kind, sc.rows, sc.set_ptr, f, l, d, w, b, x, S->s));
+                HZB_TRY(gs_run<double>(A, kind, sc.rows, sc.set_ptr, f, l, sc.run_max[q], d, w,
+                                       b, x, S->s));
             }
         }
     } else {

@@ -263,6 +263,9 @@ int batch_solve(hzb_solver *S, const double *b, double *x, double tol, int maxit
 void batch_release(hzb_solver *S);
 // ERROR_SOLVER_MISC if a device wait of the cycle (a grid barrier) ran out
 int check_waits(hzb_solver *S);
+// that word as an int for the kernels' bounded waits (null before the
+// handle's Krylov scratch exists: the caller then avoids the waits)
+int *wait_err(hzb_solver *S);
 // terminal levels of the batched systems, called by setup's level loop in
 // batch mode: which systems end on level lvl (their dense inverses; *live =
 // rows of the others), then after the aggregation the removal of their rows
