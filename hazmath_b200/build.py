@@ -24,6 +24,7 @@ ROOT = os.path.dirname(HERE)
 
 SOURCES = [
     ("hzb_kernels.cu", False),
+    ("hzb_sell.cu", False),
     ("hzb_setup.cu", False),
     ("hzb_dense.cu", True),
     ("hzb_solver.cu", False),

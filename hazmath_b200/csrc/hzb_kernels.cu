@@ -501,6 +501,8 @@ static int spmv_mode(const DCsr<T> &A, const T *x, const T *b, T *y, T alpha, T 
                      cudaStream_t s) {
     if (A.n <= 0) return SUCCESS;
     if constexpr (sizeof(T) == 4 && MODE != SPMV_Y_DOT) {
+        if (A.vec_lanes == SELL_LANES && A.sell.npad > 0 && !A.act)
+            return sell_spmv(A, MODE, x, b, y, alpha, s);
         if (A.vec_lanes > 0) return spmv_vec_launch<MODE>(A, x, b, y, alpha, s);
     }
     switch (A.bundle_rows) {
@@ -581,21 +583,27 @@ int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s)
     return SUCCESS;
 }
 
-// FP32 schedule of a level: the staged bundles (vec_lanes 0) or 4/8/16 lanes
-// per row, whichever runs this level's l1-Jacobi sweep fastest.
+bool fp32_schedule_known(int n, int nnz, int *lanes) {
+    return tune_lookup(tune_fp32_lanes, n, nnz, lanes);
+}
+
+// FP32 schedule of a level: the staged bundles (vec_lanes 0), 4/8/16 lanes
+// per row or the sliced-ELL copy (when A.sell holds one), whichever runs
+// this level's l1-Jacobi sweep fastest.
 int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cudaStream_t s) {
     int known = 0;
     if (tune_lookup(tune_fp32_lanes, A.n, A.nnz, &known)) {
         A.vec_lanes = known;
         return SUCCESS;
     }
-    const int cands[4] = {0, 4, 8, 16};
+    const int cands[5] = {0, 4, 8, 16, SELL_LANES};
     cudaEvent_t e0, e1;
     HZB_CUDA(cudaEventCreate(&e0));
     HZB_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     int pick = 0;
     for (int c : cands) {
+        if (c == SELL_LANES && A.sell.npad == 0) continue;
         DCsr<float> B = A;
         B.vec_lanes = c;
         HZB_TRY(l1_sweep<float>(B, b, x, xn, nullptr, s));   // warm
@@ -808,6 +816,8 @@ int l1_sweep(const DCsr<T> &A, const T *b, const T *x, T *xn,
              const float *omega, cudaStream_t s) {
     if (A.n <= 0) return SUCCESS;
     if constexpr (sizeof(T) == 4) {
+        if (A.vec_lanes == SELL_LANES && A.sell.npad > 0 && !A.act)
+            return sell_l1_sweep(A, b, x, xn, omega, s);
         if (A.vec_lanes > 0) return l1_vec_launch(A, b, x, xn, omega, s);
     }
     switch (A.bundle_rows) {
@@ -946,10 +956,21 @@ __device__ __forceinline__ void gs_row_load(GsRowData<T, P> &r, const int *__res
 // row in set s+2 and the first P column indices and values of its row in
 // set s+1, each from values that arrived during the previous set, so the
 // chain set pointer -> row -> row bounds -> entries costs no barrier period
-// of its own.  Only the x gathers remain between barriers.  The run's set
-// pointers sit in shared memory, and so does x when the level fits (XS): the
-// run then reads x once, sweeps in shared memory and writes x back.  The row
-// sum runs in CSR order from b_i with the diagonal skipped, as gs_row's.
+// of its own.  The four sets in flight live in four register stages whose
+// roles rotate through an unrolled loop: a stage is never copied, so no
+// instruction waits on a load issued for a later set.  Only the x gathers
+// remain between barriers.  The run's set pointers sit in shared memory, and
+// so does x when the level fits (XS): the run then reads x once, sweeps in
+// shared memory and writes x back.  The row sum runs in CSR order from b_i
+// with the diagonal skipped, as gs_row's.
+template <typename T, int P>
+struct GsStage {
+    int i, k0, k1;
+    T bi, di;
+    int c[P];
+    T v[P];
+};
+
 template <typename T, int NT, int P, bool XS>
 __global__ void __launch_bounds__(NT)
 k_gs_pipe(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first, int last,
@@ -968,87 +989,81 @@ k_gs_pipe(const int *__restrict__ rows, const int *__restrict__ set_ptr, int fir
     __syncthreads();
     T *x = XS ? xs : xg;
     const int t = threadIdx.x;
-    auto row_of = [&](int r) -> int {   // this thread's row in set r of the run, or -1
-        if (r >= ns) return -1;
-        const int q = sp[r] + t;
-        return q < sp[r + 1] ? __ldg(rows + q) : -1;
-    };
-    auto bounds = [&](int i, int &k0, int &k1, T &bi, T &di) {
-        k0 = k1 = 0;
-        bi = di = T(0);
-        if (i >= 0) {
-            k0 = __ldg(ia + i);
-            k1 = __ldg(ia + i + 1);
-            bi = __ldg(b + i);
-            di = __ldg(d + i);
+    using St = GsStage<T, P>;
+    auto row_of = [&](St &S, int r) {   // this thread's row in set r of the run, or -1
+        S.i = -1;
+        if (r < ns) {
+            const int q = sp[r] + t;
+            if (q < sp[r + 1]) S.i = __ldg(rows + q);
         }
     };
-    auto entries = [&](int k0, int k1, int *col, T *val) {
+    auto bounds = [&](St &S) {
+        S.k0 = S.k1 = 0;
+        S.bi = S.di = T(0);
+        if (S.i >= 0) {
+            S.k0 = __ldg(ia + S.i);
+            S.k1 = __ldg(ia + S.i + 1);
+            S.bi = __ldg(b + S.i);
+            S.di = __ldg(d + S.i);
+        }
+    };
+    auto entries = [&](St &S) {
 #pragma unroll
         for (int u = 0; u < P; ++u) {
-            col[u] = 0;
-            val[u] = T(0);
-            if (k0 + u < k1) {
-                col[u] = __ldg(ja + k0 + u);
-                val[u] = __ldg(a + k0 + u);
+            S.c[u] = 0;
+            S.v[u] = T(0);
+            if (S.k0 + u < S.k1) {
+                S.c[u] = __ldg(ja + S.k0 + u);
+                S.v[u] = __ldg(a + S.k0 + u);
             }
         }
     };
-    // pipeline registers: suffix 0 = set s, 1 = set s+1, 2 = set s+2
-    int i0 = row_of(0), i1 = row_of(1), i2 = row_of(2);
-    int k00, k10, k01, k11;
-    T b0, d0, b1, d1;
-    bounds(i0, k00, k10, b0, d0);
-    bounds(i1, k01, k11, b1, d1);
-    int c0[P];
-    T v0[P];
-    entries(k00, k10, c0, v0);
-    for (int s = 0; s < ns; ++s) {
-        // loads for the next sets first, so that they overlap the gathers
-        int c1[P];
-        T v1[P];
-        entries(k01, k11, c1, v1);
-        int k02, k12;
-        T b2, d2;
-        bounds(i2, k02, k12, b2, d2);
-        const int i3 = row_of(s + 3);
-        if (i0 >= 0 && i0 != skip) {
-            T xv[P];
+    auto apply = [&](const St &S) {
+        const int i = S.i;
+        if (i < 0 || i == skip) return;
+        T xv[P];
 #pragma unroll
-            for (int u = 0; u < P; ++u) xv[u] = k00 + u < k10 ? x[c0[u]] : T(0);
-            T tv = b0;
+        for (int u = 0; u < P; ++u) xv[u] = S.k0 + u < S.k1 ? x[S.c[u]] : T(0);
+        T tv = S.bi;
 #pragma unroll
-            for (int u = 0; u < P; ++u)
-                if (k00 + u < k10 && c0[u] != i0) tv -= v0[u] * xv[u];
-            for (int k = k00 + P; k < k10; ++k) {
-                const int j = __ldg(ja + k);
-                if (j != i0) tv -= __ldg(a + k) * x[j];
-            }
-            if (kind == 0) {
-                x[i0] = tv * d0;
-            } else if (kind == 1) {
-                if (fabs(d0) > T(SMALLREAL)) x[i0] = w * (tv / d0) + (1 - w) * x[i0];
-            } else {
-                if (fabs(d0) > T(SMALLREAL)) x[i0] = tv / d0;
-            }
+        for (int u = 0; u < P; ++u)
+            if (S.k0 + u < S.k1 && S.c[u] != i) tv -= S.v[u] * xv[u];
+        for (int k = S.k0 + P; k < S.k1; ++k) {
+            const int j = __ldg(ja + k);
+            if (j != i) tv -= __ldg(a + k) * x[j];
         }
+        const T di = S.di;
+        if (kind == 0) {
+            x[i] = tv * di;
+        } else if (kind == 1) {
+            if (fabs(di) > T(SMALLREAL)) x[i] = w * (tv / di) + (1 - w) * x[i];
+        } else {
+            if (fabs(di) > T(SMALLREAL)) x[i] = tv / di;
+        }
+    };
+    // set s+3 (row), s+2 (bounds), s+1 (entries) loaded; set s swept
+    auto step = [&](int s, St &A3, St &B2, St &C1, const St &D0) {
+        entries(C1);
+        bounds(B2);
+        row_of(A3, s + 3);
+        apply(D0);
         __syncthreads();
-        i0 = i1;
-        i1 = i2;
-        i2 = i3;
-        k00 = k01;
-        k10 = k11;
-        b0 = b1;
-        d0 = d1;
-        k01 = k02;
-        k11 = k12;
-        b1 = b2;
-        d1 = d2;
-#pragma unroll
-        for (int u = 0; u < P; ++u) {
-            c0[u] = c1[u];
-            v0[u] = v1[u];
-        }
+    };
+    St S0, S1, S2, S3;
+    row_of(S0, 0);
+    row_of(S1, 1);
+    row_of(S2, 2);
+    bounds(S0);
+    bounds(S1);
+    entries(S0);
+    for (int s = 0; s < ns; s += 4) {
+        step(s, S3, S2, S1, S0);
+        if (s + 1 >= ns) break;
+        step(s + 1, S0, S3, S2, S1);
+        if (s + 2 >= ns) break;
+        step(s + 2, S1, S0, S3, S2);
+        if (s + 3 >= ns) break;
+        step(s + 3, S2, S1, S0, S3);
     }
     if (XS) {
 #pragma unroll 4
@@ -1100,12 +1115,17 @@ int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
     if (last - first > GS_RUN_SETS || max_set > GS_SMALL_SET) return ERROR_INPUT_PAR;
     const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
     const int kd = kind & 15;
-    // 4 entries per row ahead at 1024 threads (64 registers a thread), 16 below
+    // entries per row held ahead in each of the four register stages: 8 up
+    // to 512 threads, fewer at 1024 (64 registers a thread)
+    constexpr int P1024 = sizeof(T) == 8 ? 2 : 4;
     if (max_set <= 128)
-        return gs_pipe_launch<T, 128, 16>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+        return gs_pipe_launch<T, 128, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
     if (max_set <= 256)
-        return gs_pipe_launch<T, 256, 16>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
-    return gs_pipe_launch<T, 1024, 4>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+        return gs_pipe_launch<T, 256, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+    if (max_set <= 512)
+        return gs_pipe_launch<T, 512, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+    return gs_pipe_launch<T, 1024, P1024>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip,
+                                          s);
 }
 // ---------------------------------------------------------------------------
 // Consecutive large level sets in one cooperative launch, the sets separated

@@ -9,6 +9,26 @@
 
 namespace hzb {
 
+// FP32 sliced-ELL copy of a level's matrix (hzb_sell.cu): slot r of a
+// 256-row window holds row row[r] (-1: none) of len[r] entries, stored at
+// col/val[ptr[r / 32] + 32 u + r % 32]; npad = 0: none.
+struct SellView {
+    int npad = 0;
+    const int *ptr = nullptr, *row = nullptr, *len = nullptr, *col = nullptr;
+    const float *val = nullptr;
+};
+struct SellArrays {
+    int npad = 0;
+    int *ptr = nullptr, *row = nullptr, *len = nullptr, *col = nullptr;
+    float *val = nullptr;
+    SellView view() const {
+        SellView v;
+        v.npad = npad; v.ptr = ptr; v.row = row; v.len = len; v.col = col; v.val = val;
+        return v;
+    }
+    void release();
+};
+
 // A CSR matrix resident in device memory (int32 pattern).
 template <typename T>
 struct DCsr {
@@ -18,14 +38,17 @@ struct DCsr {
     int bundle_cap = 0;   // max entries in any bundle of bundle_rows rows (0: none)
     int bundle_rows = 128;   // rows per CTA of the staged kernels: 64, 128 or 256
     // FP32 only: lanes per row of the vector-CSR kernels (2..16), 0 for the
-    // staged bundles.  A row's partial sums are combined across its lanes,
-    // so this is not the sequential CSR-order sum of the FP64 kernels.
+    // staged bundles, SELL_LANES for the sliced-ELL copy in `sell`.  A row's
+    // partial sums are combined across its lanes, so the lanes kernels do
+    // not give the sequential CSR-order sum of the FP64 kernels.
     int vec_lanes = 0;
+    SellView sell;
     // Optional activity of 256-row blocks (ACT_ROWS): kernels skip the rows
     // of a block whose byte is 0 (batched solves skip converged systems).
     const unsigned char *act = nullptr;
 };
 constexpr int ACT_ROWS = 256;
+constexpr int SELL_LANES = -1;
 
 constexpr int SPMV_ROWS = 128;          // rows per CTA in the row-bundle SpMV
 constexpr int SPMV_SMEM_MAX = 160 * 1024;
@@ -40,6 +63,19 @@ int autotune_bundle(DCsr<double> &A, const double *x, double *y, cudaStream_t s)
 // Picks the FP32 schedule (staged bundles or 4/8/16 lanes per row) by timing
 // the l1-Jacobi sweep of A on b, x -> xn.
 int autotune_fp32(DCsr<float> &A, const float *b, const float *x, float *xn, cudaStream_t s);
+// the FP32 schedule an earlier autotune_fp32 picked for a level of this
+// shape, if any
+bool fp32_schedule_known(int n, int nnz, int *lanes);
+
+// Sliced-ELL copy of an FP32 CSR matrix (hzb_sell.cu); *out stays empty
+// (npad 0) when its slice offsets would overflow int.  Sweep and SpMV on it
+// (no activity array, no SPMV_Y_DOT).
+int sell_build(int n, const int *ia, const int *ja, const float *a, SellArrays *out,
+               cudaStream_t s);
+int sell_l1_sweep(const DCsr<float> &A, const float *b, const float *x, float *xn,
+                  const float *omega, cudaStream_t s);
+int sell_spmv(const DCsr<float> &A, int mode, const float *x, const float *b, float *y,
+              float alpha, cudaStream_t s);
 int spmv_blocks_rows(int n, int rows);
 
 // y = A x (SPMV_Y); y = b - A x (SPMV_RES); y += alpha A x with the

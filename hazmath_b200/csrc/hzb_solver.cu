@@ -111,6 +111,7 @@ void Level::release() {
     ia = ja = nullptr; val = nullptr;
     dfree(val32);
     dfree(val64nz);
+    sell32.release();
     if (own32) { dfree(ia32); dfree(ja32); }
     ia32 = ja32 = nullptr;
     own32 = false;
@@ -558,18 +559,30 @@ int ensure_fp32(hzb_solver *S) {
         if (!L.l1_32) {
             HZB_TRY(dalloc(&L.l1_32, L.n));
             HZB_TRY(l1_norms<float>(L.A32(), L.l1_32, S->s));
-            // staged bundles or lanes per row, by timing; HZB_FP32_LANES
-            // (0, 2, 4, 8 or 16) names one for every level instead
+            // staged bundles, lanes per row or the sliced-ELL copy, by
+            // timing; HZB_FP32_LANES (0, 2, 4, 8, 16 or "sell") names one for
+            // every level instead.  Batched solves run the kernels with an
+            // activity array, which the sliced-ELL kernels do not take.
             const char *force = getenv("HZB_FP32_LANES");
-            const int fl = force ? atoi(force) : -1;
-            if (fl == 0 || fl == 2 || fl == 4 || fl == 8 || fl == 16) {
+            const bool force_sell = force && strcmp(force, "sell") == 0;
+            const int fl = force && !force_sell ? atoi(force) : -1;
+            const bool sell_ok = !S->batch && L.n >= 4096;
+            if (force_sell && sell_ok) {
+                HZB_TRY(sell_build(L.n, L.ia32, L.ja32, L.val32, &L.sell32, S->s));
+                L.vec32 = SELL_LANES;
+            } else if (fl == 0 || fl == 2 || fl == 4 || fl == 8 || fl == 16) {
                 L.vec32 = fl;
             } else if (L.n >= 4096) {
+                int known = 0;
+                const bool have = fp32_schedule_known(L.n, L.nnz32, &known);
+                if (sell_ok && (!have || known == SELL_LANES))
+                    HZB_TRY(sell_build(L.n, L.ia32, L.ja32, L.val32, &L.sell32, S->s));
                 HZB_TRY(vzero<float>(L.n, L.b32, S->s));
                 HZB_TRY(vzero<float>(L.n, L.x32, S->s));
                 DCsr<float> A = L.A32();
                 HZB_TRY(autotune_fp32(A, L.b32, L.x32, L.w32, S->s));
                 L.vec32 = A.vec_lanes;
+                if (L.vec32 != SELL_LANES) L.sell32.release();
             }
         }
         if (S->amg.smoother == SMOOTHER_GS && l < S->nl - 1 && !L.d_gs32) {

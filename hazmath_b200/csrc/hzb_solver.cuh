@@ -17,13 +17,15 @@ struct Level {
     // FP32 copy for the mixed cycle without the stored exact zeros (a zero
     // entry adds nothing to a row sum); aliases ia/ja when there are none
     int nnz32 = 0, bundle_cap32 = 0;
-    int vec32 = 0;                    // FP32 schedule: lanes per row, 0 = bundles
+    int vec32 = 0;                    // FP32 schedule: lanes per row, 0 = bundles,
+                                      // SELL_LANES = the sliced-ELL copy
     // activity of 256-row blocks while a batched solve runs (else null):
     // the level kernels skip blocks of converged systems
     const unsigned char *act = nullptr;
     int *ia32 = nullptr, *ja32 = nullptr;
     float *val32 = nullptr;
     bool own32 = false;
+    SellArrays sell32;                // sliced-ELL copy, when vec32 = SELL_LANES
     // level 0 of the mixed solve with stored exact zeros: the FP64 values of
     // the FP32 copy's pattern, for the outer Krylov loop's SpMV (a zero adds
     // nothing to a row sum, so its result is the full matrix's)
@@ -87,6 +89,7 @@ struct Level {
         m.bundle_cap = bundle_cap32;
         m.bundle_rows = bundle_rows;
         m.vec_lanes = vec32;
+        m.sell = sell32.view();
         m.act = act;
         return m;
     }
