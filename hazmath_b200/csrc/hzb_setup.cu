@@ -762,11 +762,17 @@ int hem_exact(int n, const int *nia, const int *nja, const double *nval,
 
 // ---------------------------------------------------------------------------
 // deterministic parallel matching (fast mode)
-//   rounds: every free vertex points at its preferred free neighbour (the
-//   reference's preference: heaviest |a_ij|, later row position on ties);
-//   mutual pairs match, numbered by the lower vertex through a scan.
+//   PM_LEAD rounds of mutual choice: every free vertex points at its heaviest
+//   free neighbour and mutual pairs match -- the edges that dominate both
+//   their ends, which the reference's greedy walk takes too; then red/blue
+//   handshake rounds until no pair forms.  Pairs are numbered through a scan.
 //   Leftovers join the adjacent aggregate with the fewest members counted
-//   before the leftover pass (first such neighbour on ties).
+//   before the leftover pass (first such neighbour on ties).  Mutual choice
+//   alone stalls on chains of ever heavier edges (smooth coefficient fields);
+//   the handshake alone pairs a vertex only with a neighbour of the other
+//   colour, which on the 128^3 log-normal problem (sigma 1) left coarser
+//   levels and 43 instead of the reference's 38 iterations; a few mutual
+//   rounds first gave 39.
 // ---------------------------------------------------------------------------
 __global__ void k_pm_init(int n, const int *__restrict__ ia, int *state) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
@@ -802,18 +808,23 @@ __device__ __forceinline__ bool pm_better(float w, unsigned h, int j, float bw,
     return best < 0 || w > bw || (w == bw && (h > bh || (h == bh && j > best)));
 }
 
+constexpr int PM_LEAD = 4;
+
+// red k proposes to its heaviest free blue neighbour; in a mutual round
+// (round < PM_LEAD) every free k points at its heaviest free neighbour
 __global__ void k_pm_propose(int n, int round, const int *__restrict__ ia,
                              const int *__restrict__ ja, const double *__restrict__ a,
                              const int *__restrict__ state, int *ptr) {
+    const bool mutual = round < PM_LEAD;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += gridDim.x * blockDim.x) {
         int best = -1;
-        if (state[k] == -1 && pm_red(k, round)) {
+        if (state[k] == -1 && (mutual || pm_red(k, round))) {
             float bw = -1.0f;
             unsigned bh = 0u;
             for (int p = ia[k]; p < ia[k + 1]; ++p) {
                 const int j = ja[p];
-                if (j == k || state[j] != -1 || pm_red(j, round)) continue;
+                if (j == k || state[j] != -1 || (!mutual && pm_red(j, round))) continue;
                 const float w = (float)fabs(a[p]);
                 const unsigned h = edge_hash(k, j);
                 if (pm_better(w, h, j, bw, bh, best)) { best = j; bw = w; bh = h; }
@@ -846,6 +857,22 @@ __global__ void k_pm_accept(int n, int round, const int *__restrict__ ia,
         acc[j] = best;
         flag[j] = best >= 0;
         if (best >= 0) *any = 1;
+    }
+}
+
+// mutual round: j pairs with i = ptr[j] when ptr[i] = j, numbered by the
+// higher end
+__global__ void k_pm_mutual(int n, const int *__restrict__ state, const int *__restrict__ ptr,
+                            int *acc, int *flag, int *any) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        int i = -1;
+        if (state[j] == -1) {
+            const int p = ptr[j];
+            if (p >= 0 && p < j && ptr[p] == j) i = p;
+        }
+        acc[j] = i;
+        flag[j] = i >= 0;
+        if (i >= 0) *any = 1;
     }
 }
 
@@ -937,10 +964,14 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
     cudaMemsetAsync(dflag + 1, 0, sizeof(int), s);   // the aggregate count
     int nc = 0;
     int *acc = size;   // free during the rounds
-    for (int round = 0, idle = 0; round < 96 && idle < 4; ++round) {
+    for (int round = 0, idle = 0; round < 96 + PM_LEAD && idle < 4; ++round) {
         cudaMemsetAsync(dflag, 0, sizeof(int), s);
         k_pm_propose<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr);
-        k_pm_accept<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr, acc, flag, dflag);
+        if (round < PM_LEAD)
+            k_pm_mutual<<<g, 256, 0, s>>>(n, state, ptr, acc, flag, dflag);
+        else
+            k_pm_accept<<<g, 256, 0, s>>>(n, round, nia, nja, nval, state, ptr, acc, flag,
+                                          dflag);
         count_launch(2);
         int rc = scan_exclusive(flag, pos, n, tmp, s);
         if (rc) { dfree(dflag); return rc; }
@@ -952,8 +983,8 @@ int hem_parallel(int n, const int *nia, const int *nja, const double *nval,
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { dfree(dflag); set_error(e, __FILE__, __LINE__); return ERROR_SOLVER_MISC; }
         nc = h[1];
-        // stop after a few rounds in a row without a new pair
-        idle = h[0] ? 0 : idle + 1;
+        // stop after a few handshake rounds in a row without a new pair
+        idle = h[0] || round < PM_LEAD ? 0 : idle + 1;
     }
     cudaMemsetAsync(size, 0, sizeof(int) * (nc > 0 ? nc : 1), s);
     k_pm_sizes<<<g, 256, 0, s>>>(n, state, size);
