@@ -662,6 +662,7 @@ def run_single(args, rank, world, local, dist):
             print(json.dumps({"metric": METRIC, "value": step_s, "unit": "s",
                               "steps_only": True, "iterations": int(iters),
                               "setup_s": statistics.mean(setup_s),
+                              "setup_s_steps": [round(v, 4) for v in setup_s],
                               "solve_s": statistics.mean(solve_s),
                               "final_relres": relres, "config": desc}))
         S.close()
@@ -767,6 +768,7 @@ def run_single(args, rank, world, local, dist):
                            parallelism="replicas", l2="inputs larger than L2 (no flush)"),
             "iterations": int(iters), "final_relres": relres,
             "setup_s": statistics.mean(setup_s),
+            "setup_s_steps": [round(v, 4) for v in setup_s],
             "solve_s": solve_ml, "dof_per_s": n / solve_ml,
             "mixed_learned": learned,
             "learned_c4": c4,
