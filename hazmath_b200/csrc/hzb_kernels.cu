@@ -5,8 +5,10 @@
 // one thread; coalescing comes from staging each row bundle's entries in
 // shared memory (the CSR-stream schedule), not from splitting rows.
 #include "hzb_kernels.cuh"
+#include <cooperative_groups.h>
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -1071,6 +1073,154 @@ k_gs_pipe(const int *__restrict__ rows, const int *__restrict__ set_ptr, int fir
     }
 }
 
+// The same sweep for runs of sets of at most 256 rows per CTA with the
+// pipeline twice as deep: a thread loads its row index in set s+6, the
+// bounds of its row in set s+4 and the entries of its row in set s+2, so
+// every load has two barrier periods to arrive before anything uses it.
+// Seven register stages rotate through a seven-fold unrolled loop.  Where x
+// lives (XM):
+//   GS_X_GLOBAL  global memory (one CTA);
+//   GS_X_SMEM    the CTA's shared memory, read once and written back;
+//   GS_X_CLUSTER the distributed shared memory of a cluster of CL CTAs: CTA
+//                r holds rows [r << cshift, (r + 1) << cshift), the set's
+//                rows are dealt over the cluster's threads, and the sets are
+//                separated by cluster barriers (whose release / acquire order
+//                makes a set's writes visible to every CTA).  Levels whose x
+//                does not fit one CTA's shared memory keep their gathers on
+//                chip this way: a global-memory x misses L1 after every write.
+constexpr int GS_X_GLOBAL = 0, GS_X_SMEM = 1, GS_X_CLUSTER = 2;
+template <typename T, int NT, int P, int XM>
+__global__ void __launch_bounds__(NT)
+k_gs_deep(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first, int last,
+          int n, const int *__restrict__ ia, const int *__restrict__ ja,
+          const T *__restrict__ a, const T *__restrict__ d, int kind, T w,
+          const T *__restrict__ b, T *xg, int skip, int cshift) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char gs_smem[];
+    const int ns = last - first;
+    int *sp = reinterpret_cast<int *>(gs_smem);
+    T *xs = reinterpret_cast<T *>(gs_smem + gs_sp_bytes(ns));
+    const int crank = XM == GS_X_CLUSTER ? (int)cg::this_cluster().block_rank() : 0;
+    const int csize = XM == GS_X_CLUSTER ? (int)cg::this_cluster().num_blocks() : 1;
+    const int cmask = (1 << cshift) - 1;
+    for (int k = threadIdx.x; k <= ns; k += NT) sp[k] = set_ptr[first + k];
+    if (XM == GS_X_SMEM) {
+#pragma unroll 4
+        for (int k = threadIdx.x; k < n; k += NT) xs[k] = xg[k];
+    } else if (XM == GS_X_CLUSTER) {
+        const int r0 = crank << cshift, r1 = min(n, r0 + (1 << cshift));
+#pragma unroll 4
+        for (int k = r0 + (int)threadIdx.x; k < r1; k += NT) xs[k - r0] = xg[k];
+    }
+    if (XM == GS_X_CLUSTER) cg::this_cluster().sync();
+    else __syncthreads();
+    auto xat = [&](int j) -> T * {
+        if (XM == GS_X_GLOBAL) return xg + j;
+        if (XM == GS_X_SMEM) return xs + j;
+        return cg::this_cluster().map_shared_rank(xs + (j & cmask), j >> cshift);
+    };
+    const int t = (int)threadIdx.x + crank * NT;   // this thread's slot in a set
+    using St = GsStage<T, P>;
+    auto row_of = [&](St &S, int r) {
+        S.i = -1;
+        if (r < ns) {
+            const int q = sp[r] + t;
+            if (q < sp[r + 1]) S.i = __ldg(rows + q);
+        }
+    };
+    auto bounds = [&](St &S) {
+        S.k0 = S.k1 = 0;
+        S.bi = S.di = T(0);
+        if (S.i >= 0) {
+            S.k0 = __ldg(ia + S.i);
+            S.k1 = __ldg(ia + S.i + 1);
+            S.bi = __ldg(b + S.i);
+            S.di = __ldg(d + S.i);
+        }
+    };
+    auto entries = [&](St &S) {
+#pragma unroll
+        for (int u = 0; u < P; ++u) {
+            S.c[u] = 0;
+            S.v[u] = T(0);
+            if (S.k0 + u < S.k1) {
+                S.c[u] = __ldg(ja + S.k0 + u);
+                S.v[u] = __ldg(a + S.k0 + u);
+            }
+        }
+    };
+    auto apply = [&](const St &S) {
+        const int i = S.i;
+        if (i < 0 || i == skip) return;
+        T xv[P];
+#pragma unroll
+        for (int u = 0; u < P; ++u) xv[u] = S.k0 + u < S.k1 ? *xat(S.c[u]) : T(0);
+        T tv = S.bi;
+#pragma unroll
+        for (int u = 0; u < P; ++u)
+            if (S.k0 + u < S.k1 && S.c[u] != i) tv -= S.v[u] * xv[u];
+        for (int k = S.k0 + P; k < S.k1; ++k) {
+            const int j = __ldg(ja + k);
+            if (j != i) tv -= __ldg(a + k) * *xat(j);
+        }
+        const T di = S.di;
+        T *xi = xat(i);
+        if (kind == 0) {
+            *xi = tv * di;
+        } else if (kind == 1) {
+            if (fabs(di) > T(SMALLREAL)) *xi = w * (tv / di) + (1 - w) * *xi;
+        } else {
+            if (fabs(di) > T(SMALLREAL)) *xi = tv / di;
+        }
+    };
+    auto step = [&](int s, St &R6, St &B4, St &E2, const St &D0) {
+        entries(E2);
+        bounds(B4);
+        row_of(R6, s + 6);
+        apply(D0);
+        if (XM == GS_X_CLUSTER) cg::this_cluster().sync();
+        else __syncthreads();
+    };
+    St S0, S1, S2, S3, S4, S5, S6;
+    row_of(S0, 0);
+    row_of(S1, 1);
+    row_of(S2, 2);
+    row_of(S3, 3);
+    row_of(S4, 4);
+    row_of(S5, 5);
+    bounds(S0);
+    bounds(S1);
+    bounds(S2);
+    bounds(S3);
+    entries(S0);
+    entries(S1);
+    for (int s = 0; s < ns; s += 7) {
+        step(s, S6, S4, S2, S0);
+        if (s + 1 >= ns) break;
+        step(s + 1, S0, S5, S3, S1);
+        if (s + 2 >= ns) break;
+        step(s + 2, S1, S6, S4, S2);
+        if (s + 3 >= ns) break;
+        step(s + 3, S2, S0, S5, S3);
+        if (s + 4 >= ns) break;
+        step(s + 4, S3, S1, S6, S4);
+        if (s + 5 >= ns) break;
+        step(s + 5, S4, S2, S0, S5);
+        if (s + 6 >= ns) break;
+        step(s + 6, S5, S3, S1, S6);
+    }
+    // every step ended with a barrier, so no CTA reads another's x any more
+    if (XM == GS_X_SMEM) {
+#pragma unroll 4
+        for (int k = threadIdx.x; k < n; k += NT) xg[k] = xs[k];
+    } else if (XM == GS_X_CLUSTER) {
+        const int r0 = crank << cshift, r1 = min(n, r0 + (1 << cshift));
+#pragma unroll 4
+        for (int k = r0 + (int)threadIdx.x; k < r1; k += NT) xg[k] = xs[k - r0];
+    }
+    (void)csize;
+}
+
 template <typename T>
 int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt, const T *d,
             T w, const T *b, T *x, cudaStream_t s) {
@@ -1082,6 +1232,18 @@ int gs_rows(const DCsr<T> &A, int kind, const int *rows, int cnt, const T *d,
     HZB_LAUNCH_CHECK();
     return SUCCESS;
 }
+// raise a kernel's dynamic shared memory limit once per process
+template <typename K>
+static void gs_smem_limit(K kernel, bool &done) {
+    if (!done) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)GS_SMEM_MAX);
+        done = true;
+    }
+}
+
+// the four-stage run kernel (any thread count): x in shared memory when the
+// level fits, else in global memory
 template <typename T, int NT, int P>
 static int gs_pipe_launch(const DCsr<T> &A, int kd, const int *rows, const int *set_ptr,
                           int first, int last, const T *d, T w, const T *b, T *x, int skip,
@@ -1089,12 +1251,8 @@ static int gs_pipe_launch(const DCsr<T> &A, int kd, const int *rows, const int *
     const size_t spb = gs_sp_bytes(last - first);
     const size_t xsb = sizeof(T) * (size_t)A.n;
     if (spb + xsb <= GS_SMEM_MAX) {
-        static bool done = false;   // per instantiation: raise the limit once
-        if (!done) {
-            cudaFuncSetAttribute(k_gs_pipe<T, NT, P, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GS_SMEM_MAX);
-            done = true;
-        }
+        static bool done = false;
+        gs_smem_limit(k_gs_pipe<T, NT, P, true>, done);
         k_gs_pipe<T, NT, P, true><<<1, NT, spb + xsb, s>>>(rows, set_ptr, first, last, A.n,
                                                            A.ia, A.ja, A.val, d, kd, w, b, x,
                                                            skip);
@@ -1102,6 +1260,62 @@ static int gs_pipe_launch(const DCsr<T> &A, int kd, const int *rows, const int *
         k_gs_pipe<T, NT, P, false><<<1, NT, spb, s>>>(rows, set_ptr, first, last, A.n, A.ia,
                                                       A.ja, A.val, d, kd, w, b, x, skip);
     }
+    count_launch();
+    HZB_LAUNCH_CHECK();
+    return SUCCESS;
+}
+
+// the deep run kernel (at most 256 threads a CTA): x in shared memory when
+// the level fits one CTA, else (FP64) in the distributed shared memory of a
+// cluster of up to 8 CTAs when it fits that, else in global memory
+template <typename T, int NT, int P>
+static int gs_deep_launch(const DCsr<T> &A, int kd, const int *rows, const int *set_ptr,
+                          int first, int last, const T *d, T w, const T *b, T *x, int skip,
+                          cudaStream_t s) {
+    const size_t spb = gs_sp_bytes(last - first);
+    const size_t xsb = sizeof(T) * (size_t)A.n;
+    if (spb + xsb <= GS_SMEM_MAX) {
+        static bool done = false;
+        gs_smem_limit(k_gs_deep<T, NT, P, GS_X_SMEM>, done);
+        k_gs_deep<T, NT, P, GS_X_SMEM><<<1, NT, spb + xsb, s>>>(
+            rows, set_ptr, first, last, A.n, A.ia, A.ja, A.val, d, kd, w, b, x, skip, 0);
+        count_launch();
+        HZB_LAUNCH_CHECK();
+        return SUCCESS;
+    }
+    // rows per cluster CTA: the largest power of two whose x fits beside the
+    // set pointers; the smallest cluster (2, 4 or 8 CTAs) that holds the level
+    static const bool cluster_ok = [] {
+        const char *e = getenv("HZB_GS_CLUSTER");
+        return !(e && e[0] == '0');
+    }();
+    int cshift = 0;
+    while (cshift < 24 && (sizeof(T) << (cshift + 1)) + spb <= GS_SMEM_MAX) ++cshift;
+    int cl = 2;
+    while (cl < 8 && ((long long)cl << cshift) < A.n) cl *= 2;
+    if (sizeof(T) == 8 && cluster_ok && ((long long)cl << cshift) >= A.n) {
+        static bool done = false;
+        gs_smem_limit(k_gs_deep<T, NT, P, GS_X_CLUSTER>, done);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cl);
+        cfg.blockDim = dim3(NT);
+        cfg.dynamicSmemBytes = spb + (sizeof(T) << cshift);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        HZB_CUDA(cudaLaunchKernelEx(&cfg, k_gs_deep<T, NT, P, GS_X_CLUSTER>, rows, set_ptr,
+                                    first, last, A.n, A.ia, A.ja, A.val, d, kd, w, b, x, skip,
+                                    cshift));
+        count_launch();
+        return SUCCESS;
+    }
+    k_gs_deep<T, NT, P, GS_X_GLOBAL><<<1, NT, spb, s>>>(rows, set_ptr, first, last, A.n, A.ia,
+                                                        A.ja, A.val, d, kd, w, b, x, skip, 0);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;
@@ -1115,15 +1329,27 @@ int gs_run(const DCsr<T> &A, int kind, const int *rows, const int *set_ptr,
     if (last - first > GS_RUN_SETS || max_set > GS_SMALL_SET) return ERROR_INPUT_PAR;
     const int skip = (kind & GS_SKIP_LAST) ? A.n - 1 : -1;
     const int kd = kind & 15;
-    // entries per row held ahead in each of the four register stages: 8 up
-    // to 512 threads, fewer at 1024 (64 registers a thread)
+    // up to 256 rows a set: the deep pipeline (HZB_GS_DEEP=0: the four-stage
+    // one; same results); larger sets: four stages, 8 entries per row held
+    // ahead up to 512 threads, fewer at 1024 (64 registers a thread)
     constexpr int P1024 = sizeof(T) == 8 ? 2 : 4;
+    static const bool deep = [] {
+        const char *e = getenv("HZB_GS_DEEP");
+        return !(e && e[0] == '0');
+    }();
     if (max_set <= 128)
-        return gs_pipe_launch<T, 128, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+        return deep ? gs_deep_launch<T, 128, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x,
+                                                skip, s)
+                    : gs_pipe_launch<T, 128, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x,
+                                                skip, s);
     if (max_set <= 256)
-        return gs_pipe_launch<T, 256, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+        return deep ? gs_deep_launch<T, 256, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x,
+                                                skip, s)
+                    : gs_pipe_launch<T, 256, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x,
+                                                skip, s);
     if (max_set <= 512)
-        return gs_pipe_launch<T, 512, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip, s);
+        return gs_pipe_launch<T, 512, 8>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip,
+                                         s);
     return gs_pipe_launch<T, 1024, P1024>(A, kd, rows, set_ptr, first, last, d, w, b, x, skip,
                                           s);
 }

@@ -9,6 +9,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <chrono>
 
 namespace hzb {
 
@@ -621,8 +623,58 @@ int level_smoother_data(hzb_solver *S, Level &L) {
     return SUCCESS;
 }
 
+// HZB_SETUP_TRACE=1: each setup prints to stderr the host time of its phases
+// (the stream synchronised at every mark) and how much the device's memory
+// pool grew, for finding where a slow setup spent its time.
+namespace {
+struct SetupTrace {
+    bool on = false;
+    cudaStream_t s = nullptr;
+    std::chrono::steady_clock::time_point t0, last;
+    unsigned long long pool0 = 0;
+    std::string line;
+    static unsigned long long reserved() {
+        int dev = 0;
+        cudaMemPool_t pool;
+        unsigned long long v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v);
+        return v;
+    }
+    explicit SetupTrace(cudaStream_t st) : s(st) {
+        const char *e = getenv("HZB_SETUP_TRACE");
+        on = e && e[0] == '1';
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        t0 = last = std::chrono::steady_clock::now();
+        pool0 = reserved();
+    }
+    void mark(const char *what) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto t = std::chrono::steady_clock::now();
+        char buf[96];
+        snprintf(buf, sizeof(buf), " %s %.2f", what,
+                 std::chrono::duration<double, std::milli>(t - last).count());
+        line += buf;
+        last = t;
+    }
+    ~SetupTrace() {
+        if (!on) return;
+        const double tot =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                .count();
+        const long long grew = (long long)reserved() - (long long)pool0;
+        fprintf(stderr, "hzb setup trace (ms):%s total %.2f pool_growth_MB %.1f\n", line.c_str(),
+                tot, grew / 1048576.0);
+    }
+};
+}  // namespace
+
 int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
           const double *d_val, bool copy_in) {
+    SetupTrace trace(S->s);
     S->g64.release();
     S->g32.release();
     S->g32c.release();
@@ -634,6 +686,7 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
     dfree(S->Ainv);
     S->nl = 0;
     cudaStream_t s = S->s;
+    trace.mark("release");
     HZB_CUDA(cudaEventRecord(S->e0, s));
     S->lv.emplace_back();
     {
@@ -777,6 +830,7 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
         int live = 0;
         HZB_TRY(batch_level_begin(S, lvl, true, &live));
     }
+    trace.mark("levels");
     // coarsest level: dense inverse (coarse_solver 32, and always for the
     // FP32 cycle); batched systems use their terminal blocks instead
     if (!batch &&
@@ -787,6 +841,7 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
         HZB_TRY(transpose_csr(C.A64(), &C.tia, &C.tja, &C.tval, s));
         HZB_TRY(dense_inverse(C.AT64(), &S->Ainv, s));
     }
+    trace.mark("coarse");
     for (int l = 0; l < S->nl; ++l) {
         Level &L = S->lv[l];
         HZB_TRY(dalloc(&L.b, L.n));
@@ -802,10 +857,12 @@ int setup(hzb_solver *S, int n, int nnz, const int *d_ia, const int *d_ja,
             L.bundle_cap = A.bundle_cap;
         }
     }
+    trace.mark("smoothers");
     HZB_TRY(S->kw.alloc(n, s));
     if (S->amg.coarse_solver != SOLVER_UMFPACK)
         HZB_TRY(S->kwc.alloc(S->lv[S->nl - 1].n, s));
     if (S->bp.precision == HZB_PREC_MIXED) HZB_TRY(ensure_fp32(S));
+    trace.mark("fp32");
     HZB_CUDA(cudaEventRecord(S->e1, s));
     HZB_CUDA(cudaEventSynchronize(S->e1));
     float ms = 0.f;
