@@ -5,7 +5,6 @@
 // one thread; coalescing comes from staging each row bundle's entries in
 // shared memory (the CSR-stream schedule), not from splitting rows.
 #include "hzb_kernels.cuh"
-#include <cooperative_groups.h>
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -1073,53 +1072,33 @@ k_gs_pipe(const int *__restrict__ rows, const int *__restrict__ set_ptr, int fir
     }
 }
 
-// The same sweep for runs of sets of at most 256 rows per CTA with the
-// pipeline twice as deep: a thread loads its row index in set s+6, the
-// bounds of its row in set s+4 and the entries of its row in set s+2, so
-// every load has two barrier periods to arrive before anything uses it.
-// Seven register stages rotate through a seven-fold unrolled loop.  Where x
-// lives (XM):
-//   GS_X_GLOBAL  global memory (one CTA);
-//   GS_X_SMEM    the CTA's shared memory, read once and written back;
-//   GS_X_CLUSTER the distributed shared memory of a cluster of CL CTAs: CTA
-//                r holds rows [r << cshift, (r + 1) << cshift), the set's
-//                rows are dealt over the cluster's threads, and the sets are
-//                separated by cluster barriers (whose release / acquire order
-//                makes a set's writes visible to every CTA).  Levels whose x
-//                does not fit one CTA's shared memory keep their gathers on
-//                chip this way: a global-memory x misses L1 after every write.
-constexpr int GS_X_GLOBAL = 0, GS_X_SMEM = 1, GS_X_CLUSTER = 2;
-template <typename T, int NT, int P, int XM>
+// The same sweep for runs of sets of at most 256 rows with the pipeline
+// twice as deep: a thread loads its row index in set s+6, the bounds of its
+// row in set s+4 and the entries of its row in set s+2, so every load has
+// two barrier periods to arrive before anything uses it.  Seven register
+// stages rotate through a seven-fold unrolled loop.  x lives in the CTA's
+// shared memory when the level fits (XS), else in global memory.  (Holding
+// x in the distributed shared memory of a cluster of 2-8 CTAs instead, with
+// a cluster barrier between sets, measured slower on the 2D 255^2 levels:
+// 854 against 612 us for the 509 sets of level 0.)
+template <typename T, int NT, int P, bool XS>
 __global__ void __launch_bounds__(NT)
 k_gs_deep(const int *__restrict__ rows, const int *__restrict__ set_ptr, int first, int last,
           int n, const int *__restrict__ ia, const int *__restrict__ ja,
           const T *__restrict__ a, const T *__restrict__ d, int kind, T w,
-          const T *__restrict__ b, T *xg, int skip, int cshift) {
-    namespace cg = cooperative_groups;
+          const T *__restrict__ b, T *xg, int skip) {
     extern __shared__ __align__(16) unsigned char gs_smem[];
     const int ns = last - first;
     int *sp = reinterpret_cast<int *>(gs_smem);
     T *xs = reinterpret_cast<T *>(gs_smem + gs_sp_bytes(ns));
-    const int crank = XM == GS_X_CLUSTER ? (int)cg::this_cluster().block_rank() : 0;
-    const int csize = XM == GS_X_CLUSTER ? (int)cg::this_cluster().num_blocks() : 1;
-    const int cmask = (1 << cshift) - 1;
     for (int k = threadIdx.x; k <= ns; k += NT) sp[k] = set_ptr[first + k];
-    if (XM == GS_X_SMEM) {
+    if (XS) {
 #pragma unroll 4
         for (int k = threadIdx.x; k < n; k += NT) xs[k] = xg[k];
-    } else if (XM == GS_X_CLUSTER) {
-        const int r0 = crank << cshift, r1 = min(n, r0 + (1 << cshift));
-#pragma unroll 4
-        for (int k = r0 + (int)threadIdx.x; k < r1; k += NT) xs[k - r0] = xg[k];
     }
-    if (XM == GS_X_CLUSTER) cg::this_cluster().sync();
-    else __syncthreads();
-    auto xat = [&](int j) -> T * {
-        if (XM == GS_X_GLOBAL) return xg + j;
-        if (XM == GS_X_SMEM) return xs + j;
-        return cg::this_cluster().map_shared_rank(xs + (j & cmask), j >> cshift);
-    };
-    const int t = (int)threadIdx.x + crank * NT;   // this thread's slot in a set
+    __syncthreads();
+    auto xat = [&](int j) -> T * { return XS ? xs + j : xg + j; };
+    const int t = threadIdx.x;
     using St = GsStage<T, P>;
     auto row_of = [&](St &S, int r) {
         S.i = -1;
@@ -1178,8 +1157,7 @@ k_gs_deep(const int *__restrict__ rows, const int *__restrict__ set_ptr, int fir
         bounds(B4);
         row_of(R6, s + 6);
         apply(D0);
-        if (XM == GS_X_CLUSTER) cg::this_cluster().sync();
-        else __syncthreads();
+        __syncthreads();
     };
     St S0, S1, S2, S3, S4, S5, S6;
     row_of(S0, 0);
@@ -1209,16 +1187,10 @@ k_gs_deep(const int *__restrict__ rows, const int *__restrict__ set_ptr, int fir
         if (s + 6 >= ns) break;
         step(s + 6, S5, S3, S1, S6);
     }
-    // every step ended with a barrier, so no CTA reads another's x any more
-    if (XM == GS_X_SMEM) {
+    if (XS) {
 #pragma unroll 4
         for (int k = threadIdx.x; k < n; k += NT) xg[k] = xs[k];
-    } else if (XM == GS_X_CLUSTER) {
-        const int r0 = crank << cshift, r1 = min(n, r0 + (1 << cshift));
-#pragma unroll 4
-        for (int k = r0 + (int)threadIdx.x; k < r1; k += NT) xg[k] = xs[k - r0];
     }
-    (void)csize;
 }
 
 template <typename T>
@@ -1265,9 +1237,8 @@ static int gs_pipe_launch(const DCsr<T> &A, int kd, const int *rows, const int *
     return SUCCESS;
 }
 
-// the deep run kernel (at most 256 threads a CTA): x in shared memory when
-// the level fits one CTA, else (FP64) in the distributed shared memory of a
-// cluster of up to 8 CTAs when it fits that, else in global memory
+// the deep run kernel (at most 256 threads): x in shared memory when the
+// level fits, else in global memory
 template <typename T, int NT, int P>
 static int gs_deep_launch(const DCsr<T> &A, int kd, const int *rows, const int *set_ptr,
                           int first, int last, const T *d, T w, const T *b, T *x, int skip,
@@ -1276,46 +1247,14 @@ static int gs_deep_launch(const DCsr<T> &A, int kd, const int *rows, const int *
     const size_t xsb = sizeof(T) * (size_t)A.n;
     if (spb + xsb <= GS_SMEM_MAX) {
         static bool done = false;
-        gs_smem_limit(k_gs_deep<T, NT, P, GS_X_SMEM>, done);
-        k_gs_deep<T, NT, P, GS_X_SMEM><<<1, NT, spb + xsb, s>>>(
-            rows, set_ptr, first, last, A.n, A.ia, A.ja, A.val, d, kd, w, b, x, skip, 0);
-        count_launch();
-        HZB_LAUNCH_CHECK();
-        return SUCCESS;
+        gs_smem_limit(k_gs_deep<T, NT, P, true>, done);
+        k_gs_deep<T, NT, P, true><<<1, NT, spb + xsb, s>>>(rows, set_ptr, first, last, A.n,
+                                                           A.ia, A.ja, A.val, d, kd, w, b, x,
+                                                           skip);
+    } else {
+        k_gs_deep<T, NT, P, false><<<1, NT, spb, s>>>(rows, set_ptr, first, last, A.n, A.ia,
+                                                      A.ja, A.val, d, kd, w, b, x, skip);
     }
-    // rows per cluster CTA: the largest power of two whose x fits beside the
-    // set pointers; the smallest cluster (2, 4 or 8 CTAs) that holds the level
-    static const bool cluster_ok = [] {
-        const char *e = getenv("HZB_GS_CLUSTER");
-        return !(e && e[0] == '0');
-    }();
-    int cshift = 0;
-    while (cshift < 24 && (sizeof(T) << (cshift + 1)) + spb <= GS_SMEM_MAX) ++cshift;
-    int cl = 2;
-    while (cl < 8 && ((long long)cl << cshift) < A.n) cl *= 2;
-    if (sizeof(T) == 8 && cluster_ok && ((long long)cl << cshift) >= A.n) {
-        static bool done = false;
-        gs_smem_limit(k_gs_deep<T, NT, P, GS_X_CLUSTER>, done);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(cl);
-        cfg.blockDim = dim3(NT);
-        cfg.dynamicSmemBytes = spb + (sizeof(T) << cshift);
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cl;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        HZB_CUDA(cudaLaunchKernelEx(&cfg, k_gs_deep<T, NT, P, GS_X_CLUSTER>, rows, set_ptr,
-                                    first, last, A.n, A.ia, A.ja, A.val, d, kd, w, b, x, skip,
-                                    cshift));
-        count_launch();
-        return SUCCESS;
-    }
-    k_gs_deep<T, NT, P, GS_X_GLOBAL><<<1, NT, spb, s>>>(rows, set_ptr, first, last, A.n, A.ia,
-                                                        A.ja, A.val, d, kd, w, b, x, skip, 0);
     count_launch();
     HZB_LAUNCH_CHECK();
     return SUCCESS;

@@ -1547,6 +1547,7 @@ __global__ void k_indeg(int n, const int *__restrict__ ia, const int *__restrict
             c += backward ? (j > i) : (j < i);
         }
         indeg[i] = c;
+        atomicMax(tail + 1, c);
         if (c == 0) rows[atomicAdd(tail, 1)] = i;
     }
 }
@@ -1622,6 +1623,89 @@ k_kahn_all(int n, const int *__restrict__ ia, const int *__restrict__ ja,
     }
 }
 
+// The same rounds for levels of at most KAHN_SMEM_ROWS rows whose in-degrees
+// fit 16 bits: the in-degree counters sit in shared memory (two to a word;
+// a counter is decremented exactly as often as it counts, so a halfword
+// never borrows from its neighbour), and each round's new frontier is also
+// kept in shared memory (double-buffered, up to KAHN_FRONT rows) for the next
+// round to read, so a round costs two dependent global loads (row bounds,
+// then columns) instead of a chain through global atomics.  The column
+// indices of a row are loaded eight at a time before their counters are
+// decremented.  Same sets as k_kahn_all (the order of rows inside a set may
+// differ; the rows of a set are independent).
+constexpr int KAHN_SMEM_ROWS = 96 * 1024;
+constexpr int KAHN_FRONT = 4096;
+constexpr size_t kahn_smem_bytes(int n) {
+    return sizeof(unsigned) * ((size_t)(n + 1) / 2) + sizeof(int) * 2 * KAHN_FRONT;
+}
+__global__ void __launch_bounds__(1024)
+k_kahn_smem(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+            const int *__restrict__ tia, const int *__restrict__ tja, int backward,
+            const int *__restrict__ indeg, int *rows, const int *__restrict__ tail0, int *ptr,
+            int *nsets) {
+    extern __shared__ unsigned kahn_sm[];
+    const int nw = (n + 1) / 2;
+    unsigned *deg = kahn_sm;
+    int *front = reinterpret_cast<int *>(kahn_sm + nw);
+    __shared__ int s_tail, s_head, s_cur, s_ns;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+        const unsigned lo = (unsigned)indeg[2 * w];
+        const unsigned hi = 2 * w + 1 < n ? (unsigned)indeg[2 * w + 1] : 0u;
+        deg[w] = lo | (hi << 16);
+    }
+    if (threadIdx.x == 0) {
+        s_head = 0;
+        s_cur = *tail0;
+        s_tail = s_cur;
+        s_ns = 0;
+        ptr[0] = 0;
+    }
+    __syncthreads();
+    for (int round = 0; round < n; ++round) {
+        const int head = s_head, cur = s_cur;
+        if (cur <= head) break;
+        if (threadIdx.x == 0) ptr[++s_ns] = cur;
+        const bool fin_ok = round > 0 && cur - head <= KAHN_FRONT;
+        const int *fin = front + (round & 1) * KAHN_FRONT;
+        int *fout = front + ((round + 1) & 1) * KAHN_FRONT;
+        auto release = [&](int j) {
+            const unsigned sh = 16u * (unsigned)(j & 1);
+            const unsigned old = atomicSub(deg + (j >> 1), 1u << sh);
+            if (((old >> sh) & 0xFFFFu) == 1u) {
+                const int p = atomicAdd(&s_tail, 1);
+                rows[p] = j;
+                if (p - cur < KAHN_FRONT) fout[p - cur] = j;
+            }
+        };
+        auto visit = [&](int i, const int *__restrict__ xa, const int *__restrict__ xj) {
+            const int k1 = xa[i + 1];
+            for (int k0 = xa[i]; k0 < k1; k0 += 8) {
+                int c[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) c[u] = k0 + u < k1 ? xj[k0 + u] : -1;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (c[u] >= 0 && (backward ? (c[u] < i) : (c[u] > i))) release(c[u]);
+            }
+        };
+        for (int q = head + threadIdx.x; q < cur; q += blockDim.x) {
+            const int i = fin_ok ? fin[q - head] : rows[q];
+            visit(i, ia, ja);
+            visit(i, tia, tja);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_head = cur;
+            s_cur = s_tail;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        nsets[0] = s_ns;
+        nsets[1] = s_head;   // rows placed
+    }
+}
+
 static void make_runs(Schedule *sch) {
     const int ns = (int)sch->h_ptr.size() - 1;
     int k = 0;
@@ -1660,11 +1744,11 @@ int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,
     if ((rc = dalloc(&tja, nnz))) goto done;
     if ((rc = dalloc(&fillc, n))) goto done;
     if ((rc = dalloc(&indeg, n))) goto done;
-    if ((rc = dalloc(&tail, 1))) goto done;
+    if ((rc = dalloc(&tail, 2))) goto done;   // frontier end, largest in-degree
     if ((rc = dalloc(&tmp, scan_tmp_size(n + 1)))) goto done;
     if ((rc = dalloc(&sch->rows, n))) goto done;
     cudaMemsetAsync(fillc, 0, sizeof(int) * n, s);
-    cudaMemsetAsync(tail, 0, sizeof(int), s);
+    cudaMemsetAsync(tail, 0, 2 * sizeof(int), s);
     k_transpose_count<<<g, 256, 0, s>>>(n, ia, ja, fillc);
     count_launch();
     if ((rc = scan_exclusive(fillc, tia, n, tmp, s))) goto done;
@@ -1679,8 +1763,29 @@ int gs_schedule(int n, const int *ia, const int *ja, int nnz, int backward,
             dfree(dptr);
             goto done;
         }
-        k_kahn_all<<<1, 1024, 0, s>>>(n, ia, ja, tia, tja, backward, indeg, sch->rows, tail,
-                                       dptr, dns);
+        int maxdeg = 0;
+        e = cudaMemcpyAsync(&maxdeg, tail + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            dfree(dptr);
+            dfree(dns);
+            set_error(e, __FILE__, __LINE__);
+            rc = ERROR_SOLVER_MISC;
+            goto done;
+        }
+        if (n <= KAHN_SMEM_ROWS && maxdeg <= 0xFFFF) {
+            static bool attr = false;
+            if (!attr) {
+                cudaFuncSetAttribute(k_kahn_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kahn_smem_bytes(KAHN_SMEM_ROWS));
+                attr = true;
+            }
+            k_kahn_smem<<<1, 1024, kahn_smem_bytes(n), s>>>(n, ia, ja, tia, tja, backward,
+                                                            indeg, sch->rows, tail, dptr, dns);
+        } else {
+            k_kahn_all<<<1, 1024, 0, s>>>(n, ia, ja, tia, tja, backward, indeg, sch->rows,
+                                          tail, dptr, dns);
+        }
         count_launch();
         int hns[2] = {0, 0};
         e = cudaMemcpyAsync(hns, dns, sizeof(hns), cudaMemcpyDeviceToHost, s);
