@@ -69,6 +69,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import datetime
 import json
 import os
 import statistics
@@ -144,41 +145,64 @@ def cpu_sample(name: str, variant: str = ""):
 
 
 class Clocks:
-    """nvidia-smi sampler during the timed region."""
+    """nvidia-smi sampler (every 200 ms).  Started before the warm-up steps, so
+    that its start-up (NVML initialisation, which can hold up the driver for a
+    few hundred ms) falls outside the timed region; mark() records the start
+    of the timed region and stop() keeps the samples taken after it (all of
+    them when none is, or when the timestamps do not parse)."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
         self.p = None
+        self.t_mark = None
         self.path = os.path.join("/tmp", f"hzb_clocks_{os.getpid()}.csv")
         try:
             self.p = subprocess.Popen(
-                ["nvidia-smi", f"--id={index}",
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+
+    def mark(self):
+        self.t_mark = datetime.datetime.now()
+
+    @staticmethod
+    def summary(lines, t_mark=None) -> dict:
+        rows = []
+        for ln in lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) >= 8:
+                rows.append(f)
+        if t_mark is not None:
+            def after(r):
+                try:
+                    return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f") >= t_mark
+                except ValueError:
+                    return True
+            timed = [r for r in rows if after(r)]
+            rows = timed or rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit()
+                else None, "reasons": reasons, "samples": len(rows)}
 
     def stop(self) -> dict:
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
         self.p.wait()
-        rows = []
-        for ln in open(self.path):
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) >= 7:
-                rows.append(f)
+        with open(self.path) as fh:
+            lines = fh.readlines()
         os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
-        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit()
-                else None, "reasons": reasons, "samples": len(rows)}
+        return self.summary(lines, self.t_mark)
 
 
 def hbm_peak():
@@ -292,15 +316,16 @@ def run_variant(args, rank, world, local, dist):
         check(S.setup_device(n, nnz, p(dia), p(dja), p(dval)), "setup")
         return check(S.solve_device(p(db), p(dx)), "solve")
 
+    clocks = Clocks(local)
     for _ in range(args.warmup):
         step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     setup_s, solve_s, launches, iters = [], [], 0, 0
     torch.cuda.profiler.start()
+    clocks.mark()
     ev0.record()
     for _ in range(args.steps):
         iters = step()
@@ -559,7 +584,6 @@ def main():
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
@@ -632,15 +656,16 @@ def run_single(args, rank, world, local, dist):
     # learned weights, which do not reduce this problem's iteration count,
     # are measured beside it below)
     S = hz.Solver(amg_l1(hz), itparam(hz), bp_mixed)
+    clocks = Clocks(local)
     for _ in range(args.warmup):
         step(S, False)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     setup_s, solve_s, launches, iters = [], [], 0, 0
     torch.cuda.profiler.start()
+    clocks.mark()
     ev0.record()
     for _ in range(args.steps):
         iters, _ = step(S, False)
@@ -1119,14 +1144,15 @@ def run_bsr(args, rank, world, local, dist):
         check(S.setup_bsr_device(nrow, nnzb, BSR_NB, p(dia), p(dja), p(dval)), "bsr setup")
         return check(S.bsr_solve_device(p(db), p(dx)), "bsr solve")
 
+    clocks = Clocks(local)
     for _ in range(args.warmup):
         step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     setup_s, solve_s, launches, iters = [], [], 0, 0
+    clocks.mark()
     ev0.record()
     for _ in range(args.steps):
         iters = step()
@@ -1227,16 +1253,17 @@ def run_batch(args, rank, world, local, dist):
             raise RuntimeError(f"batch solve {rc}: {hz.last_error()}")
         return su, S.stats().solve_seconds, its, rel, sec
 
+    clocks = Clocks(local)
     for _ in range(args.warmup):
         step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     res = []
     launches = 0
     torch.cuda.profiler.start()
+    clocks.mark()
     ev0.record()
     for _ in range(args.steps):
         res.append(step())
