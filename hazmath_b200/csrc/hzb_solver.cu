@@ -136,7 +136,11 @@ enum { SC_T1 = 0, SC_T2 = 1, SC_RR = 2, SC_UM = 3, SC_UU = 4, SC_PP = 5,
        SC_T3 = 6, SC_ZT = 7, SC_X = 8, SC_ERR = 15, SC_N = 16 };
 
 int KrylovWork::alloc(int nn, cudaStream_t st) {
-    release();
+    // the device arrays follow the system size; the pinned host mirror of the
+    // scalars has a fixed size and stays: page-locking host memory (and
+    // freeing it, which waits for the whole device) took from a few to a few
+    // hundred ms per setup
+    release_device();
     n = nn;
     const int G = reduce_blocks(n);
     const int np = 4 * G + spmv_blocks_rows(n, 64) + 8;   // smallest bundle
@@ -148,14 +152,17 @@ int KrylovWork::alloc(int nn, cudaStream_t st) {
     HZB_TRY(dalloc(&sc, SC_N));
     // on the stream the allocations were made on (the entry point's)
     HZB_CUDA(cudaMemsetAsync(sc, 0, SC_N * sizeof(double), st ? st : cur_stream()));
-    HZB_CUDA(cudaMallocHost((void **)&h_sc, SC_N * sizeof(double)));
+    if (!h_sc) HZB_CUDA(cudaMallocHost((void **)&h_sc, SC_N * sizeof(double)));
     return SUCCESS;
 }
-void KrylovWork::release() {
+void KrylovWork::release_device() {
     dfree(p); dfree(z); dfree(r); dfree(t); dfree(part); dfree(sc);
+    n = 0;
+}
+void KrylovWork::release() {
+    release_device();
     if (h_sc) cudaFreeHost(h_sc);
     h_sc = nullptr;
-    n = 0;
 }
 
 static int fetch(hzb_solver *S, KrylovWork &w) {
@@ -516,8 +523,26 @@ forward:
 }
 
 int ensure_fp32(hzb_solver *S) {
+    // HZB_SETUP_TRACE=1: the stream synchronised after each part, and a level
+    // whose parts took more than 20 ms reported to stderr
+    static const bool trace = [] {
+        const char *e = getenv("HZB_SETUP_TRACE");
+        return e && e[0] == '1';
+    }();
+    using clk = std::chrono::steady_clock;
+    auto lap = [&](clk::time_point &t) {
+        if (!trace) return 0.0;
+        cudaStreamSynchronize(S->s);
+        const auto now = clk::now();
+        const double ms = std::chrono::duration<double, std::milli>(now - t).count();
+        t = now;
+        return ms;
+    };
     for (int l = 0; l < S->nl; ++l) {
         Level &L = S->lv[l];
+        clk::time_point t = clk::now();
+        double ms_count = 0, ms_copy = 0, ms_vec = 0, ms_norms = 0, ms_sell = 0, ms_sched = 0;
+        lap(t);
         if (!L.val32) {
             // drop the stored exact zeros: they add nothing to a row sum
             int *cnt = nullptr, *ia32 = nullptr, *tmp = nullptr;
@@ -529,6 +554,7 @@ int ensure_fp32(hzb_solver *S) {
             int nz = 0;
             HZB_CUDA(cudaMemcpyAsync(&nz, ia32 + L.n, sizeof(int), cudaMemcpyDeviceToHost, S->s));
             HZB_CUDA(cudaStreamSynchronize(S->s));
+            ms_count = lap(t);
             dfree(cnt);
             dfree(tmp);
             if (nz == L.nnz) {   // nothing to drop: share the pattern
@@ -552,15 +578,18 @@ int ensure_fp32(hzb_solver *S) {
             L.nnz32 = nz;
             HZB_TRY(bundle_capacity_rows(L.n, L.bundle_rows, L.ia32, S->s, &L.bundle_cap32));
         }
+        ms_copy = lap(t);
         if (!L.b32) {
             HZB_TRY(dalloc(&L.b32, L.n));
             HZB_TRY(dalloc(&L.x32, L.n));
             HZB_TRY(dalloc(&L.w32, L.n));
             HZB_TRY(dalloc(&L.t32, L.n));
         }
+        ms_vec = lap(t);
         if (!L.l1_32) {
             HZB_TRY(dalloc(&L.l1_32, L.n));
             HZB_TRY(l1_norms<float>(L.A32(), L.l1_32, S->s));
+            ms_norms = lap(t);
             // staged bundles, lanes per row or the sliced-ELL copy, by
             // timing; HZB_FP32_LANES (0, 2, 4, 8, 16 or "sell") names one for
             // every level instead.  Batched solves run the kernels with an
@@ -579,6 +608,7 @@ int ensure_fp32(hzb_solver *S) {
                 const bool have = fp32_schedule_known(L.n, L.nnz32, &known);
                 if (sell_ok && (!have || known == SELL_LANES))
                     HZB_TRY(sell_build(L.n, L.ia32, L.ja32, L.val32, &L.sell32, S->s));
+                ms_sell = lap(t);
                 HZB_TRY(vzero<float>(L.n, L.b32, S->s));
                 HZB_TRY(vzero<float>(L.n, L.x32, S->s));
                 DCsr<float> A = L.A32();
@@ -587,6 +617,11 @@ int ensure_fp32(hzb_solver *S) {
                 if (L.vec32 != SELL_LANES) L.sell32.release();
             }
         }
+        ms_sched = lap(t);
+        if (trace && ms_count + ms_copy + ms_vec + ms_norms + ms_sell + ms_sched > 1.0)
+            fprintf(stderr, "hzb setup trace: fp32 level %d (%d rows): count %.2f copy %.2f "
+                    "vectors %.2f norms %.2f sell %.2f schedule %.2f ms\n", l, L.n, ms_count,
+                    ms_copy, ms_vec, ms_norms, ms_sell, ms_sched);
         if (S->amg.smoother == SMOOTHER_GS && l < S->nl - 1 && !L.d_gs32) {
             if (!L.col.rows) HZB_TRY(multicolor(L.n, L.ia, L.ja, &L.col, S->s));
             HZB_TRY(dalloc(&L.d_gs32, L.n));

@@ -104,6 +104,7 @@ struct KrylovWork {
     double *sc = nullptr;     // device scalars
     double *h_sc = nullptr;   // pinned host mirror
     int alloc(int n, cudaStream_t s = nullptr);   // scalars zeroed on s (or the current stream)
+    void release_device();   // the device arrays (the pinned host mirror stays)
     void release();
 };
 
