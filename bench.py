@@ -805,13 +805,14 @@ def run_single(args, rank, world, local, dist):
             "speedup_solve_vs_plain": st64.solve_seconds / solve_ml,
             "err_vs_fp64": err_vs_fp64,
             "roofline": {"bound": "hbm", "kernel": "level-0 FP32 l1-Jacobi sweep of the "
-                         "mixed cycle (k_l1_vec / k_l1_bundle<float>, autotuned), with the "
-                         "weights the step ran", "achieved": l1_gbs, "peak": peak,
+                         "mixed cycle (k_l1_sell / k_l1_vec / k_l1_bundle<float>, autotuned), "
+                         "with the weights the step ran", "achieved": l1_gbs, "peak": peak,
                          "unit": "GB/s", "frac": l1_gbs / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": l1_by, "ms_per_launch": l1_ms,
                          "traffic": TRAFFIC_PER_BYTE["l1_32"] * l1_by,
-                         "traffic_source": "ncu DRAM bytes per algorithmic byte of this "
-                         "kernel on the 128^3 case, times this launch's bytes"},
+                         "traffic_source": "ncu DRAM bytes per algorithmic byte of the "
+                         "sliced-ELL sweep (level 1 of the 192^3 instance), times this "
+                         "launch's bytes"},
             "solve_roofline": {"bound": "hbm", "bytes": solve_by,
                                "seconds": solve_ml, "achieved": solve_by / solve_ml / 1e9,
                                "peak": peak, "unit": "GB/s",
@@ -1113,12 +1114,15 @@ def parity_vs_fixture(name, st, iters):
 
 
 # DRAM bytes (read + written) per algorithmic byte of one launch, measured by
-# ncu on the level-0 kernels of the 128^3 case (dram__bytes_read.sum +
-# dram__bytes_write.sum over the bytes hzb_time_kernel counts): the FP32
-# l1-Jacobi sweep in its lanes-per-row schedule, and the drop-in's FP64 SpMV.
-# The 256^3 launches run the same kernels over 8.1x the entries, and their
-# traffic is this ratio times their algorithmic bytes.
-TRAFFIC_PER_BYTE = {"l1_32": 143.73e6 / 146709388.0, "spmv64": 404.52e6 / 405049716.0}
+# ncu over the bytes hzb_time_kernel counts: the FP32 l1-Jacobi sweep in the
+# sliced-ELL schedule the autotuner picks on the fine levels (level 1 of the
+# 192^3 instance of the family: dram__bytes.sum.per_second 4.804 TB/s over
+# 68.288 us = 328.1 MB for 311,596,604 algorithmic bytes), and the drop-in's
+# FP64 SpMV on level 0 of the 128^3 case.  The 256^3 launches run the same
+# kernels over more entries, and their traffic is this ratio times their
+# algorithmic bytes.
+TRAFFIC_PER_BYTE = {"l1_32": 4.804461e12 * 68.288e-6 / 311596604.0,
+                    "spmv64": 404.52e6 / 405049716.0}
 
 
 def run_bsr(args, rank, world, local, dist):
