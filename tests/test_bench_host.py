@@ -80,3 +80,26 @@ def test_solve_bytes_model():
     # the learned weights add 4 bytes per fine row to the first and three full sweeps
     assert bench.solve_bytes_mixed(levels, 10, True) - bench.solve_bytes_mixed(
         levels, 10, False) == 11 * 4 * (4 * n0)
+
+
+def test_clock_samples_after_mark():
+    """The clock summary keeps the nvidia-smi samples taken after the start of
+    the timed region (the sampler starts before the warm-up steps), falls back
+    to all samples when none is later, and reports the throttle reasons seen."""
+    import datetime
+    sys.path.insert(0, ROOT)
+    import bench
+    rows = ["2026/12/04 01:00:00.000, 1500, 1965, 300.1, Not Active, Not Active, Not Active, "
+            "Not Active\n",
+            "2026/12/04 01:00:01.000, 1965, 1965, 900.0, Not Active, Not Active, Not Active, "
+            "Active\n",
+            "2026/12/04 01:00:01.200, 1905, 1965, 950.0, Not Active, Not Active, Not Active, "
+            "Not Active\n",
+            "garbled\n"]
+    mark = datetime.datetime(2026, 12, 4, 1, 0, 0, 500000)
+    s = bench.Clocks.summary(rows, mark)
+    assert s["samples"] == 2 and s["sm_mhz"] == 1935.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
+    late = bench.Clocks.summary(rows, datetime.datetime(2027, 1, 1))
+    assert late["samples"] == 3 and late["sm_mhz"] == 1905.0
+    assert bench.Clocks.summary([], mark)["sm_mhz"] is None
